@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: accepted cell-steps/s of the 3-D mechanics step at 100k cells.
+
+Workload (one "step" = one accepted iteration of the runSimulation loop body,
+ABM-3d/ABM-3d-cpp/include/simulation.hpp:1617-1864): 100,000 cells, centres
+uniform in a 300 um disk with z in [R, 10] um, no growth or division, Heun-Euler
+2(1) (the 3-D driver's default), RK tolerance 1e-8, dt capped at 1e-6 h,
+isotropic JKR cell-cell adhesion (gamma = 100) and cell-surface Hertz + JKR.
+Inputs are seeded synthetic states (no dataset is involved).
+
+  value     device-resident throughput, CUDA events on the context stream, L2
+            flushed (256 MB write) between timed steps, max over ranks
+  e2e       through the C ABI with pinned host buffers: upload cells -> one
+            iteration -> download cells, every step
+  roofline  the dominant kernel's algorithmic bytes per launch / its
+            event-timed duration, against MEASURED_PEAKS.json
+  cpu_baseline / --impl reference
+            the oracle (a C++ restatement of the reference path, run the way
+            the reference runs it: O(n^2) neighbor build, serial pair loops,
+            pair forces recomputed per stage, OpenMP on the per-cell loops)
+
+Multi-GPU: replicas only (each rank advances its own biofilm; no collective on
+the data path), scaling "weak".
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "biofilm-abms_b200"))
+
+METRIC = "accepted cell-steps/s @100k 3D cells"
+UNIT = "cell-steps/s"
+N_CELLS = 100_000
+SEED = 1
+P_CONTACT = 0.9
+FLUSH_BYTES = 256 << 20
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS)
+    ap.add_argument("--tableau", type=int, default=1, help="1 HE21, 2 BS32, 3 RKF45, 4 DP54")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--profile-steps", type=int, default=200)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def dist_init(backend):
+    import datetime
+    import torch.distributed as dist
+    rank, world, _ = dist_env()
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(x, device, world):
+    """Max of a float over ranks (identity for one rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.rows = []
+        self.t0 = self.t1 = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=timestamp," + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def mark(self, which):
+        setattr(self, which, time.time())
+
+    def stop(self):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.f.read().splitlines() if ln.strip()]
+        self.f.close()
+        os.unlink(self.f.name)
+        out = []
+        for r in rows:
+            if len(r) < 10:
+                continue
+            try:
+                out.append(dict(sm=float(r[2]), sm_max=float(r[3]), power=float(r[4]),
+                                hw=r[6], hw_thermal=r[7], sw_thermal=r[8], sw_power=r[9]))
+            except ValueError:
+                continue
+        self.rows = out
+        return self.summary()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        reasons = set()
+        for r in self.rows:
+            for k, name in (("hw", "hw_slowdown"), ("hw_thermal", "hw_thermal_slowdown"),
+                            ("sw_thermal", "sw_thermal_slowdown"), ("sw_power", "sw_power_cap")):
+                if r[k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in self.rows),
+                "sm_max_mhz": max(r["sm_max"] for r in self.rows), "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload(n, seed):
+    from abm_b200 import workloads
+    radius = 300.0 * (n / 100000.0) ** 0.5
+    return workloads.biofilm_3d(n=n, seed=seed, disk_radius=radius, p_contact=P_CONTACT)
+
+
+def sim_params(args, n):
+    return dict(cap_cells=n, integration_mode=args.tableau,
+                precision=1 if args.precision == "mixed" else 0, pair_lanes=args.lanes,
+                max_stepsize=1e-6, max_error_allowed=1e-8, iter_update_neighbors=100)
+
+
+def config(args, info, extra=None):
+    c = {"workload": "3d_mechanics_n%d_disk300um_z10um_%s_tol1e-8" %
+                     (args.n, {1: "HE21", 2: "BS32", 3: "RKF45", 4: "DP54"}[args.tableau]),
+         "cells": args.n, "tableau": {1: "HE21", 2: "BS32", 3: "RKF45", 4: "DP54"}[args.tableau],
+         "rk_tol": 1e-8, "max_stepsize_h": 1e-6, "iter_update_neighbors": 100,
+         "adhesion": "JKR isotropic gamma=100", "precision": args.precision,
+         "mean_contacts_per_cell": round(info["mean_contacts_per_cell"], 3),
+         "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# algorithmic (unique) bytes per launch of each kernel, per cell
+def pair_force_bytes(n, n_dir):
+    # own geometry record 64 B + row_ptr 8 B + its neighbor indices 4 B each + dE/dq write 48 B
+    return n * (64 + 8 + 48) + 4 * n_dir
+
+
+def attempt_bytes(n, final):
+    # geometry 64 + stored velocity 48 + physical record 64 + pair force 48 read;
+    # the accepted attempt also writes geometry 64 + velocity 48 + length 8
+    return n * (224 + (120 if final else 0))
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle run the way the reference runs
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(cells, args, steps, n_threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import abm_b200
+    import oracle_ref as orc
+    _, pd = abm_b200.make_params(**{k: v for k, v in sim_params(args, args.n).items()
+                                   if k not in ("cap_cells", "precision", "pair_lanes")})
+    o = orc.Oracle(pd, jkr=orc.jkr_table(0.8, 0.5, 3900.0, 100.0, 100), n_threads=n_threads)
+    o.set_cells(cells)
+    t0 = time.perf_counter()
+    o.loop_init()                                  # O(n^2) getCellNeighbors
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.iterate(steps, 0, 0)                         # pair forces recomputed per stage
+    t_steps = time.perf_counter() - t0
+    k = pd["iter_update_neighbors"]
+    t_amort = t_steps + t_build * steps / k
+    value = args.n * steps / t_amort
+    sample = ("%d accepted steps at n=%d (%.2f s) + one O(n^2) neighbor build (%.2f s) charged at the "
+              "reference cadence of one rebuild per %d steps" % (steps, args.n, t_steps, t_build, k))
+    return value, sample, dict(t_build_s=t_build, t_steps_s=t_steps)
+
+
+def cpu_info():
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return os.cpu_count() or 1, model
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return                                     # rank 0 alone times the host reference
+    cells, info = workload(args.n, SEED)
+    cores, model = cpu_info()
+    # each reference step is one accepted iteration at n = 100k (~0.1-0.5 s on the host);
+    # the run is bounded to about two minutes of CPU work
+    steps = max(1, min(args.steps, 60))
+    value, sample, extra = cpu_reference_rate(cells, args, steps, cores)
+    ms = 1000.0 * args.n / value
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded biofilm state)",
+            "impl": "reference",
+            "config": config(args, info, {"cpu_model": model, "requested_steps": args.steps}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    import abm_b200
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        dist_init("nccl")
+    cells, info = workload(args.n, SEED + rank)
+    sim = abm_b200.Simulation(**sim_params(args, args.n))
+    sim.upload_cells(cells)
+    pairs = sim.get_cell_neighbors()
+    stream = torch.cuda.ExternalStream(sim.stream, device=device)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    # warm-up (untimed)
+    sim.iterate(max(args.warmup, 0), stats=False)
+    sim.synchronize()
+    s0 = sim.stats()
+
+    # timed region: device-resident, L2 flushed between steps
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            sim.iterate(1, stats=False)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    sim.synchronize()
+    ms_total = sum(a.elapsed_time(b) for a, b in ev)
+    ms_total = reduce_max(ms_total, device, world)
+    s1 = sim.stats()
+    iters = s1["iterations"] - s0["iterations"]
+    attempts = s1["attempts"] - s0["attempts"]
+    rebuilds = s1["rebuilds"] - s0["rebuilds"]
+    value = world * args.n * args.steps / (ms_total / 1000.0)
+    # per iteration: pair force, trial, max_tries retries (exit at once when idle), final;
+    # per rebuild: bbox, bin count, 3 scan passes, scatter, pair build, 3 scan passes, CSR fill, counter
+    launches_per_iter = 3 + sim.params.max_tries_update_stepsize
+    gpu_launches = args.steps * launches_per_iter + rebuilds * 12
+
+    # per-kernel event timing for the roofline (same iteration loop without the graph)
+    prof = sim.profile_iterations(max(1, min(args.profile_steps, args.steps)))
+    n_dir = 2 * sim.stats()["n_pairs"]
+    pf_ms = prof["pair_force_ms"] / prof["pair_force_launches"]
+    at_ms = prof["attempt_ms"] / prof["iterations"]
+    peak, peak_kind = measured_peak_hbm()
+    traffic = load_traffic()
+    kernels = {
+        "k_pair_force": (pair_force_bytes(args.n, n_dir), pf_ms),
+        "k_attempt(trial+final)": (attempt_bytes(args.n, False) + attempt_bytes(args.n, True), at_ms),
+    }
+    dom = max(kernels, key=lambda k: kernels[k][1])
+    b, ms = kernels[dom]
+    achieved = b / (ms / 1000.0) / 1e9
+    tr = traffic.get(dom, {}).get("bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": tr, "kernel": dom,
+                "algorithmic_bytes_per_launch": b, "ms_per_launch": ms, "peak_source": peak_kind,
+                "other_kernels": {k: {"ms_per_launch": v[1], "algorithmic_bytes_per_launch": v[0],
+                                      "achieved_gbs": v[0] / (v[1] / 1000.0) / 1e9}
+                                  for k, v in kernels.items() if k != dom},
+                "rebuild_ms_per_rebuild": prof["rebuild_ms"] / max(prof["rebuild_launches"], 1)}
+
+    # e2e through the C ABI with pinned host buffers
+    ncols = cells.shape[1]
+    host = torch.empty((ncols, args.n), dtype=torch.float64, pin_memory=True)
+    host_np = host.numpy()
+    host_np[:] = sim.download_cells().T
+    ptr = host.data_ptr()
+    e2e_steps = max(1, min(args.steps, 200))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload_cells_raw(ptr, args.n, ncols, args.n)
+        sim.iterate(1, stats=False)
+        sim.download_cells_raw(ptr, args.n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), device, world)
+    e2e_value = world * args.n * e2e_steps / (e2e_ms / 1000.0)
+    nbytes = args.n * ncols * 8
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded biofilm state, p_contact=%g)" % P_CONTACT,
+            "config": config(args, info, {"pairs_per_cell": round(pairs / args.n, 3),
+                                          "rk_evals_per_step": round(attempts / max(iters, 1), 3),
+                                          "rebuilds_in_timed_region": rebuilds}),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
+            "gpu_launches": gpu_launches, "roofline": roofline,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores, model = cpu_info()
+        v, sample, extra = cpu_reference_rate(cells, args, args.cpu_steps, cores)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": sample + " on " + model}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,352 @@
+"""Python binding of the B200 mechanics step (ctypes over include/abm_capi.h).
+
+The names mirror the reference functions the C ABI stands in for
+(kmnam/biofilm-ABMs, ABM-3d/ABM-3d-cpp/include):
+
+    Simulation.get_cell_neighbors()        getCellNeighbors          mechanics.hpp:520-593
+    Simulation.neighbors()                 the neighbor table after updateNeighborDistances (:604-648)
+    Simulation.cell_cell_forces()          cellCellInteractionForces mechanics.hpp:1209-1659
+    Simulation.get_velocities()            getVelocities             mechanics.hpp:2011-2347
+    Simulation.step_runge_kutta_adaptive() stepRungeKuttaAdaptive    mechanics.hpp:2406-2612
+    Simulation.grow_cells()                growCells                 growth.hpp:51-57
+    Simulation.iterate()                   runSimulation loop body   simulation.hpp:1617-1864
+
+Arrays use the reference layout: cells are (n, ncols) float64 with the column
+order of indices.hpp (column 21 = gamma when adhesion is on); neighbor rows
+are (m, 7) = (i, j, dx, dy, dz, si, sj).  Errors raise RuntimeError, like the
+reference's std::runtime_error.  There is no CPU fallback: importing this
+module without the built library raises ImportError.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libabm_b200.so")
+
+ABM_OK = 0
+ERRORS = {-1: "ABM_ERR_ARG", -2: "ABM_ERR_CUDA", -3: "ABM_ERR_CAPACITY", -4: "ABM_ERR_NAN",
+          -5: "ABM_ERR_STATE"}
+HEUN_EULER, BOGACKI_SHAMPINE, RUNGE_KUTTA_FEHLBERG, DORMAND_PRINCE = 1, 2, 3, 4
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+# Column indices of the 3-D cell array (ABM-3d/ABM-3d-cpp/include/indices.hpp:17-47)
+COL = dict(id=0, rx=1, ry=2, rz=3, nx=4, ny=5, nz=6, drx=7, dry=8, drz=9, dnx=10, dny=11,
+           dnz=12, l=13, half_l=14, t0=15, growth=16, eta0=17, eta1=18, sigma0=19, group=20,
+           gamma=21)
+
+
+class AbmParams(ctypes.Structure):
+    _fields_ = [
+        ("R", ctypes.c_double), ("Rcell", ctypes.c_double), ("E0", ctypes.c_double),
+        ("Ecell", ctypes.c_double), ("L0", ctypes.c_double), ("Ldiv", ctypes.c_double),
+        ("neighbor_threshold", ctypes.c_double), ("nz_threshold", ctypes.c_double),
+        ("adhesion_mode", ctypes.c_int), ("integration_mode", ctypes.c_int),
+        ("max_stepsize", ctypes.c_double), ("min_stepsize", ctypes.c_double),
+        ("max_error_allowed", ctypes.c_double), ("min_error", ctypes.c_double),
+        ("max_tries_update_stepsize", ctypes.c_int), ("iter_update_stepsize", ctypes.c_int),
+        ("iter_update_neighbors", ctypes.c_int),
+        ("max_rxy_noise", ctypes.c_double), ("max_rz_noise", ctypes.c_double),
+        ("max_nxy_noise", ctypes.c_double), ("max_nz_noise", ctypes.c_double),
+        ("cell_surface_coulomb_coeff", ctypes.c_double), ("no_surface", ctypes.c_int),
+        ("growth_mean", ctypes.c_double), ("growth_std", ctypes.c_double),
+        ("daughter_length_std", ctypes.c_double), ("daughter_angle_xy_bound", ctypes.c_double),
+        ("daughter_angle_z_bound", ctypes.c_double), ("rng_seed", ctypes.c_ulonglong),
+        ("precision", ctypes.c_int), ("cap_cells", ctypes.c_int),
+        ("cap_neighbors_per_cell", ctypes.c_int), ("pair_lanes", ctypes.c_int),
+        ("use_graphs", ctypes.c_int),
+    ]
+
+
+class AbmStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_longlong), ("attempts", ctypes.c_longlong),
+        ("retries", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong),
+        ("divisions", ctypes.c_longlong), ("t", ctypes.c_double), ("dt", ctypes.c_double),
+        ("last_max_error", ctypes.c_double), ("n_cells", ctypes.c_int), ("n_pairs", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class AbmProfile(ctypes.Structure):
+    _fields_ = [
+        ("pair_force_ms", ctypes.c_double), ("attempt_ms", ctypes.c_double), ("rebuild_ms", ctypes.c_double),
+        ("pair_force_launches", ctypes.c_longlong), ("attempt_launches", ctypes.c_longlong),
+        ("rebuild_launches", ctypes.c_longlong), ("iterations", ctypes.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Defaults: the reference's 3-D driver (ABM-3d/ABM-3d-cpp/src/abmConstAdhesion.cpp) with
+# R = 0.8, Rcell = 0.5, E0 = 3900, Ecell = 3.9e6 (testTwoCellSimulations.cpp:46-48),
+# L0 = 2 so Ldiv = 2 L0 + 2 R (:41) and neighbor_threshold = 0.5 (2R + Ldiv) (:53).
+DEFAULTS = dict(
+    R=0.8, Rcell=0.5, E0=3900.0, Ecell=3.9e6, L0=2.0, Ldiv=5.6, neighbor_threshold=3.6,
+    nz_threshold=1e-8, adhesion_mode=1, integration_mode=HEUN_EULER, max_stepsize=1e-6,
+    min_stepsize=1e-9, max_error_allowed=1e-8, min_error=1e-30, max_tries_update_stepsize=3,
+    iter_update_stepsize=1, iter_update_neighbors=100, max_rxy_noise=0.0, max_rz_noise=0.0,
+    max_nxy_noise=0.0, max_nz_noise=0.0, cell_surface_coulomb_coeff=1.0, no_surface=0,
+    growth_mean=0.0, growth_std=0.0, daughter_length_std=0.0, daughter_angle_xy_bound=0.0,
+    daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
+    cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1,
+)
+
+
+def make_params(**kw):
+    d = dict(DEFAULTS)
+    for k in kw:
+        if k not in d:
+            raise KeyError("unknown parameter %s" % k)
+    d.update(kw)
+    p = AbmParams()
+    for k, v in d.items():
+        setattr(p, k, v)
+    return p, d
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libabm_b200.so is not built (%s); run __graft_entry__.build() or "
+                          "make -C biofilm-abms_b200" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    d, i, vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+    dp, ip = P(d), P(i)
+    sig = {
+        "abm_create": ([P(AbmParams), P(vp)], i),
+        "abm_destroy": ([vp], i),
+        "abm_last_error": ([vp], ctypes.c_char_p),
+        "abm_get_stream": ([vp, P(vp)], i),
+        "abm_synchronize": ([vp], i),
+        "abm_jkr_contact_radius": ([d, d, d, d, dp], i),
+        "abm_jkr_radius_table": ([d, d, d, d, i, dp, dp], i),
+        "abm_set_jkr_table": ([vp, dp, dp, i], i),
+        "abm_upload_cells": ([vp, dp, i, i, i], i),
+        "abm_download_cells": ([vp, dp, i], i),
+        "abm_get_num_cells": ([vp, ip], i),
+        "abm_set_clock": ([vp, d, d, i], i),
+        "abm_get_clock": ([vp, dp, dp, ip], i),
+        "abm_set_parents": ([vp, ip, i], i),
+        "abm_get_parents": ([vp, ip, i, ip], i),
+        "abm_build_neighbors": ([vp, ip], i),
+        "abm_download_neighbors": ([vp, dp, i, i, ip], i),
+        "abm_upload_neighbors": ([vp, dp, i, i], i),
+        "abm_cell_cell_forces": ([vp, dp], i),
+        "abm_get_velocities": ([vp, dp], i),
+        "abm_rk_attempt": ([vp, d, i, dp, dp, dp], i),
+        "abm_grow": ([vp, d], i),
+        "abm_divide": ([vp, ip], i),
+        "abm_iterate": ([vp, i, i, P(AbmStats)], i),
+        "abm_get_stats": ([vp, P(AbmStats)], i),
+        "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+LIB = _load()
+EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchronize "
+            "abm_jkr_contact_radius abm_jkr_radius_table abm_set_jkr_table abm_upload_cells "
+            "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
+            "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
+            "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
+            "abm_iterate abm_get_stats abm_profile_iterations").split()
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def jkr_contact_radius(delta, Req, E, gamma):
+    """jkrContactRadius(delta, Req, E, gamma).second (jkr.hpp:67-144)."""
+    out = ctypes.c_double()
+    rc = LIB.abm_jkr_contact_radius(delta, Req, E, gamma, ctypes.byref(out))
+    if rc:
+        raise RuntimeError("abm_jkr_contact_radius failed (%s)" % ERRORS.get(rc, rc))
+    return out.value
+
+
+def jkr_radius_table(R, Rcell, E0, gamma, n_mesh=100):
+    """Overlap mesh LinSpaced(n, 0, 2(R - Rcell)) and radii (simulation.hpp:86-104, 1379-1382)."""
+    delta = np.zeros(n_mesh)
+    radius = np.zeros(n_mesh)
+    rc = LIB.abm_jkr_radius_table(R, Rcell, E0, gamma, n_mesh, _dptr(delta), _dptr(radius))
+    if rc:
+        raise RuntimeError("abm_jkr_radius_table failed (%s)" % ERRORS.get(rc, rc))
+    return delta, radius
+
+
+class Simulation:
+    """One device context: state, neighbor set, controller and CUDA graphs."""
+
+    def __init__(self, gamma=100.0, n_mesh_overlap=100, jkr_table=None, **params):
+        self.params, self.pdict = make_params(**params)
+        if self.params.cap_cells <= 0:
+            raise ValueError("cap_cells must be set")
+        self._ctx = ctypes.c_void_p()
+        rc = LIB.abm_create(ctypes.byref(self.params), ctypes.byref(self._ctx))
+        if rc:
+            msg = LIB.abm_last_error(self._ctx).decode() if self._ctx else ""
+            if self._ctx:
+                LIB.abm_destroy(self._ctx)
+            self._ctx = None
+            raise RuntimeError("abm_create failed (%s): %s" % (ERRORS.get(rc, rc), msg))
+        self.ncols = None
+        if self.params.adhesion_mode:
+            if jkr_table is None:
+                jkr_table = jkr_radius_table(self.params.R, self.params.Rcell, self.params.E0, gamma,
+                                             n_mesh_overlap)
+            self.set_jkr_table(*jkr_table)
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, rc, what):
+        if rc:
+            raise RuntimeError("%s failed (%s): %s" % (what, ERRORS.get(rc, rc),
+                                                       LIB.abm_last_error(self._ctx).decode()))
+
+    def close(self):
+        if self._ctx:
+            LIB.abm_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(LIB.abm_get_stream(self._ctx, ctypes.byref(s)), "abm_get_stream")
+        return s.value
+
+    def synchronize(self):
+        self._check(LIB.abm_synchronize(self._ctx), "abm_synchronize")
+
+    # -- state ----------------------------------------------------------------
+    def set_jkr_table(self, delta, radius):
+        delta = np.ascontiguousarray(delta, dtype=np.float64)
+        radius = np.ascontiguousarray(radius, dtype=np.float64)
+        self._check(LIB.abm_set_jkr_table(self._ctx, _dptr(delta), _dptr(radius), len(delta)),
+                    "abm_set_jkr_table")
+
+    def upload_cells(self, cells):
+        """cells: (n, ncols) float64 array in the reference's column order."""
+        a = np.asfortranarray(cells, dtype=np.float64)
+        n, ncols = a.shape
+        self._check(LIB.abm_upload_cells(self._ctx, _dptr(a), n, ncols, max(n, 1)), "abm_upload_cells")
+        self.ncols = ncols
+
+    def upload_cells_raw(self, ptr, n, ncols, ld):
+        """Upload from a raw column-major host pointer (e.g. pinned memory)."""
+        self._check(LIB.abm_upload_cells(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                                         n, ncols, ld), "abm_upload_cells")
+        self.ncols = ncols
+
+    def download_cells(self):
+        n = self.num_cells()
+        out = np.zeros((n, self.ncols), dtype=np.float64, order="F")
+        self._check(LIB.abm_download_cells(self._ctx, _dptr(out), max(n, 1)), "abm_download_cells")
+        return out
+
+    def download_cells_raw(self, ptr, ld):
+        self._check(LIB.abm_download_cells(self._ctx, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)), ld),
+                    "abm_download_cells")
+
+    def num_cells(self):
+        n = ctypes.c_int()
+        self._check(LIB.abm_get_num_cells(self._ctx, ctypes.byref(n)), "abm_get_num_cells")
+        return n.value
+
+    def set_clock(self, t, dt, iteration):
+        self._check(LIB.abm_set_clock(self._ctx, t, dt, iteration), "abm_set_clock")
+
+    def clock(self):
+        t, dt, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(LIB.abm_get_clock(self._ctx, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it)),
+                    "abm_get_clock")
+        return t.value, dt.value, it.value
+
+    def set_parents(self, parents):
+        a = np.ascontiguousarray(parents, dtype=np.int32)
+        self._check(LIB.abm_set_parents(self._ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)),
+                    "abm_set_parents")
+
+    def parents(self):
+        n = ctypes.c_int()
+        self._check(LIB.abm_get_parents(self._ctx, None, 0, ctypes.byref(n)), "abm_get_parents")
+        a = np.zeros(n.value, dtype=np.int32)
+        self._check(LIB.abm_get_parents(self._ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n.value,
+                                        ctypes.byref(n)), "abm_get_parents")
+        return a
+
+    # -- hot path ---------------------------------------------------------------
+    def get_cell_neighbors(self):
+        m = ctypes.c_int()
+        self._check(LIB.abm_build_neighbors(self._ctx, ctypes.byref(m)), "abm_build_neighbors")
+        return m.value
+
+    def neighbors(self):
+        """(m, 7) table in the reference's row order with current distances."""
+        m = ctypes.c_int()
+        self._check(LIB.abm_download_neighbors(self._ctx, None, 0, 0, ctypes.byref(m)), "abm_download_neighbors")
+        out = np.zeros((m.value, 7), dtype=np.float64, order="F")
+        ld = max(m.value, 1)
+        self._check(LIB.abm_download_neighbors(self._ctx, _dptr(out), ld, m.value, ctypes.byref(m)),
+                    "abm_download_neighbors")
+        return out
+
+    def set_neighbors(self, rows):
+        a = np.asfortranarray(rows, dtype=np.float64)
+        self._check(LIB.abm_upload_neighbors(self._ctx, _dptr(a), a.shape[0], max(a.shape[0], 1)),
+                    "abm_upload_neighbors")
+
+    def cell_cell_forces(self):
+        n = self.num_cells()
+        out = np.zeros((n, 6), dtype=np.float64, order="F")
+        self._check(LIB.abm_cell_cell_forces(self._ctx, _dptr(out)), "abm_cell_cell_forces")
+        return out
+
+    def get_velocities(self):
+        n = self.num_cells()
+        out = np.zeros((n, 6), dtype=np.float64, order="F")
+        self._check(LIB.abm_get_velocities(self._ctx, _dptr(out)), "abm_get_velocities")
+        return out
+
+    def step_runge_kutta_adaptive(self, dt, attempt=0):
+        """One RK attempt at dt (not accepted): (new cells, errors, scaled max error)."""
+        n = self.num_cells()
+        cells = np.zeros((n, self.ncols), dtype=np.float64, order="F")
+        errors = np.zeros((n, 6), dtype=np.float64, order="F")
+        e = ctypes.c_double()
+        self._check(LIB.abm_rk_attempt(self._ctx, dt, attempt, _dptr(cells), _dptr(errors), ctypes.byref(e)),
+                    "abm_rk_attempt")
+        return cells, errors, e.value
+
+    def grow_cells(self, dt):
+        self._check(LIB.abm_grow(self._ctx, dt), "abm_grow")
+
+    def iterate(self, n_iters, n_cells_stop=0, stats=True):
+        s = AbmStats()
+        self._check(LIB.abm_iterate(self._ctx, n_iters, n_cells_stop, ctypes.byref(s) if stats else None),
+                    "abm_iterate")
+        return s.as_dict() if stats else None
+
+    def profile_iterations(self, n_iters):
+        p = AbmProfile()
+        self._check(LIB.abm_profile_iterations(self._ctx, n_iters, ctypes.byref(p)), "abm_profile_iterations")
+        return p.as_dict()
+
+    def stats(self):
+        s = AbmStats()
+        self._check(LIB.abm_get_stats(self._ctx, ctypes.byref(s)), "abm_get_stats")
+        return s.as_dict()

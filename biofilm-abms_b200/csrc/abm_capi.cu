@@ -1,0 +1,729 @@
+// C ABI of the B200 mechanics step (declared in include/abm_capi.h).
+//
+// A context owns the device state (cell records, CSR neighbor set, cell-list
+// buffers, controller state), one CUDA stream and two CUDA graphs: one loop
+// iteration (pair force -> trial attempt -> retries -> final attempt with
+// growth) and one neighbor rebuild (bbox -> counting sort -> pair build ->
+// CSR).  All sizes that change during a run (cell count, pair count, bin
+// count) live in device memory, so the graphs are captured once and replayed.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "abm_kernels.cuh"
+#include "../../include/abm_capi.h"
+
+using namespace abm;
+
+struct abm_ctx {
+    abm_params p;
+    std::string err;
+    int dev = 0, num_sms = 148;
+    cudaStream_t st = nullptr;
+    int cap = 0, cap_bins = 0, cap_nbr = 0;
+    int ncols = 0, has_gamma = 0;
+    int n_host = 0;
+    bool cells_loaded = false, nbrs_valid = false;
+    int host_iter = 0;
+    // device state
+    Geom* geom = nullptr; Vel* vel = nullptr; Phys* phys = nullptr; Gen6* fcc = nullptr;
+    Geom* geom_c = nullptr; Vel* vel_c = nullptr; Gen6* gen_tmp = nullptr;
+    Ctrl* ctrl = nullptr; Grid* grid = nullptr;
+    unsigned long long* bbox_acc = nullptr; unsigned int* bbox_counter = nullptr;
+    int *bin_count = nullptr, *bin_start = nullptr, *key = nullptr, *slot = nullptr, *sorted_cell = nullptr;
+    Geom* sorted_geom = nullptr;
+    int *scratch = nullptr, *nbr_count = nullptr, *row_ptr = nullptr, *col = nullptr;
+    int* scan_sums = nullptr;
+    double *jkr_delta = nullptr, *jkr_radius = nullptr;
+    int jkr_n = 0;
+    double* staging = nullptr;   // cap x (ncols max 32) doubles
+    std::vector<int> parents;
+    // parameters
+    ForceParams fp; StepParams sp; BuildParams bp;
+    // graphs
+    cudaGraphExec_t g_iter = nullptr, g_rebuild = nullptr;
+};
+
+static const int STAGING_COLS = 32;
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { \
+    if (c) c->err = std::string(#call) + ": " + cudaGetErrorString(e_); return ABM_ERR_CUDA; } } while (0)
+
+static int fail(abm_ctx* c, int code, const std::string& msg) { if (c) c->err = msg; return code; }
+
+// --------------------------------------------------------------------------
+// JKR contact radius: the largest real root of
+//   p(a) = a^4 - 2 Req delta a^2 - (4 pi gamma Req^2 / E) a + delta^2 Req^2
+// (jkr.hpp:81-84).  Newton's method started at the Cauchy bound converges
+// monotonically from above to the largest real root, because by Gauss-Lucas
+// the roots of p' and p'' also lie below that bound.
+// --------------------------------------------------------------------------
+static double jkr_radius_host(double delta, double Req, double E, double gamma)
+{
+    typedef long double LD;
+    const LD pi = 3.141592653589793238462643383279502884L;
+    LD c2 = -2.0L * Req * delta, c1 = -4.0L * pi * gamma * (LD)Req * Req / E, c0 = (LD)delta * delta * Req * Req;
+    LD x = 1.0L + std::max(std::fabs(c2), std::max(std::fabs(c1), std::fabs(c0)));
+    for (int it = 0; it < 500; ++it)
+    {
+        LD p = ((x * x + c2) * x + c1) * x + c0;
+        LD dp = (4.0L * x * x + 2.0L * c2) * x + c1;
+        if (dp <= 0) break;
+        LD xn = x - p / dp;
+        if (!(xn < x)) break;
+        x = xn;
+    }
+    return (double)x;
+}
+
+extern "C" {
+
+int abm_jkr_contact_radius(double delta, double Req, double E, double gamma, double* radius)
+{
+    if (!radius || Req <= 0 || E <= 0 || gamma < 0 || delta < 0) return ABM_ERR_ARG;
+    *radius = jkr_radius_host(delta, Req, E, gamma);
+    return ABM_OK;
+}
+
+int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_mesh,
+                         double* delta_out, double* radius_out)
+{
+    if (n_mesh < 2 || !delta_out || !radius_out) return ABM_ERR_ARG;
+    // Eigen LinSpaced(n, 0, 2 (R - Rcell)): low + i * step, last entry exactly high
+    const double high = 2 * (R - Rcell), step = (high - 0.0) / double(n_mesh - 1);
+    for (int i = 0; i < n_mesh; ++i)
+    {
+        delta_out[i] = (i == n_mesh - 1) ? high : 0.0 + double(i) * step;
+        radius_out[i] = jkr_radius_host(delta_out[i], R / 2, E0, gamma);
+    }
+    return ABM_OK;
+}
+
+const char* abm_last_error(const abm_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+static void free_all(abm_ctx* c)
+{
+    if (c->g_iter) cudaGraphExecDestroy(c->g_iter);
+    if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
+    void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->ctrl, c->grid,
+                    c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
+                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col,
+                    c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    if (c->st) cudaStreamDestroy(c->st);
+}
+
+static void fill_tableau(StepParams& sp, int mode, bool& ok)
+{
+    ok = true;
+    memset(sp.A, 0, sizeof(sp.A)); memset(sp.b, 0, sizeof(sp.b)); memset(sp.bs, 0, sizeof(sp.bs));
+    double q = 0;
+    // simulation.hpp:1207-1268
+    if (mode == ABM_HEUN_EULER)
+    {
+        sp.s = 2; sp.A[1][0] = 1; sp.b[0] = 0.5; sp.b[1] = 0.5; sp.bs[0] = 1; sp.bs[1] = 0; q = 1;
+    }
+    else if (mode == ABM_BOGACKI_SHAMPINE)
+    {
+        sp.s = 4;
+        sp.A[1][0] = 1. / 2.; sp.A[2][1] = 3. / 4.; sp.A[3][0] = 2. / 9.; sp.A[3][1] = 1. / 3.; sp.A[3][2] = 4. / 9.;
+        double b[4] = {2. / 9., 1. / 3., 4. / 9., 0}, bs[4] = {7. / 24., 1. / 4., 1. / 3., 1. / 8.};
+        for (int i = 0; i < 4; ++i) { sp.b[i] = b[i]; sp.bs[i] = bs[i]; }
+        q = 2;
+    }
+    else if (mode == ABM_RUNGE_KUTTA_FEHLBERG)
+    {
+        sp.s = 6;
+        double A[6][6] = {{0, 0, 0, 0, 0, 0}, {1. / 4., 0, 0, 0, 0, 0}, {3. / 32., 9. / 32., 0, 0, 0, 0},
+                          {1932. / 2197., -7200. / 2197., 7296. / 2197., 0, 0, 0},
+                          {439. / 216., -8.0, 3680. / 513., -845. / 4104., 0, 0},
+                          {-8. / 27., 2.0, -3544. / 2565., 1859. / 4104., -11. / 40., 0}};
+        double b[6] = {16. / 135., 0, 6656. / 12825., 28561. / 56430., -9. / 50., 2. / 55.};
+        double bs[6] = {25. / 216., 0, 1408. / 2565., 2197. / 4104., -1. / 5., 0};
+        for (int i = 0; i < 6; ++i) { for (int j = 0; j < 6; ++j) sp.A[i][j] = A[i][j]; sp.b[i] = b[i]; sp.bs[i] = bs[i]; }
+        q = 4;
+    }
+    else if (mode == ABM_DORMAND_PRINCE)
+    {
+        sp.s = 7;
+        double A[7][7] = {{0, 0, 0, 0, 0, 0, 0}, {1. / 5., 0, 0, 0, 0, 0, 0}, {3. / 40., 9. / 40., 0, 0, 0, 0, 0},
+                          {44. / 45., -56. / 15., 32. / 9., 0, 0, 0, 0},
+                          {19372. / 6561., -25360. / 2187., 64448. / 6561., -212. / 729, 0, 0, 0},
+                          {9017. / 3168., -355. / 33., 46732. / 5247., 49. / 176., -5103. / 18656., 0, 0},
+                          {35. / 384., 0, 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84., 0}};
+        double b[7] = {35. / 384., 0, 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84., 0};
+        double bs[7] = {5179. / 57600., 0, 7571. / 16695., 393. / 640., -92097. / 339200., 187. / 2100., 1. / 40.};
+        for (int i = 0; i < 7; ++i) { for (int j = 0; j < 7; ++j) sp.A[i][j] = A[i][j]; sp.b[i] = b[i]; sp.bs[i] = bs[i]; }
+        q = 4;
+    }
+    else ok = false;
+    sp.inv_q1 = 1.0 / (q + 1);
+}
+
+__global__ void k_set_n(Ctrl* c, int n) { c->n = n; }
+__global__ void k_set_clock(Ctrl* c, double t, double dt, int iter)
+{
+    c->t = t; c->dt = dt; c->iter = iter; c->mode = MODE_TRIAL; c->tries = 0; c->attempt = 0;
+    c->err_bits = 0; c->blocks_done = 0;
+}
+__global__ void k_count_rebuild(Ctrl* c) { c->rebuilds += 1; }
+
+int abm_create(const abm_params* q, abm_ctx** out)
+{
+    if (!q || !out) return ABM_ERR_ARG;
+    *out = nullptr;
+    abm_ctx* c = new abm_ctx();
+    c->p = *q;
+    abm_params& p = c->p;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+    {
+        c->err = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        *out = c;
+        return ABM_ERR_CUDA;
+    }
+    if (p.cap_cells <= 0 || p.R <= 0 || p.neighbor_threshold <= 0 || p.max_stepsize <= 0 ||
+        p.iter_update_stepsize <= 0 || p.iter_update_neighbors <= 0)
+    {
+        c->err = "invalid parameters";
+        *out = c;
+        return ABM_ERR_ARG;
+    }
+    bool ok;
+    fill_tableau(c->sp, p.integration_mode, ok);
+    if (!ok) { c->err = "unsupported integration_mode"; *out = c; return ABM_ERR_ARG; }
+    if (p.pair_lanes == 0) p.pair_lanes = 8;
+    if (p.pair_lanes != 4 && p.pair_lanes != 8 && p.pair_lanes != 16 && p.pair_lanes != 32)
+    {
+        c->err = "pair_lanes must be 4, 8, 16 or 32"; *out = c; return ABM_ERR_ARG;
+    }
+    c->cap = p.cap_cells;
+    c->cap_nbr = p.cap_neighbors_per_cell > 0 ? p.cap_neighbors_per_cell : 64;
+    *out = c;
+    CK(cudaGetDevice(&c->dev));
+    CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    // bins: at least one per 2 cells, at most 4M
+    c->cap_bins = std::min(std::max(c->cap * 2, 1 << 16), 1 << 22);
+    const size_t cap = c->cap;
+    CK(cudaMalloc(&c->geom, cap * sizeof(Geom)));
+    CK(cudaMalloc(&c->vel, cap * sizeof(Vel)));
+    CK(cudaMalloc(&c->phys, cap * sizeof(Phys)));
+    CK(cudaMalloc(&c->fcc, cap * sizeof(Gen6)));
+    CK(cudaMalloc(&c->geom_c, cap * sizeof(Geom)));
+    CK(cudaMalloc(&c->vel_c, cap * sizeof(Vel)));
+    CK(cudaMalloc(&c->gen_tmp, cap * sizeof(Gen6)));
+    CK(cudaMalloc(&c->ctrl, sizeof(Ctrl)));
+    CK(cudaMalloc(&c->grid, sizeof(Grid)));
+    CK(cudaMalloc(&c->bbox_acc, 8 * sizeof(unsigned long long)));
+    CK(cudaMalloc(&c->bbox_counter, sizeof(unsigned int)));
+    CK(cudaMalloc(&c->bin_count, (size_t)c->cap_bins * sizeof(int)));
+    CK(cudaMalloc(&c->bin_start, ((size_t)c->cap_bins + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->key, cap * sizeof(int)));
+    CK(cudaMalloc(&c->slot, cap * sizeof(int)));
+    CK(cudaMalloc(&c->sorted_cell, cap * sizeof(int)));
+    CK(cudaMalloc(&c->sorted_geom, cap * sizeof(Geom)));
+    CK(cudaMalloc(&c->scratch, cap * c->cap_nbr * sizeof(int)));
+    CK(cudaMalloc(&c->nbr_count, cap * sizeof(int)));
+    CK(cudaMalloc(&c->row_ptr, (cap + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->col, cap * c->cap_nbr * sizeof(int)));
+    size_t ns = std::max(scan_block_sums_size((int)cap + 1), scan_block_sums_size(c->cap_bins + 1)) + 1;
+    CK(cudaMalloc(&c->scan_sums, ns * sizeof(int)));
+    CK(cudaMalloc(&c->staging, cap * STAGING_COLS * sizeof(double)));
+    CK(cudaMemset(c->row_ptr, 0, (cap + 1) * sizeof(int)));
+    Ctrl h;
+    memset(&h, 0, sizeof(h));
+    h.dt = p.max_stepsize;
+    h.mode = MODE_TRIAL;
+    CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
+    unsigned long long acc0[8] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+    CK(cudaMemcpy(c->bbox_acc, acc0, sizeof(acc0), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->bbox_counter, 0, sizeof(unsigned int)));
+    // parameters of the kernels
+    MechParams mp;
+    mp.R = p.R; mp.Rcell = p.Rcell; mp.E0 = p.E0; mp.Ecell = p.Ecell; mp.sqrtR = std::sqrt(p.R);
+    mp.nz_threshold = p.nz_threshold; mp.coulomb = p.cell_surface_coulomb_coeff; mp.no_surface = p.no_surface;
+    StepParams& sp = c->sp;
+    sp.mp = mp;
+    sp.tol = p.max_error_allowed; sp.min_error = p.min_error;
+    sp.min_stepsize = p.min_stepsize; sp.max_stepsize = p.max_stepsize;
+    sp.max_tries = p.max_tries_update_stepsize; sp.iter_update_stepsize = p.iter_update_stepsize;
+    double nm[6] = {p.max_rxy_noise, p.max_rxy_noise, p.max_rz_noise, p.max_nxy_noise, p.max_nxy_noise, p.max_nz_noise};
+    for (int k = 0; k < 6; ++k) sp.noise_max[k] = nm[k];
+    sp.noise_on = (p.max_rxy_noise > 0 || p.max_rz_noise > 0 || p.max_nxy_noise > 0 || p.max_nz_noise > 0);
+    sp.seed = p.rng_seed;
+    ForceParams& fp = c->fp;
+    fp.R = p.R; fp.Rcell = p.Rcell; fp.E0 = p.E0;
+    // simulation.hpp:1270-1274
+    fp.pf0 = (4. / 3.) * p.E0 * std::sqrt(p.R / 2);
+    fp.pf1 = (4. / 3.) * p.Ecell * std::sqrt(p.Rcell / 2);
+    fp.pf2 = (4. / 3.) * p.E0 * std::sqrt(p.R / 2) * std::pow(2 * (p.R - p.Rcell), 1.5);
+    fp.max_overlap = 2 * (p.R - p.Rcell);
+    fp.adhesion = p.adhesion_mode != 0;
+    fp.jkr_n = 0; fp.jkr_step = 1.0;
+    c->bp.threshold = p.neighbor_threshold;
+    c->bp.prefilter = p.neighbor_threshold + p.Ldiv + 2 * p.R;
+    c->bp.cap_per_cell = c->cap_nbr;
+    if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
+        return fail(c, ABM_ERR_ARG, "adhesion_mode must be 0 (none) or 1 (isotropic JKR, fixed gamma)");
+    c->parents.clear();
+    return ABM_OK;
+}
+
+int abm_destroy(abm_ctx* c)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (c->st) cudaStreamSynchronize(c->st);
+    free_all(c);
+    delete c;
+    return ABM_OK;
+}
+
+int abm_get_stream(abm_ctx* c, void** stream)
+{
+    if (!c || !stream) return ABM_ERR_ARG;
+    *stream = (void*)c->st;
+    return ABM_OK;
+}
+
+static int check_status(abm_ctx* c)
+{
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (h.status & ST_NAN) return fail(c, ABM_ERR_NAN, "NaN/Inf in the RK error norm or velocities");
+    if (h.status & ST_NBR_OVERFLOW) return fail(c, ABM_ERR_CAPACITY, "neighbors per cell exceed cap_neighbors_per_cell");
+    if (h.status & ST_BIN_OVERFLOW) return fail(c, ABM_ERR_CAPACITY, "cell-list grid exceeds the bin capacity");
+    if (h.status & ST_CELL_OVERFLOW) return fail(c, ABM_ERR_CAPACITY, "division exceeds cap_cells");
+    return ABM_OK;
+}
+
+int abm_synchronize(abm_ctx* c)
+{
+    if (!c) return ABM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    return check_status(c);
+}
+
+int abm_set_jkr_table(abm_ctx* c, const double* delta, const double* radius, int n)
+{
+    if (!c || !delta || !radius || n < 2 || n > 512) return fail(c, ABM_ERR_ARG, "JKR table needs 2..512 entries");
+    for (int i = 1; i < n; ++i)
+        if (!(delta[i] > delta[i - 1])) return fail(c, ABM_ERR_ARG, "JKR overlap mesh must be increasing");
+    if (c->jkr_delta) { cudaFree(c->jkr_delta); cudaFree(c->jkr_radius); c->jkr_delta = c->jkr_radius = nullptr; }
+    CK(cudaMalloc(&c->jkr_delta, n * sizeof(double)));
+    CK(cudaMalloc(&c->jkr_radius, n * sizeof(double)));
+    CK(cudaMemcpy(c->jkr_delta, delta, n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->jkr_radius, radius, n * sizeof(double), cudaMemcpyHostToDevice));
+    c->jkr_n = n;
+    c->fp.jkr_n = n;
+    c->fp.jkr_step = (delta[n - 1] - delta[0]) / double(n - 1);
+    if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+    return ABM_OK;
+}
+
+int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
+{
+    if (!c || !cm || n < 0 || ld < n) return fail(c, ABM_ERR_ARG, "bad cell array");
+    if (n > c->cap) return fail(c, ABM_ERR_CAPACITY, "more cells than cap_cells");
+    if (ncols < 21 || ncols > STAGING_COLS) return fail(c, ABM_ERR_ARG, "cell arrays need 21..32 columns");
+    if (c->p.adhesion_mode != 0 && ncols < 22) return fail(c, ABM_ERR_ARG, "adhesion needs the gamma column (21)");
+    c->ncols = ncols;
+    c->has_gamma = (c->p.adhesion_mode != 0);
+    if (n > 0)
+    {
+        CK(cudaMemcpy2DAsync(c->staging, (size_t)n * sizeof(double), cm, (size_t)ld * sizeof(double),
+                             (size_t)n * sizeof(double), ncols, cudaMemcpyHostToDevice, c->st));
+        launch_cells_from_colmajor(c->staging, n, ncols, n, c->has_gamma, c->geom, c->vel, c->phys, c->st);
+    }
+    k_set_n<<<1, 1, 0, c->st>>>(c->ctrl, n);
+    CK(cudaGetLastError());
+    if (c->n_host != n) c->nbrs_valid = false;
+    c->n_host = n;
+    c->cells_loaded = true;
+    return ABM_OK;
+}
+
+int abm_download_cells(abm_ctx* c, double* cm, int ld)
+{
+    if (!c || !cm) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int n = h.n;
+    c->n_host = n;
+    if (ld < n) return fail(c, ABM_ERR_ARG, "ld smaller than the cell count");
+    if (n > 0)
+    {
+        launch_cells_to_colmajor(c->geom, c->vel, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        CK(cudaMemcpy2DAsync(cm, (size_t)ld * sizeof(double), c->staging, (size_t)n * sizeof(double),
+                             (size_t)n * sizeof(double), c->ncols, cudaMemcpyDeviceToHost, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
+int abm_get_num_cells(abm_ctx* c, int* n)
+{
+    if (!c || !n) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *n = h.n;
+    return ABM_OK;
+}
+
+int abm_set_clock(abm_ctx* c, double t, double dt, int iter)
+{
+    if (!c || !(dt > 0)) return ABM_ERR_ARG;
+    k_set_clock<<<1, 1, 0, c->st>>>(c->ctrl, t, dt, iter);
+    CK(cudaGetLastError());
+    c->host_iter = iter;
+    return ABM_OK;
+}
+
+int abm_get_clock(abm_ctx* c, double* t, double* dt, int* iter)
+{
+    if (!c) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (t) *t = h.t;
+    if (dt) *dt = h.dt;
+    if (iter) *iter = h.iter;
+    return ABM_OK;
+}
+
+int abm_set_parents(abm_ctx* c, const int* parents, int n)
+{
+    if (!c || (n > 0 && !parents) || n < 0) return ABM_ERR_ARG;
+    c->parents.assign(parents, parents + n);
+    return ABM_OK;
+}
+
+int abm_get_parents(abm_ctx* c, int* out, int cap, int* n)
+{
+    if (!c) return ABM_ERR_ARG;
+    int m = (int)c->parents.size();
+    if (n) *n = m;
+    if (out) for (int i = 0; i < m && i < cap; ++i) out[i] = c->parents[i];
+    return ABM_OK;
+}
+
+// neighbor rebuild sequence (getCellNeighbors, mechanics.hpp:520-593)
+static void enqueue_rebuild(abm_ctx* c)
+{
+    cudaStream_t st = c->st;
+    launch_bbox(c->geom, c->ctrl, c->grid, c->bbox_acc, c->bbox_counter, c->bp.prefilter, c->cap_bins, c->cap, st);
+    cudaMemsetAsync(c->bin_count, 0, (size_t)c->cap_bins * sizeof(int), st);
+    launch_bin_count(c->geom, c->ctrl, c->grid, c->bin_count, c->key, c->slot, c->cap, st);
+    launch_scan(c->bin_count, &c->grid->nbins, c->bin_start, c->scan_sums, c->cap_bins, st);
+    launch_bin_scatter(c->geom, c->ctrl, c->bin_start, c->key, c->slot, c->sorted_cell, c->sorted_geom, c->cap, st);
+    launch_pair_build(c->grid, c->bin_start, c->sorted_cell, c->sorted_geom, c->ctrl, c->bp, c->scratch,
+                      c->nbr_count, c->cap_bins, c->num_sms, st);
+    launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
+    launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
+    k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
+}
+
+// one iteration of the loop body without division
+static void enqueue_iteration(abm_ctx* c)
+{
+    cudaStream_t st = c->st;
+    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, st);
+    launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                   0.0, 0, c->cap, st);
+    for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
+        launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                       0.0, 0, c->cap, st);
+    launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                   0.0, 0, c->cap, st);
+}
+
+static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
+{
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    fn(c);
+    CK(cudaStreamEndCapture(c->st, &g));
+    cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    return ABM_OK;
+}
+
+static int ready_for_forces(abm_ctx* c)
+{
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    if (c->p.adhesion_mode != 0 && c->jkr_n < 2) return fail(c, ABM_ERR_STATE, "JKR table not set");
+    return ABM_OK;
+}
+
+int abm_build_neighbors(abm_ctx* c, int* m)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    enqueue_rebuild(c);
+    CK(cudaGetLastError());
+    c->nbrs_valid = true;
+    int rc = check_status(c);
+    if (rc) return rc;
+    if (m)
+    {
+        Ctrl h;
+        CK(cudaMemcpy(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+        *m = h.n_dir / 2;
+    }
+    return ABM_OK;
+}
+
+int abm_download_neighbors(abm_ctx* c, double* rows, int ld, int cap, int* m)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int mm = h.n_dir / 2;
+    if (m) *m = mm;
+    if (!rows) return ABM_OK;
+    if (cap < mm || ld < mm) return fail(c, ABM_ERR_CAPACITY, "row buffer too small");
+    launch_count_lower(c->ctrl, c->row_ptr, c->col, c->nbr_count, c->cap, c->st);
+    launch_scan(c->nbr_count, &c->ctrl->n, c->key, c->scan_sums, c->cap, c->st);
+    double* d_rows = nullptr;
+    CK(cudaMallocAsync(&d_rows, (size_t)std::max(mm, 1) * 7 * sizeof(double), c->st));
+    launch_table_rows(c->ctrl, c->row_ptr, c->col, c->key, c->geom, d_rows, std::max(mm, 1), c->cap, c->st);
+    if (mm > 0)
+        CK(cudaMemcpy2DAsync(rows, (size_t)ld * sizeof(double), d_rows, (size_t)mm * sizeof(double),
+                             (size_t)mm * sizeof(double), 7, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaFreeAsync(d_rows, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
+int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
+{
+    if (!c || (m > 0 && !rows) || ld < m) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    const int n = c->n_host;
+    std::vector<std::vector<int>> adj(n);
+    for (int k = 0; k < m; ++k)
+    {
+        int i = (int)rows[k], j = (int)rows[(size_t)ld + k];
+        if (i < 0 || j < 0 || i >= n || j >= n || i == j) return fail(c, ABM_ERR_ARG, "bad neighbor row");
+        adj[i].push_back(j); adj[j].push_back(i);
+    }
+    std::vector<int> rp(n + 1, 0), cl;
+    for (int i = 0; i < n; ++i)
+    {
+        std::sort(adj[i].begin(), adj[i].end());
+        if ((int)adj[i].size() > c->cap_nbr) return fail(c, ABM_ERR_CAPACITY, "neighbors per cell exceed capacity");
+        rp[i + 1] = rp[i] + (int)adj[i].size();
+        cl.insert(cl.end(), adj[i].begin(), adj[i].end());
+    }
+    CK(cudaMemcpyAsync(c->row_ptr, rp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    if (!cl.empty()) CK(cudaMemcpyAsync(c->col, cl.data(), cl.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    h.n_dir = (int)cl.size();
+    CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
+    c->nbrs_valid = true;
+    return ABM_OK;
+}
+
+static int download_gen6(abm_ctx* c, const Gen6* src, double* out)
+{
+    int n = c->n_host;
+    if (n == 0) return ABM_OK;
+    launch_gen6_to_colmajor(src, n, c->staging, c->st);
+    CK(cudaMemcpyAsync(out, c->staging, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
+int abm_cell_cell_forces(abm_ctx* c, double* out)
+{
+    if (!c || !out) return ABM_ERR_ARG;
+    int rc = ready_for_forces(c);
+    if (rc) return rc;
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    CK(cudaGetLastError());
+    return download_gen6(c, c->fcc, out);
+}
+
+int abm_get_velocities(abm_ctx* c, double* out)
+{
+    if (!c || !out) return ABM_ERR_ARG;
+    int rc = ready_for_forces(c);
+    if (rc) return rc;
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    launch_velocities(c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->gen_tmp, c->cap, c->st);
+    CK(cudaGetLastError());
+    rc = download_gen6(c, c->gen_tmp, out);
+    if (rc) return rc;
+    return check_status(c);
+}
+
+__global__ void k_clear_eval(Ctrl* c) { c->eval_err_bits = 0ull; }
+
+int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double* errors_out,
+                   double* max_scaled_error)
+{
+    if (!c || !(dt > 0)) return ABM_ERR_ARG;
+    int rc = ready_for_forces(c);
+    if (rc) return rc;
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    k_clear_eval<<<1, 1, 0, c->st>>>(c->ctrl);
+    launch_attempt(3, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->gen_tmp,
+                   dt, attempt, c->cap, c->st);
+    CK(cudaGetLastError());
+    const int n = c->n_host;
+    if (cells_out && n > 0)
+    {
+        launch_cells_to_colmajor(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        CK(cudaMemcpyAsync(cells_out, c->staging, (size_t)n * c->ncols * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    }
+    if (errors_out)
+    {
+        rc = download_gen6(c, c->gen_tmp, errors_out);
+        if (rc) return rc;
+    }
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (max_scaled_error)
+    {
+        double e;
+        memcpy(&e, &h.eval_err_bits, sizeof(double));
+        *max_scaled_error = std::max(e, c->p.min_error);
+    }
+    return check_status(c);
+}
+
+int abm_grow(abm_ctx* c, double dt)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    launch_grow(c->geom, c->phys, c->ctrl, c->p.R, dt, c->cap, c->st);
+    CK(cudaGetLastError());
+    return ABM_OK;
+}
+
+int abm_divide(abm_ctx* c, int* n_divided)
+{
+    (void)n_divided;
+    return fail(c, ABM_ERR_ARG, "division is not available in this build");
+}
+
+int abm_get_stats(abm_ctx* c, abm_stats* s)
+{
+    if (!c || !s) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    s->iterations = h.iterations; s->attempts = h.attempts; s->retries = h.retries;
+    s->rebuilds = h.rebuilds; s->divisions = h.divisions;
+    s->t = h.t; s->dt = h.dt; s->last_max_error = h.last_max_error;
+    s->n_cells = h.n; s->n_pairs = h.n_dir / 2;
+    return check_status(c);
+}
+
+int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
+{
+    if (!c || n_iters < 0) return ABM_ERR_ARG;
+    int rc = ready_for_forces(c);
+    if (rc) return rc;
+    if (c->p.growth_mean != 0 || c->p.growth_std != 0)
+    {
+        // cells may cross Ldiv; division is handled by abm_divide's kernels when present
+    }
+    if (!c->nbrs_valid)
+    {
+        enqueue_rebuild(c);
+        c->nbrs_valid = true;
+    }
+    (void)n_cells_stop;
+    if (c->p.use_graphs)
+    {
+        if (!c->g_iter) { rc = capture(c, enqueue_iteration, &c->g_iter); if (rc) return rc; }
+        if (!c->g_rebuild) { rc = capture(c, enqueue_rebuild, &c->g_rebuild); if (rc) return rc; }
+    }
+    for (int k = 0; k < n_iters; ++k)
+    {
+        if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
+        else enqueue_iteration(c);
+        c->host_iter += 1;
+        if (c->host_iter % c->p.iter_update_neighbors == 0)
+        {
+            if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_rebuild, c->st));
+            else enqueue_rebuild(c);
+        }
+    }
+    CK(cudaGetLastError());
+    if (stats) return abm_get_stats(c, stats);
+    return ABM_OK;
+}
+
+int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
+{
+    if (!c || !prof || n_iters < 0) return ABM_ERR_ARG;
+    int rc = ready_for_forces(c);
+    if (rc) return rc;
+    if (!c->nbrs_valid) { enqueue_rebuild(c); c->nbrs_valid = true; }
+    memset(prof, 0, sizeof(*prof));
+    std::vector<cudaEvent_t> ev((size_t)n_iters * 4);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    std::vector<int> rebuilt(n_iters, 0);
+    cudaStream_t st = c->st;
+    for (int k = 0; k < n_iters; ++k)
+    {
+        cudaEvent_t* e = &ev[(size_t)k * 4];
+        CK(cudaEventRecord(e[0], st));
+        launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                          c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, st);
+        CK(cudaEventRecord(e[1], st));
+        launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                       0.0, 0, c->cap, st);
+        for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
+            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr,
+                           nullptr, 0.0, 0, c->cap, st);
+        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                       0.0, 0, c->cap, st);
+        CK(cudaEventRecord(e[2], st));
+        c->host_iter += 1;
+        if (c->host_iter % c->p.iter_update_neighbors == 0) { enqueue_rebuild(c); rebuilt[k] = 1; }
+        CK(cudaEventRecord(e[3], st));
+    }
+    CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < n_iters; ++k)
+    {
+        cudaEvent_t* e = &ev[(size_t)k * 4];
+        float a, b, d;
+        CK(cudaEventElapsedTime(&a, e[0], e[1]));
+        CK(cudaEventElapsedTime(&b, e[1], e[2]));
+        CK(cudaEventElapsedTime(&d, e[2], e[3]));
+        prof->pair_force_ms += a;
+        prof->attempt_ms += b;
+        prof->pair_force_launches += 1;
+        prof->attempt_launches += 2 + c->p.max_tries_update_stepsize;
+        if (rebuilt[k]) { prof->rebuild_ms += d; prof->rebuild_launches += 1; }
+    }
+    prof->iterations = n_iters;
+    for (auto& e : ev) cudaEventDestroy(e);
+    return check_status(c);
+}
+
+}   // extern "C"

@@ -1,0 +1,486 @@
+// Device-side building blocks of the B200 mechanics step: state records,
+// exact-rounding segment distance, surface integrals, the per-cell velocity
+// solve and the Philox counter RNG.  Every function names the reference
+// file:line (kmnam/biofilm-ABMs, ABM-3d/ABM-3d-cpp/include) whose arithmetic
+// it reproduces.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace abm {
+
+// ---------------------------------------------------------------------------
+// State records.  Cell geometry is gathered at random by the pair kernels, so
+// it is one 64-byte record per cell (two 32-byte sectors, read as four 16-byte
+// loads); everything else is streamed once per cell per kernel.
+// ---------------------------------------------------------------------------
+struct __align__(64) Geom {     // position, half-length, orientation, gamma
+    double rx, ry, rz, h;
+    double nx, ny, nz, gamma;
+};
+struct __align__(16) Vel {      // stored velocities of the last accepted step (dr, dn)
+    double v[6];
+};
+struct __align__(64) Phys {     // l, growth, eta0, eta1, sigma0, t0, id, group
+    double l, growth, eta0, eta1, sigma0, t0, id, group;
+};
+struct __align__(16) Gen6 {     // generalised force / dE/dq
+    double f[6];
+};
+
+__device__ __forceinline__ Geom load_geom(const Geom* __restrict__ g, int i)
+{
+    const double2* p = reinterpret_cast<const double2*>(g + i);
+    double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    Geom o;
+    o.rx = a.x; o.ry = a.y; o.rz = b.x; o.h = b.y;
+    o.nx = c.x; o.ny = c.y; o.nz = d.x; o.gamma = d.y;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// Exact-rounding vector arithmetic.  The neighbor decision |d| < threshold
+// must come out identically on the GPU and in the CPU restatement, so the
+// segment distance uses only correctly rounded +, -, *, /, sqrt with no
+// fused multiply-add (the __d*_rn intrinsics are never contracted), summing
+// dot products as ((x + y) + z).
+// ---------------------------------------------------------------------------
+struct X3 { double x, y, z; };
+__device__ __forceinline__ X3 x3(double x, double y, double z) { X3 v; v.x = x; v.y = y; v.z = z; return v; }
+__device__ __forceinline__ X3 xadd(X3 a, X3 b) { return x3(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y), __dadd_rn(a.z, b.z)); }
+__device__ __forceinline__ X3 xsub(X3 a, X3 b) { return x3(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)); }
+__device__ __forceinline__ X3 xscale(double s, X3 a) { return x3(__dmul_rn(s, a.x), __dmul_rn(s, a.y), __dmul_rn(s, a.z)); }
+__device__ __forceinline__ double xdot(X3 a, X3 b)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ double xnorm(X3 a) { return __dsqrt_rn(xdot(a, a)); }
+
+// distances.hpp:92-105 (nearestCellBodyCoordToPoint)
+__device__ __forceinline__ double nearest_body_coord(X3 r, X3 n, double h, X3 q)
+{
+    double s = xdot(xsub(q, r), n);
+    if (fabs(s) <= h) return s;
+    else if (s > h) return h;
+    return -h;
+}
+
+__device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+// Closest-point parameters of two segments p1 + x (q1 - p1), p2 + y (q2 - p2),
+// standing in for CGAL's Segment_3/Segment_3 squared_distance result
+// (distances.hpp:341).  Method: Ericson, Real-Time Collision Detection (2005),
+// sec. 5.1.9.
+__device__ __forceinline__ void closest_params(X3 p1, X3 q1, X3 p2, X3 q2, double& x, double& y)
+{
+    X3 d1 = xsub(q1, p1), d2 = xsub(q2, p2), r = xsub(p1, p2);
+    double a = xdot(d1, d1), e = xdot(d2, d2), f = xdot(d2, r);
+    if (a <= 0.0 && e <= 0.0) { x = 0.0; y = 0.0; return; }
+    if (a <= 0.0) { x = 0.0; y = clamp01(__ddiv_rn(f, e)); return; }
+    double c = xdot(d1, r);
+    if (e <= 0.0) { y = 0.0; x = clamp01(__ddiv_rn(-c, a)); return; }
+    double b = xdot(d1, d2);
+    double denom = __dsub_rn(__dmul_rn(a, e), __dmul_rn(b, b));
+    double s = (denom != 0.0)
+        ? clamp01(__ddiv_rn(__dsub_rn(__dmul_rn(b, f), __dmul_rn(c, e)), denom)) : 0.0;
+    double t = __ddiv_rn(__dadd_rn(__dmul_rn(b, s), f), e);
+    if (t < 0.0) { t = 0.0; s = clamp01(__ddiv_rn(-c, a)); }
+    else if (t > 1.0) { t = 1.0; s = clamp01(__ddiv_rn(__dsub_rn(b, c), a)); }
+    x = s; y = t;
+}
+
+struct Dist { double dx, dy, dz, s, t; };
+
+// distances.hpp:206-357 (distBetweenCells): d runs from cell 1 to cell 2.
+__device__ __forceinline__ Dist dist_between_cells(X3 r1, X3 n1, double h1, X3 r2, X3 n2, double h2)
+{
+    Dist o;
+    double cos_theta = xdot(n1, n2);
+    X3 p1 = xsub(r1, xscale(h1, n1)), q1 = xadd(r1, xscale(h1, n1));
+    X3 p2 = xsub(r2, xscale(h2, n2)), q2 = xadd(r2, xscale(h2, n2));
+    X3 d; double s, t;
+    if (cos_theta >= 0.9999 || cos_theta <= -0.9999)
+    {
+        double s_p1 = nearest_body_coord(r2, n2, h2, p1);
+        double s_q1 = nearest_body_coord(r2, n2, h2, q1);
+        X3 d_p1 = xsub(xadd(r2, xscale(s_p1, n2)), p1);
+        X3 d_q1 = xsub(xadd(r2, xscale(s_q1, n2)), q1);
+        double dist_p1 = xnorm(d_p1), dist_q1 = xnorm(d_q1);
+        if (s_p1 == s_q1)
+        {
+            if (dist_p1 < dist_q1) { s = -h1; t = s_p1; d = d_p1; }
+            else { s = h1; t = s_q1; d = d_q1; }
+        }
+        else
+        {
+            double s_p2 = nearest_body_coord(r1, n1, h1, p2);
+            double s_q2 = nearest_body_coord(r1, n1, h1, q2);
+            X3 d_p2 = xsub(xadd(r1, xscale(s_p2, n1)), p2);
+            X3 d_q2 = xsub(xadd(r1, xscale(s_q2, n1)), q2);
+            double dist_p2 = xnorm(d_p2), dist_q2 = xnorm(d_q2);
+            // the two smallest of four distances; ties keep index order, as the
+            // reference's std::sort of a 4-element range does (insertion sort)
+            double dv[4] = {dist_p1, dist_q1, dist_p2, dist_q2};
+            int iv[4] = {0, 1, 2, 3};
+#pragma unroll
+            for (int a = 1; a < 4; ++a)
+            {
+                double kd = dv[a]; int ki = iv[a]; int b = a - 1;
+                while (b >= 0 && kd < dv[b]) { dv[b + 1] = dv[b]; iv[b + 1] = iv[b]; --b; }
+                dv[b + 1] = kd; iv[b + 1] = ki;
+            }
+            bool m0 = (iv[0] == 0 || iv[1] == 0), m1 = (iv[0] == 1 || iv[1] == 1);
+            bool m2 = (iv[0] == 2 || iv[1] == 2);
+            if (m0 && m1)
+            {
+                s = 0.0;
+                t = nearest_body_coord(r2, n2, h2, r1);
+                d = xsub(xadd(r2, xscale(t, n2)), r1);
+            }
+            else if (!m0 && !m1)
+            {
+                t = 0.0;
+                s = nearest_body_coord(r1, n1, h1, r2);
+                d = xsub(xsub(r2, r1), xscale(s, n1));
+            }
+            else
+            {
+                double end1 = m0 ? -h1 : h1;
+                double end2 = m2 ? s_p2 : s_q2;
+                s = __ddiv_rn(__dadd_rn(end1, end2), 2.0);
+                t = nearest_body_coord(r2, n2, h2, xadd(r1, xscale(s, n1)));
+                d = xsub(xsub(xadd(r2, xscale(t, n2)), r1), xscale(s, n1));
+            }
+        }
+    }
+    else
+    {
+        double x, y;
+        closest_params(p1, q1, p2, q2, x, y);
+        s = __dsub_rn(__dmul_rn(__dmul_rn(x, 2.0), h1), h1);
+        t = __dsub_rn(__dmul_rn(__dmul_rn(y, 2.0), h2), h2);
+        d = xsub(xsub(xadd(r2, xscale(t, n2)), r1), xscale(s, n1));
+    }
+    o.dx = d.x; o.dy = d.y; o.dz = d.z; o.s = s; o.t = t;
+    return o;
+}
+
+__device__ __forceinline__ Dist dist_geom(const Geom& a, const Geom& b)
+{
+    return dist_between_cells(x3(a.rx, a.ry, a.rz), x3(a.nx, a.ny, a.nz), a.h,
+                              x3(b.rx, b.ry, b.rz), x3(b.nx, b.ny, b.nz), b.h);
+}
+
+// Mixed-precision variant: the generic (skew) branch in FP32, the
+// near-parallel branch (|cos| >= 0.9999, ill-conditioned s, t) in FP64.
+__device__ __forceinline__ Dist dist_geom_mixed(const Geom& a, const Geom& b)
+{
+    float n1x = (float)a.nx, n1y = (float)a.ny, n1z = (float)a.nz;
+    float n2x = (float)b.nx, n2y = (float)b.ny, n2z = (float)b.nz;
+    double cos_theta = xdot(x3(a.nx, a.ny, a.nz), x3(b.nx, b.ny, b.nz));
+    if (cos_theta >= 0.9999 || cos_theta <= -0.9999) return dist_geom(a, b);
+    // relative coordinates keep FP32 well conditioned far from the origin
+    float rx = (float)(b.rx - a.rx), ry = (float)(b.ry - a.ry), rz = (float)(b.rz - a.rz);
+    float h1 = (float)a.h, h2 = (float)b.h;
+    // segment 1: -h1 n1 .. +h1 n1 (origin at r1); segment 2: r - h2 n2 .. r + h2 n2
+    float d1x = 2.f * h1 * n1x, d1y = 2.f * h1 * n1y, d1z = 2.f * h1 * n1z;
+    float d2x = 2.f * h2 * n2x, d2y = 2.f * h2 * n2y, d2z = 2.f * h2 * n2z;
+    float p2x = rx - h2 * n2x, p2y = ry - h2 * n2y, p2z = rz - h2 * n2z;
+    float wx = -h1 * n1x - p2x, wy = -h1 * n1y - p2y, wz = -h1 * n1z - p2z;   // p1 - p2
+    float aa = d1x * d1x + d1y * d1y + d1z * d1z;
+    float e = d2x * d2x + d2y * d2y + d2z * d2z;
+    float f = d2x * wx + d2y * wy + d2z * wz;
+    float c = d1x * wx + d1y * wy + d1z * wz;
+    float bb = d1x * d2x + d1y * d2y + d1z * d2z;
+    float x, y;
+    if (aa <= 0.f && e <= 0.f) { x = 0.f; y = 0.f; }
+    else if (aa <= 0.f) { x = 0.f; y = fminf(fmaxf(f / e, 0.f), 1.f); }
+    else if (e <= 0.f) { y = 0.f; x = fminf(fmaxf(-c / aa, 0.f), 1.f); }
+    else
+    {
+        float denom = aa * e - bb * bb;
+        float s = denom != 0.f ? fminf(fmaxf((bb * f - c * e) / denom, 0.f), 1.f) : 0.f;
+        float t = (bb * s + f) / e;
+        if (t < 0.f) { t = 0.f; s = fminf(fmaxf(-c / aa, 0.f), 1.f); }
+        else if (t > 1.f) { t = 1.f; s = fminf(fmaxf((bb - c) / aa, 0.f), 1.f); }
+        x = s; y = t;
+    }
+    float s1 = x * 2.f * h1 - h1, t2 = y * 2.f * h2 - h2;
+    Dist o;
+    o.dx = (double)(rx + t2 * n2x - s1 * n1x);
+    o.dy = (double)(ry + t2 * n2y - s1 * n1y);
+    o.dz = (double)(rz + t2 * n2z - s1 * n1z);
+    o.s = (double)s1; o.t = (double)t2;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11), the counter-based draw policy shared
+// with the CPU restatement.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r)
+    {
+        uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t y0 = hi1 ^ c[1] ^ k0, y2 = hi0 ^ c[3] ^ k1;
+        c[0] = y0; c[1] = lo1; c[2] = y2; c[3] = lo0;
+        k0 += W0; k1 += W1;
+    }
+}
+__host__ __device__ __forceinline__ double philox_u01(uint32_t hi, uint32_t lo)
+{
+    uint64_t bits = (((uint64_t)hi << 32) | lo) >> 12;
+    return ((double)bits + 0.5) * (1.0 / 4503599627370496.0);
+}
+const uint32_t RNG_PURPOSE_NOISE = 0x4E6F6973u;
+const uint32_t RNG_PURPOSE_DIVIDE = 0x44697669u;
+
+__host__ __device__ __forceinline__ double rng_uniform(uint64_t seed, uint32_t purpose, uint32_t a,
+                                                       uint32_t b, uint32_t c, uint32_t d)
+{
+    uint32_t x[4] = {a, b, c, d};
+    philox4x32_10(x, (uint32_t)seed, (uint32_t)(seed >> 32) ^ purpose);
+    return philox_u01(x[0], x[1]);
+}
+
+// ---------------------------------------------------------------------------
+// Surface integrals (integrals.hpp) with the overlap powers taken from one
+// square root: p^{k+1/2} = p^k sqrt(p).
+// ---------------------------------------------------------------------------
+struct EndPow {               // powers of the end overlaps phi(-h) (1) and phi(+h) (2)
+    double p1, q1;            // p^1/2
+    double p2, q2;            // p^1
+    double p3, q3;            // p^3/2
+    double p4, q4;            // p^2
+    double p5, q5;            // p^5/2
+    double p6, q6;            // p^3
+    double p7, q7;            // p^7/2
+};
+
+// exponent index e = 2 (gamma + 1): 1 -> p^0.5, 2 -> p, 3 -> p^1.5, ...
+__device__ __forceinline__ double epw(const EndPow& w, int e, bool second)
+{
+    switch (e)
+    {
+        case 1: return second ? w.q1 : w.p1;
+        case 2: return second ? w.q2 : w.p2;
+        case 3: return second ? w.q3 : w.p3;
+        case 4: return second ? w.q4 : w.p4;
+        case 5: return second ? w.q5 : w.p5;
+        case 6: return second ? w.q6 : w.p6;
+        default: return second ? w.q7 : w.p7;
+    }
+}
+
+__device__ __forceinline__ void fill_pows(double p, double& r1, double& r2, double& r3, double& r4,
+                                          double& r5, double& r6, double& r7)
+{
+    double sq = sqrt(p);
+    r1 = sq; r2 = p; r3 = p * sq; r4 = p * p; r5 = r4 * sq; r6 = r4 * p; r7 = r6 * sq;
+}
+
+// integrals.hpp:116-140 (integral1) with gamma + 1 = e / 2
+__device__ __forceinline__ double integral1(const EndPow& w, double nz, double h, int e, double ss)
+{
+    double g1 = 0.5 * e;
+    if (ss > h) return (epw(w, e, false) - epw(w, e, true)) / (nz * g1);
+    else if (ss > -h) return epw(w, e, false) / (nz * g1);
+    return 0.0;
+}
+
+// integrals.hpp:159-184 (integral2) with gamma + 1 = e / 2
+__device__ __forceinline__ double integral2(const EndPow& w, double nz, double h, int e, double ss)
+{
+    double term1 = integral1(w, nz, h, e + 2, ss);
+    double term2 = 0.0;
+    if (ss > h) term2 = -h * (epw(w, e, false) + epw(w, e, true));
+    else if (ss > -h) term2 = -h * epw(w, e, false);
+    return (term1 + term2) / (nz * (0.5 * e));
+}
+
+// The end overlaps that integral1/2 and areaIntegrals read (integrals.hpp:56-60,
+// 431-441): both ends when ss > h, the lower end when -h < ss <= h.
+__device__ __forceinline__ EndPow end_pows(double rz, double nz, double R, double h, double ss)
+{
+    EndPow w;
+    double o1 = 0.0, o2 = 0.0;
+    if (ss > h) { o1 = R - rz - (-h) * nz; o2 = R - rz - h * nz; }
+    else if (ss > -h) { o1 = R - rz - (-h) * nz; }
+    fill_pows(o1, w.p1, w.p2, w.p3, w.p4, w.p5, w.p6, w.p7);
+    fill_pows(o2, w.q1, w.q2, w.q3, w.q4, w.q5, w.q6, w.q7);
+    return w;
+}
+
+struct MechParams {
+    double R, Rcell, E0, Ecell;
+    double sqrtR;
+    double nz_threshold;
+    double coulomb;          // cell_surface_coulomb_coeff
+    int no_surface;
+};
+
+// Cell-surface repulsion + adhesion dE/dq components 2 and 5
+// (mechanics.hpp:673-780 and 800-910, include_constraint = false).
+__device__ __forceinline__ void surface_dEdq(const MechParams& P, bool assume_2d, double rz, double nz,
+                                             double l, double h, double sigma0, double ss,
+                                             const EndPow& w, double& rep2, double& rep5,
+                                             double& adh2, double& adh5)
+{
+    const double R = P.R, E0 = P.E0;
+    rep2 = rep5 = adh2 = adh5 = 0.0;
+    if (assume_2d)
+    {
+        double ph = R - rz;
+        if (ph > 0)
+        {
+            rep2 = -(2 * E0) * ph * l;
+            adh2 = sigma0 * (P.sqrtR / 2) * l / sqrt(ph);
+        }
+        return;
+    }
+    const double pf0 = 2 * E0, pf1 = (8. / 3.) * E0 * P.sqrtR, pf2 = 2 * E0 * P.sqrtR;
+    double nz2 = nz * nz;
+    double int1 = integral1(w, nz, h, 4, ss);   // delta
+    double int2 = integral1(w, nz, h, 3, ss);   // sqrt(delta)
+    rep2 = -pf0 * ((1.0 - nz2) * int1 + P.sqrtR * nz2 * int2);
+    double int3 = integral1(w, nz, h, 6, ss);   // delta^2
+    double int4 = integral2(w, nz, h, 4, ss);   // s delta
+    double int5 = integral1(w, nz, h, 5, ss);   // delta^1.5
+    double int6 = integral2(w, nz, h, 3, ss);   // s sqrt(delta)
+    double d5 = 0.0;
+    d5 -= pf0 * nz * int3;
+    d5 -= pf0 * (1 - nz2) * int4;
+    d5 += pf1 * nz * int5;
+    d5 -= pf2 * nz2 * int6;
+    rep5 = d5;
+    // adhesion
+    const double a0 = P.sqrtR / 2, a1 = 2 * M_PI * R, a2 = 2 * P.sqrtR;
+    double i1 = integral1(w, nz, h, 1, ss);     // delta^-1/2
+    bool partial = fabs(ss) < h;
+    double term2 = partial ? (a1 / 2) * nz : 0.0;
+    adh2 = (a0 * (1 - nz2) * i1 + term2) * sigma0;
+    double i2 = integral1(w, nz, h, 3, ss);     // delta^1/2
+    double i3 = integral2(w, nz, h, 1, ss);     // s delta^-1/2
+    double i4 = (ss > h) ? 2 * h : ((ss > -h) ? ss + h : 0.0);   // integral4
+    double term4 = partial ? (a1 / 2) * (R - rz) : 0.0;
+    double e5 = 0.0;
+    e5 += a2 * nz * i2;
+    e5 += a0 * (1 - nz2) * i3;
+    e5 -= a1 * nz * i4;
+    e5 += term4;
+    adh5 = e5 * sigma0;
+}
+
+// integrals.hpp:400-463 (areaIntegrals)
+__device__ __forceinline__ void area_integrals(const MechParams& P, double nz, double h, double ss,
+                                               const EndPow& w, double& A1, double& A2, double& A3)
+{
+    const double R = P.R;
+    double int4 = (ss > h) ? 2 * h : ((ss > -h) ? ss + h : 0.0);
+    double int5 = (-h < ss && ss <= h) ? (ss * ss - h * h) / 2.0 : 0.0;
+    double int6 = (ss > h) ? 2 * h * h * h / 3.0 : ((ss > -h) ? (ss * ss * ss + h * h * h) / 3.0 : 0.0);
+    double int1a = integral1(w, nz, h, 3, ss);
+    double int1b = integral1(w, nz, h, 5, ss);
+    double int1c = integral1(w, nz, h, 7, ss);
+    double onz = 1 - nz * nz;
+    double piRnz2 = M_PI * R * nz * nz;
+    A1 = P.sqrtR * onz * int1a + piRnz2 * int4;
+    double term2 = -h * (w.p3 + w.q3);
+    double int2a = (int1b + term2) / (1.5 * nz);
+    A2 = P.sqrtR * onz * int2a + piRnz2 * int5;
+    term2 = -h * (w.p5 + w.q5);
+    double int2b = (int1c + term2) / (2.5 * nz);
+    double int3 = (2 * int2b + h * h * (w.p3 - w.q3)) / (1.5 * nz);
+    A3 = P.sqrtR * onz * int3 + piRnz2 * int6;
+}
+
+// Velocity of one cell from its generalised force (mechanics.hpp:2011-2347,
+// the three branches: no surface contact, horizontal contact, full 3-D contact).
+// dr, dn: stored velocities of the previous accepted step (Coulomb truncation).
+__device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_2d, const double y[6],
+                                               double l, double h, double eta0, double eta1_in,
+                                               double ss, const EndPow& w, const double dr[6],
+                                               const double f[6], double v[6])
+{
+    const double R = P.R, E0 = P.E0, coul = P.coulomb;
+    const double rz = y[2], nx = y[3], ny = y[4], nz = y[5];
+    bool contacting;
+    if (!assume_2d) contacting = (rz - h * nz < R) || (rz + h * nz < R);
+    else contacting = rz < R;
+    if (P.no_surface || !contacting)
+    {
+        double K = eta0 * l, L = K * l * l / 12;
+        double mult = -((nx * f[3] + ny * f[4]) + nz * f[5]);
+        v[0] = f[0] / K; v[1] = f[1] / K; v[2] = f[2] / K;
+        v[3] = (f[3] + mult * nx) / L; v[4] = (f[4] + mult * ny) / L; v[5] = (f[5] + mult * nz) / L;
+    }
+    else if (assume_2d)
+    {
+        double K, L;
+        double a = sqrt(R * (R - rz));
+        if (coul == 0)
+        {
+            double eta_c = eta0 + eta1_in * a / R;
+            K = eta_c * l; L = K * l * l / 12;
+        }
+        else
+        {
+            double K_vis = eta0 * l, L_vis = K_vis * l * l / 12;
+            double K_fric = eta1_in * l * a / R;
+            double drxy = sqrt(dr[0] * dr[0] + dr[1] * dr[1]);
+            double max_norm = coul * (2 * E0 * (R - rz) * l);
+            if (K_fric * drxy > max_norm)
+            {
+                double eta1_tr = max_norm * R / (drxy * l * a);
+                K_fric = eta1_tr * l * a / R;
+            }
+            K = K_vis + K_fric; L = L_vis + K_fric * l * l / 12;
+        }
+        double mult = -(nx * f[3] + ny * f[4]);
+        v[0] = f[0] / K; v[1] = f[1] / K;
+        v[3] = (f[3] + mult * nx) / L; v[4] = (f[4] + mult * ny) / L;
+        v[2] = f[2] / (eta0 * l);
+        v[5] = 12 * f[5] / (eta0 * l * l * l);
+    }
+    else
+    {
+        double eta1 = eta1_in;
+        double A1, A2, A3;
+        area_integrals(P, nz, h, ss, w, A1, A2, A3);
+        if (coul > 0)
+        {
+            double drxy = sqrt(dr[0] * dr[0] + dr[1] * dr[1]);
+            double dnxy = sqrt(dr[3] * dr[3] + dr[4] * dr[4]);
+            double friction_norm = (A1 * drxy + A2 * dnxy) * (eta1 / R);
+            double max_norm = (1 - nz * nz) * integral1(w, nz, h, 4, ss)
+                            + P.sqrtR * nz * nz * integral1(w, nz, h, 3, ss);
+            max_norm *= (2 * E0 * coul);
+            if (friction_norm > max_norm) eta1 = max_norm * R / (A1 * drxy + A2 * dnxy);
+        }
+        const double c1 = eta0 * l + (eta1 / R) * A1;
+        const double c2 = eta0 * l;
+        const double c4 = c2 * l * l / 12;
+        const double c3 = c4 + (eta1 / R) * A3;
+        const double c5 = (eta1 / R) * A2;
+        const double term1 = c3 - (c5 * c5 / c1);
+        const double w4 = f[3] - f[0] * (c5 / c1);
+        const double w5 = f[4] - f[1] * (c5 / c1);
+        const double nx2 = nx / term1, ny2 = ny / term1, nz2 = nz / c4;
+        const double alpha = 2 * ((nx * nx2 + ny * ny2) + nz * nz2);
+        const double beta = -((w4 * nx2 + w5 * ny2) + f[5] * nz2);
+        const double lambda = beta / alpha;
+        v[5] = (f[5] + 2 * nz * lambda) / c4;
+        v[4] = (w5 + 2 * ny * lambda) / term1;
+        v[3] = (w4 + 2 * nx * lambda) / term1;
+        v[2] = f[2] / c2;
+        v[1] = (f[1] - c5 * v[4]) / c1;
+        v[0] = (f[0] - c5 * v[3]) / c1;
+    }
+}
+
+}   // namespace abm

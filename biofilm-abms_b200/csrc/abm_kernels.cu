@@ -1,0 +1,945 @@
+// CUDA kernels of the B200 mechanics step (sm_100a).
+//
+//   cell list      k_bbox -> k_bin_count -> scan -> k_bin_scatter        (uniform grid,
+//                  counting sort by bin, bins staged through shared memory)
+//   pair set       k_pair_build -> scan -> k_csr_fill                   (getCellNeighbors,
+//                  mechanics.hpp:520-593; CSR rows sorted by neighbor index)
+//   pair force     k_pair_force<G>                                      (cellCellInteractionForces,
+//                  mechanics.hpp:1209-1659; G lanes per cell, shuffle reduction)
+//   RK attempt     k_attempt<S, KIND>                                   (stepRungeKuttaAdaptive,
+//                  mechanics.hpp:2406-2612; all stages of a cell in registers, the error
+//                  norm reduced in the same kernel, the step-size controller of
+//                  simulation.hpp:1690-1769 run by the last block to finish)
+#include <cstdio>
+#include "abm_kernels.cuh"
+
+namespace abm {
+
+static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// Order-preserving double <-> uint64 maps for atomic min/max
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ord_enc(double x)
+{
+    unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_dec(unsigned long long u)
+{
+    u = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+    return __longlong_as_double((long long)u);
+}
+
+// ---------------------------------------------------------------------------
+// Column-major cell arrays <-> device records
+// ---------------------------------------------------------------------------
+__global__ void k_cells_from_colmajor(const double* __restrict__ cm, int n, int ncols, int ld,
+                                      int has_gamma, Geom* geom, Vel* vel, Phys* phys)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto c = [&](int col) { return cm[(size_t)col * ld + i]; };
+    Geom g;
+    g.rx = c(1); g.ry = c(2); g.rz = c(3); g.h = c(14);
+    g.nx = c(4); g.ny = c(5); g.nz = c(6); g.gamma = has_gamma ? c(21) : 0.0;
+    geom[i] = g;
+    Vel v;
+    for (int k = 0; k < 6; ++k) v.v[k] = c(7 + k);
+    vel[i] = v;
+    Phys p;
+    p.l = c(13); p.growth = c(16); p.eta0 = c(17); p.eta1 = c(18); p.sigma0 = c(19);
+    p.t0 = c(15); p.id = c(0); p.group = c(20);
+    phys[i] = p;
+}
+
+__global__ void k_cells_to_colmajor(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
+                                    const Phys* __restrict__ phys, int n, int ncols, int ld,
+                                    int has_gamma, double* cm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Geom g = geom[i]; Vel v = vel[i]; Phys p = phys[i];
+    auto w = [&](int col, double x) { cm[(size_t)col * ld + i] = x; };
+    w(0, p.id); w(1, g.rx); w(2, g.ry); w(3, g.rz); w(4, g.nx); w(5, g.ny); w(6, g.nz);
+    for (int k = 0; k < 6; ++k) w(7 + k, v.v[k]);
+    w(13, p.l); w(14, g.h); w(15, p.t0); w(16, p.growth); w(17, p.eta0); w(18, p.eta1);
+    w(19, p.sigma0); w(20, p.group);
+    if (has_gamma && ncols > 21) w(21, g.gamma);
+}
+
+__global__ void k_gen6_to_colmajor(const Gen6* __restrict__ g, int n, double* cm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Gen6 v = g[i];
+    for (int k = 0; k < 6; ++k) cm[(size_t)k * n + i] = v.f[k];
+}
+
+void launch_cells_from_colmajor(const double* cm, int n, int ncols, int ld, int has_gamma,
+                                Geom* geom, Vel* vel, Phys* phys, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_cells_from_colmajor<<<cdiv(n, 256), 256, 0, st>>>(cm, n, ncols, ld, has_gamma, geom, vel, phys);
+}
+void launch_cells_to_colmajor(const Geom* geom, const Vel* vel, const Phys* phys, int n, int ncols,
+                              int ld, int has_gamma, double* cm, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_cells_to_colmajor<<<cdiv(n, 256), 256, 0, st>>>(geom, vel, phys, n, ncols, ld, has_gamma, cm);
+}
+void launch_gen6_to_colmajor(const Gen6* g, int n, double* cm, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_gen6_to_colmajor<<<cdiv(n, 256), 256, 0, st>>>(g, n, cm);
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Cell list: bounding box -> grid (last block), counting sort by bin
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_bbox(const Geom* __restrict__ geom, Ctrl* ctrl, Grid* grid,
+                                              unsigned long long* acc, unsigned int* counter,
+                                              double edge, int cap_bins)
+{
+    __shared__ double sh[7][8];
+    __shared__ bool last;
+    const int n = ctrl->n;
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, mh = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        Geom g = load_geom(geom, i);
+        mn[0] = fmin(mn[0], g.rx); mn[1] = fmin(mn[1], g.ry); mn[2] = fmin(mn[2], g.rz);
+        mx[0] = fmax(mx[0], g.rx); mx[1] = fmax(mx[1], g.ry); mx[2] = fmax(mx[2], g.rz);
+        mh = fmax(mh, g.h);
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double v[7] = {mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], mh};
+    for (int k = 0; k < 3; ++k) v[k] = warp_min(v[k]);
+    for (int k = 3; k < 7; ++k) v[k] = warp_max(v[k]);
+    if (lane == 0) for (int k = 0; k < 7; ++k) sh[k][wid] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        {
+            for (int k = 0; k < 3; ++k) v[k] = fmin(v[k], sh[k][w]);
+            for (int k = 3; k < 7; ++k) v[k] = fmax(v[k], sh[k][w]);
+        }
+        for (int k = 0; k < 3; ++k) atomicMin(&acc[k], ord_enc(v[k]));
+        for (int k = 3; k < 7; ++k) atomicMax(&acc[k], ord_enc(v[k]));
+        __threadfence();
+        unsigned int done = atomicAdd(counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        __threadfence();
+        double lo[3], hi[3];
+        for (int k = 0; k < 3; ++k)
+        {
+            lo[k] = ord_dec(atomicAdd(&acc[k], 0ull));
+            hi[k] = ord_dec(atomicAdd(&acc[3 + k], 0ull));
+        }
+        double maxh = ord_dec(atomicAdd(&acc[6], 0ull));
+        if (n <= 0) { for (int k = 0; k < 3; ++k) { lo[k] = 0; hi[k] = 0; } maxh = 0; }
+        double e = edge;
+        long long nb[3];
+        for (int tries = 0; tries < 64; ++tries)
+        {
+            for (int k = 0; k < 3; ++k) nb[k] = (long long)floor((hi[k] - lo[k]) / e) + 1;
+            if (nb[0] * nb[1] * nb[2] <= (long long)cap_bins) break;
+            e *= 1.5;
+        }
+        if (nb[0] * nb[1] * nb[2] > (long long)cap_bins) atomicOr(&ctrl->status, (int)ST_BIN_OVERFLOW);
+        Grid g;
+        g.x0 = lo[0]; g.y0 = lo[1]; g.z0 = lo[2]; g.edge = e; g.inv_edge = 1.0 / e;
+        g.nx = (int)nb[0]; g.ny = (int)nb[1]; g.nz = (int)nb[2];
+        g.nbins = (int)min((long long)cap_bins, nb[0] * nb[1] * nb[2]);
+        g.max_half_l = maxh;
+        *grid = g;
+        // reset accumulators for the next rebuild
+        for (int k = 0; k < 3; ++k) { acc[k] = 0xffffffffffffffffull; acc[3 + k] = 0ull; }
+        acc[6] = 0ull;
+        *counter = 0u;
+    }
+}
+
+void launch_bbox(const Geom* geom, Ctrl* ctrl, Grid* grid, unsigned long long* acc,
+                 unsigned int* counter, double edge, int cap_bins, int cap_cells, cudaStream_t st)
+{
+    int blocks = min(cdiv(cap_cells, 256), 592);
+    k_bbox<<<max(blocks, 1), 256, 0, st>>>(geom, ctrl, grid, acc, counter, edge, cap_bins);
+}
+
+__device__ __forceinline__ int bin_coord(double x, double x0, double inv_edge, int nb)
+{
+    int b = (int)floor((x - x0) * inv_edge);
+    return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+
+__global__ void k_bin_count(const Geom* __restrict__ geom, const Ctrl* ctrl, const Grid* grid,
+                            int* bin_count, int* key, int* slot)
+{
+    const int n = ctrl->n;
+    const Grid g = *grid;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        Geom c = load_geom(geom, i);
+        int bx = bin_coord(c.rx, g.x0, g.inv_edge, g.nx);
+        int by = bin_coord(c.ry, g.y0, g.inv_edge, g.ny);
+        int bz = bin_coord(c.rz, g.z0, g.inv_edge, g.nz);
+        int k = (bz * g.ny + by) * g.nx + bx;
+        if (k >= g.nbins) k = g.nbins - 1;
+        key[i] = k;
+        slot[i] = atomicAdd(&bin_count[k], 1);
+    }
+}
+
+void launch_bin_count(const Geom* geom, const Ctrl* ctrl, const Grid* grid, int* bin_count,
+                      int* key, int* slot, int cap_cells, cudaStream_t st)
+{
+    k_bin_count<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(geom, ctrl, grid, bin_count, key, slot);
+}
+
+__global__ void k_bin_scatter(const Geom* __restrict__ geom, const Ctrl* ctrl, const int* bin_start,
+                              const int* key, const int* slot, int* sorted_cell, Geom* sorted_geom)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        int pos = bin_start[key[i]] + slot[i];
+        sorted_cell[pos] = i;
+        sorted_geom[pos] = load_geom(geom, i);
+    }
+}
+
+void launch_bin_scatter(const Geom* geom, const Ctrl* ctrl, const int* bin_start, const int* key,
+                        const int* slot, int* sorted_cell, Geom* sorted_geom, int cap_cells,
+                        cudaStream_t st)
+{
+    k_bin_scatter<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(geom, ctrl, bin_start, key, slot,
+                                                                 sorted_cell, sorted_geom);
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan (three passes: block sums, one-block scan of the sums,
+// block scan + offset).  Up to 4096 * 4096 entries.
+// ---------------------------------------------------------------------------
+const int SCAN_T = 1024, SCAN_PER = 4, SCAN_TILE = SCAN_T * SCAN_PER;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sh_warp, int& total)
+{
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0)
+    {
+        int w = (lane < (int)(blockDim.x >> 5)) ? sh_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        sh_warp[lane] = w;
+    }
+    __syncthreads();
+    int warp_off = wid > 0 ? sh_warp[wid - 1] : 0;
+    total = sh_warp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_off + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_sums(const int* __restrict__ in, const int* len_p,
+                                                      int* block_sums)
+{
+    __shared__ int sh[32];
+    const int len = *len_p;
+    long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_PER;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) if (base + k < len) s += in[base + k];
+    int total;
+    block_exclusive_scan(s, sh, total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_top(int* block_sums, int nblocks)
+{
+    __shared__ int sh[32];
+    int base = threadIdx.x * SCAN_PER;
+    int v[SCAN_PER], s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) { v[k] = (base + k < nblocks) ? block_sums[base + k] : 0; s += v[k]; }
+    int total;
+    int off = block_exclusive_scan(s, sh, total);
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) { if (base + k < nblocks) block_sums[base + k] = off; off += v[k]; }
+    if (threadIdx.x == 0) block_sums[nblocks] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_final(const int* __restrict__ in, const int* len_p,
+                                                       const int* block_sums, int* out, int nblocks)
+{
+    __shared__ int sh[32];
+    const int len = *len_p;
+    long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_PER;
+    int v[SCAN_PER], s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) { v[k] = (base + k < len) ? in[base + k] : 0; s += v[k]; }
+    int total;
+    int off = block_exclusive_scan(s, sh, total) + block_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) { if (base + k < len) out[base + k] = off; off += v[k]; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[len] = block_sums[nblocks];
+}
+
+size_t scan_block_sums_size(int cap) { return (size_t)cdiv(cap, SCAN_TILE) + 1; }
+
+void launch_scan(const int* in, const int* len, int* out, int* block_sums, int cap, cudaStream_t st)
+{
+    int nb = max(cdiv(cap, SCAN_TILE), 1);
+    k_scan_sums<<<nb, SCAN_T, 0, st>>>(in, len, block_sums);
+    k_scan_top<<<1, SCAN_T, 0, st>>>(block_sums, nb);
+    k_scan_final<<<nb, SCAN_T, 0, st>>>(in, len, block_sums, out, nb);
+}
+
+// ---------------------------------------------------------------------------
+// Pair build: one block per bin (grid-stride over bins).  Candidate cells of
+// the 27 surrounding bins are staged through shared memory in chunks; each
+// thread owns one cell of the bin and keeps the candidates that pass the
+// reference's two tests: centre distance < threshold + Ldiv + 2R and
+// segment distance < threshold (mechanics.hpp:548-577).  The segment distance
+// is always evaluated with the larger index as cell 1, as the reference's
+// j < i loop does, so both cells of a pair reach the same decision.
+// ---------------------------------------------------------------------------
+const int PB_T = 128, PB_CHUNK = 128;
+
+__global__ void __launch_bounds__(PB_T) k_pair_build(const Grid* grid, const int* __restrict__ bin_start,
+                                                    const int* __restrict__ sorted_cell,
+                                                    const Geom* __restrict__ sorted_geom, const Ctrl* ctrl,
+                                                    BuildParams bp, int* scratch, int* count)
+{
+    __shared__ Geom sg[PB_CHUNK];
+    __shared__ int sc[PB_CHUNK];
+    const Grid g = *grid;
+    const int cap = bp.cap_per_cell;
+    for (int bin = blockIdx.x; bin < g.nbins; bin += gridDim.x)
+    {
+        const int s0 = bin_start[bin], s1 = bin_start[bin + 1];
+        if (s0 == s1) continue;
+        const int bx = bin % g.nx, by = (bin / g.nx) % g.ny, bz = bin / (g.nx * g.ny);
+        for (int base = s0; base < s1; base += PB_T)
+        {
+            const int my = base + threadIdx.x;
+            const bool act = my < s1;
+            Geom gm;
+            int cm = -1, cnt = 0;
+            if (act) { gm = sorted_geom[my]; cm = sorted_cell[my]; }
+            for (int dz = -1; dz <= 1; ++dz)
+            {
+                int zz = bz + dz;
+                if (zz < 0 || zz >= g.nz) continue;
+                for (int dy = -1; dy <= 1; ++dy)
+                {
+                    int yy = by + dy;
+                    if (yy < 0 || yy >= g.ny) continue;
+                    for (int dx = -1; dx <= 1; ++dx)
+                    {
+                        int xx = bx + dx;
+                        if (xx < 0 || xx >= g.nx) continue;
+                        int nbin = (zz * g.ny + yy) * g.nx + xx;
+                        if (nbin >= g.nbins) continue;
+                        const int c0 = bin_start[nbin], c1 = bin_start[nbin + 1];
+                        for (int ch = c0; ch < c1; ch += PB_CHUNK)
+                        {
+                            const int len = min(PB_CHUNK, c1 - ch);
+                            __syncthreads();
+                            for (int q = threadIdx.x; q < len; q += PB_T)
+                            {
+                                sg[q] = sorted_geom[ch + q];
+                                sc[q] = sorted_cell[ch + q];
+                            }
+                            __syncthreads();
+                            if (act)
+                            {
+                                for (int q = 0; q < len; ++q)
+                                {
+                                    const int o = sc[q];
+                                    if (o == cm) continue;
+                                    const Geom go = sg[q];
+                                    const Geom& gi = (cm > o) ? gm : go;
+                                    const Geom& gj = (cm > o) ? go : gm;
+                                    double cd = xnorm(xsub(x3(gi.rx, gi.ry, gi.rz), x3(gj.rx, gj.ry, gj.rz)));
+                                    if (!(cd < bp.prefilter)) continue;
+                                    Dist d = dist_geom(gi, gj);
+                                    if (xnorm(x3(d.dx, d.dy, d.dz)) < bp.threshold)
+                                    {
+                                        if (cnt < cap) scratch[(size_t)cm * cap + cnt] = o;
+                                        ++cnt;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            if (act)
+            {
+                if (cnt > cap) { atomicOr((int*)&ctrl->status, (int)ST_NBR_OVERFLOW); cnt = cap; }
+                count[cm] = cnt;
+            }
+        }
+    }
+}
+
+void launch_pair_build(const Grid* grid, const int* bin_start, const int* sorted_cell,
+                       const Geom* sorted_geom, const Ctrl* ctrl, BuildParams bp, int* scratch,
+                       int* count, int cap_bins, int num_sms, cudaStream_t st)
+{
+    int blocks = min(cap_bins, num_sms * 16);
+    k_pair_build<<<max(blocks, 1), PB_T, 0, st>>>(grid, bin_start, sorted_cell, sorted_geom, ctrl, bp,
+                                                  scratch, count);
+}
+
+// CSR rows: copy the per-cell lists and sort each ascending (deterministic
+// order for the force reduction; the reference's table is i-major, j ascending).
+__global__ void k_csr_fill(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ scratch,
+                           int cap, int* col, Ctrl* ctrl_w)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
+        const int* src = scratch + (size_t)i * cap;
+        for (int k = 0; k < r1 - r0; ++k)
+        {
+            int v = src[k];
+            int j = r0 + k - 1;
+            while (j >= r0 && col[j] > v) { col[j + 1] = col[j]; --j; }
+            col[j + 1] = v;
+        }
+        if (i == n - 1) ctrl_w->n_dir = r1;
+    }
+    if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) ctrl_w->n_dir = 0;
+}
+
+void launch_csr_fill(const Ctrl* ctrl, const int* row_ptr, const int* scratch, int cap_per_cell,
+                     int* col, Ctrl* ctrl_w, int cap_cells, cudaStream_t st)
+{
+    k_csr_fill<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, scratch, cap_per_cell, col, ctrl_w);
+}
+
+// ---------------------------------------------------------------------------
+// Pair force: G lanes per cell walk its CSR row; each lane evaluates the
+// distance (larger index as cell 1) and the Hertz / JKR + hard-core magnitude
+// of mechanics.hpp:1390-1659 (or :1209-1350 without adhesion), accumulates the
+// cell's share of dE/dq, and the G partial sums are combined by xor shuffles.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pow15(double x) { return x * sqrt(x); }
+
+// adhesion.hpp:282-370: magnitude (term1 - term2) of the isotropic JKR force
+// from the fixed-gamma radius table, overlap capped at max_overlap
+__device__ __forceinline__ double jkr_magnitude(double dist, double gamma, const ForceParams& fp,
+                                                const double* td, const double* tr)
+{
+    double delta = 2 * fp.R - dist;
+    if (fp.max_overlap >= 0 && delta > fp.max_overlap) delta = fp.max_overlap;
+    const int nm = fp.jkr_n;
+    int k = (int)(delta / fp.jkr_step);
+    k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
+    while (k > 0 && td[k] > delta) --k;
+    while (k < nm - 2 && td[k + 1] <= delta) ++k;
+    double d1 = td[k], d2 = td[k + 1], r1 = tr[k], r2 = tr[k + 1];
+    double radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
+    double Req = fp.R / 2;
+    double a3 = radius * radius * radius;
+    double term1 = 4 * fp.E0 * a3 / (3 * Req);
+    double term2 = 4 * sqrt(M_PI * a3 * gamma * fp.E0);
+    return term1 - term2;
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void pair_contribution(int cell, int o, const Geom& gc, const Geom& go,
+                                                  const ForceParams& fp, const double* td,
+                                                  const double* tr, double acc[6])
+{
+    const bool first = cell > o;                 // cell is "cell 1" (row index i) of the pair
+    const Geom& gi = first ? gc : go;
+    const Geom& gj = first ? go : gc;
+    Dist d = MIXED ? dist_geom_mixed(gi, gj) : dist_geom(gi, gj);
+    double dist = xnorm(x3(d.dx, d.dy, d.dz));
+    double overlap = 2 * fp.R - dist;
+    if (!(overlap > 0)) return;
+    double ux = d.dx / dist, uy = d.dy / dist, uz = d.dz / dist;
+    double m;
+    double gamma = fp.adhesion ? fmin(gi.gamma, gj.gamma) : 0.0;
+    if (fp.adhesion && gamma > 0) m = jkr_magnitude(dist, gamma, fp, td, tr);
+    else if (overlap <= fp.max_overlap) m = fp.pf0 * pow15(overlap);
+    else
+    {
+        m = fp.pf2;
+        if (!fp.adhesion) m += fp.pf1 * pow15(overlap - fp.max_overlap);
+    }
+    if (fp.adhesion && overlap > fp.max_overlap) m += fp.pf1 * pow15(overlap - fp.max_overlap);
+    double vx = m * ux, vy = m * uy, vz = m * uz;
+    if (first)
+    {
+        acc[0] += vx; acc[1] += vy; acc[2] += vz;
+        acc[3] += d.s * vx; acc[4] += d.s * vy; acc[5] += d.s * vz;
+    }
+    else
+    {
+        acc[0] -= vx; acc[1] -= vy; acc[2] -= vz;
+        acc[3] -= d.t * vx; acc[4] -= d.t * vy; acc[5] -= d.t * vz;
+    }
+}
+
+const int PF_T = 256, JKR_MAX = 512;
+
+template <int G, bool MIXED>
+__global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ geom, const int* __restrict__ row_ptr,
+                                                    const int* __restrict__ col, const Ctrl* ctrl, ForceParams fp,
+                                                    const double* __restrict__ jkr_delta,
+                                                    const double* __restrict__ jkr_radius, Gen6* fcc)
+{
+    __shared__ double td[JKR_MAX], tr[JKR_MAX];
+    for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
+    __syncthreads();
+    const int n = ctrl->n;
+    const int lane = threadIdx.x & (G - 1);
+    const unsigned gmask = (G == 32) ? 0xffffffffu
+                                     : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    const int groups_per_grid = gridDim.x * (blockDim.x / G);
+    for (int cell = (blockIdx.x * blockDim.x + threadIdx.x) / G; cell < n; cell += groups_per_grid)
+    {
+        const Geom gc = load_geom(geom, cell);
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        const int r0 = row_ptr[cell], r1 = row_ptr[cell + 1];
+        for (int k = r0 + lane; k < r1; k += G)
+        {
+            const int o = col[k];
+            const Geom go = load_geom(geom, o);
+            pair_contribution<MIXED>(cell, o, gc, go, fp, td, tr, acc);
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc[c] += __shfl_xor_sync(gmask, acc[c], off, G);
+        if (lane == 0)
+        {
+            Gen6 out;
+            for (int c = 0; c < 6; ++c) out.f[c] = acc[c];
+            fcc[cell] = out;
+        }
+    }
+}
+
+void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, const Ctrl* ctrl,
+                       ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Gen6* fcc, int lanes, int mixed, int cap_cells, cudaStream_t st)
+{
+    int blocks = max(cdiv((long long)cap_cells * lanes, PF_T), 1);
+#define PF_CASE(G) \
+    if (lanes == G) { \
+        if (mixed) k_pair_force<G, true><<<blocks, PF_T, 0, st>>>(geom, row_ptr, col, ctrl, fp, jkr_delta, jkr_radius, fcc); \
+        else k_pair_force<G, false><<<blocks, PF_T, 0, st>>>(geom, row_ptr, col, ctrl, fp, jkr_delta, jkr_radius, fcc); \
+        return; }
+    PF_CASE(4) PF_CASE(8) PF_CASE(16) PF_CASE(32)
+#undef PF_CASE
+}
+
+// ---------------------------------------------------------------------------
+// RK attempt: one thread per cell runs every stage of stepRungeKuttaAdaptive
+// (mechanics.hpp:2406-2612) in registers.  3-D pair forces are stage-invariant
+// (the table is not refreshed between stages and include_constraint = false,
+// mechanics.hpp:2064), so each stage needs only the cell's own state, its
+// precomputed pair force and the surface terms.
+// ---------------------------------------------------------------------------
+const int AT_T = 256;
+
+__device__ __forceinline__ void normalize_n(double y[6])
+{
+    double nrm = sqrt((y[3] * y[3] + y[4] * y[4]) + y[5] * y[5]);
+    y[3] /= nrm; y[4] /= nrm; y[5] /= nrm;
+    if (y[5] < 0) { y[3] = -y[3]; y[4] = -y[4]; y[5] = -y[5]; }
+}
+
+// getVelocities (mechanics.hpp:2011-2347) of one cell at state y
+__device__ __forceinline__ void cell_velocity(const StepParams& sp, bool a2, const double y[6],
+                                              const Phys& ph, double h, const double dr[6],
+                                              const Gen6& cc, const double noise[6], double v[6])
+{
+    const MechParams& P = sp.mp;
+    double ss = a2 ? __longlong_as_double(0x7ff8000000000000ll) : (P.R - y[2]) / y[5];
+    EndPow w;
+    if (!a2) w = end_pows(y[2], y[5], P.R, h, ss);
+    double rep2 = 0, rep5 = 0, adh2 = 0, adh5 = 0;
+    if (!P.no_surface) surface_dEdq(P, a2, y[2], y[5], ph.l, h, ph.sigma0, ss, w, rep2, rep5, adh2, adh5);
+    double f[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) f[c] = -cc.f[c];
+    f[2] = (f[2] - rep2) - adh2;
+    f[5] = (f[5] - rep5) - adh5;
+    if (sp.noise_on)
+    {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) f[c] += noise[c];
+    }
+    velocity_solve(P, a2, y, ph.l, h, ph.eta0, ph.eta1, ss, w, dr, f, v);
+}
+
+__device__ __forceinline__ void cell_noise(const StepParams& sp, int iter, int attempt, int i, double noise[6])
+{
+#pragma unroll
+    for (int c = 0; c < 6; ++c) noise[c] = 0.0;
+    if (!sp.noise_on) return;
+    for (int c = 0; c < 3; ++c)
+    {
+        uint32_t x[4] = {(uint32_t)iter, (uint32_t)attempt, (uint32_t)i, (uint32_t)c};
+        philox4x32_10(x, (uint32_t)sp.seed, (uint32_t)(sp.seed >> 32) ^ RNG_PURPOSE_NOISE);
+        double u0 = philox_u01(x[0], x[1]), u1 = philox_u01(x[2], x[3]);
+        noise[2 * c] = -sp.noise_max[2 * c] + 2 * sp.noise_max[2 * c] * u0;
+        noise[2 * c + 1] = -sp.noise_max[2 * c + 1] + 2 * sp.noise_max[2 * c + 1] * u1;
+    }
+}
+
+// Step-size controller, run once per attempt by the last block
+// (simulation.hpp:1690-1769; the final re-run is accepted unconditionally).
+__device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, double E)
+{
+    c->attempts += 1;
+    if (kind == MODE_TRIAL)
+    {
+        c->last_trial_error = E;
+        bool exceeded = E > 1.0;
+        double factor = 0.9 * pow(1.0 / E, sp.inv_q1);
+        if (factor >= 10) factor = 10;
+        else if (factor < 0.2) factor = 0.2;
+        c->factor = factor;
+        c->tries = 0;
+        c->attempt = 1;
+        if (exceeded && 0 < sp.max_tries) { c->mode = MODE_RETRY; c->dt_try = c->dt * factor; return; }
+    }
+    else if (kind == MODE_RETRY)
+    {
+        c->retries += 1;
+        c->attempt += 1;
+        bool exceeded = E > 1.0;
+        double factor = c->factor * (0.9 * pow(1.0 / E, sp.inv_q1));
+        bool brk = false;
+        if (factor >= 10) { factor = 10; brk = true; }
+        else if (factor < 0.2) { factor = 0.2; brk = true; }
+        c->factor = factor;
+        if (!brk)
+        {
+            c->tries += 1;
+            if (exceeded && c->tries < sp.max_tries) { c->mode = MODE_RETRY; c->dt_try = c->dt * factor; return; }
+        }
+    }
+    else   // MODE_FINAL: accepted
+    {
+        c->last_max_error = E;
+        c->t += c->dt;
+        c->iter += 1;
+        c->iterations += 1;
+        c->mode = MODE_TRIAL;
+        c->tries = 0;
+        c->attempt = 0;
+        return;
+    }
+    // clamp and schedule the final re-run (simulation.hpp:1752-1760)
+    double factor = c->factor;
+    if (c->dt * factor < sp.min_stepsize) factor = sp.min_stepsize / c->dt;
+    else if (c->dt * factor > sp.max_stepsize) factor = sp.max_stepsize / c->dt;
+    c->dt *= factor;
+    c->dt_try = c->dt;
+    c->mode = MODE_FINAL;
+}
+
+template <int S, int KIND>
+__global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* __restrict__ fcc,
+                                                 Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
+                                                 Gen6* err_out, double eval_dt, int eval_attempt)
+{
+    __shared__ double sh_max[AT_T / 32];
+    __shared__ bool last;
+    const int n = ctrl->n;
+    const int mode = ctrl->mode;
+    const int iter = ctrl->iter;
+    double dt;
+    int attempt;
+    if (KIND == MODE_TRIAL)
+    {
+        if (iter % sp.iter_update_stepsize != 0) return;   // no step-size update: FINAL runs at dt
+        dt = ctrl->dt; attempt = 0;
+    }
+    else if (KIND == MODE_RETRY)
+    {
+        if (mode != MODE_RETRY) return;
+        dt = ctrl->dt_try; attempt = ctrl->attempt;
+    }
+    else if (KIND == MODE_FINAL)
+    {
+        dt = (mode == MODE_FINAL) ? ctrl->dt_try : ctrl->dt;
+        attempt = (mode == MODE_FINAL) ? ctrl->attempt : 0;
+    }
+    else { dt = eval_dt; attempt = eval_attempt; }
+
+    double local_max = 0.0;
+    bool bad = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom g = geom[i];
+        const Vel vv = vel[i];
+        const Phys ph = phys[i];
+        const Gen6 cc = fcc[i];
+        const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
+        const bool a2 = y0[5] < sp.mp.nz_threshold;
+        double noise[6];
+        cell_noise(sp, iter, attempt, i, noise);
+        double k[S][6];
+#pragma unroll
+        for (int st = 0; st < S; ++st)
+        {
+            double y[6];
+            if (st == 0)
+            {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) y[c] = y0[c];
+            }
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                {
+                    double m = 0.0;
+#pragma unroll
+                    for (int j = 0; j < st; ++j) m += k[j][c] * sp.A[st][j];
+                    y[c] = y0[c] + m * dt;
+                }
+                normalize_n(y);
+            }
+            cell_velocity(sp, a2, y, ph, g.h, vv.v, cc, noise, k[st]);
+        }
+        double vf1[6], d1[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+        {
+            double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+            for (int st = 0; st < S; ++st) { s1 += k[st][c] * sp.b[st]; s2 += k[st][c] * sp.bs[st]; }
+            vf1[c] = s1;
+            d1[c] = s1 * dt;
+            double err = d1[c] - s2 * dt;
+            double scaled = err / (sp.tol * (1.0 + fabs(y0[c])));
+            if (isnan(scaled) || isinf(scaled)) bad = true;
+            local_max = fmax(local_max, scaled);
+            if (KIND == 3 && err_out) err_out[i].f[c] = err;
+        }
+        if (KIND == MODE_FINAL || KIND == 3)
+        {
+            double y1[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) y1[c] = y0[c] + d1[c];
+            normalize_n(y1);
+            Geom go = g;
+            go.rx = y1[0]; go.ry = y1[1]; go.rz = y1[2]; go.nx = y1[3]; go.ny = y1[4]; go.nz = y1[5];
+            Vel vo;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) vo.v[c] = vf1[c];
+            if (KIND == MODE_FINAL)
+            {
+                // growCells (growth.hpp:51-57) fused with the accepted step
+                double l = ph.l + ph.growth * (4 * sp.mp.R / 3 + ph.l) * dt;
+                go.h = l / 2;
+                phys[i].l = l;
+                geom[i] = go;
+                vel[i] = vo;
+            }
+            else
+            {
+                geom_c[i] = go;
+                vel_c[i] = vo;
+            }
+        }
+    }
+    // block max of the scaled error, floored at min_error (simulation.hpp:1703)
+    local_max = fmax(local_max, sp.min_error);
+    if (bad) local_max = __longlong_as_double(0x7ff0000000000000ll);
+    local_max = warp_max(local_max);
+    if ((threadIdx.x & 31) == 0) sh_max[threadIdx.x >> 5] = local_max;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double m = sh_max[0];
+        for (int w = 1; w < AT_T / 32; ++w) m = fmax(m, sh_max[w]);
+        unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+        if (bad) atomicOr(&ctrl->status, (int)ST_NAN);
+        if (KIND == 3) { atomicMax(&ctrl->eval_err_bits, bits); last = false; }
+        else
+        {
+            atomicMax(&ctrl->err_bits, bits);
+            __threadfence();
+            unsigned int done = atomicAdd(&ctrl->blocks_done, 1u);
+            last = (done == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (KIND != 3 && last && threadIdx.x == 0)
+    {
+        __threadfence();
+        double E = __longlong_as_double((long long)atomicAdd(&ctrl->err_bits, 0ull));
+        E = fmax(E, sp.min_error);
+        ctrl->err_bits = 0ull;
+        ctrl->blocks_done = 0u;
+        controller_finish(ctrl, sp, KIND, E);
+    }
+}
+
+template <int S>
+static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
+                             Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
+                             double eval_dt, int eval_attempt, cudaStream_t st)
+{
+    switch (kind)
+    {
+        case MODE_TRIAL: k_attempt<S, MODE_TRIAL><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
+        case MODE_RETRY: k_attempt<S, MODE_RETRY><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
+        case MODE_FINAL: k_attempt<S, MODE_FINAL><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
+        default: k_attempt<S, 3><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
+    }
+}
+
+void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
+                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
+                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st)
+{
+    int blocks = max(cdiv(cap_cells, AT_T), 1);
+    switch (sp.s)
+    {
+        case 2: launch_attempt_s<2>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
+        case 4: launch_attempt_s<4>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
+        case 6: launch_attempt_s<6>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
+        case 7: launch_attempt_s<7>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
+        default: break;
+    }
+}
+
+__global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
+                             const Phys* __restrict__ phys, const Gen6* __restrict__ fcc, const Ctrl* ctrl,
+                             StepParams sp, Gen6* v_out)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom g = geom[i];
+        const double y[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
+        const bool a2 = y[5] < sp.mp.nz_threshold;
+        double noise[6] = {0, 0, 0, 0, 0, 0};
+        StepParams q = sp;
+        q.noise_on = 0;
+        Gen6 out;
+        cell_velocity(q, a2, y, phys[i], g.h, vel[i].v, fcc[i], noise, out.f);
+        v_out[i] = out;
+    }
+}
+
+void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
+                       const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
+                       cudaStream_t st)
+{
+    k_velocities<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, v_out);
+}
+
+// growCells (growth.hpp:51-57)
+__global__ void k_grow(Geom* geom, Phys* phys, const Ctrl* ctrl, double R, double dt)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        double l = phys[i].l;
+        l += phys[i].growth * (4 * R / 3 + l) * dt;
+        phys[i].l = l;
+        geom[i].h = l / 2;
+    }
+}
+
+void launch_grow(Geom* geom, Phys* phys, const Ctrl* ctrl, double R, double dt, int cap_cells,
+                 cudaStream_t st)
+{
+    k_grow<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(geom, phys, ctrl, R, dt);
+}
+
+// ---------------------------------------------------------------------------
+// Neighbor table in the reference's row order (i ascending, j < i ascending)
+// ---------------------------------------------------------------------------
+__global__ void k_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, int* cnt)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        int c = 0;
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) c += col[k] < i;
+        cnt[i] = c;
+    }
+}
+
+void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, int* cnt,
+                        int cap_cells, cudaStream_t st)
+{
+    k_count_lower<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(ctrl, row_ptr, col, cnt);
+}
+
+__global__ void k_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
+                             const Geom* __restrict__ geom, double* out, int ld)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        int p = pos[i];
+        Geom gi = load_geom(geom, i);
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+        {
+            int j = col[k];
+            if (j >= i) continue;
+            Dist d = dist_geom(gi, load_geom(geom, j));
+            out[p] = i; out[(size_t)ld + p] = j;
+            out[(size_t)2 * ld + p] = d.dx; out[(size_t)3 * ld + p] = d.dy; out[(size_t)4 * ld + p] = d.dz;
+            out[(size_t)5 * ld + p] = d.s; out[(size_t)6 * ld + p] = d.t;
+            ++p;
+        }
+    }
+}
+
+void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
+                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st)
+{
+    k_table_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, pos, geom, out, ld);
+}
+
+}   // namespace abm

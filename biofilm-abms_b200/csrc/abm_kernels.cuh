@@ -1,0 +1,132 @@
+// Kernel-side shared types and launch wrappers of the B200 mechanics step.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "abm_device.cuh"
+
+namespace abm {
+
+const int MAX_STAGES = 7;
+
+// Controller modes of one iteration (simulation.hpp:1690-1769)
+enum CtrlMode { MODE_TRIAL = 0, MODE_RETRY = 1, MODE_FINAL = 2 };
+
+// Status bits raised on the device and turned into ABM_ERR_* by the host.
+enum StatusBits {
+    ST_NAN = 1,            // NaN/Inf in the error norm or velocities
+    ST_NBR_OVERFLOW = 2,   // more neighbors than cap_neighbors_per_cell
+    ST_BIN_OVERFLOW = 4,   // grid needs more bins than allocated
+    ST_CELL_OVERFLOW = 8,  // division would exceed cap_cells
+};
+
+// Device-resident clock, controller and population state.
+struct Ctrl {
+    double t, dt;               // simulated time, current step size
+    double dt_try;              // step size of the next attempt
+    double factor;              // controller factor (simulation.hpp:1710-1757)
+    double last_max_error;
+    double last_trial_error;
+    unsigned long long err_bits;    // max scaled error of the running attempt (ordered bits)
+    unsigned int blocks_done;       // last-block counter of the running attempt
+    int iter;
+    int mode;                   // CtrlMode
+    int tries;                  // j in simulation.hpp:1716
+    int attempt;                // attempt index within the iteration (noise stream)
+    int status;                 // StatusBits
+    int n;                      // cells
+    int n_dir;                  // directed neighbor entries (2 x pairs)
+    int n_divide;               // mothers in the pending division
+    long long attempts, retries, iterations, rebuilds, divisions;
+    unsigned long long eval_err_bits;   // scaled max error of the last API attempt
+};
+
+struct Grid {
+    double x0, y0, z0, edge, inv_edge;
+    int nx, ny, nz, nbins;
+    double max_half_l;
+};
+
+struct StepParams {
+    MechParams mp;
+    int s;                      // stages
+    double A[MAX_STAGES][MAX_STAGES], b[MAX_STAGES], bs[MAX_STAGES];
+    double inv_q1;              // 1 / (error_order + 1)
+    double tol, min_error, min_stepsize, max_stepsize;
+    int max_tries, iter_update_stepsize;
+    double noise_max[6];
+    int noise_on;
+    uint64_t seed;
+};
+
+struct ForceParams {
+    double R, Rcell, E0;
+    double pf0, pf1, pf2;       // repulsion prefactors (simulation.hpp:1270-1274)
+    double max_overlap;         // 2 (R - Rcell)
+    int adhesion;
+    int jkr_n;
+    double jkr_step;            // spacing of the overlap mesh
+};
+
+struct BuildParams {
+    double threshold;           // neighbor_threshold
+    double prefilter;           // neighbor_threshold + Ldiv + 2 R (mechanics.hpp:551)
+    int cap_per_cell;
+};
+
+// ---- launch wrappers (abm_kernels.cu) ----
+void launch_cells_from_colmajor(const double* cm, int n, int ncols, int ld, int has_gamma,
+                                Geom* geom, Vel* vel, Phys* phys, cudaStream_t st);
+void launch_cells_to_colmajor(const Geom* geom, const Vel* vel, const Phys* phys, int n, int ncols,
+                              int ld, int has_gamma, double* cm, cudaStream_t st);
+void launch_gen6_to_colmajor(const Gen6* g, int n, double* cm, cudaStream_t st);
+
+void launch_bbox(const Geom* geom, Ctrl* ctrl, Grid* grid, unsigned long long* scratch8,
+                 unsigned int* counter, double edge, int cap_bins, int cap_cells, cudaStream_t st);
+void launch_bin_count(const Geom* geom, const Ctrl* ctrl, const Grid* grid, int* bin_count,
+                      int* key, int* slot, int cap_cells, cudaStream_t st);
+void launch_bin_scatter(const Geom* geom, const Ctrl* ctrl, const int* bin_start, const int* key,
+                        const int* slot, int* sorted_cell, Geom* sorted_geom, int cap_cells,
+                        cudaStream_t st);
+void launch_pair_build(const Grid* grid, const int* bin_start, const int* sorted_cell,
+                       const Geom* sorted_geom, const Ctrl* ctrl, BuildParams bp, int* scratch,
+                       int* count, int cap_bins, int num_sms, cudaStream_t st);
+void launch_csr_fill(const Ctrl* ctrl, const int* row_ptr, const int* scratch, int cap_per_cell,
+                     int* col, Ctrl* ctrl_w, int cap_cells, cudaStream_t st);
+
+// exclusive scan of len (device int) entries; out has len + 1 entries, out[len] = total
+void launch_scan(const int* in, const int* len, int* out, int* block_sums, int cap, cudaStream_t st);
+size_t scan_block_sums_size(int cap);
+
+void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, const Ctrl* ctrl,
+                       ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Gen6* fcc, int lanes, int mixed, int cap_cells, cudaStream_t st);
+
+// kind: MODE_TRIAL / MODE_RETRY / MODE_FINAL for the loop, 3 = evaluation for the API
+// (writes candidates and errors without touching the controller)
+void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
+                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
+                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st);
+void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
+                       const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
+                       cudaStream_t st);
+void launch_grow(Geom* geom, Phys* phys, const Ctrl* ctrl, double R, double dt, int cap_cells,
+                 cudaStream_t st);
+
+void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, int* cnt,
+                        int cap_cells, cudaStream_t st);
+void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
+                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st);
+
+// division (growth.hpp:66-426)
+struct DivideParams {
+    double R, Rcell, Ldiv;
+    double growth_mean, growth_std, daughter_length_std, angle_xy_bound, angle_z_bound;
+    uint64_t seed;
+    int cap_cells;
+};
+void launch_divide(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp,
+                   int* flags, int* ranks, int* block_sums, int* mothers, double* scratch_d,
+                   int* scratch_i, int* parents, int* n_parents, const Grid* grid,
+                   const int* bin_start, const int* sorted_cell, int cap_bins, cudaStream_t st);
+
+}   // namespace abm

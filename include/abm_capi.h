@@ -1,0 +1,163 @@
+/*
+ * C ABI of the B200 mechanics step for the kmnam/biofilm-ABMs 3-D model.
+ *
+ * The reference exposes no plugin or FFI layer: its seam is the set of
+ * templated free functions that ABM-3d/ABM-3d-cpp/include/simulation.hpp's
+ * runSimulation loop calls.  Each entry point below names the reference
+ * function (file:line) it stands in for.  Arrays cross this boundary in the
+ * reference's own layout: column-major double arrays (Eigen::Array<double,
+ * Dynamic, Dynamic>), cells n x ncols with the column order of
+ * ABM-3d/ABM-3d-cpp/include/indices.hpp:17-47 (+ gamma in column 21 when
+ * cell-cell adhesion is on), neighbor rows m x 7 (i, j, dx, dy, dz, si, sj).
+ *
+ * Ownership: the caller owns every host buffer; a context owns its device
+ * buffers, its CUDA stream and its CUDA graphs.  A context is not thread-safe;
+ * use one context per host thread.  Every call returns ABM_OK (0) or a negative
+ * status; abm_last_error() gives the message.  No call falls back to the CPU:
+ * without a usable CUDA device abm_create() fails with ABM_ERR_CUDA.
+ */
+#ifndef ABM_CAPI_H
+#define ABM_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABM_OK 0
+#define ABM_ERR_ARG -1          /* invalid argument or unsupported option */
+#define ABM_ERR_CUDA -2         /* CUDA runtime error (device missing, launch failure, ...) */
+#define ABM_ERR_CAPACITY -3     /* a device capacity (cells, neighbors per cell, bins) was exceeded */
+#define ABM_ERR_NAN -4          /* NaN/Inf in forces, velocities or the error norm */
+#define ABM_ERR_STATE -5        /* call order violated (e.g. iterate before upload) */
+
+/* Integration modes, as IntegrationMode in simulation.hpp:45-55 */
+#define ABM_HEUN_EULER 1
+#define ABM_BOGACKI_SHAMPINE 2
+#define ABM_RUNGE_KUTTA_FEHLBERG 3
+#define ABM_DORMAND_PRINCE 4
+
+/* Pair-force precision */
+#define ABM_PRECISION_FP64 0    /* everything in FP64 */
+#define ABM_PRECISION_MIXED 1   /* segment distance + pair force in FP32; near-parallel branch,
+                                   positions, orientations, stage sums and error norm in FP64 */
+
+typedef struct abm_params {
+    /* geometry and mechanics (runSimulation arguments, simulation.hpp:1106-1165) */
+    double R, Rcell, E0, Ecell;
+    double L0, Ldiv;
+    double neighbor_threshold;   /* abmConstAdhesion.cpp:53: 0.5 (2R + Ldiv) */
+    double nz_threshold;
+    int adhesion_mode;           /* 0 = NONE, 1 = JKR_ISOTROPIC with a fixed-gamma radius table */
+    int integration_mode;        /* ABM_HEUN_EULER ... ABM_DORMAND_PRINCE */
+    double max_stepsize, min_stepsize;
+    double max_error_allowed, min_error;
+    int max_tries_update_stepsize;
+    int iter_update_stepsize, iter_update_neighbors;
+    double max_rxy_noise, max_rz_noise, max_nxy_noise, max_nz_noise;
+    double cell_surface_coulomb_coeff;
+    int no_surface;
+    /* growth and division (growth.hpp:51-426) */
+    double growth_mean, growth_std, daughter_length_std;
+    double daughter_angle_xy_bound, daughter_angle_z_bound;
+    unsigned long long rng_seed;
+    /* device-side choices */
+    int precision;               /* ABM_PRECISION_FP64 or ABM_PRECISION_MIXED */
+    int cap_cells;               /* device capacity in cells (>= the largest population) */
+    int cap_neighbors_per_cell;  /* directed neighbor slots per cell (0 = default 64) */
+    int pair_lanes;              /* lanes per cell in the pair-force kernel: 4, 8, 16 or 32 (0 = 8) */
+    int use_graphs;              /* 1 = capture the iteration in a CUDA graph */
+} abm_params;
+
+typedef struct abm_stats {
+    long long iterations;        /* accepted steps taken by abm_iterate */
+    long long attempts;          /* RK evaluations (stepRungeKuttaAdaptive calls) */
+    long long retries;           /* controller re-runs at a reduced step (simulation.hpp:1717) */
+    long long rebuilds;          /* neighbor-table rebuilds */
+    long long divisions;         /* cells divided */
+    double t, dt;                /* simulated time and current step size */
+    double last_max_error;       /* scaled max error of the accepted attempt */
+    int n_cells, n_pairs;        /* current population and neighbor pairs (unordered) */
+} abm_stats;
+
+/* Device time per kernel group, from CUDA events on the context stream. */
+typedef struct abm_profile {
+    double pair_force_ms;        /* cellCellInteractionForces (+ distance refresh) */
+    double attempt_ms;           /* all RK attempts incl. controller and growth */
+    double rebuild_ms;           /* getCellNeighbors rebuilds */
+    long long pair_force_launches, attempt_launches, rebuild_launches;
+    long long iterations;
+} abm_profile;
+
+typedef struct abm_ctx abm_ctx;
+
+/* Create a context on the current CUDA device.  No reference counterpart: the
+ * reference keeps this state on the stack of runSimulation (simulation.hpp:1106-1170). */
+int abm_create(const abm_params* params, abm_ctx** ctx);
+int abm_destroy(abm_ctx* ctx);
+const char* abm_last_error(const abm_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work after it. */
+int abm_get_stream(abm_ctx* ctx, void** stream);
+int abm_synchronize(abm_ctx* ctx);
+
+/* JKR contact radius, the larger root of the jkr.hpp:67-144 quartic (jkrContactRadius(...).second). */
+int abm_jkr_contact_radius(double delta, double Req, double E, double gamma, double* radius);
+/* Radius table over LinSpaced(n, 0, 2 (R - Rcell)): calculateJKRContactRadii, simulation.hpp:86-104
+ * with the mesh of simulation.hpp:1379-1382. */
+int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_mesh,
+                         double* delta_out, double* radius_out);
+/* Install the fixed-gamma table (IsotropicJKRDataFixedGamma, mechanics.hpp:113-153). */
+int abm_set_jkr_table(abm_ctx* ctx, const double* delta, const double* radius, int n);
+
+/* Cell state in and out (the cells array of runSimulation).  ld >= n. */
+int abm_upload_cells(abm_ctx* ctx, const double* colmajor, int n, int ncols, int ld);
+int abm_download_cells(abm_ctx* ctx, double* colmajor, int ld);
+int abm_get_num_cells(abm_ctx* ctx, int* n);
+/* Simulation clock (t, dt, iter of runSimulation, simulation.hpp:1166-1168). */
+int abm_set_clock(abm_ctx* ctx, double t, double dt, int iter);
+int abm_get_clock(abm_ctx* ctx, double* t, double* dt, int* iter);
+/* Lineage vector (parents) of runSimulation; cell IDs index it. */
+int abm_set_parents(abm_ctx* ctx, const int* parents, int n);
+int abm_get_parents(abm_ctx* ctx, int* out, int cap, int* n);
+
+/* getCellNeighbors (mechanics.hpp:520-593): rebuild the neighbor pair set with a
+ * uniform-grid cell list; *m receives the number of unordered pairs. */
+int abm_build_neighbors(abm_ctx* ctx, int* m);
+/* The table in the reference's row order (i ascending, then j < i ascending),
+ * m x 7 column-major with leading dimension ld >= m.  Distances are those of
+ * updateNeighborDistances (mechanics.hpp:604-648) on the current cells. */
+int abm_download_neighbors(abm_ctx* ctx, double* rows, int ld, int cap, int* m);
+/* Replace the pair set by the given rows (columns 0 and 1 are read). */
+int abm_upload_neighbors(abm_ctx* ctx, const double* rows, int m, int ld);
+
+/* cellCellInteractionForces (mechanics.hpp:1209-1350, 1390-1659): dE/dq, n x 6. */
+int abm_cell_cell_forces(abm_ctx* ctx, double* dEdq_colmajor);
+/* getVelocities (mechanics.hpp:2011-2347) of the current cells, no noise: n x 6. */
+int abm_get_velocities(abm_ctx* ctx, double* v_colmajor);
+/* stepRungeKuttaAdaptive (mechanics.hpp:2406-2612) at dt without accepting it.
+ * Optional outputs: the new cell array (n x ncols), the error array (n x 6) and
+ * the controller's scaled max error (simulation.hpp:1697-1705).  `attempt`
+ * selects the noise stream. */
+int abm_rk_attempt(abm_ctx* ctx, double dt, int attempt, double* cells_out,
+                   double* errors_out, double* max_scaled_error);
+/* growCells (growth.hpp:51-57). */
+int abm_grow(abm_ctx* ctx, double dt);
+/* divideMaxLength + divideCells (growth.hpp:66-71, 166-426) at the current clock;
+ * *n_divided receives the number of mothers. */
+int abm_divide(abm_ctx* ctx, int* n_divided);
+
+/* n_iters iterations of the runSimulation loop body (simulation.hpp:1617-1864):
+ * divide -> rebuild if divided -> adaptive RK step with the step-size
+ * controller -> grow -> refresh distances -> t, iter -> rebuild every
+ * iter_update_neighbors.  Stops early when n_cells_stop > 0 and the population
+ * reaches it.  Runs asynchronously on the context stream; stats (optional)
+ * forces a synchronisation. */
+int abm_iterate(abm_ctx* ctx, int n_iters, int n_cells_stop, abm_stats* stats);
+int abm_get_stats(abm_ctx* ctx, abm_stats* stats);
+/* Same as abm_iterate without graphs, with CUDA events around each kernel group
+ * (no reference counterpart; measurement only). */
+int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABM_CAPI_H */

@@ -1,0 +1,1181 @@
+// ORACLE — test infrastructure only.  A plain C++17 restatement of the 3-D
+// mechanics step of kmnam/biofilm-ABMs (ABM-3d/ABM-3d-cpp), used by tests/,
+// __graft_entry__.smoke() and bench.py's CPU baseline leg as the checker.  The
+// product library never links, includes or calls anything under oracle/.
+//
+// Every function names the reference file:line it restates.  The reference
+// itself cannot be compiled here (Eigen, Boost and CGAL are absent), so:
+//   * CGAL's Segment_3/Segment_3 squared_distance (distances.hpp:341) is
+//     replaced by Ericson's clamped closest-point method for two segments
+//     (C. Ericson, Real-Time Collision Detection, 2005, sec. 5.1.9), which
+//     returns the same unique minimiser for non-parallel segments; it is pinned
+//     against the reference's own known-answer cases (testDistBetweenCells.cpp).
+//   * the MPFR Aberth quartic solve for the JKR radius table (jkr.hpp:67-144)
+//     is replaced by a bracketed Newton solve of the same quartic in long
+//     double, pinned by the invariants of testJKR.cpp:26-83.
+//   * boost::random::mt19937 draws are replaced by the counter-based Philox
+//     policy of philox.hpp (no reference test pins the mt19937 stream).
+// Arrays are column-major (n rows x ncols), exactly like the reference's
+// Eigen::Array<double, Dynamic, Dynamic>, so a reference cell array can be
+// handed in unchanged.  Vector sums are evaluated as ((x + y) + z) and the
+// file is compiled with -ffp-contract=off.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "philox.hpp"
+
+namespace oracle {
+
+// ABM-3d/ABM-3d-cpp/include/indices.hpp:17-47 ; gamma column simulation.hpp:1180
+enum Col3 {
+    C_ID = 0, C_RX = 1, C_RY = 2, C_RZ = 3, C_NX = 4, C_NY = 5, C_NZ = 6,
+    C_DRX = 7, C_DRY = 8, C_DRZ = 9, C_DNX = 10, C_DNY = 11, C_DNZ = 12,
+    C_L = 13, C_HALF_L = 14, C_T0 = 15, C_GROWTH = 16, C_ETA0 = 17,
+    C_ETA1 = 18, C_SIGMA0 = 19, C_GROUP = 20, C_GAMMA = 21
+};
+const int NCOLS_REQUIRED_3D = 21;
+const double PI = 3.141592653589793238462643383279502884;
+const double TWO_PI = 6.283185307179586476925286766559005768;
+
+struct Cells {
+    int n = 0, ncols = 0;
+    std::vector<double> a;   // column-major, leading dimension n
+    Cells() {}
+    Cells(int n_, int ncols_) : n(n_), ncols(ncols_), a((size_t)n_ * ncols_, 0.0) {}
+    double& operator()(int i, int j) { return a[(size_t)j * n + i]; }
+    double operator()(int i, int j) const { return a[(size_t)j * n + i]; }
+};
+
+struct V3 { double x, y, z; };
+inline V3 v3(double x, double y, double z) { V3 v = {x, y, z}; return v; }
+inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 operator*(double s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+inline double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline double norm(V3 a) { return std::sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
+
+inline V3 cell_r(const Cells& c, int i) { return v3(c(i, C_RX), c(i, C_RY), c(i, C_RZ)); }
+inline V3 cell_n(const Cells& c, int i) { return v3(c(i, C_NX), c(i, C_NY), c(i, C_NZ)); }
+
+// ------------------------------------------------------------------------
+// Segment distance (ABM-3d/ABM-3d-cpp/include/distances.hpp)
+// ------------------------------------------------------------------------
+
+// distances.hpp:92-105
+inline double nearest_body_coord(V3 r, V3 n, double half_l, V3 q)
+{
+    double s = dot(q - r, n);
+    if (std::fabs(s) <= half_l) return s;
+    else if (s > half_l) return half_l;
+    else return -half_l;
+}
+
+inline double clamp01(double x) { return x < 0 ? 0 : (x > 1 ? 1 : x); }
+
+// Stand-in for CGAL::Distance_3::internal::squared_distance(Segment_3, Segment_3)
+// (distances.hpp:341): returns the parameters (x, y) in [0, 1] of the closest
+// points p1 + x (q1 - p1) and p2 + y (q2 - p2).  Method: Ericson, Real-Time
+// Collision Detection (2005), sec. 5.1.9, "ClosestPtSegmentSegment".
+inline void closest_params_segments(V3 p1, V3 q1, V3 p2, V3 q2, double& x, double& y)
+{
+    V3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+    double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    if (a <= 0 && e <= 0) { x = 0; y = 0; return; }
+    if (a <= 0) { x = 0; y = clamp01(f / e); return; }
+    double c = dot(d1, r);
+    if (e <= 0) { y = 0; x = clamp01(-c / a); return; }
+    double b = dot(d1, d2);
+    double denom = a * e - b * b;
+    double s = (denom != 0) ? clamp01((b * f - c * e) / denom) : 0.0;
+    double t = (b * s + f) / e;
+    if (t < 0) { t = 0; s = clamp01(-c / a); }
+    else if (t > 1) { t = 1; s = clamp01((b - c) / a); }
+    x = s; y = t;
+}
+
+struct DistResult { V3 d; double s, t; };
+
+// distances.hpp:206-357 (distBetweenCells); segment endpoints as in
+// generateSegments (distances.hpp:59-80)
+inline DistResult dist_between_cells(V3 r1, V3 n1, double half_l1, V3 r2, V3 n2, double half_l2)
+{
+    DistResult out;
+    out.d = v3(0, 0, 0); out.s = 0; out.t = 0;
+    double cos_theta = dot(n1, n2);
+    if (cos_theta >= 0.9999 || cos_theta <= -0.9999)
+    {
+        V3 p1 = r1 - half_l1 * n1, q1 = r1 + half_l1 * n1;
+        V3 p2 = r2 - half_l2 * n2, q2 = r2 + half_l2 * n2;
+        double s_p1 = nearest_body_coord(r2, n2, half_l2, p1);
+        double s_q1 = nearest_body_coord(r2, n2, half_l2, q1);
+        V3 d_p1 = (r2 + s_p1 * n2) - p1;
+        V3 d_q1 = (r2 + s_q1 * n2) - q1;
+        double dist_p1 = norm(d_p1), dist_q1 = norm(d_q1);
+        if (s_p1 == s_q1)
+        {
+            if (dist_p1 < dist_q1) { out.s = -half_l1; out.t = s_p1; out.d = d_p1; }
+            else { out.s = half_l1; out.t = s_q1; out.d = d_q1; }
+        }
+        else
+        {
+            double s_p2 = nearest_body_coord(r1, n1, half_l1, p2);
+            double s_q2 = nearest_body_coord(r1, n1, half_l1, q2);
+            V3 d_p2 = (r1 + s_p2 * n1) - p2;
+            V3 d_q2 = (r1 + s_q2 * n1) - q2;
+            double dist_p2 = norm(d_p2), dist_q2 = norm(d_q2);
+            // std::sort of four (dist, idx) pairs by dist (distances.hpp:274-286):
+            // libstdc++ sorts a 4-element range by insertion sort, which keeps
+            // ties in their original order, so a stable insertion sort is used.
+            double dv[4] = {dist_p1, dist_q1, dist_p2, dist_q2};
+            int iv[4] = {0, 1, 2, 3};
+            for (int a = 1; a < 4; ++a)
+            {
+                double kd = dv[a]; int ki = iv[a]; int b = a - 1;
+                while (b >= 0 && kd < dv[b]) { dv[b + 1] = dv[b]; iv[b + 1] = iv[b]; --b; }
+                dv[b + 1] = kd; iv[b + 1] = ki;
+            }
+            bool m0 = (iv[0] == 0 || iv[1] == 0), m1 = (iv[0] == 1 || iv[1] == 1);
+            bool m2 = (iv[0] == 2 || iv[1] == 2);
+            if (m0)
+            {
+                if (m1)
+                {
+                    out.s = 0.0;
+                    out.t = nearest_body_coord(r2, n2, half_l2, r1);
+                    out.d = (r2 + out.t * n2) - r1;
+                }
+                else if (m2)
+                {
+                    out.s = (-half_l1 + s_p2) / 2;
+                    out.t = nearest_body_coord(r2, n2, half_l2, r1 + out.s * n1);
+                    out.d = ((r2 + out.t * n2) - r1) - out.s * n1;
+                }
+                else
+                {
+                    out.s = (-half_l1 + s_q2) / 2;
+                    out.t = nearest_body_coord(r2, n2, half_l2, r1 + out.s * n1);
+                    out.d = ((r2 + out.t * n2) - r1) - out.s * n1;
+                }
+            }
+            else if (m1)
+            {
+                if (m2)
+                {
+                    out.s = (half_l1 + s_p2) / 2;
+                    out.t = nearest_body_coord(r2, n2, half_l2, r1 + out.s * n1);
+                    out.d = ((r2 + out.t * n2) - r1) - out.s * n1;
+                }
+                else
+                {
+                    out.s = (half_l1 + s_q2) / 2;
+                    out.t = nearest_body_coord(r2, n2, half_l2, r1 + out.s * n1);
+                    out.d = ((r2 + out.t * n2) - r1) - out.s * n1;
+                }
+            }
+            else
+            {
+                out.t = 0.0;
+                out.s = nearest_body_coord(r1, n1, half_l1, r2);
+                out.d = (r2 - r1) - out.s * n1;
+            }
+        }
+    }
+    else
+    {
+        V3 p1 = r1 - half_l1 * n1, q1 = r1 + half_l1 * n1;
+        V3 p2 = r2 - half_l2 * n2, q2 = r2 + half_l2 * n2;
+        double x, y;
+        closest_params_segments(p1, q1, p2, q2, x, y);
+        out.s = x * 2 * half_l1 - half_l1;
+        out.t = y * 2 * half_l2 - half_l2;
+        out.d = ((r2 + out.t * n2) - r1) - out.s * n1;
+    }
+    return out;
+}
+
+inline DistResult dist_cells(const Cells& c, int i, int j)
+{
+    return dist_between_cells(cell_r(c, i), cell_n(c, i), c(i, C_HALF_L),
+                              cell_r(c, j), cell_n(c, j), c(j, C_HALF_L));
+}
+
+// ------------------------------------------------------------------------
+// Neighbor table (mechanics.hpp:520-648).  Row = (i, j, dx, dy, dz, si, sj)
+// ------------------------------------------------------------------------
+struct Neighbors {
+    std::vector<int> i, j;
+    std::vector<double> dx, dy, dz, si, sj;
+    int size() const { return (int)i.size(); }
+};
+
+// mechanics.hpp:520-593 (getCellNeighbors): O(n^2), rows i-major, j < i ascending
+inline Neighbors get_cell_neighbors(const Cells& cells, double neighbor_threshold,
+                                    double R, double Ldiv)
+{
+    Neighbors nb;
+    int n = cells.n;
+    if (n == 1) return nb;
+    const double prefilter = neighbor_threshold + Ldiv + 2 * R;
+    for (int i = 0; i < n; ++i)
+    {
+        V3 ri = cell_r(cells, i);
+        for (int j = 0; j < i; ++j)
+        {
+            double dist_rij = norm(ri - cell_r(cells, j));
+            if (dist_rij < prefilter)
+            {
+                DistResult res = dist_cells(cells, i, j);
+                if (norm(res.d) < neighbor_threshold)
+                {
+                    nb.i.push_back(i); nb.j.push_back(j);
+                    nb.dx.push_back(res.d.x); nb.dy.push_back(res.d.y); nb.dz.push_back(res.d.z);
+                    nb.si.push_back(res.s); nb.sj.push_back(res.t);
+                }
+            }
+        }
+    }
+    return nb;
+}
+
+// mechanics.hpp:604-648 (updateNeighborDistances)
+inline void update_neighbor_distances(const Cells& cells, Neighbors& nb)
+{
+    for (int k = 0; k < nb.size(); ++k)
+    {
+        DistResult res = dist_cells(cells, nb.i[k], nb.j[k]);
+        nb.dx[k] = res.d.x; nb.dy[k] = res.d.y; nb.dz[k] = res.d.z;
+        nb.si[k] = res.s; nb.sj[k] = res.t;
+    }
+}
+
+// ------------------------------------------------------------------------
+// Auxiliary integrals (ABM-3d/ABM-3d-cpp/include/integrals.hpp)
+// ------------------------------------------------------------------------
+inline double sstar(double rz, double nz, double R) { return (R - rz) / nz; }        // :35-45
+inline double phi(double rz, double nz, double R, double s) { return R - rz - s * nz; }  // :56-60
+
+// integrals.hpp:116-140
+inline double integral1(double rz, double nz, double R, double half_l, double gamma, double ss)
+{
+    if (ss > half_l)
+    {
+        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        return (o1 - o2) / (nz * (gamma + 1));
+    }
+    else if (ss > -half_l)
+    {
+        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        return o1 / (nz * (gamma + 1));
+    }
+    return 0;
+}
+
+// integrals.hpp:159-184
+inline double integral2(double rz, double nz, double R, double half_l, double gamma, double ss)
+{
+    double term1 = integral1(rz, nz, R, half_l, gamma + 1, ss);
+    double term2 = 0;
+    if (ss > half_l)
+    {
+        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        term2 = -half_l * (o1 + o2);
+    }
+    else if (ss > -half_l)
+    {
+        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        term2 = -half_l * o1;
+    }
+    return (term1 + term2) / (nz * (gamma + 1));
+}
+
+// integrals.hpp:250-266
+inline double integral4(double nz, double half_l, double ss)
+{
+    (void)nz;
+    if (ss > half_l) return 2 * half_l;
+    else if (ss > -half_l) return ss + half_l;
+    return 0;
+}
+// integrals.hpp:279-291
+inline double integral5(double nz, double half_l, double ss)
+{
+    (void)nz;
+    if (-half_l < ss && ss <= half_l) return (ss * ss - half_l * half_l) / 2.0;
+    return 0.0;
+}
+// integrals.hpp:304-318
+inline double integral6(double nz, double half_l, double ss)
+{
+    (void)nz;
+    if (ss > half_l) return 2 * half_l * half_l * half_l / 3.0;
+    else if (ss > -half_l) return (ss * ss * ss + half_l * half_l * half_l) / 3.0;
+    return 0.0;
+}
+
+// integrals.hpp:400-463 (areaIntegrals)
+inline void area_integrals(double rz, double nz, double R, double half_l, double ss,
+                           double& area1, double& area2, double& area3)
+{
+    double int4 = integral4(nz, half_l, ss);
+    double int5 = integral5(nz, half_l, ss);
+    double int6 = integral6(nz, half_l, ss);
+    double int1a = integral1(rz, nz, R, half_l, 0.5, ss);
+    double int1b = integral1(rz, nz, R, half_l, 1.5, ss);
+    double int1c = integral1(rz, nz, R, half_l, 2.5, ss);
+    double term1 = std::sqrt(R) * (1 - nz * nz) * int1a;
+    double term2 = PI * R * nz * nz * int4;
+    area1 = term1 + term2;
+    double overlap1 = 0, overlap2 = 0;
+    if (ss > half_l) { overlap1 = phi(rz, nz, R, -half_l); overlap2 = phi(rz, nz, R, half_l); }
+    else if (ss > -half_l) { overlap1 = phi(rz, nz, R, -half_l); }
+    double o1p1 = std::pow(overlap1, 1.5), o2p1 = std::pow(overlap2, 1.5);
+    term2 = -half_l * (o1p1 + o2p1);
+    double int2a = (int1b + term2) / (1.5 * nz);
+    term1 = std::sqrt(R) * (1 - nz * nz) * int2a;
+    term2 = PI * R * nz * nz * int5;
+    area2 = term1 + term2;
+    double o1p2 = o1p1 * overlap1, o2p2 = o2p1 * overlap2;
+    term2 = -half_l * (o1p2 + o2p2);
+    double int2b = (int1c + term2) / (2.5 * nz);
+    term1 = 2 * int2b;
+    term2 = half_l * half_l * (o1p1 - o2p1);
+    double int3 = (term1 + term2) / (1.5 * nz);
+    term1 = std::sqrt(R) * (1 - nz * nz) * int3;
+    term2 = PI * R * nz * nz * int6;
+    area3 = term1 + term2;
+}
+
+// ------------------------------------------------------------------------
+// JKR radius table and lookup
+// ------------------------------------------------------------------------
+
+// Eigen::Matrix::LinSpaced(n, low, high) for a real scalar with |high| >= |low|:
+// low + i * step for i < n - 1 and exactly high at the last entry.
+inline std::vector<double> linspaced(int n, double low, double high)
+{
+    std::vector<double> v(n);
+    if (n == 1) { v[0] = high; return v; }
+    double step = (high - low) / double(n - 1);
+    for (int i = 0; i < n; ++i) v[i] = (i == n - 1) ? high : low + double(i) * step;
+    return v;
+}
+
+// jkr.hpp:67-144 (jkrContactRadius(delta, Req, E, gamma).second): the larger
+// positive real root a of  a^4 - 2 Req delta a^2 - (4 pi gamma Req^2 / E) a
+// + delta^2 Req^2 = 0, i.e. the root of  g(a) = a^2/Req - 2 sqrt(pi gamma a/E)
+// - delta  on the branch where g increases.  Solved in long double by
+// bracketing plus Newton steps (the reference uses 100-digit MPFR Aberth).
+inline double jkr_contact_radius(double delta, double Req, double E, double gamma)
+{
+    typedef long double LD;
+    LD d = delta, R = Req, Ee = E, g = gamma, pi = 3.141592653589793238462643383279502884L;
+    if (g <= 0) return (double)std::sqrt(R * d);
+    // g(a) = a^2/R - 2 sqrt(pi g a / E) - d, minimum at a_min where g'(a) = 0
+    auto G = [&](LD a) { return a * a / R - 2 * std::sqrt(pi * g * a / Ee) - d; };
+    auto dG = [&](LD a) { return 2 * a / R - std::sqrt(pi * g / (Ee * a)); };
+    LD a_min = std::cbrt(R * R * pi * g / (4 * Ee));
+    LD lo = a_min, hi = std::max(a_min * 2, std::sqrt(R * std::max(d, (LD)0)) + a_min * 4 + 1e-6L);
+    while (G(hi) < 0) hi *= 2;
+    LD a = hi;
+    for (int it = 0; it < 200; ++it)
+    {
+        LD ga = G(a);
+        if (ga > 0) hi = a; else lo = a;
+        LD step = ga / dG(a);
+        LD an = a - step;
+        if (!(an > lo && an < hi)) an = (lo + hi) / 2;
+        if (std::fabs(an - a) <= 1e-19L * std::fabs(a)) { a = an; break; }
+        a = an;
+    }
+    return (double)a;
+}
+
+// simulation.hpp:86-104 (calculateJKRContactRadii) over the overlap mesh of
+// simulation.hpp:1379-1382
+inline std::vector<double> jkr_radius_table(const std::vector<double>& overlaps, double gamma,
+                                            double R, double E0)
+{
+    std::vector<double> radii(overlaps.size());
+    for (size_t i = 0; i < overlaps.size(); ++i)
+        radii[i] = jkr_contact_radius(overlaps[i], R / 2, E0, gamma);
+    return radii;
+}
+
+// utils.hpp:1169-1215 (nearestValue)
+inline int nearest_value(const std::vector<double>& values, double x)
+{
+    int sz = (int)values.size();
+    if (x <= values[0]) return 0;
+    else if (x >= values[sz - 1]) return sz - 1;
+    int low = 0, high = sz - 1, nearest_idx = 0;
+    while (low <= high)
+    {
+        int mid = (low + high) / 2;
+        if (values[mid] <= x && x < values[mid + 1]) { nearest_idx = mid; break; }
+        else if (x >= values[mid + 1]) low = mid + 1;
+        else high = mid - 1;
+    }
+    if (low > high) throw std::runtime_error("Unexpected error during binary search");
+    if (x - values[nearest_idx] < values[nearest_idx + 1] - x) return nearest_idx;
+    return nearest_idx + 1;
+}
+
+// ------------------------------------------------------------------------
+// Parameters
+// ------------------------------------------------------------------------
+struct Params3 {
+    double R = 0.8, Rcell = 0.5, E0 = 3900.0, Ecell = 3.9e6;
+    double L0 = 2.0, Ldiv = 5.6;
+    double neighbor_threshold = 3.6, nz_threshold = 1e-8;
+    int adhesion_mode = 1;            // 0 none, 1 isotropic JKR with a fixed-gamma radius table
+    int integration_mode = 1;         // 1 HE21, 2 BS32, 3 RKF45, 4 DP54 (simulation.hpp:45-55)
+    double max_stepsize = 1e-6, min_stepsize = 1e-9;
+    double max_error_allowed = 1e-8, min_error = 1e-30;
+    int max_tries_update_stepsize = 3;
+    int iter_update_stepsize = 1, iter_update_neighbors = 100;
+    double max_rxy_noise = 0, max_rz_noise = 0, max_nxy_noise = 0, max_nz_noise = 0;
+    double cell_surface_coulomb_coeff = 1.0;
+    int no_surface = 0;
+    double growth_mean = 0, growth_std = 0, daughter_length_std = 0;
+    double daughter_angle_xy_bound = 0, daughter_angle_z_bound = 0;
+    uint64_t rng_seed = 42;
+    int n_start_multithread = 50;
+    std::vector<double> jkr_overlaps, jkr_radii;
+};
+
+struct Tableau {
+    int s = 0; double error_order = 0;
+    std::vector<double> A, b, bs;   // A row-major s x s
+    double a(int i, int j) const { return A[(size_t)i * s + j]; }
+};
+
+// simulation.hpp:1207-1268
+inline Tableau make_tableau(int mode)
+{
+    Tableau t;
+    if (mode == 1)
+    {
+        t.s = 2; t.A = {0, 0, 1, 0}; t.b = {0.5, 0.5}; t.bs = {1, 0}; t.error_order = 1;
+    }
+    else if (mode == 2)
+    {
+        t.s = 4;
+        t.A = {0, 0, 0, 0,  1. / 2., 0, 0, 0,  0, 3. / 4., 0, 0,  2. / 9., 1. / 3., 4. / 9., 0};
+        t.b = {2. / 9., 1. / 3., 4. / 9., 0};
+        t.bs = {7. / 24., 1. / 4., 1. / 3., 1. / 8.};
+        t.error_order = 2;
+    }
+    else if (mode == 3)
+    {
+        t.s = 6;
+        t.A = {0, 0, 0, 0, 0, 0,
+               1. / 4., 0, 0, 0, 0, 0,
+               3. / 32., 9. / 32., 0, 0, 0, 0,
+               1932. / 2197., -7200. / 2197., 7296. / 2197., 0, 0, 0,
+               439. / 216., -8.0, 3680. / 513., -845. / 4104., 0, 0,
+               -8. / 27., 2.0, -3544. / 2565., 1859. / 4104., -11. / 40., 0};
+        t.b = {16. / 135., 0, 6656. / 12825., 28561. / 56430., -9. / 50., 2. / 55.};
+        t.bs = {25. / 216., 0, 1408. / 2565., 2197. / 4104., -1. / 5., 0};
+        t.error_order = 4;
+    }
+    else if (mode == 4)
+    {
+        t.s = 7;
+        t.A = {0, 0, 0, 0, 0, 0, 0,
+               1. / 5., 0, 0, 0, 0, 0, 0,
+               3. / 40., 9. / 40., 0, 0, 0, 0, 0,
+               44. / 45., -56. / 15., 32. / 9., 0, 0, 0, 0,
+               19372. / 6561., -25360. / 2187., 64448. / 6561., -212. / 729, 0, 0, 0,
+               9017. / 3168., -355. / 33., 46732. / 5247., 49. / 176., -5103. / 18656., 0, 0,
+               35. / 384., 0, 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84., 0};
+        t.b = {35. / 384., 0, 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84., 0};
+        t.bs = {5179. / 57600., 0, 7571. / 16695., 393. / 640., -92097. / 339200., 187. / 2100., 1. / 40.};
+        t.error_order = 4;
+    }
+    else throw std::runtime_error("unsupported integration mode");
+    return t;
+}
+
+// simulation.hpp:1270-1274
+inline void repulsion_prefactors(const Params3& p, double pf[3])
+{
+    pf[0] = (4. / 3.) * p.E0 * std::sqrt(p.R / 2);
+    pf[1] = (4. / 3.) * p.Ecell * std::sqrt(p.Rcell / 2);
+    pf[2] = (4. / 3.) * p.E0 * std::sqrt(p.R / 2) * std::pow(2 * (p.R - p.Rcell), 1.5);
+}
+
+// ------------------------------------------------------------------------
+// Generalised forces (mechanics.hpp)
+// ------------------------------------------------------------------------
+typedef std::vector<double> Arr6;   // n x 6, column-major (ld = n)
+inline double& A6(Arr6& a, int n, int i, int k) { return a[(size_t)k * n + i]; }
+inline double A6c(const Arr6& a, int n, int i, int k) { return a[(size_t)k * n + i]; }
+
+// adhesion.hpp:282-370 (forcesIsotropicJKRLagrange, include_constraint = false,
+// interpolate = true) with max_overlap = 2 (R - Rcell); rows = cells i, j
+inline void jkr_forces(V3 d12, double R, double E0, double gamma, double s, double t,
+                       const std::vector<double>& tab_delta, const std::vector<double>& tab_radius,
+                       double max_overlap, double out[2][6])
+{
+    for (int a = 0; a < 2; ++a) for (int k = 0; k < 6; ++k) out[a][k] = 0;
+    double dist = norm(d12);
+    if (dist < 2 * R)
+    {
+        V3 d12n = v3(d12.x / dist, d12.y / dist, d12.z / dist);
+        double delta = 2 * R - dist;
+        if (max_overlap >= 0 && delta > max_overlap) delta = max_overlap;
+        int idx_d1 = nearest_value(tab_delta, delta);
+        int idx_d2 = (tab_delta[idx_d1] < delta ? idx_d1 + 1 : idx_d1 - 1);
+        if (idx_d1 > idx_d2) std::swap(idx_d1, idx_d2);
+        double d1 = tab_delta[idx_d1], d2 = tab_delta[idx_d2];
+        double r1 = tab_radius[idx_d1], r2 = tab_radius[idx_d2];
+        double radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
+        double Req = R / 2;
+        double a3 = radius * radius * radius;
+        double term1 = 4 * E0 * a3 / (3 * Req);
+        double term2 = 4 * std::sqrt(PI * a3 * gamma * E0);
+        V3 v = (term2 - term1) * d12n;
+        out[0][0] = -v.x; out[0][1] = -v.y; out[0][2] = -v.z;
+        out[1][0] = v.x; out[1][1] = v.y; out[1][2] = v.z;
+        out[0][3] = -s * v.x; out[0][4] = -s * v.y; out[0][5] = -s * v.z;
+        out[1][3] = t * v.x; out[1][4] = t * v.y; out[1][5] = t * v.z;
+    }
+}
+
+// mechanics.hpp:1209-1350 (Hertz only) and :1390-1659 (Hertz + isotropic JKR),
+// include_constraint = false, no cell-cell friction.  Returns dE/dq (n x 6).
+inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Params3& p)
+{
+    const int n = cells.n, m = nb.size();
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    if (m == 0) return dEdq;
+    const double R = p.R, Rcell = p.Rcell;
+    double pf[3]; repulsion_prefactors(p, pf);
+    const bool adhesion = (p.adhesion_mode != 0);
+    for (int k = 0; k < m; ++k)
+    {
+        int i = nb.i[k], j = nb.j[k];
+        V3 dij = v3(nb.dx[k], nb.dy[k], nb.dz[k]);
+        double dist = norm(dij);
+        double overlap = 2 * R - dist;
+        if (!(overlap > 0)) continue;
+        double si = nb.si[k], sj = nb.sj[k];
+        V3 dijn = v3(dij.x / dist, dij.y / dist, dij.z / dist);
+        double f[2][6];
+        double max_overlap = 2 * (R - Rcell);
+        double gamma = adhesion ? std::min(cells(i, C_GAMMA), cells(j, C_GAMMA)) : 0.0;
+        if (adhesion && gamma > 0)
+        {
+            jkr_forces(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_radii, max_overlap, f);
+        }
+        else
+        {
+            double magnitude;
+            if (overlap <= max_overlap) magnitude = pf[0] * std::pow(overlap, 1.5);
+            else
+            {
+                magnitude = pf[2];
+                if (!adhesion) magnitude += pf[1] * std::pow(overlap - max_overlap, 1.5);
+            }
+            V3 vij = magnitude * dijn;
+            f[0][0] = vij.x; f[0][1] = vij.y; f[0][2] = vij.z;
+            f[1][0] = -vij.x; f[1][1] = -vij.y; f[1][2] = -vij.z;
+            f[0][3] = si * vij.x; f[0][4] = si * vij.y; f[0][5] = si * vij.z;
+            f[1][3] = -sj * vij.x; f[1][4] = -sj * vij.y; f[1][5] = -sj * vij.z;
+        }
+        for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += f[0][c]; A6(dEdq, n, j, c) += f[1][c]; }
+        if (adhesion && overlap > 2 * (R - Rcell))
+        {
+            double magnitude = pf[1] * std::pow(overlap - 2 * (R - Rcell), 1.5);
+            V3 vij = magnitude * dijn;
+            double h[2][6] = {{vij.x, vij.y, vij.z, si * vij.x, si * vij.y, si * vij.z},
+                              {-vij.x, -vij.y, -vij.z, -sj * vij.x, -sj * vij.y, -sj * vij.z}};
+            for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += h[0][c]; A6(dEdq, n, j, c) += h[1][c]; }
+        }
+    }
+    return dEdq;
+}
+
+// mechanics.hpp:673-780 (cellSurfaceRepulsionForces, include_constraint = false)
+inline Arr6 cell_surface_repulsion_forces(const Cells& cells, const std::vector<double>& ss,
+                                          double R, double E0, const std::vector<int>& assume_2d,
+                                          bool multithread)
+{
+    const int n = cells.n;
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    const double prefactor0 = 2 * E0;
+    const double prefactor1 = (8. / 3.) * E0 * std::pow(R, 0.5);
+    const double prefactor2 = 2 * E0 * std::pow(R, 0.5);
+    #pragma omp parallel for if(multithread)
+    for (int i = 0; i < n; ++i)
+    {
+        double rz = cells(i, C_RZ), nz = cells(i, C_NZ), hl = cells(i, C_HALF_L);
+        if (assume_2d[i])
+        {
+            double ph = R - rz;
+            if (ph > 0) A6(dEdq, n, i, 2) = -prefactor0 * ph * cells(i, C_L);
+        }
+        else
+        {
+            double nz2 = nz * nz;
+            double int1 = integral1(rz, nz, R, hl, 1.0, ss[i]);
+            double int2 = integral1(rz, nz, R, hl, 0.5, ss[i]);
+            A6(dEdq, n, i, 2) = -prefactor0 * ((1.0 - nz2) * int1 + std::sqrt(R) * nz2 * int2);
+            double int3 = integral1(rz, nz, R, hl, 2.0, ss[i]);
+            double int4 = integral2(rz, nz, R, hl, 1.0, ss[i]);
+            double int5 = integral1(rz, nz, R, hl, 1.5, ss[i]);
+            double int6 = integral2(rz, nz, R, hl, 0.5, ss[i]);
+            double& d5 = A6(dEdq, n, i, 5);
+            d5 -= prefactor0 * nz * int3;
+            d5 -= prefactor0 * (1 - nz2) * int4;
+            d5 += prefactor1 * nz * int5;
+            d5 -= prefactor2 * nz2 * int6;
+        }
+    }
+    return dEdq;
+}
+
+// mechanics.hpp:800-910 (cellSurfaceAdhesionForces, include_constraint = false)
+inline Arr6 cell_surface_adhesion_forces(const Cells& cells, const std::vector<double>& ss,
+                                         double R, const std::vector<int>& assume_2d,
+                                         bool multithread)
+{
+    const int n = cells.n;
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    const double prefactor0 = std::pow(R, 0.5) / 2;
+    const double prefactor1 = 2 * PI * R;
+    const double prefactor2 = 2 * std::pow(R, 0.5);
+    #pragma omp parallel for if(multithread)
+    for (int i = 0; i < n; ++i)
+    {
+        double rz = cells(i, C_RZ), nz = cells(i, C_NZ), hl = cells(i, C_HALF_L);
+        double sig = cells(i, C_SIGMA0);
+        if (assume_2d[i])
+        {
+            double ph = R - rz;
+            if (ph > 0) A6(dEdq, n, i, 2) = sig * prefactor0 * cells(i, C_L) / std::pow(ph, 0.5);
+        }
+        else
+        {
+            double nz2 = nz * nz;
+            double int1 = integral1(rz, nz, R, hl, -0.5, ss[i]);
+            double term2 = 0.0;
+            if (std::fabs(ss[i]) < hl) term2 = (prefactor1 / 2) * nz;
+            double d2 = prefactor0 * (1 - nz2) * int1 + term2;
+            A6(dEdq, n, i, 2) = d2 * sig;
+            double int2 = integral1(rz, nz, R, hl, 0.5, ss[i]);
+            double int3 = integral2(rz, nz, R, hl, -0.5, ss[i]);
+            double int4 = integral4(nz, hl, ss[i]);
+            double term4 = 0.0;
+            if (std::fabs(ss[i]) < hl) term4 = (prefactor1 / 2) * (R - rz);
+            double d5 = 0;
+            d5 += prefactor2 * nz * int2;
+            d5 += prefactor0 * (1 - nz2) * int3;
+            d5 -= prefactor1 * nz * int4;
+            d5 += term4;
+            A6(dEdq, n, i, 5) = d5 * sig;
+        }
+    }
+    return dEdq;
+}
+
+// mechanics.hpp:1702-1769 (getConservativeForces): -(dE_cc) - dE_rep - dE_adh
+inline Arr6 get_conservative_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
+                                    const std::vector<int>& assume_2d, bool multithread,
+                                    const Arr6* dEdq_cc_cached = nullptr)
+{
+    const int n = cells.n;
+    std::vector<double> ss(n);
+    for (int i = 0; i < n; ++i)
+        ss[i] = assume_2d[i] ? std::numeric_limits<double>::quiet_NaN()
+                             : sstar(cells(i, C_RZ), cells(i, C_NZ), p.R);
+    Arr6 cc = dEdq_cc_cached ? *dEdq_cc_cached : cell_cell_forces(cells, nb, p);
+    Arr6 rep((size_t)n * 6, 0.0), adh((size_t)n * 6, 0.0);
+    if (!p.no_surface)
+    {
+        rep = cell_surface_repulsion_forces(cells, ss, p.R, p.E0, assume_2d, multithread);
+        adh = cell_surface_adhesion_forces(cells, ss, p.R, assume_2d, multithread);
+    }
+    Arr6 out((size_t)n * 6);
+    for (size_t k = 0; k < out.size(); ++k) out[k] = ((-cc[k]) - rep[k]) - adh[k];
+    return out;
+}
+
+// mechanics.hpp:1918-1959 (normalizeOrientations)
+inline void normalize_orientations(Cells& cells)
+{
+    for (int i = 0; i < cells.n; ++i)
+    {
+        double nx = cells(i, C_NX), ny = cells(i, C_NY), nz = cells(i, C_NZ);
+        double nrm = std::sqrt((nx * nx + ny * ny) + nz * nz);
+        cells(i, C_NX) = nx / nrm; cells(i, C_NY) = ny / nrm; cells(i, C_NZ) = nz / nrm;
+    }
+    for (int i = 0; i < cells.n; ++i)
+    {
+        if (cells(i, C_NZ) < 0)
+        {
+            cells(i, C_NX) *= -1; cells(i, C_NY) *= -1; cells(i, C_NZ) *= -1;
+        }
+    }
+}
+
+// mechanics.hpp:2011-2347 (getVelocities) with friction NONE.  `noise` is n x 6.
+inline Arr6 get_velocities(const Cells& cells, const Neighbors& nb, const Params3& p,
+                           const std::vector<int>& assume_2d, const Arr6& noise,
+                           bool multithread, const Arr6* dEdq_cc_cached = nullptr)
+{
+    const int n = cells.n;
+    const double R = p.R, E0 = p.E0;
+    const double coul = p.cell_surface_coulomb_coeff;
+    Arr6 v((size_t)n * 6, 0.0);
+    std::vector<double> ss(n);
+    for (int i = 0; i < n; ++i)
+        ss[i] = assume_2d[i] ? std::numeric_limits<double>::quiet_NaN()
+                             : sstar(cells(i, C_RZ), cells(i, C_NZ), R);
+    Arr6 F = get_conservative_forces(cells, nb, p, assume_2d, multithread, dEdq_cc_cached);
+    for (size_t k = 0; k < F.size(); ++k) F[k] += noise[k];
+    #pragma omp parallel for if(multithread)
+    for (int i = 0; i < n; ++i)
+    {
+        const double rz = cells(i, C_RZ), nx = cells(i, C_NX), ny = cells(i, C_NY), nz = cells(i, C_NZ);
+        const double l = cells(i, C_L), hl = cells(i, C_HALF_L);
+        const double eta0 = cells(i, C_ETA0);
+        double f[6]; for (int k = 0; k < 6; ++k) f[k] = A6c(F, n, i, k);
+        double out[6] = {0, 0, 0, 0, 0, 0};
+        bool contacting = false;
+        if (!assume_2d[i])
+        {
+            double z1 = rz - hl * nz, z2 = rz + hl * nz;
+            contacting = (z1 < R || z2 < R);
+        }
+        else contacting = (rz < R);
+        if (p.no_surface || !contacting)
+        {
+            double K = eta0 * l;
+            double L = K * l * l / 12;
+            double mult = -((nx * f[3] + ny * f[4]) + nz * f[5]);
+            out[0] = f[0] / K; out[1] = f[1] / K; out[2] = f[2] / K;
+            out[3] = (f[3] + mult * nx) / L; out[4] = (f[4] + mult * ny) / L; out[5] = (f[5] + mult * nz) / L;
+        }
+        else if (assume_2d[i])
+        {
+            double K, L;
+            if (coul == 0)
+            {
+                double a = std::sqrt(R * (R - rz));
+                double eta_c = eta0 + cells(i, C_ETA1) * a / R;
+                K = eta_c * l;
+                L = K * l * l / 12;
+            }
+            else
+            {
+                double K_vis = eta0 * l;
+                double L_vis = K_vis * l * l / 12;
+                double a = std::sqrt(R * (R - rz));
+                double K_fric = cells(i, C_ETA1) * l * a / R;
+                double drx = cells(i, C_DRX), dry = cells(i, C_DRY);
+                double drxy = std::sqrt(drx * drx + dry * dry);
+                double friction_norm = K_fric * drxy;
+                double max_norm = coul * (2 * E0 * (R - rz) * l);
+                if (friction_norm > max_norm)
+                {
+                    double eta1_tr = max_norm * R / (drxy * l * a);
+                    K_fric = eta1_tr * l * a / R;
+                }
+                double L_fric = K_fric * l * l / 12;
+                K = K_vis + K_fric;
+                L = L_vis + L_fric;
+            }
+            double mult = -(nx * f[3] + ny * f[4]);
+            out[0] = f[0] / K; out[1] = f[1] / K;
+            out[3] = (f[3] + mult * nx) / L; out[4] = (f[4] + mult * ny) / L;
+            out[2] = f[2] / (eta0 * l);
+            out[5] = 12 * f[5] / (eta0 * l * l * l);
+        }
+        else
+        {
+            double eta1 = cells(i, C_ETA1);
+            double A1, A2, A3;
+            area_integrals(rz, nz, R, hl, ss[i], A1, A2, A3);
+            if (coul > 0)
+            {
+                double drx = cells(i, C_DRX), dry = cells(i, C_DRY);
+                double dnx = cells(i, C_DNX), dny = cells(i, C_DNY);
+                double drxy = std::sqrt(drx * drx + dry * dry);
+                double dnxy = std::sqrt(dnx * dnx + dny * dny);
+                double friction_norm = A1 * drxy;
+                friction_norm += A2 * dnxy;
+                friction_norm *= (eta1 / R);
+                double max_norm = (1 - nz * nz) * integral1(rz, nz, R, hl, 1, ss[i]);
+                max_norm += std::sqrt(R) * nz * nz * integral1(rz, nz, R, hl, 0.5, ss[i]);
+                max_norm *= (2 * E0 * coul);
+                if (friction_norm > max_norm)
+                    eta1 = max_norm * R / (A1 * drxy + A2 * dnxy);
+            }
+            const double c1 = eta0 * l + (eta1 / R) * A1;
+            const double c2 = eta0 * l;
+            const double c3 = c2 * l * l / 12 + (eta1 / R) * A3;
+            const double c4 = c2 * l * l / 12;
+            const double c5 = (eta1 / R) * A2;
+            const double term1 = c3 - (c5 * c5 / c1);
+            const double w4 = f[3] - f[0] * (c5 / c1);
+            const double w5 = f[4] - f[1] * (c5 / c1);
+            const double nx2 = nx / term1, ny2 = ny / term1, nz2 = nz / c4;
+            const double alpha = 2 * ((nx * nx2 + ny * ny2) + nz * nz2);
+            const double beta = -((w4 * nx2 + w5 * ny2) + f[5] * nz2);
+            const double lambda = beta / alpha;
+            out[5] = (f[5] + 2 * nz * lambda) / c4;
+            out[4] = (w5 + 2 * ny * lambda) / term1;
+            out[3] = (w4 + 2 * nx * lambda) / term1;
+            out[2] = f[2] / c2;
+            out[1] = (f[1] - c5 * out[4]) / c1;
+            out[0] = (f[0] - c5 * out[3]) / c1;
+        }
+        for (int k = 0; k < 6; ++k) A6(v, n, i, k) = out[k];
+    }
+    return v;
+}
+
+// Noise for one RK attempt (mechanics.hpp:2489-2510): uniform on
+// [-max, max] per component, drawn once per stepRungeKuttaAdaptive call.
+// Counter policy: (iter, attempt, cell, pair-of-components).
+inline Arr6 sample_noise(int n, const Params3& p, int iter, int attempt)
+{
+    Arr6 noise((size_t)n * 6, 0.0);
+    if (!(p.max_rxy_noise > 0 || p.max_rz_noise > 0 || p.max_nxy_noise > 0 || p.max_nz_noise > 0))
+        return noise;
+    uint32_t k0, k1;
+    rng_key(p.rng_seed, RNG_PURPOSE_NOISE, k0, k1);
+    const double mx[6] = {p.max_rxy_noise, p.max_rxy_noise, p.max_rz_noise,
+                          p.max_nxy_noise, p.max_nxy_noise, p.max_nz_noise};
+    for (int i = 0; i < n; ++i)
+    {
+        for (int c = 0; c < 3; ++c)
+        {
+            Philox4 x = philox4x32_10((uint32_t)iter, (uint32_t)attempt, (uint32_t)i, (uint32_t)c, k0, k1);
+            double u0 = philox_u01(x.v[0], x.v[1]), u1 = philox_u01(x.v[2], x.v[3]);
+            A6(noise, n, i, 2 * c) = -mx[2 * c] + 2 * mx[2 * c] * u0;
+            A6(noise, n, i, 2 * c + 1) = -mx[2 * c + 1] + 2 * mx[2 * c + 1] * u1;
+        }
+    }
+    return noise;
+}
+
+// mechanics.hpp:2406-2612 (stepRungeKuttaAdaptive).  Returns the new cell
+// array; `errors` receives the n x 6 embedded error estimate.  Pair forces are
+// taken from the neighbor table, which this function never refreshes, so they
+// are the same in every stage (include_constraint = false); `cc_once` computes
+// them once instead of per stage, which changes no arithmetic.
+inline Cells step_rk_adaptive(const Tableau& tab, const Cells& cells, const Neighbors& nb,
+                              double dt, const Params3& p, int iter, int attempt, Arr6& errors,
+                              bool cc_once = false)
+{
+    const int n = cells.n;
+    std::vector<int> assume_2d(n);
+    for (int i = 0; i < n; ++i) assume_2d[i] = (cells(i, C_NZ) < p.nz_threshold);
+    Arr6 noise = sample_noise(n, p, iter, attempt);
+    const int s = tab.s;
+    const bool multithread = (n >= p.n_start_multithread);
+    Arr6 cc;
+    const Arr6* ccp = nullptr;
+    if (cc_once) { cc = cell_cell_forces(cells, nb, p); ccp = &cc; }
+    std::vector<Arr6> vel;
+    vel.push_back(get_velocities(cells, nb, p, assume_2d, noise, multithread, ccp));
+    for (int i = 1; i < s; ++i)
+    {
+        Arr6 mult((size_t)n * 6, 0.0);
+        for (int j = 0; j < i; ++j)
+            for (size_t k = 0; k < mult.size(); ++k) mult[k] += vel[j][k] * tab.a(i, j);
+        Cells ci(cells);
+        for (int c = 0; c < 6; ++c)
+            for (int r = 0; r < n; ++r) ci(r, C_RX + c) += A6(mult, n, r, c) * dt;
+        normalize_orientations(ci);
+        vel.push_back(get_velocities(ci, nb, p, assume_2d, noise, multithread, ccp));
+    }
+    Cells cn(cells);
+    Arr6 vf1((size_t)n * 6, 0.0), vf2((size_t)n * 6, 0.0);
+    for (int i = 0; i < s; ++i)
+        for (size_t k = 0; k < vf1.size(); ++k) { vf1[k] += vel[i][k] * tab.b[i]; vf2[k] += vel[i][k] * tab.bs[i]; }
+    errors.assign((size_t)n * 6, 0.0);
+    for (int c = 0; c < 6; ++c)
+        for (int r = 0; r < n; ++r)
+        {
+            double d1 = A6(vf1, n, r, c) * dt, d2 = A6(vf2, n, r, c) * dt;
+            cn(r, C_RX + c) += d1;
+            A6(errors, n, r, c) = d1 - d2;
+        }
+    for (int c = 0; c < 6; ++c)
+        for (int r = 0; r < n; ++r) cn(r, C_DRX + c) = A6(vf1, n, r, c);
+    normalize_orientations(cn);
+    return cn;
+}
+
+// simulation.hpp:1697-1705: max over cells/components of err / (tol (1 + |y0|)),
+// floored at min_error (signed errors, as in the reference)
+inline double max_scaled_error(const Cells& cells, const Arr6& errors, double tol, double min_error)
+{
+    const int n = cells.n;
+    double mx = -std::numeric_limits<double>::infinity();
+    for (int c = 0; c < 6; ++c)
+        for (int r = 0; r < n; ++r)
+        {
+            double z = 1.0 + std::fabs(cells(r, C_RX + c));
+            double v = A6c(errors, n, r, c) / (tol * z);
+            if (v > mx) mx = v;
+        }
+    return std::max(mx, min_error);
+}
+
+// growth.hpp:51-57 (growCells)
+inline void grow_cells(Cells& cells, double dt, double R)
+{
+    for (int i = 0; i < cells.n; ++i)
+    {
+        cells(i, C_L) += cells(i, C_GROWTH) * (4 * R / 3 + cells(i, C_L)) * dt;
+        cells(i, C_HALF_L) = cells(i, C_L) / 2;
+    }
+}
+
+// growth.hpp:82-117 (minDistToCell)
+inline double min_dist_to_cell(const Cells& cells, int i)
+{
+    double mindist = std::numeric_limits<double>::infinity();
+    for (int j = 0; j < cells.n; ++j)
+    {
+        if (i == j) continue;
+        double d = norm(dist_cells(cells, i, j).d);
+        if (d < mindist) mindist = d;
+    }
+    return mindist;
+}
+
+// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms
+inline double standard_normal(double u, double v)
+{
+    double c = std::sqrt(-2 * std::log(u));
+    return c * std::cos(TWO_PI * v);
+}
+
+// utils.hpp:791-801 (rotateXY)
+inline V3 rotate_xy(V3 n, double theta)
+{
+    double st = std::sin(theta), ct = std::cos(theta);
+    return v3(ct * n.x + (-st) * n.y + 0 * n.z, st * n.x + ct * n.y + 0 * n.z, (0 * n.x + 0 * n.y) + 1 * n.z);
+}
+
+// utils.hpp:814-829 (rotateOutOfXY)
+inline V3 rotate_out_of_xy(V3 n, double theta)
+{
+    V3 v = v3(n.y * 1 - n.z * 0, n.z * 0 - n.x * 1, n.x * 0 - n.y * 0);   // n x z
+    double nv = norm(v);
+    v = v3(v.x / nv, v.y / nv, v.z / nv);
+    double st = std::sin(theta), ct = std::cos(theta);
+    V3 w = v3(v.y * n.z - v.z * n.y, v.z * n.x - v.x * n.z, v.x * n.y - v.y * n.x);   // v x n
+    return v3(n.x * ct + w.x * st, n.y * ct + w.y * st, n.z * ct + w.z * st);
+}
+
+// Draw slots of one division try (policy): 0-3 angles, 4-5 length fraction,
+// 6-7 mother growth rate, 8-9 daughter growth rate.
+inline double div_uniform(const Params3& p, int iter, int k, int tr, int slot)
+{
+    return rng_uniform(p.rng_seed, RNG_PURPOSE_DIVIDE, (uint32_t)iter, (uint32_t)k,
+                       (uint32_t)tr, (uint32_t)slot);
+}
+
+// growth.hpp:166-426 (divideCells, one group).  Mothers keep their row
+// (daughter 1); daughter 2 rows are appended in ascending mother order; IDs are
+// max_id + 2k + 1 and max_id + 2k + 2.  `ntries_out` is the number of tries.
+inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double t, const Params3& p,
+                          const std::vector<int>& to_divide, int iter, int* ntries_out = nullptr)
+{
+    int n_divide = 0;
+    for (int v : to_divide) n_divide += v;
+    if (ntries_out) *ntries_out = 0;
+    if (n_divide == 0) return cells;
+    const int n = cells.n;
+    const double R = p.R;
+    std::vector<int> idx_divide;
+    for (int i = 0; i < n; ++i) if (to_divide[i]) idx_divide.push_back(i);
+    Cells total(n + n_divide, cells.ncols);
+    std::vector<int> check_distance(n_divide, 1);
+    const double mindist_default = 2 * p.Rcell;
+    for (int m = 0; m < n_divide; ++m)
+        if (min_dist_to_cell(cells, idx_divide[m]) < mindist_default) check_distance[m] = 0;
+    std::vector<int> satisfies(n_divide, 0);
+    for (int m = 0; m < n_divide; ++m) if (check_distance[m] == 0) satisfies[m] = 1;
+    int ntries = 0;
+    const int ntries_total = 10;
+    auto sum = [](const std::vector<int>& v) { int s = 0; for (int x : v) s += x; return s; };
+    while (ntries == 0 || (ntries < ntries_total && sum(satisfies) < n_divide))
+    {
+        for (int c = 0; c < cells.ncols; ++c)
+            for (int r = 0; r < n; ++r) total(r, c) = cells(r, c);
+        Cells nc(n_divide, cells.ncols);
+        for (int m = 0; m < n_divide; ++m)
+            for (int c = 0; c < cells.ncols; ++c) nc(m, c) = cells(idx_divide[m], c);
+        std::vector<double> txy1(n_divide, 0), tz1(n_divide, 0), txy2(n_divide, 0), tz2(n_divide, 0);
+        for (int m = 0; m < n_divide; ++m)
+        {
+            if (ntries < ntries_total - 1 && check_distance[m] == 1)
+            {
+                double bxy = p.daughter_angle_xy_bound, bz = p.daughter_angle_z_bound;
+                txy1[m] = -bxy + 2 * bxy * div_uniform(p, iter, m, ntries, 0);
+                tz1[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 1);
+                txy2[m] = -bxy + 2 * bxy * div_uniform(p, iter, m, ntries, 2);
+                tz2[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 3);
+            }
+        }
+        for (int m = 0; m < n_divide; ++m)
+        {
+            V3 u = cell_n(nc, m);
+            V3 a1 = rotate_out_of_xy(rotate_xy(u, txy1[m]), tz1[m]);
+            V3 a2 = rotate_out_of_xy(rotate_xy(u, txy2[m]), tz2[m]);
+            int im = idx_divide[m];
+            total(im, C_NX) = a1.x; total(im, C_NY) = a1.y; total(im, C_NZ) = a1.z;
+            nc(m, C_NX) = a2.x; nc(m, C_NY) = a2.y; nc(m, C_NZ) = a2.z;
+        }
+        for (int m = 0; m < n_divide; ++m)
+        {
+            double r = 0.5 + p.daughter_length_std *
+                standard_normal(div_uniform(p, iter, m, ntries, 4), div_uniform(p, iter, m, ntries, 5));
+            double M = (r < 0) ? 0.0 : (r > 1 ? 1.0 : r);
+            int im = idx_divide[m];
+            double Ld = total(im, C_L) - 2 * R;
+            double L1 = M * Ld, L2 = (1 - M) * Ld;
+            double div = -total(im, C_HALF_L) + L1 + R;
+            double delta1 = L1 / 2 + R, delta2 = L2 / 2 + R;
+            total(im, C_L) = L1; total(im, C_HALF_L) = L1 / 2;
+            nc(m, C_L) = L2; nc(m, C_HALF_L) = L2 / 2;
+            for (int c = 0; c < 3; ++c)
+            {
+                total(im, C_RX + c) = total(im, C_RX + c) + (div - delta1) * total(im, C_NX + c);
+                nc(m, C_RX + c) = nc(m, C_RX + c) + (div + delta2) * nc(m, C_NX + c);
+            }
+            total(im, C_T0) = t; nc(m, C_T0) = t;
+        }
+        for (int m = 0; m < n_divide; ++m)
+            total(idx_divide[m], C_GROWTH) = p.growth_mean + p.growth_std *
+                standard_normal(div_uniform(p, iter, m, ntries, 6), div_uniform(p, iter, m, ntries, 7));
+        for (int m = 0; m < n_divide; ++m)
+            nc(m, C_GROWTH) = p.growth_mean + p.growth_std *
+                standard_normal(div_uniform(p, iter, m, ntries, 8), div_uniform(p, iter, m, ntries, 9));
+        for (int m = 0; m < n_divide; ++m)
+            for (int c = 0; c < cells.ncols; ++c) total(n + m, c) = nc(m, c);
+        std::vector<double> md1(n_divide, 0), md2(n_divide, 0);
+        for (int m = 0; m < n_divide; ++m)
+            if (check_distance[m] == 1) md1[m] = min_dist_to_cell(total, idx_divide[m]);
+        for (int m = 0; m < n_divide; ++m)
+            if (check_distance[m] == 1) md2[m] = min_dist_to_cell(total, n + m);
+        for (int m = 0; m < n_divide; ++m)
+            if (check_distance[m] == 1 && md1[m] >= mindist_default && md2[m] >= mindist_default)
+                satisfies[m] = 1;
+        ntries++;
+    }
+    if (ntries_out) *ntries_out = ntries;
+    int max_id = (int)parents.size() - 1;
+    for (int m = 0; m < n_divide; ++m)
+    {
+        int id1 = max_id + (2 * m + 1), id2 = max_id + (2 * m + 2);
+        int parent_id = (int)total(idx_divide[m], C_ID);
+        total(idx_divide[m], C_ID) = id1;
+        total(n + m, C_ID) = id2;
+        parents.push_back(parent_id);
+        parents.push_back(parent_id);
+    }
+    return total;
+}
+
+// ------------------------------------------------------------------------
+// Simulation loop body (simulation.hpp:1617-1864, switching, writing,
+// basal_only and pole tracking excluded)
+// ------------------------------------------------------------------------
+struct LoopState {
+    Cells cells;
+    Neighbors nb;
+    std::vector<int> parents;
+    double t = 0, dt = 0;
+    int iter = 0;
+    // statistics
+    long long attempts = 0, rebuilds = 0, divisions = 0;
+    double last_max_error = 0;
+};
+
+inline void loop_init(LoopState& st, const Params3& p)
+{
+    st.dt = p.max_stepsize;                      // simulation.hpp:1167
+    st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);   // :1277
+    st.rebuilds = 1;
+}
+
+// One iteration of `while (!terminate)`; `cc_once` evaluates the stage-
+// invariant pair forces once per attempt instead of once per stage.
+inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false)
+{
+    const Tableau tab = make_tableau(p.integration_mode);
+    std::vector<int> to_divide(st.cells.n);
+    int ndiv = 0;
+    for (int i = 0; i < st.cells.n; ++i) { to_divide[i] = st.cells(i, C_L) > p.Ldiv; ndiv += to_divide[i]; }
+    st.cells = divide_cells(st.cells, st.parents, st.t, p, to_divide, st.iter);
+    if (ndiv > 0)
+    {
+        st.divisions += ndiv;
+        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.rebuilds++;
+    }
+    const int n = st.cells.n;
+    Arr6 errors;
+    int attempt = 0;
+    Cells cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
+    st.attempts++;
+    double max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+    if (st.iter % p.iter_update_stepsize == 0)
+    {
+        bool exceeded = (max_error > 1.0);
+        double q1 = 1.0 / (tab.error_order + 1);
+        double factor = 0.9 * std::pow(1.0 / max_error, q1);
+        if (factor >= 10) factor = 10;
+        else if (factor < 0.2) factor = 0.2;
+        int j = 0;
+        while (exceeded && j < p.max_tries_update_stepsize)
+        {
+            double dt_new = st.dt * factor;
+            cn = step_rk_adaptive(tab, st.cells, st.nb, dt_new, p, st.iter, attempt++, errors, cc_once);
+            st.attempts++;
+            max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+            exceeded = (max_error > 1.0);
+            factor *= 0.9 * std::pow(1.0 / max_error, q1);
+            if (factor >= 10) { factor = 10; break; }
+            else if (factor < 0.2) { factor = 0.2; break; }
+            j++;
+        }
+        if (st.dt * factor < p.min_stepsize) factor = p.min_stepsize / st.dt;
+        else if (st.dt * factor > p.max_stepsize) factor = p.max_stepsize / st.dt;
+        st.dt *= factor;
+        cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
+        st.attempts++;
+        max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+    }
+    st.last_max_error = max_error;
+    (void)n;
+    st.cells = cn;
+    grow_cells(st.cells, st.dt, p.R);
+    update_neighbor_distances(st.cells, st.nb);
+    st.t += st.dt;
+    st.iter++;
+    if (st.iter % p.iter_update_neighbors == 0)
+    {
+        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.rebuilds++;
+    }
+}
+
+}   // namespace oracle

@@ -1,0 +1,230 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle_abm.so) for the tests.
+
+The oracle is test infrastructure: a C++ restatement of the reference's 3-D
+mechanics step (see oracle/abm3d.hpp).  It is only used here as the checker.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "liboracle_abm.so")
+
+
+def build_oracle():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("R", ctypes.c_double), ("Rcell", ctypes.c_double), ("E0", ctypes.c_double),
+        ("Ecell", ctypes.c_double), ("L0", ctypes.c_double), ("Ldiv", ctypes.c_double),
+        ("neighbor_threshold", ctypes.c_double), ("nz_threshold", ctypes.c_double),
+        ("adhesion_mode", ctypes.c_int), ("integration_mode", ctypes.c_int),
+        ("max_stepsize", ctypes.c_double), ("min_stepsize", ctypes.c_double),
+        ("max_error_allowed", ctypes.c_double), ("min_error", ctypes.c_double),
+        ("max_tries_update_stepsize", ctypes.c_int), ("iter_update_stepsize", ctypes.c_int),
+        ("iter_update_neighbors", ctypes.c_int),
+        ("max_rxy_noise", ctypes.c_double), ("max_rz_noise", ctypes.c_double),
+        ("max_nxy_noise", ctypes.c_double), ("max_nz_noise", ctypes.c_double),
+        ("cell_surface_coulomb_coeff", ctypes.c_double), ("no_surface", ctypes.c_int),
+        ("growth_mean", ctypes.c_double), ("growth_std", ctypes.c_double),
+        ("daughter_length_std", ctypes.c_double), ("daughter_angle_xy_bound", ctypes.c_double),
+        ("daughter_angle_z_bound", ctypes.c_double), ("rng_seed", ctypes.c_ulonglong),
+        ("n_start_multithread", ctypes.c_int), ("n_threads", ctypes.c_int),
+    ]
+
+
+def _load():
+    if not os.path.exists(ORACLE_LIB):
+        build_oracle()
+    lib = ctypes.CDLL(ORACLE_LIB)
+    P = ctypes.POINTER
+    d, i, vp, dp, ip = ctypes.c_double, ctypes.c_int, ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int)
+    sig = {
+        "oracle_create": ([P(OracleParams), P(vp)], i),
+        "oracle_destroy": ([vp], None),
+        "oracle_last_error": ([], ctypes.c_char_p),
+        "oracle_max_threads": ([], i),
+        "oracle_set_jkr_table": ([vp, dp, dp, i], i),
+        "oracle_jkr_table": ([d, d, d, d, i, dp, dp], i),
+        "oracle_jkr_contact_radius": ([d, d, d, d], d),
+        "oracle_set_cells": ([vp, dp, i, i, i], i),
+        "oracle_get_num_cells": ([vp], i),
+        "oracle_get_cells": ([vp, dp, i], i),
+        "oracle_set_parents": ([vp, ip, i], i),
+        "oracle_get_parents": ([vp, ip, i], i),
+        "oracle_set_clock": ([vp, d, d, i], None),
+        "oracle_get_clock": ([vp, dp, dp, ip], None),
+        "oracle_build_neighbors": ([vp], i),
+        "oracle_num_neighbors": ([vp], i),
+        "oracle_get_neighbors": ([vp, dp, i], i),
+        "oracle_set_neighbors": ([vp, dp, i, i], i),
+        "oracle_update_neighbor_distances": ([vp], i),
+        "oracle_dist_between_cells": ([dp, dp, d, dp, dp, d, dp], None),
+        "oracle_nearest_body_coord": ([dp, dp, d, dp], d),
+        "oracle_cell_cell_forces": ([vp, dp], i),
+        "oracle_conservative_forces": ([vp, dp], i),
+        "oracle_get_velocities": ([vp, dp], i),
+        "oracle_rk_attempt": ([vp, d, i, i, dp, dp, dp], i),
+        "oracle_loop_init": ([vp], i),
+        "oracle_iterate": ([vp, i, i, i], i),
+        "oracle_get_stats": ([vp, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_longlong), dp], None),
+        "oracle_grow": ([vp, d], i),
+        "oracle_divide": ([vp, d, i], i),
+        "oracle_min_dist_to_cell": ([vp, i], d),
+        "oracle_rng_uniform": ([ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                                ctypes.c_uint, ctypes.c_uint], d),
+        "oracle_area_integrals": ([d, d, d, d, dp], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+LIB = _load()
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def dist_between_cells(r1, n1, h1, r2, n2, h2):
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (r1, n1, r2, n2)]
+    out = np.zeros(5)
+    LIB.oracle_dist_between_cells(_dp(a[0]), _dp(a[1]), h1, _dp(a[2]), _dp(a[3]), h2, _dp(out))
+    return out[:3], out[3], out[4]
+
+
+def nearest_body_coord(r, n, h, q):
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (r, n, q)]
+    return LIB.oracle_nearest_body_coord(_dp(a[0]), _dp(a[1]), h, _dp(a[2]))
+
+
+def jkr_table(R, Rcell, E0, gamma, n_mesh=100):
+    d, r = np.zeros(n_mesh), np.zeros(n_mesh)
+    LIB.oracle_jkr_table(R, Rcell, E0, gamma, n_mesh, _dp(d), _dp(r))
+    return d, r
+
+
+class Oracle:
+    """The oracle's loop state; parameters use the same names as abm_b200.DEFAULTS."""
+
+    def __init__(self, pdict, jkr=None, n_threads=0, n_start_multithread=50):
+        p = OracleParams()
+        for name, _ in OracleParams._fields_:
+            if name in pdict:
+                setattr(p, name, pdict[name])
+        p.n_start_multithread = n_start_multithread
+        p.n_threads = n_threads
+        self.pdict = dict(pdict)
+        self._c = ctypes.c_void_p()
+        LIB.oracle_create(ctypes.byref(p), ctypes.byref(self._c))
+        if jkr is not None:
+            self.set_jkr_table(*jkr)
+        self.ncols = None
+
+    def __del__(self):
+        if getattr(self, "_c", None):
+            LIB.oracle_destroy(self._c)
+            self._c = None
+
+    def set_jkr_table(self, delta, radius):
+        d = np.ascontiguousarray(delta, dtype=np.float64)
+        r = np.ascontiguousarray(radius, dtype=np.float64)
+        LIB.oracle_set_jkr_table(self._c, _dp(d), _dp(r), len(d))
+
+    def set_cells(self, cells):
+        a = np.asfortranarray(cells, dtype=np.float64)
+        LIB.oracle_set_cells(self._c, _dp(a), a.shape[0], a.shape[1], a.shape[0])
+        self.ncols = a.shape[1]
+
+    def cells(self):
+        n = LIB.oracle_get_num_cells(self._c)
+        out = np.zeros((n, self.ncols), order="F")
+        LIB.oracle_get_cells(self._c, _dp(out), max(n, 1))
+        return out
+
+    def set_clock(self, t, dt, iteration):
+        LIB.oracle_set_clock(self._c, t, dt, iteration)
+
+    def clock(self):
+        t, dt, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        LIB.oracle_get_clock(self._c, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it))
+        return t.value, dt.value, it.value
+
+    def set_parents(self, parents):
+        a = np.ascontiguousarray(parents, dtype=np.int32)
+        LIB.oracle_set_parents(self._c, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a))
+
+    def parents(self):
+        n = LIB.oracle_get_parents(self._c, None, 0)
+        a = np.zeros(n, dtype=np.int32)
+        LIB.oracle_get_parents(self._c, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+        return a
+
+    def build_neighbors(self):
+        return LIB.oracle_build_neighbors(self._c)
+
+    def neighbors(self):
+        m = LIB.oracle_num_neighbors(self._c)
+        out = np.zeros((m, 7), order="F")
+        LIB.oracle_get_neighbors(self._c, _dp(out), max(m, 1))
+        return out
+
+    def set_neighbors(self, rows):
+        a = np.asfortranarray(rows, dtype=np.float64)
+        LIB.oracle_set_neighbors(self._c, _dp(a), a.shape[0], max(a.shape[0], 1))
+
+    def update_neighbor_distances(self):
+        LIB.oracle_update_neighbor_distances(self._c)
+
+    def _n6(self, fn):
+        n = LIB.oracle_get_num_cells(self._c)
+        out = np.zeros((n, 6), order="F")
+        fn(self._c, _dp(out))
+        return out
+
+    def cell_cell_forces(self):
+        return self._n6(LIB.oracle_cell_cell_forces)
+
+    def conservative_forces(self):
+        return self._n6(LIB.oracle_conservative_forces)
+
+    def get_velocities(self):
+        return self._n6(LIB.oracle_get_velocities)
+
+    def rk_attempt(self, dt, iteration=0, attempt=0):
+        n = LIB.oracle_get_num_cells(self._c)
+        cells = np.zeros((n, self.ncols), order="F")
+        errors = np.zeros((n, 6), order="F")
+        e = ctypes.c_double()
+        LIB.oracle_rk_attempt(self._c, dt, iteration, attempt, _dp(cells), _dp(errors), ctypes.byref(e))
+        return cells, errors, e.value
+
+    def loop_init(self):
+        return LIB.oracle_loop_init(self._c)
+
+    def iterate(self, n_iters, n_cells=0, fast_cc=1):
+        rc = LIB.oracle_iterate(self._c, n_iters, n_cells, fast_cc)
+        if rc:
+            raise RuntimeError(LIB.oracle_last_error().decode())
+
+    def stats(self):
+        a, r, dv = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        e = ctypes.c_double()
+        LIB.oracle_get_stats(self._c, ctypes.byref(a), ctypes.byref(r), ctypes.byref(dv), ctypes.byref(e))
+        return dict(attempts=a.value, rebuilds=r.value, divisions=dv.value, last_max_error=e.value)
+
+    def grow(self, dt):
+        LIB.oracle_grow(self._c, dt)
+
+    def divide(self, t, iteration):
+        return LIB.oracle_divide(self._c, t, iteration)
+
+    def min_dist_to_cell(self, i):
+        return LIB.oracle_min_dist_to_cell(self._c, i)

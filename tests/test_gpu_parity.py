@@ -1,0 +1,224 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bars (stated here and in the design notes):
+  * neighbor pair set and the table's (d, s, t): bit for bit (both sides use
+    correctly rounded arithmetic without FMA for the segment distance);
+  * forces, velocities, RK states and error norms: normwise relative error
+    max|gpu - oracle| / max|oracle| <= 1e-10 per column (FP64 path).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import abm_b200
+from abm_b200 import workloads
+import oracle_ref as orc
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+RTOL = 1e-10
+JKR = orc.jkr_table(0.8, 0.5, 3900.0, 100.0, 100)
+
+
+def colwise_relerr(a, b):
+    """max over columns of max|a - b| / max|b| (0 where the column of b is zero)."""
+    a, b = np.asarray(a), np.asarray(b)
+    scale = np.abs(b).max(axis=0)
+    diff = np.abs(a - b).max(axis=0)
+    return float(np.max(np.where(scale > 0, diff / np.where(scale > 0, scale, 1), diff)))
+
+
+def make_pair(cells, **kw):
+    kw.setdefault("cap_cells", max(len(cells), 1) + 16)
+    sim = abm_b200.Simulation(jkr_table=JKR, **kw)
+    sim.upload_cells(cells)
+    o = orc.Oracle(sim.pdict, jkr=JKR)
+    o.set_cells(cells)
+    return sim, o
+
+
+def patch_state(n, seed, p_contact=0.9):
+    # same density as the 100k / 300 um benchmark disk
+    radius = 300.0 * np.sqrt(n / 100000.0)
+    cells, _ = workloads.biofilm_3d(n=n, seed=seed, disk_radius=radius, p_contact=p_contact)
+    return cells
+
+
+def parallel_bundle(n_side=8, spacing=1.3, jitter=0.0, seed=0):
+    """Cells on a lattice, all along x (exercises the near-parallel branch)."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for a in range(n_side):
+        for b in range(n_side):
+            for c in range(2):
+                n = np.array([1.0, 0.0, 0.0]) + jitter * rng.normal(size=3)
+                n /= np.linalg.norm(n)
+                if n[2] < 0:
+                    n = -n
+                rows.append(([c * 4.2 + 0.3 * (a % 2), a * spacing, 0.8 + b * spacing], n))
+    cells = np.zeros((len(rows), 22), order="F")
+    for k, (r, n) in enumerate(rows):
+        cells[k, 0] = k
+        cells[k, 1:4] = r
+        cells[k, 4:7] = n
+        cells[k, 13], cells[k, 14] = 3.0, 1.5
+        cells[k, 17], cells[k, 18], cells[k, 19], cells[k, 20], cells[k, 21] = 100, 720, 100, 1, 100
+    return cells
+
+
+# ---------------------------------------------------------------------------
+# segment distance: the reference's known-answer cases and the oracle, bit for bit
+# ---------------------------------------------------------------------------
+def test_gpu_distance_golden_cases():
+    with open(os.path.join(GOLDEN, "dist3d_cases.json")) as f:
+        cases = json.load(f)["dist_cases"]
+    for c in cases:
+        # cell 1 of the case is row index 1 so the table's d runs from it to cell 2
+        cells = workloads.two_cell_3d(c["r2"], c["n2"], c["r1"], c["n1"])
+        cells[0, 13], cells[0, 14] = 2 * c["half_l2"], c["half_l2"]
+        cells[1, 13], cells[1, 14] = 2 * c["half_l1"], c["half_l1"]
+        sim, o = make_pair(cells, neighbor_threshold=100.0, Ldiv=20.0)
+        assert sim.get_cell_neighbors() == 1
+        row = sim.neighbors()[0]
+        assert row[0] == 1 and row[1] == 0
+        np.testing.assert_allclose(row[2:5], c["d"], atol=1e-8, rtol=0)
+        assert abs(row[5] - c["s"]) <= 1e-8 and abs(row[6] - c["t"]) <= 1e-8
+        o.build_neighbors()
+        assert np.array_equal(sim.neighbors(), o.neighbors())
+
+
+# ---------------------------------------------------------------------------
+# neighbor set (getCellNeighbors): identical rows, bit for bit
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("state", ["patch1", "patch2", "patch_uniform", "bundle", "bundle_jitter"])
+def test_gpu_neighbor_table_bitexact(state):
+    cells = {"patch1": lambda: patch_state(3000, 1), "patch2": lambda: patch_state(5000, 2),
+             "patch_uniform": lambda: patch_state(3000, 3, p_contact=0.0),
+             "bundle": lambda: parallel_bundle(), "bundle_jitter": lambda: parallel_bundle(jitter=0.004)}[state]()
+    sim, o = make_pair(cells)
+    m = sim.get_cell_neighbors()
+    mo = o.build_neighbors()
+    assert m == mo and m > 0
+    g, r = sim.neighbors(), o.neighbors()
+    assert np.array_equal(g, r)
+
+
+def test_gpu_neighbor_edge_sizes():
+    for n in (1, 2, 3, 64):
+        cells = patch_state(max(n, 2), 7)[:n]
+        sim, o = make_pair(cells)
+        m = sim.get_cell_neighbors()
+        assert m == o.build_neighbors()
+        assert np.array_equal(sim.neighbors(), o.neighbors())
+
+
+def test_gpu_neighbor_overflow_is_reported():
+    cells = parallel_bundle(n_side=8, spacing=1.2)
+    sim = abm_b200.Simulation(jkr_table=JKR, cap_cells=len(cells), cap_neighbors_per_cell=4)
+    sim.upload_cells(cells)
+    with pytest.raises(RuntimeError, match="ABM_ERR_CAPACITY"):
+        sim.get_cell_neighbors()
+
+
+# ---------------------------------------------------------------------------
+# forces, velocities, one RK attempt
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("adhesion", [1, 0])
+def test_gpu_cell_cell_forces(adhesion):
+    cells = patch_state(4000, 11)
+    sim, o = make_pair(cells, adhesion_mode=adhesion)
+    sim.get_cell_neighbors()
+    o.build_neighbors()
+    err = colwise_relerr(sim.cell_cell_forces(), o.cell_cell_forces())
+    assert err <= RTOL, err
+
+
+def test_gpu_velocities():
+    cells = patch_state(4000, 12)
+    sim, o = make_pair(cells)
+    sim.get_cell_neighbors()
+    o.build_neighbors()
+    err = colwise_relerr(sim.get_velocities(), o.get_velocities())
+    assert err <= RTOL, err
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+def test_gpu_rk_attempt(mode):
+    cells = patch_state(3000, 13)
+    sim, o = make_pair(cells, integration_mode=mode)
+    sim.get_cell_neighbors()
+    o.build_neighbors()
+    for dt in (1e-6, 1e-4):
+        cg, eg, mg = sim.step_runge_kutta_adaptive(dt)
+        co, eo, mo = o.rk_attempt(dt)
+        assert colwise_relerr(cg, co) <= RTOL
+        assert colwise_relerr(eg, eo) <= 1e-8       # an O(dt^q) difference of two sums
+        assert abs(mg - mo) <= 1e-8 * max(mo, 1e-30)
+
+
+def test_gpu_rk_attempt_with_noise():
+    cells = patch_state(2000, 14)
+    kw = dict(max_rxy_noise=50.0, max_rz_noise=20.0, max_nxy_noise=5.0, max_nz_noise=2.0)
+    sim, o = make_pair(cells, **kw)
+    sim.get_cell_neighbors()
+    o.build_neighbors()
+    cg, eg, mg = sim.step_runge_kutta_adaptive(1e-5, attempt=3)
+    co, eo, mo = o.rk_attempt(1e-5, 0, 3)
+    assert colwise_relerr(cg, co) <= RTOL
+
+
+# ---------------------------------------------------------------------------
+# the loop body (divide-free): controller, growth, rebuild cadence
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_gpu_iterations_match_oracle(graphs):
+    cells = patch_state(2000, 21)
+    sim, o = make_pair(cells, use_graphs=graphs, iter_update_neighbors=10, max_stepsize=1e-4)
+    sim.get_cell_neighbors()
+    o.loop_init()
+    for _ in range(3):
+        s = sim.iterate(12)
+        o.iterate(12)
+        t, dt, it = sim.clock()
+        to, dto, ito = o.clock()
+        assert it == ito
+        assert abs(t - to) <= 1e-10 * to and abs(dt - dto) <= 1e-10 * dto
+        assert colwise_relerr(sim.download_cells(), o.cells()) <= 1e-9
+        assert s["attempts"] == o.stats()["attempts"]
+        assert np.array_equal(sim.neighbors()[:, :2], o.neighbors()[:, :2])
+
+
+def test_gpu_iterations_with_growth_no_division():
+    cells = patch_state(1500, 22)
+    cells[:, 16] = 0.5                      # growth rate; lengths stay below Ldiv
+    cells[:, 13] = np.minimum(cells[:, 13], 4.0)
+    cells[:, 14] = cells[:, 13] / 2
+    sim, o = make_pair(cells, iter_update_neighbors=5, max_stepsize=1e-4)
+    sim.get_cell_neighbors()
+    o.loop_init()
+    sim.iterate(20)
+    o.iterate(20)
+    assert colwise_relerr(sim.download_cells(), o.cells()) <= 1e-9
+
+
+# ---------------------------------------------------------------------------
+# full size (100k cells): pair set bit for bit, forces normwise
+# ---------------------------------------------------------------------------
+def test_gpu_full_size_neighbor_set_and_forces():
+    cells, _ = workloads.biofilm_3d(n=100000, seed=1, p_contact=0.9)
+    sim, o = make_pair(cells)
+    m = sim.get_cell_neighbors()
+    assert m == o.build_neighbors()
+    g = sim.neighbors()
+    assert np.array_equal(g, o.neighbors())
+    err = colwise_relerr(sim.cell_cell_forces(), o.cell_cell_forces())
+    assert err <= RTOL, err
+    cg, eg, mg = sim.step_runge_kutta_adaptive(1e-6)
+    co, eo, mo = o.rk_attempt(1e-6)
+    assert colwise_relerr(cg, co) <= RTOL
+    # Newton's third law: translational pair forces sum to zero
+    f = sim.cell_cell_forces()
+    assert np.abs(f[:, :3].sum(0)).max() <= 1e-9 * np.abs(f[:, :3]).sum()

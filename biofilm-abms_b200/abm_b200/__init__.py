@@ -141,6 +141,7 @@ def _load():
         "abm_rk_attempt": ([vp, d, i, dp, dp, dp], i),
         "abm_grow": ([vp, d], i),
         "abm_divide": ([vp, ip], i),
+        "abm_last_division_tries": ([vp, ip], i),
         "abm_iterate": ([vp, i, i, P(AbmStats)], i),
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
@@ -158,7 +159,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
-            "abm_iterate abm_get_stats abm_profile_iterations").split()
+            "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries").split()
 
 
 def _dptr(a):
@@ -334,6 +335,20 @@ class Simulation:
 
     def grow_cells(self, dt):
         self._check(LIB.abm_grow(self._ctx, dt), "abm_grow")
+
+    def divide_cells(self):
+        """divideMaxLength + divideCells (growth.hpp:66-71, 166-426) at the current clock.
+
+        Returns the number of mothers; the neighbor set must be rebuilt afterwards,
+        as the reference loop does."""
+        nd = ctypes.c_int()
+        self._check(LIB.abm_divide(self._ctx, ctypes.byref(nd)), "abm_divide")
+        return nd.value
+
+    def last_division_tries(self):
+        t = ctypes.c_int()
+        self._check(LIB.abm_last_division_tries(self._ctx, ctypes.byref(t)), "abm_last_division_tries")
+        return t.value
 
     def iterate(self, n_iters, n_cells_stop=0, stats=True):
         s = AbmStats()

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <functional>
 #include "abm_kernels.cuh"
 #include "../../include/abm_capi.h"
 
@@ -29,7 +30,7 @@ struct abm_ctx {
     int host_iter = 0;
     // device state
     Geom* geom = nullptr; Vel* vel = nullptr; Phys* phys = nullptr; Gen6* fcc = nullptr;
-    Geom* geom_c = nullptr; Vel* vel_c = nullptr; Gen6* gen_tmp = nullptr;
+    Geom* geom_c = nullptr; Vel* vel_c = nullptr; Gen6* gen_tmp = nullptr; Gen6* k0buf = nullptr;
     Ctrl* ctrl = nullptr; Grid* grid = nullptr;
     unsigned long long* bbox_acc = nullptr; unsigned int* bbox_counter = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *key = nullptr, *slot = nullptr, *sorted_cell = nullptr;
@@ -39,7 +40,14 @@ struct abm_ctx {
     double *jkr_delta = nullptr, *jkr_radius = nullptr;
     int jkr_n = 0;
     double* staging = nullptr;   // cap x (ncols max 32) doubles
-    std::vector<int> parents;
+    // division
+    DivideParams dp;
+    bool div_enabled = false;
+    int cap_parents = 0;
+    int *div_flags = nullptr, *div_rank = nullptr, *mothers = nullptr, *div_check = nullptr, *div_sat = nullptr;
+    int *div_ok = nullptr, *parents_dev = nullptr;
+    Geom *d1 = nullptr, *d2 = nullptr;
+    double *dlen = nullptr, *dgrowth = nullptr;
     // parameters
     ForceParams fp; StepParams sp; BuildParams bp;
     // graphs
@@ -107,10 +115,12 @@ static void free_all(abm_ctx* c)
 {
     if (c->g_iter) cudaGraphExecDestroy(c->g_iter);
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
-    void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->ctrl, c->grid,
+    void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col,
-                    c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging};
+                    c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
+                    c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
+                    c->dgrowth};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -216,6 +226,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     CK(cudaMalloc(&c->geom_c, cap * sizeof(Geom)));
     CK(cudaMalloc(&c->vel_c, cap * sizeof(Vel)));
     CK(cudaMalloc(&c->gen_tmp, cap * sizeof(Gen6)));
+    CK(cudaMalloc(&c->k0buf, cap * sizeof(Gen6)));
     CK(cudaMalloc(&c->ctrl, sizeof(Ctrl)));
     CK(cudaMalloc(&c->grid, sizeof(Grid)));
     CK(cudaMalloc(&c->bbox_acc, 8 * sizeof(unsigned long long)));
@@ -233,6 +244,18 @@ int abm_create(const abm_params* q, abm_ctx** out)
     size_t ns = std::max(scan_block_sums_size((int)cap + 1), scan_block_sums_size(c->cap_bins + 1)) + 1;
     CK(cudaMalloc(&c->scan_sums, ns * sizeof(int)));
     CK(cudaMalloc(&c->staging, cap * STAGING_COLS * sizeof(double)));
+    CK(cudaMalloc(&c->div_flags, cap * sizeof(int)));
+    CK(cudaMalloc(&c->div_rank, (cap + 1) * sizeof(int)));
+    CK(cudaMalloc(&c->mothers, cap * sizeof(int)));
+    CK(cudaMalloc(&c->div_check, cap * sizeof(int)));
+    CK(cudaMalloc(&c->div_sat, cap * sizeof(int)));
+    CK(cudaMalloc(&c->div_ok, 2 * cap * sizeof(int)));
+    CK(cudaMalloc(&c->d1, cap * sizeof(Geom)));
+    CK(cudaMalloc(&c->d2, cap * sizeof(Geom)));
+    CK(cudaMalloc(&c->dlen, 2 * cap * sizeof(double)));
+    CK(cudaMalloc(&c->dgrowth, 2 * cap * sizeof(double)));
+    c->cap_parents = 2 * (int)cap + 1024;
+    CK(cudaMalloc(&c->parents_dev, (size_t)c->cap_parents * sizeof(int)));
     CK(cudaMemset(c->row_ptr, 0, (cap + 1) * sizeof(int)));
     Ctrl h;
     memset(&h, 0, sizeof(h));
@@ -267,9 +290,14 @@ int abm_create(const abm_params* q, abm_ctx** out)
     c->bp.threshold = p.neighbor_threshold;
     c->bp.prefilter = p.neighbor_threshold + p.Ldiv + 2 * p.R;
     c->bp.cap_per_cell = c->cap_nbr;
+    DivideParams& dp = c->dp;
+    dp.R = p.R; dp.Rcell = p.Rcell; dp.Ldiv = p.Ldiv;
+    dp.growth_mean = p.growth_mean; dp.growth_std = p.growth_std;
+    dp.daughter_length_std = p.daughter_length_std;
+    dp.angle_xy_bound = p.daughter_angle_xy_bound; dp.angle_z_bound = p.daughter_angle_z_bound;
+    dp.seed = p.rng_seed; dp.cap_cells = c->cap;
     if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
         return fail(c, ABM_ERR_ARG, "adhesion_mode must be 0 (none) or 1 (isotropic JKR, fixed gamma)");
-    c->parents.clear();
     return ABM_OK;
 }
 
@@ -345,6 +373,12 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     if (c->n_host != n) c->nbrs_valid = false;
     c->n_host = n;
     c->cells_loaded = true;
+    // division is possible when a cell already exceeds Ldiv or any cell can grow
+    bool grows = (c->p.growth_mean != 0 || c->p.growth_std != 0);
+    for (int i = 0; i < n && !grows; ++i)
+        grows = cm[(size_t)16 * ld + i] != 0 || cm[(size_t)13 * ld + i] > c->p.Ldiv;
+    if (grows != c->div_enabled && c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+    c->div_enabled = grows;
     return ABM_OK;
 }
 
@@ -399,19 +433,27 @@ int abm_get_clock(abm_ctx* c, double* t, double* dt, int* iter)
     return ABM_OK;
 }
 
+__global__ void k_set_n_parents(Ctrl* c, int n) { c->n_parents = n; }
+
 int abm_set_parents(abm_ctx* c, const int* parents, int n)
 {
     if (!c || (n > 0 && !parents) || n < 0) return ABM_ERR_ARG;
-    c->parents.assign(parents, parents + n);
+    if (n > c->cap_parents - 2 * c->cap) return fail(c, ABM_ERR_CAPACITY, "lineage longer than capacity");
+    if (n > 0) CK(cudaMemcpyAsync(c->parents_dev, parents, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    k_set_n_parents<<<1, 1, 0, c->st>>>(c->ctrl, n);
+    CK(cudaStreamSynchronize(c->st));
     return ABM_OK;
 }
 
 int abm_get_parents(abm_ctx* c, int* out, int cap, int* n)
 {
     if (!c) return ABM_ERR_ARG;
-    int m = (int)c->parents.size();
-    if (n) *n = m;
-    if (out) for (int i = 0; i < m && i < cap; ++i) out[i] = c->parents[i];
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (n) *n = h.n_parents;
+    if (out && h.n_parents > 0)
+        CK(cudaMemcpy(out, c->parents_dev, (size_t)std::min(cap, h.n_parents) * sizeof(int), cudaMemcpyDeviceToHost));
     return ABM_OK;
 }
 
@@ -431,19 +473,31 @@ static void enqueue_rebuild(abm_ctx* c)
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
 }
 
-// one iteration of the loop body without division
-static void enqueue_iteration(abm_ctx* c)
+// one iteration of the loop body without division: stage-invariant pair
+// forces, then the trial attempt, up to max_tries retries and the accepted
+// final attempt (simulation.hpp:1677-1769), each an early exit when idle
+static void enqueue_pair_force(abm_ctx* c)
+{
+    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+}
+
+static void enqueue_attempts(abm_ctx* c)
 {
     cudaStream_t st = c->st;
-    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
-                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, st);
     launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                   0.0, 0, c->cap, st);
+                   c->k0buf, 0.0, 0, c->cap, st);
     for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
         launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       0.0, 0, c->cap, st);
+                       c->k0buf, 0.0, 0, c->cap, st);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                   0.0, 0, c->cap, st);
+                   c->k0buf, 0.0, 0, c->cap, st);
+}
+
+static void enqueue_iteration(abm_ctx* c)
+{
+    enqueue_pair_force(c);
+    enqueue_attempts(c);
 }
 
 static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
@@ -455,6 +509,142 @@ static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
     cudaError_t e = cudaGraphInstantiate(exec, g, 0);
     cudaGraphDestroy(g);
     CK(e);
+    return ABM_OK;
+}
+
+// division body (after the flag count): ranks, room checks on a fresh cell list,
+// the ten tries, commit, then the neighbor rebuild the reference does after any
+// division (simulation.hpp:1654-1660)
+static void enqueue_division_body(abm_ctx* c)
+{
+    cudaStream_t st = c->st;
+    launch_scan(c->div_flags, &c->ctrl->n, c->div_rank, c->scan_sums, c->cap, st);
+    launch_div_body_pre(c->ctrl, c->div_flags, c->div_rank, c->mothers, c->cap, st);
+    launch_bbox(c->geom, c->ctrl, c->grid, c->bbox_acc, c->bbox_counter, c->bp.prefilter, c->cap_bins, c->cap, st);
+    cudaMemsetAsync(c->bin_count, 0, (size_t)c->cap_bins * sizeof(int), st);
+    launch_bin_count(c->geom, c->ctrl, c->grid, c->bin_count, c->key, c->slot, c->cap, st);
+    launch_scan(c->bin_count, &c->grid->nbins, c->bin_start, c->scan_sums, c->cap_bins, st);
+    launch_bin_scatter(c->geom, c->ctrl, c->bin_start, c->key, c->slot, c->sorted_cell, c->sorted_geom, c->cap, st);
+    launch_div_check(c->geom, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell, c->sorted_geom, c->div_flags,
+                     c->mothers, c->div_check, c->div_sat, st);
+    launch_div_tries(c->geom, c->phys, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell, c->sorted_geom,
+                     c->div_flags, c->mothers, c->div_check, c->div_sat, c->d1, c->d2, c->dlen, c->dgrowth,
+                     c->div_ok, st);
+    launch_div_commit(c->geom, c->vel, c->phys, c->ctrl, c->dp, c->mothers, c->d1, c->d2, c->dlen, c->dgrowth,
+                      c->parents_dev, st);
+}
+
+static void enqueue_division_body_and_rebuild(abm_ctx* c)
+{
+    enqueue_division_body(c);
+    enqueue_rebuild(c);
+}
+
+// Capture fn into `graph` after `deps`; `deps` becomes the leaf set of the capture.
+static int capture_into(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphNode_t>& deps,
+                        const std::function<void()>& fn)
+{
+    CK(cudaStreamBeginCaptureToGraph(c->st, graph, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                     cudaStreamCaptureModeThreadLocal));
+    fn();
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t* leaves = nullptr;
+    size_t nleaves = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(c->st, &status, nullptr, nullptr, &leaves, &nleaves);
+    std::vector<cudaGraphNode_t> next(leaves, leaves + (e == cudaSuccess ? nleaves : 0));
+    cudaGraph_t out;
+    CK(cudaStreamEndCapture(c->st, &out));
+    CK(e);
+    deps = next;
+    return ABM_OK;
+}
+
+static int add_conditional(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphNode_t>& deps,
+                           cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                           cudaGraph_t* body)
+{
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams* np = reinterpret_cast<cudaGraphNodeParams*>(raw);
+    np->type = cudaGraphNodeTypeConditional;
+    np->conditional.handle = h;
+    np->conditional.type = type;
+    np->conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, graph, deps.empty() ? nullptr : deps.data(), deps.size(), np));
+    *body = np->conditional.phGraph_out[0];
+    deps.assign(1, node);
+    return ABM_OK;
+}
+
+// One loop iteration as a graph with conditional nodes:
+//   [division count] -> IF(n_divide > 0){division + rebuild}
+//   -> pair force -> trial -> WHILE(retry requested){retry} -> final
+static int build_iteration_graph(abm_ctx* c)
+{
+    cudaGraph_t G;
+    CK(cudaGraphCreate(&G, 0));
+    cudaGraphConditionalHandle h_div, h_retry;
+    CK(cudaGraphConditionalHandleCreate(&h_div, G, 0, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
+    std::vector<cudaGraphNode_t> deps;
+    int rc;
+    if (c->div_enabled)
+    {
+        rc = capture_into(c, G, deps, [&]() { launch_div_count(c->phys, c->ctrl, c->dp, c->div_flags, h_div, 1, c->st); });
+        if (rc) return rc;
+        cudaGraph_t body;
+        rc = add_conditional(c, G, deps, h_div, cudaGraphCondTypeIf, &body);
+        if (rc) return rc;
+        std::vector<cudaGraphNode_t> bd;
+        rc = capture_into(c, body, bd, [&]() { enqueue_division_body_and_rebuild(c); });
+        if (rc) return rc;
+    }
+    rc = capture_into(c, G, deps, [&]() {
+        enqueue_pair_force(c);
+        launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1);
+    });
+    if (rc) return rc;
+    if (c->p.max_tries_update_stepsize > 0)
+    {
+        cudaGraph_t body;
+        rc = add_conditional(c, G, deps, h_retry, cudaGraphCondTypeWhile, &body);
+        if (rc) return rc;
+        std::vector<cudaGraphNode_t> bd;
+        rc = capture_into(c, body, bd, [&]() {
+            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                           c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1);
+        });
+        if (rc) return rc;
+    }
+    rc = capture_into(c, G, deps, [&]() {
+        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+                       c->k0buf, 0.0, 0, c->cap, c->st);
+    });
+    if (rc) return rc;
+    cudaError_t e = cudaGraphInstantiate(&c->g_iter, G, 0);
+    cudaGraphDestroy(G);
+    CK(e);
+    return ABM_OK;
+}
+
+// Division outside a graph: the flag count decides on the host whether the
+// body and the neighbor rebuild run.
+static int divide_now(abm_ctx* c, bool rebuild, int* n_divided)
+{
+    launch_div_count(c->phys, c->ctrl, c->dp, c->div_flags, 0, 0, c->st);
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (n_divided) *n_divided = h.n_divide;
+    if (h.n_divide > 0)
+    {
+        enqueue_division_body(c);
+        if (rebuild) enqueue_rebuild(c);
+        else c->nbrs_valid = false;
+        CK(cudaGetLastError());
+    }
     return ABM_OK;
 }
 
@@ -588,7 +778,7 @@ int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double
                       c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
     k_clear_eval<<<1, 1, 0, c->st>>>(c->ctrl);
     launch_attempt(3, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->gen_tmp,
-                   dt, attempt, c->cap, c->st);
+                   c->k0buf, dt, attempt, c->cap, c->st);
     CK(cudaGetLastError());
     const int n = c->n_host;
     if (cells_out && n > 0)
@@ -624,8 +814,25 @@ int abm_grow(abm_ctx* c, double dt)
 
 int abm_divide(abm_ctx* c, int* n_divided)
 {
-    (void)n_divided;
-    return fail(c, ABM_ERR_ARG, "division is not available in this build");
+    if (!c) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    int rc = divide_now(c, false, n_divided);
+    if (rc) return rc;
+    rc = check_status(c);
+    Ctrl h;
+    CK(cudaMemcpy(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    c->n_host = h.n;
+    return rc;
+}
+
+int abm_last_division_tries(abm_ctx* c, int* tries)
+{
+    if (!c || !tries) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *tries = h.last_div_tries;
+    return ABM_OK;
 }
 
 int abm_get_stats(abm_ctx* c, abm_stats* s)
@@ -646,25 +853,31 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
     if (!c || n_iters < 0) return ABM_ERR_ARG;
     int rc = ready_for_forces(c);
     if (rc) return rc;
-    if (c->p.growth_mean != 0 || c->p.growth_std != 0)
-    {
-        // cells may cross Ldiv; division is handled by abm_divide's kernels when present
-    }
     if (!c->nbrs_valid)
     {
         enqueue_rebuild(c);
         c->nbrs_valid = true;
     }
-    (void)n_cells_stop;
     if (c->p.use_graphs)
     {
-        if (!c->g_iter) { rc = capture(c, enqueue_iteration, &c->g_iter); if (rc) return rc; }
+        if (!c->g_iter) { rc = build_iteration_graph(c); if (rc) return rc; }
         if (!c->g_rebuild) { rc = capture(c, enqueue_rebuild, &c->g_rebuild); if (rc) return rc; }
     }
     for (int k = 0; k < n_iters; ++k)
     {
+        if (n_cells_stop > 0 && c->div_enabled && (k % 16) == 0)
+        {
+            Ctrl h;
+            CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            if (h.n >= n_cells_stop) break;
+        }
         if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
-        else enqueue_iteration(c);
+        else
+        {
+            if (c->div_enabled) { rc = divide_now(c, true, nullptr); if (rc) return rc; }
+            enqueue_iteration(c);
+        }
         c->host_iter += 1;
         if (c->host_iter % c->p.iter_update_neighbors == 0)
         {
@@ -692,16 +905,9 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     {
         cudaEvent_t* e = &ev[(size_t)k * 4];
         CK(cudaEventRecord(e[0], st));
-        launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
-                          c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, st);
+        enqueue_pair_force(c);
         CK(cudaEventRecord(e[1], st));
-        launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       0.0, 0, c->cap, st);
-        for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
-            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr,
-                           nullptr, 0.0, 0, c->cap, st);
-        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       0.0, 0, c->cap, st);
+        enqueue_attempts(c);
         CK(cudaEventRecord(e[2], st));
         c->host_iter += 1;
         if (c->host_iter % c->p.iter_update_neighbors == 0) { enqueue_rebuild(c); rebuilt[k] = 1; }

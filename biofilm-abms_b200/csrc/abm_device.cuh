@@ -119,18 +119,14 @@ __device__ __forceinline__ Dist dist_between_cells(X3 r1, X3 n1, double h1, X3 r
             X3 d_q2 = xsub(xadd(r1, xscale(s_q2, n1)), q2);
             double dist_p2 = xnorm(d_p2), dist_q2 = xnorm(d_q2);
             // the two smallest of four distances; ties keep index order, as the
-            // reference's std::sort of a 4-element range does (insertion sort)
-            double dv[4] = {dist_p1, dist_q1, dist_p2, dist_q2};
-            int iv[4] = {0, 1, 2, 3};
-#pragma unroll
-            for (int a = 1; a < 4; ++a)
-            {
-                double kd = dv[a]; int ki = iv[a]; int b = a - 1;
-                while (b >= 0 && kd < dv[b]) { dv[b + 1] = dv[b]; iv[b + 1] = iv[b]; --b; }
-                dv[b + 1] = kd; iv[b + 1] = ki;
-            }
-            bool m0 = (iv[0] == 0 || iv[1] == 0), m1 = (iv[0] == 1 || iv[1] == 1);
-            bool m2 = (iv[0] == 2 || iv[1] == 2);
+            // reference's std::sort of a 4-element range does (insertion sort):
+            // element a lands at position #{b : d_b < d_a} + #{b < a : d_b == d_a}
+            const double dv0 = dist_p1, dv1 = dist_q1, dv2 = dist_p2, dv3 = dist_q2;
+            const int rk0 = (dv1 < dv0) + (dv2 < dv0) + (dv3 < dv0);
+            const int rk1 = (dv0 <= dv1) + (dv2 < dv1) + (dv3 < dv1);
+            const int rk2 = (dv0 <= dv2) + (dv1 <= dv2) + (dv3 < dv2);
+            bool m0 = rk0 < 2, m1 = rk1 < 2;
+            bool m2 = rk2 < 2;
             if (m0 && m1)
             {
                 s = 0.0;
@@ -250,38 +246,22 @@ __host__ __device__ __forceinline__ double rng_uniform(uint64_t seed, uint32_t p
 
 // ---------------------------------------------------------------------------
 // Surface integrals (integrals.hpp) with the overlap powers taken from one
-// square root: p^{k+1/2} = p^k sqrt(p).
+// square root per end: p^{k/2} = p^{floor(k/2)} (sqrt p)^{k mod 2}.
 // ---------------------------------------------------------------------------
-struct EndPow {               // powers of the end overlaps phi(-h) (1) and phi(+h) (2)
-    double p1, q1;            // p^1/2
-    double p2, q2;            // p^1
-    double p3, q3;            // p^3/2
-    double p4, q4;            // p^2
-    double p5, q5;            // p^5/2
-    double p6, q6;            // p^3
-    double p7, q7;            // p^7/2
+struct EndPow {               // end overlaps phi(-h) (p) and phi(+h) (q) and their roots
+    double p, q, sp, sq;
 };
 
-// exponent index e = 2 (gamma + 1): 1 -> p^0.5, 2 -> p, 3 -> p^1.5, ...
+// p^(e/2) for e = 1..7 (e = 2 (gamma + 1))
+__device__ __forceinline__ double half_pow(double x, double sx, int e)
+{
+    double r = (e & 1) ? sx : 1.0;
+    for (int k = 0; k < (e >> 1); ++k) r *= x;
+    return r;
+}
 __device__ __forceinline__ double epw(const EndPow& w, int e, bool second)
 {
-    switch (e)
-    {
-        case 1: return second ? w.q1 : w.p1;
-        case 2: return second ? w.q2 : w.p2;
-        case 3: return second ? w.q3 : w.p3;
-        case 4: return second ? w.q4 : w.p4;
-        case 5: return second ? w.q5 : w.p5;
-        case 6: return second ? w.q6 : w.p6;
-        default: return second ? w.q7 : w.p7;
-    }
-}
-
-__device__ __forceinline__ void fill_pows(double p, double& r1, double& r2, double& r3, double& r4,
-                                          double& r5, double& r6, double& r7)
-{
-    double sq = sqrt(p);
-    r1 = sq; r2 = p; r3 = p * sq; r4 = p * p; r5 = r4 * sq; r6 = r4 * p; r7 = r6 * sq;
+    return second ? half_pow(w.q, w.sq, e) : half_pow(w.p, w.sp, e);
 }
 
 // integrals.hpp:116-140 (integral1) with gamma + 1 = e / 2
@@ -308,11 +288,10 @@ __device__ __forceinline__ double integral2(const EndPow& w, double nz, double h
 __device__ __forceinline__ EndPow end_pows(double rz, double nz, double R, double h, double ss)
 {
     EndPow w;
-    double o1 = 0.0, o2 = 0.0;
-    if (ss > h) { o1 = R - rz - (-h) * nz; o2 = R - rz - h * nz; }
-    else if (ss > -h) { o1 = R - rz - (-h) * nz; }
-    fill_pows(o1, w.p1, w.p2, w.p3, w.p4, w.p5, w.p6, w.p7);
-    fill_pows(o2, w.q1, w.q2, w.q3, w.q4, w.q5, w.q6, w.q7);
+    w.p = 0.0; w.q = 0.0;
+    if (ss > h) { w.p = R - rz - (-h) * nz; w.q = R - rz - h * nz; }
+    else if (ss > -h) { w.p = R - rz - (-h) * nz; }
+    w.sp = sqrt(w.p); w.sq = sqrt(w.q);
     return w;
 }
 
@@ -390,12 +369,13 @@ __device__ __forceinline__ void area_integrals(const MechParams& P, double nz, d
     double onz = 1 - nz * nz;
     double piRnz2 = M_PI * R * nz * nz;
     A1 = P.sqrtR * onz * int1a + piRnz2 * int4;
-    double term2 = -h * (w.p3 + w.q3);
+    const double p3 = epw(w, 3, false), q3 = epw(w, 3, true);
+    double term2 = -h * (p3 + q3);
     double int2a = (int1b + term2) / (1.5 * nz);
     A2 = P.sqrtR * onz * int2a + piRnz2 * int5;
-    term2 = -h * (w.p5 + w.q5);
+    term2 = -h * (epw(w, 5, false) + epw(w, 5, true));
     double int2b = (int1c + term2) / (2.5 * nz);
-    double int3 = (2 * int2b + h * h * (w.p3 - w.q3)) / (1.5 * nz);
+    double int3 = (2 * int2b + h * h * (p3 - q3)) / (1.5 * nz);
     A3 = P.sqrtR * onz * int3 + piRnz2 * int6;
 }
 
@@ -404,7 +384,7 @@ __device__ __forceinline__ void area_integrals(const MechParams& P, double nz, d
 // dr, dn: stored velocities of the previous accepted step (Coulomb truncation).
 __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_2d, const double y[6],
                                                double l, double h, double eta0, double eta1_in,
-                                               double ss, const EndPow& w, const double dr[6],
+                                               double ss, const EndPow& w, const Vel* __restrict__ drp,
                                                const double f[6], double v[6])
 {
     const double R = P.R, E0 = P.E0, coul = P.coulomb;
@@ -432,7 +412,8 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         {
             double K_vis = eta0 * l, L_vis = K_vis * l * l / 12;
             double K_fric = eta1_in * l * a / R;
-            double drxy = sqrt(dr[0] * dr[0] + dr[1] * dr[1]);
+            const double2 d01 = __ldg(reinterpret_cast<const double2*>(drp->v));
+            double drxy = sqrt(d01.x * d01.x + d01.y * d01.y);
             double max_norm = coul * (2 * E0 * (R - rz) * l);
             if (K_fric * drxy > max_norm)
             {
@@ -454,8 +435,11 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         area_integrals(P, nz, h, ss, w, A1, A2, A3);
         if (coul > 0)
         {
-            double drxy = sqrt(dr[0] * dr[0] + dr[1] * dr[1]);
-            double dnxy = sqrt(dr[3] * dr[3] + dr[4] * dr[4]);
+            const double2 d01 = __ldg(reinterpret_cast<const double2*>(drp->v));
+            const double2 d23 = __ldg(reinterpret_cast<const double2*>(drp->v) + 1);
+            const double2 d45 = __ldg(reinterpret_cast<const double2*>(drp->v) + 2);
+            double drxy = sqrt(d01.x * d01.x + d01.y * d01.y);
+            double dnxy = sqrt(d23.y * d23.y + d45.x * d45.x);
             double friction_norm = (A1 * drxy + A2 * dnxy) * (eta1 / R);
             double max_norm = (1 - nz * nz) * integral1(w, nz, h, 4, ss)
                             + P.sqrtR * nz * nz * integral1(w, nz, h, 3, ss);

@@ -580,7 +580,7 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, con
 // mechanics.hpp:2064), so each stage needs only the cell's own state, its
 // precomputed pair force and the surface terms.
 // ---------------------------------------------------------------------------
-const int AT_T = 256;
+const int AT_T = 128;
 
 __device__ __forceinline__ void normalize_n(double y[6])
 {
@@ -589,42 +589,46 @@ __device__ __forceinline__ void normalize_n(double y[6])
     if (y[5] < 0) { y[3] = -y[3]; y[4] = -y[4]; y[5] = -y[5]; }
 }
 
-// getVelocities (mechanics.hpp:2011-2347) of one cell at state y
+// getVelocities (mechanics.hpp:2011-2347) of one cell at state y; f0 = -dE/dq of
+// the (stage-invariant) pair forces plus noise
 __device__ __forceinline__ void cell_velocity(const StepParams& sp, bool a2, const double y[6],
-                                              const Phys& ph, double h, const double dr[6],
-                                              const Gen6& cc, const double noise[6], double v[6])
+                                              double l, double h, double eta0, double eta1, double sigma0,
+                                              const Vel* __restrict__ drp, const double f0[6], double v[6])
 {
     const MechParams& P = sp.mp;
     double ss = a2 ? __longlong_as_double(0x7ff8000000000000ll) : (P.R - y[2]) / y[5];
     EndPow w;
+    w.p = w.q = w.sp = w.sq = 0.0;
     if (!a2) w = end_pows(y[2], y[5], P.R, h, ss);
     double rep2 = 0, rep5 = 0, adh2 = 0, adh5 = 0;
-    if (!P.no_surface) surface_dEdq(P, a2, y[2], y[5], ph.l, h, ph.sigma0, ss, w, rep2, rep5, adh2, adh5);
+    if (!P.no_surface) surface_dEdq(P, a2, y[2], y[5], l, h, sigma0, ss, w, rep2, rep5, adh2, adh5);
     double f[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) f[c] = -cc.f[c];
+    for (int c = 0; c < 6; ++c) f[c] = f0[c];
     f[2] = (f[2] - rep2) - adh2;
     f[5] = (f[5] - rep5) - adh5;
-    if (sp.noise_on)
-    {
-#pragma unroll
-        for (int c = 0; c < 6; ++c) f[c] += noise[c];
-    }
-    velocity_solve(P, a2, y, ph.l, h, ph.eta0, ph.eta1, ss, w, dr, f, v);
+    velocity_solve(P, a2, y, l, h, eta0, eta1, ss, w, drp, f, v);
 }
 
-__device__ __forceinline__ void cell_noise(const StepParams& sp, int iter, int attempt, int i, double noise[6])
+// -dE/dq of the pair forces (getConservativeForces, mechanics.hpp:1768) plus the
+// attempt's noise (mechanics.hpp:2489-2510, forces += noise at :2066)
+template <bool NOISE>
+__device__ __forceinline__ void base_force(const StepParams& sp, const Gen6* __restrict__ fcc, int iter,
+                                           int attempt, int i, double f0[6])
 {
-#pragma unroll
-    for (int c = 0; c < 6; ++c) noise[c] = 0.0;
-    if (!sp.noise_on) return;
-    for (int c = 0; c < 3; ++c)
+    const double2* cp = reinterpret_cast<const double2*>(fcc + i);
+    double2 a = __ldg(cp), b = __ldg(cp + 1), c = __ldg(cp + 2);
+    f0[0] = -a.x; f0[1] = -a.y; f0[2] = -b.x; f0[3] = -b.y; f0[4] = -c.x; f0[5] = -c.y;
+    if (NOISE)
     {
-        uint32_t x[4] = {(uint32_t)iter, (uint32_t)attempt, (uint32_t)i, (uint32_t)c};
-        philox4x32_10(x, (uint32_t)sp.seed, (uint32_t)(sp.seed >> 32) ^ RNG_PURPOSE_NOISE);
-        double u0 = philox_u01(x[0], x[1]), u1 = philox_u01(x[2], x[3]);
-        noise[2 * c] = -sp.noise_max[2 * c] + 2 * sp.noise_max[2 * c] * u0;
-        noise[2 * c + 1] = -sp.noise_max[2 * c + 1] + 2 * sp.noise_max[2 * c + 1] * u1;
+        for (int k = 0; k < 3; ++k)
+        {
+            uint32_t x[4] = {(uint32_t)iter, (uint32_t)attempt, (uint32_t)i, (uint32_t)k};
+            philox4x32_10(x, (uint32_t)sp.seed, (uint32_t)(sp.seed >> 32) ^ RNG_PURPOSE_NOISE);
+            double u0 = philox_u01(x[0], x[1]), u1 = philox_u01(x[2], x[3]);
+            f0[2 * k] += -sp.noise_max[2 * k] + 2 * sp.noise_max[2 * k] * u0;
+            f0[2 * k + 1] += -sp.noise_max[2 * k + 1] + 2 * sp.noise_max[2 * k + 1] * u1;
+        }
     }
 }
 
@@ -681,32 +685,46 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
     c->mode = MODE_FINAL;
 }
 
-template <int S, int KIND>
+// KIND: MODE_TRIAL / MODE_RETRY / MODE_FINAL inside the loop, 3 = API evaluation.
+// Without noise the stage-0 velocity k0 = f(y0) is the same for every attempt of an
+// iteration (y0 and the pair forces do not change), so the trial stores it in k0buf
+// and the retries and the final attempt read it back.
+template <int S, int KIND, bool NOISE>
 __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* __restrict__ fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
-                                                 Gen6* err_out, double eval_dt, int eval_attempt)
+                                                 Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
+                                                 unsigned long long cond, int use_cond)
 {
     __shared__ double sh_max[AT_T / 32];
     __shared__ bool last;
     const int n = ctrl->n;
     const int mode = ctrl->mode;
     const int iter = ctrl->iter;
+    const bool trial_ran = (iter % sp.iter_update_stepsize == 0);
     double dt;
     int attempt;
+    bool load_k0 = false, store_k0 = false;
     if (KIND == MODE_TRIAL)
     {
-        if (iter % sp.iter_update_stepsize != 0) return;   // no step-size update: FINAL runs at dt
-        dt = ctrl->dt; attempt = 0;
+        if (!trial_ran) return;   // no step-size update this iteration: FINAL runs at dt
+        dt = ctrl->dt; attempt = 0; store_k0 = !NOISE;
     }
     else if (KIND == MODE_RETRY)
     {
-        if (mode != MODE_RETRY) return;
-        dt = ctrl->dt_try; attempt = ctrl->attempt;
+        if (mode != MODE_RETRY)
+        {
+            // no retry pending: make sure an enclosing WHILE node stops
+            if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
+                cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
+            return;
+        }
+        dt = ctrl->dt_try; attempt = ctrl->attempt; load_k0 = !NOISE;
     }
     else if (KIND == MODE_FINAL)
     {
         dt = (mode == MODE_FINAL) ? ctrl->dt_try : ctrl->dt;
         attempt = (mode == MODE_FINAL) ? ctrl->attempt : 0;
+        load_k0 = !NOISE && trial_ran;
     }
     else { dt = eval_dt; attempt = eval_attempt; }
 
@@ -714,37 +732,44 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        const Geom g = geom[i];
-        const Vel vv = vel[i];
-        const Phys ph = phys[i];
-        const Gen6 cc = fcc[i];
+        const Geom g = load_geom(geom, i);
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
+        const double l = phys[i].l, eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
         const bool a2 = y0[5] < sp.mp.nz_threshold;
-        double noise[6];
-        cell_noise(sp, iter, attempt, i, noise);
+        double f0[6];
+        base_force<NOISE>(sp, fcc, iter, attempt, i, f0);
         double k[S][6];
+        if (load_k0)
+        {
+            const double2* kp = reinterpret_cast<const double2*>(k0buf + i);
+            double2 a = kp[0], b = kp[1], c = kp[2];
+            k[0][0] = a.x; k[0][1] = a.y; k[0][2] = b.x; k[0][3] = b.y; k[0][4] = c.x; k[0][5] = c.y;
+        }
+        else
+        {
+            cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[0]);
+            if (store_k0)
+            {
+                double2* kp = reinterpret_cast<double2*>(k0buf + i);
+                kp[0] = make_double2(k[0][0], k[0][1]);
+                kp[1] = make_double2(k[0][2], k[0][3]);
+                kp[2] = make_double2(k[0][4], k[0][5]);
+            }
+        }
 #pragma unroll
-        for (int st = 0; st < S; ++st)
+        for (int st = 1; st < S; ++st)
         {
             double y[6];
-            if (st == 0)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
             {
+                double m = 0.0;
 #pragma unroll
-                for (int c = 0; c < 6; ++c) y[c] = y0[c];
+                for (int j = 0; j < st; ++j) m += k[j][c] * sp.A[st][j];
+                y[c] = y0[c] + m * dt;
             }
-            else
-            {
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                {
-                    double m = 0.0;
-#pragma unroll
-                    for (int j = 0; j < st; ++j) m += k[j][c] * sp.A[st][j];
-                    y[c] = y0[c] + m * dt;
-                }
-                normalize_n(y);
-            }
-            cell_velocity(sp, a2, y, ph, g.h, vv.v, cc, noise, k[st]);
+            normalize_n(y);
+            cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[st]);
         }
         double vf1[6], d1[6];
 #pragma unroll
@@ -775,9 +800,9 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             if (KIND == MODE_FINAL)
             {
                 // growCells (growth.hpp:51-57) fused with the accepted step
-                double l = ph.l + ph.growth * (4 * sp.mp.R / 3 + ph.l) * dt;
-                go.h = l / 2;
-                phys[i].l = l;
+                double lg = l + phys[i].growth * (4 * sp.mp.R / 3 + l) * dt;
+                go.h = lg / 2;
+                phys[i].l = lg;
                 geom[i] = go;
                 vel[i] = vo;
             }
@@ -818,36 +843,46 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         ctrl->err_bits = 0ull;
         ctrl->blocks_done = 0u;
         controller_finish(ctrl, sp, KIND, E);
+        // another retry?  (bounded: the controller schedules at most max_tries of them)
+        if (use_cond && (KIND == MODE_TRIAL || KIND == MODE_RETRY))
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond,
+                                    (ctrl->mode == MODE_RETRY && ctrl->tries < sp.max_tries) ? 1u : 0u);
     }
 }
 
-template <int S>
+template <int S, bool NOISE>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
-                             double eval_dt, int eval_attempt, cudaStream_t st)
+                             Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
+                             unsigned long long cond, int use_cond)
 {
+#define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond
     switch (kind)
     {
-        case MODE_TRIAL: k_attempt<S, MODE_TRIAL><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
-        case MODE_RETRY: k_attempt<S, MODE_RETRY><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
-        case MODE_FINAL: k_attempt<S, MODE_FINAL><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
-        default: k_attempt<S, 3><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt); break;
+        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        default: k_attempt<S, 3, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
     }
+#undef AT_ARGS
 }
 
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
-                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
-                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st)
+                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
+                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
+                    unsigned long long cond, int use_cond)
 {
     int blocks = max(cdiv(cap_cells, AT_T), 1);
+#define AT_CASE(S) case S: \
+        if (sp.noise_on) launch_attempt_s<S, true>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond); \
+        else launch_attempt_s<S, false>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond); \
+        break;
     switch (sp.s)
     {
-        case 2: launch_attempt_s<2>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
-        case 4: launch_attempt_s<4>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
-        case 6: launch_attempt_s<6>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
-        case 7: launch_attempt_s<7>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, eval_dt, eval_attempt, st); break;
+        AT_CASE(2) AT_CASE(4) AT_CASE(6) AT_CASE(7)
         default: break;
     }
+#undef AT_CASE
 }
 
 __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
@@ -857,14 +892,14 @@ __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restric
     const int n = ctrl->n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        const Geom g = geom[i];
+        const Geom g = load_geom(geom, i);
         const double y[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
         const bool a2 = y[5] < sp.mp.nz_threshold;
-        double noise[6] = {0, 0, 0, 0, 0, 0};
-        StepParams q = sp;
-        q.noise_on = 0;
+        double f0[6];
+        base_force<false>(sp, fcc, 0, 0, i, f0);
         Gen6 out;
-        cell_velocity(q, a2, y, phys[i], g.h, vel[i].v, fcc[i], noise, out.f);
+        const Phys ph = phys[i];
+        cell_velocity(sp, a2, y, ph.l, g.h, ph.eta0, ph.eta1, ph.sigma0, vel + i, f0, out.f);
         v_out[i] = out;
     }
 }

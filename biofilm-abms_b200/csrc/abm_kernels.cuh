@@ -38,6 +38,12 @@ struct Ctrl {
     int n_divide;               // mothers in the pending division
     long long attempts, retries, iterations, rebuilds, divisions;
     unsigned long long eval_err_bits;   // scaled max error of the last API attempt
+    // division bookkeeping (growth.hpp:166-426)
+    int div_count;              // running count of flagged / satisfied cells
+    unsigned int div_blocks;    // last-block counter of the division kernels
+    int div_done, div_tries, last_div_tries;
+    int n_parents;              // length of the lineage vector
+    long long div_events;       // iterations in which cells divided
 };
 
 struct Grid {
@@ -103,9 +109,12 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, con
 
 // kind: MODE_TRIAL / MODE_RETRY / MODE_FINAL for the loop, 3 = evaluation for the API
 // (writes candidates and errors without touching the controller)
+// cond / use_cond: WHILE-node handle that the trial and retry attempts set to 1
+// when the controller asks for another retry (only inside a CUDA graph)
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
-                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
-                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st);
+                    const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
+                    double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
+                    unsigned long long cond = 0, int use_cond = 0);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
                        cudaStream_t st);
@@ -117,16 +126,26 @@ void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, in
 void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
                        const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st);
 
-// division (growth.hpp:66-426)
+// division (growth.hpp:66-426), abm_divide.cu
 struct DivideParams {
     double R, Rcell, Ldiv;
     double growth_mean, growth_std, daughter_length_std, angle_xy_bound, angle_z_bound;
     uint64_t seed;
     int cap_cells;
 };
-void launch_divide(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp,
-                   int* flags, int* ranks, int* block_sums, int* mothers, double* scratch_d,
-                   int* scratch_i, int* parents, int* n_parents, const Grid* grid,
-                   const int* bin_start, const int* sorted_cell, int cap_bins, cudaStream_t st);
+void launch_div_count(const Phys* phys, Ctrl* ctrl, const DivideParams& dp, int* flags,
+                      unsigned long long cond, int use_cond, cudaStream_t st);
+void launch_div_body_pre(Ctrl* ctrl, const int* flags, const int* rank, int* mothers, int cap_cells,
+                         cudaStream_t st);
+void launch_div_check(const Geom* geom, Ctrl* ctrl, const DivideParams& dp, const Grid* grid,
+                      const int* bin_start, const int* sorted_cell, const Geom* sorted_geom, const int* flags,
+                      const int* mothers, int* check, int* sat, cudaStream_t st);
+void launch_div_tries(const Geom* geom, const Phys* phys, Ctrl* ctrl, const DivideParams& dp, const Grid* grid,
+                      const int* bin_start, const int* sorted_cell, const Geom* sorted_geom, const int* flags,
+                      const int* mothers, const int* check, int* sat, Geom* d1, Geom* d2, double* dlen,
+                      double* dgrowth, int* ok, cudaStream_t st);
+void launch_div_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp, const int* mothers,
+                       const Geom* d1, const Geom* d2, const double* dlen, const double* dgrowth, int* parents,
+                       cudaStream_t st);
 
 }   // namespace abm

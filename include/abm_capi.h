@@ -144,6 +144,8 @@ int abm_grow(abm_ctx* ctx, double dt);
 /* divideMaxLength + divideCells (growth.hpp:66-71, 166-426) at the current clock;
  * *n_divided receives the number of mothers. */
 int abm_divide(abm_ctx* ctx, int* n_divided);
+/* Number of tries the last division took (the ntries loop of growth.hpp:252-398). */
+int abm_last_division_tries(abm_ctx* ctx, int* tries);
 
 /* n_iters iterations of the runSimulation loop body (simulation.hpp:1617-1864):
  * divide -> rebuild if divided -> adaptive RK step with the step-size

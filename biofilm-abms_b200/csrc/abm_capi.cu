@@ -52,6 +52,8 @@ struct abm_ctx {
     ForceParams fp; StepParams sp; BuildParams bp;
     // graphs
     cudaGraphExec_t g_iter = nullptr, g_rebuild = nullptr;
+    bool graph_fallback = false;     // conditional nodes could not be built
+    std::string graph_note;
 };
 
 static const int STAGING_COLS = 32;
@@ -506,9 +508,9 @@ static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     fn(c);
     CK(cudaStreamEndCapture(c->st, &g));
-    cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+    cudaError_t inst_plain = cudaGraphInstantiate(exec, g, 0);
     cudaGraphDestroy(g);
-    CK(e);
+    CK(inst_plain);
     return ABM_OK;
 }
 
@@ -550,11 +552,10 @@ static int capture_into(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphNode
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t* leaves = nullptr;
     size_t nleaves = 0;
-    cudaError_t e = cudaStreamGetCaptureInfo(c->st, &status, nullptr, nullptr, &leaves, &nleaves);
-    std::vector<cudaGraphNode_t> next(leaves, leaves + (e == cudaSuccess ? nleaves : 0));
-    cudaGraph_t out;
-    CK(cudaStreamEndCapture(c->st, &out));
-    CK(e);
+    cudaError_t info = cudaStreamGetCaptureInfo(c->st, &status, nullptr, nullptr, &leaves, &nleaves);
+    std::vector<cudaGraphNode_t> next(leaves, leaves + (info == cudaSuccess ? nleaves : 0));
+    CK(cudaStreamEndCapture(c->st, nullptr));
+    CK(info);
     deps = next;
     return ABM_OK;
 }
@@ -584,13 +585,15 @@ static int build_iteration_graph(abm_ctx* c)
 {
     cudaGraph_t G;
     CK(cudaGraphCreate(&G, 0));
-    cudaGraphConditionalHandle h_div, h_retry;
-    CK(cudaGraphConditionalHandleCreate(&h_div, G, 0, cudaGraphCondAssignDefault));
-    CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
+    // every handle must belong to a conditional node of this graph, or instantiation fails
+    cudaGraphConditionalHandle h_div = 0, h_retry = 0;
+    const bool retries = c->p.max_tries_update_stepsize > 0;
+    if (retries) CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
     std::vector<cudaGraphNode_t> deps;
     int rc;
     if (c->div_enabled)
     {
+        CK(cudaGraphConditionalHandleCreate(&h_div, G, 0, cudaGraphCondAssignDefault));
         rc = capture_into(c, G, deps, [&]() { launch_div_count(c->phys, c->ctrl, c->dp, c->div_flags, h_div, 1, c->st); });
         if (rc) return rc;
         cudaGraph_t body;
@@ -603,10 +606,10 @@ static int build_iteration_graph(abm_ctx* c)
     rc = capture_into(c, G, deps, [&]() {
         enqueue_pair_force(c);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1);
+                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0);
     });
     if (rc) return rc;
-    if (c->p.max_tries_update_stepsize > 0)
+    if (retries)
     {
         cudaGraph_t body;
         rc = add_conditional(c, G, deps, h_retry, cudaGraphCondTypeWhile, &body);
@@ -623,9 +626,9 @@ static int build_iteration_graph(abm_ctx* c)
                        c->k0buf, 0.0, 0, c->cap, c->st);
     });
     if (rc) return rc;
-    cudaError_t e = cudaGraphInstantiate(&c->g_iter, G, 0);
+    cudaError_t inst = cudaGraphInstantiate(&c->g_iter, G, 0);
     cudaGraphDestroy(G);
-    CK(e);
+    CK(inst);
     return ABM_OK;
 }
 
@@ -825,6 +828,13 @@ int abm_divide(abm_ctx* c, int* n_divided)
     return rc;
 }
 
+const char* abm_graph_info(const abm_ctx* c)
+{
+    if (!c) return "";
+    if (!c->g_iter) return "no iteration graph yet";
+    return c->graph_fallback ? c->graph_note.c_str() : "conditional";
+}
+
 int abm_last_division_tries(abm_ctx* c, int* tries)
 {
     if (!c || !tries) return ABM_ERR_ARG;
@@ -860,7 +870,20 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
     }
     if (c->p.use_graphs)
     {
-        if (!c->g_iter) { rc = build_iteration_graph(c); if (rc) return rc; }
+        if (!c->g_iter && !c->graph_fallback)
+        {
+            rc = build_iteration_graph(c);
+            if (rc)
+            {
+                // conditional nodes unavailable: keep the error for abm_graph_info and fall back to
+                // a straight-line graph (retries exit early) with division decided on the host
+                c->graph_note = c->err;
+                c->graph_fallback = true;
+                cudaGetLastError();
+                if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+            }
+        }
+        if (c->graph_fallback && !c->g_iter) { rc = capture(c, enqueue_iteration, &c->g_iter); if (rc) return rc; }
         if (!c->g_rebuild) { rc = capture(c, enqueue_rebuild, &c->g_rebuild); if (rc) return rc; }
     }
     for (int k = 0; k < n_iters; ++k)
@@ -872,11 +895,12 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
             CK(cudaStreamSynchronize(c->st));
             if (h.n >= n_cells_stop) break;
         }
-        if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
+        if (c->p.use_graphs && !c->graph_fallback) CK(cudaGraphLaunch(c->g_iter, c->st));
         else
         {
             if (c->div_enabled) { rc = divide_now(c, true, nullptr); if (rc) return rc; }
-            enqueue_iteration(c);
+            if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
+            else enqueue_iteration(c);
         }
         c->host_iter += 1;
         if (c->host_iter % c->p.iter_update_neighbors == 0)

@@ -155,6 +155,9 @@ int abm_last_division_tries(abm_ctx* ctx, int* tries);
  * forces a synchronisation. */
 int abm_iterate(abm_ctx* ctx, int n_iters, int n_cells_stop, abm_stats* stats);
 int abm_get_stats(abm_ctx* ctx, abm_stats* stats);
+/* "conditional" when the iteration graph uses IF/WHILE nodes, otherwise why it could not
+ * (the fallback graph launches every retry and decides division on the host). */
+const char* abm_graph_info(const abm_ctx* ctx);
 /* Same as abm_iterate without graphs, with CUDA events around each kernel group
  * (no reference counterpart; measurement only). */
 int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);

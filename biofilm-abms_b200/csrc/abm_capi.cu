@@ -36,6 +36,8 @@ struct abm_ctx {
     int *bin_count = nullptr, *bin_start = nullptr, *key = nullptr, *slot = nullptr, *sorted_cell = nullptr;
     Geom* sorted_geom = nullptr;
     int *scratch = nullptr, *nbr_count = nullptr, *row_ptr = nullptr, *col = nullptr;
+    int *lower_end = nullptr, *rev = nullptr;
+    double4* jbuf = nullptr;
     int* scan_sums = nullptr;
     double *jkr_delta = nullptr, *jkr_radius = nullptr;
     int jkr_n = 0;
@@ -119,7 +121,7 @@ static void free_all(abm_ctx* c)
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
-                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col,
+                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth};
@@ -243,6 +245,10 @@ int abm_create(const abm_params* q, abm_ctx** out)
     CK(cudaMalloc(&c->nbr_count, cap * sizeof(int)));
     CK(cudaMalloc(&c->row_ptr, (cap + 1) * sizeof(int)));
     CK(cudaMalloc(&c->col, cap * c->cap_nbr * sizeof(int)));
+    CK(cudaMalloc(&c->lower_end, cap * sizeof(int)));
+    CK(cudaMalloc(&c->rev, cap * c->cap_nbr * sizeof(int)));
+    CK(cudaMalloc(&c->jbuf, cap * c->cap_nbr * sizeof(double4)));
+    CK(cudaMemset(c->lower_end, 0, cap * sizeof(int)));
     size_t ns = std::max(scan_block_sums_size((int)cap + 1), scan_block_sums_size(c->cap_bins + 1)) + 1;
     CK(cudaMalloc(&c->scan_sums, ns * sizeof(int)));
     CK(cudaMalloc(&c->staging, cap * STAGING_COLS * sizeof(double)));
@@ -472,6 +478,7 @@ static void enqueue_rebuild(abm_ctx* c)
                       c->nbr_count, c->cap_bins, c->num_sms, st);
     launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
     launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st);
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
 }
 
@@ -480,7 +487,7 @@ static void enqueue_rebuild(abm_ctx* c)
 // final attempt (simulation.hpp:1677-1769), each an early exit when idle
 static void enqueue_pair_force(abm_ctx* c)
 {
-    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
                       c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
 }
 
@@ -727,6 +734,8 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
     CK(cudaStreamSynchronize(c->st));
     h.n_dir = (int)cl.size();
     CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st);
+    CK(cudaGetLastError());
     c->nbrs_valid = true;
     return ABM_OK;
 }
@@ -747,7 +756,7 @@ int abm_cell_cell_forces(abm_ctx* c, double* out)
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
                       c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
     CK(cudaGetLastError());
     return download_gen6(c, c->fcc, out);
@@ -759,7 +768,7 @@ int abm_get_velocities(abm_ctx* c, double* out)
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
                       c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
     launch_velocities(c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->gen_tmp, c->cap, c->st);
     CK(cudaGetLastError());
@@ -777,7 +786,7 @@ int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->col, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc,
+    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
                       c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
     k_clear_eval<<<1, 1, 0, c->st>>>(c->ctrl);
     launch_attempt(3, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->gen_tmp,

@@ -211,6 +211,51 @@ __device__ __forceinline__ Dist dist_geom_mixed(const Geom& a, const Geom& b)
 }
 
 // ---------------------------------------------------------------------------
+// Deterministic log, sin, cos for the division draws.  Two daughters of one
+// mother are placed exactly 2R apart end to end, where the JKR force jumps at
+// zero overlap, so the draws must come out bit-identical in the CPU
+// restatement: both evaluate the same sequence of correctly rounded operations.
+//   log x   frexp reduction to m in [sqrt(1/2), sqrt(2)), log m = 2 atanh((m-1)/(m+1))
+//           by its power series (to f^29);
+//   sin/cos Cody-Waite reduction by pi/2 (two-part constant), Taylor series of sin
+//           and cos on [-pi/4, pi/4] (to r^23 / r^22).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double det_log(double x)
+{
+    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+    int e;
+    double m = frexp(x, &e);
+    if (m < 0.70710678118654752440) { m = __dmul_rn(m, 2.0); e = e - 1; }
+    double f = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
+    double f2 = __dmul_rn(f, f);
+    double p = __ddiv_rn(1.0, 29.0);
+    for (int k = 27; k >= 1; k -= 2) p = __dadd_rn(__dmul_rn(p, f2), __ddiv_rn(1.0, (double)k));
+    double ed = (double)e;
+    return __dadd_rn(__dmul_rn(ed, LN2_HI), __dadd_rn(__dmul_rn(__dmul_rn(2.0, f), p), __dmul_rn(ed, LN2_LO)));
+}
+
+__device__ __forceinline__ void det_sincos(double x, double& s, double& c)
+{
+    const double TWO_OVER_PI = 0.63661977236758134308;
+    const double PIO2_HI = 1.57079632673412561417e+00, PIO2_LO = 6.07710050650619224932e-11;
+    double k = rint(__dmul_rn(x, TWO_OVER_PI));
+    double r = __dsub_rn(__dsub_rn(x, __dmul_rn(k, PIO2_HI)), __dmul_rn(k, PIO2_LO));
+    double r2 = __dmul_rn(r, r);
+    double ps = 1.0, pc = 1.0;
+    for (int n = 22; n >= 2; n -= 2)
+    {
+        ps = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(ps, r2), (double)((n + 1) * n)));
+        pc = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(pc, r2), (double)(n * (n - 1))));
+    }
+    double sr = __dmul_rn(r, ps), cr = pc;
+    int q = (int)((long long)k & 3);
+    if (q == 0) { s = sr; c = cr; }
+    else if (q == 1) { s = cr; c = -sr; }
+    else if (q == 2) { s = -sr; c = -cr; }
+    else { s = -cr; c = sr; }
+}
+
+// ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon et al., SC'11), the counter-based draw policy shared
 // with the CPU restatement.
 // ---------------------------------------------------------------------------

@@ -119,10 +119,13 @@ __global__ void k_div_check(const Geom* __restrict__ geom, Ctrl* ctrl, DividePar
     }
 }
 
-// utils.hpp:648-655 (standardNormal), on two policy uniforms
+// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms, with the
+// deterministic log / cos shared with the CPU restatement
 __device__ __forceinline__ double std_normal(double u, double v)
 {
-    return sqrt(-2 * log(u)) * cos(2 * M_PI * v);
+    double s, c;
+    det_sincos(__dmul_rn(6.283185307179586476925286766559005768, v), s, c);
+    return __dmul_rn(__dsqrt_rn(__dmul_rn(-2.0, det_log(u))), c);
 }
 
 __device__ __forceinline__ double div_u(const DivideParams& dp, int iter, int k, int tr, int slot)
@@ -130,21 +133,30 @@ __device__ __forceinline__ double div_u(const DivideParams& dp, int iter, int k,
     return rng_uniform(dp.seed, RNG_PURPOSE_DIVIDE, (uint32_t)iter, (uint32_t)k, (uint32_t)tr, (uint32_t)slot);
 }
 
-// utils.hpp:791-801 (rotateXY) then :814-829 (rotateOutOfXY)
+// utils.hpp:791-801 (rotateXY) then :814-829 (rotateOutOfXY), in correctly rounded
+// operations without FMA so daughters come out bit-identical to the CPU restatement
 __device__ __forceinline__ void rotate_daughter(double ux, double uy, double uz, double txy, double tz,
                                                 double& ox, double& oy, double& oz)
 {
-    double st = sin(txy), ct = cos(txy);
-    double ax = ct * ux + (-st) * uy + 0 * uz;
-    double ay = st * ux + ct * uy + 0 * uz;
-    double az = (0 * ux + 0 * uy) + 1 * uz;
+    double st, ct;
+    det_sincos(txy, st, ct);
+    double ax = __dadd_rn(__dadd_rn(__dmul_rn(ct, ux), __dmul_rn(-st, uy)), __dmul_rn(0.0, uz));
+    double ay = __dadd_rn(__dadd_rn(__dmul_rn(st, ux), __dmul_rn(ct, uy)), __dmul_rn(0.0, uz));
+    double az = __dadd_rn(__dadd_rn(__dmul_rn(0.0, ux), __dmul_rn(0.0, uy)), __dmul_rn(1.0, uz));
     // v = a x z, normalised; w = v x a
-    double vx = ay * 1 - az * 0, vy = az * 0 - ax * 1, vz = ax * 0 - ay * 0;
-    double vn = sqrt((vx * vx + vy * vy) + vz * vz);
-    vx /= vn; vy /= vn; vz /= vn;
-    double s2 = sin(tz), c2 = cos(tz);
-    double wx = vy * az - vz * ay, wy = vz * ax - vx * az, wz = vx * ay - vy * ax;
-    ox = ax * c2 + wx * s2; oy = ay * c2 + wy * s2; oz = az * c2 + wz * s2;
+    double vx = __dsub_rn(__dmul_rn(ay, 1.0), __dmul_rn(az, 0.0));
+    double vy = __dsub_rn(__dmul_rn(az, 0.0), __dmul_rn(ax, 1.0));
+    double vz = __dsub_rn(__dmul_rn(ax, 0.0), __dmul_rn(ay, 0.0));
+    double vn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz)));
+    vx = __ddiv_rn(vx, vn); vy = __ddiv_rn(vy, vn); vz = __ddiv_rn(vz, vn);
+    double s2, c2;
+    det_sincos(tz, s2, c2);
+    double wx = __dsub_rn(__dmul_rn(vy, az), __dmul_rn(vz, ay));
+    double wy = __dsub_rn(__dmul_rn(vz, ax), __dmul_rn(vx, az));
+    double wz = __dsub_rn(__dmul_rn(vx, ay), __dmul_rn(vy, ax));
+    ox = __dadd_rn(__dmul_rn(ax, c2), __dmul_rn(wx, s2));
+    oy = __dadd_rn(__dmul_rn(ay, c2), __dmul_rn(wy, s2));
+    oz = __dadd_rn(__dmul_rn(az, c2), __dmul_rn(wz, s2));
 }
 
 __global__ void k_div_try(const Geom* __restrict__ geom, const Phys* __restrict__ phys, Ctrl* ctrl,
@@ -162,29 +174,36 @@ __global__ void k_div_try(const Geom* __restrict__ geom, const Phys* __restrict_
         double txy1 = 0, tz1 = 0, txy2 = 0, tz2 = 0;
         if (tr < DIV_TRIES - 1 && check[k] == 1)
         {
-            txy1 = -dp.angle_xy_bound + 2 * dp.angle_xy_bound * div_u(dp, iter, k, tr, 0);
-            tz1 = -dp.angle_z_bound + 2 * dp.angle_z_bound * div_u(dp, iter, k, tr, 1);
-            txy2 = -dp.angle_xy_bound + 2 * dp.angle_xy_bound * div_u(dp, iter, k, tr, 2);
-            tz2 = -dp.angle_z_bound + 2 * dp.angle_z_bound * div_u(dp, iter, k, tr, 3);
+            const double bxy = dp.angle_xy_bound, bz = dp.angle_z_bound;
+            txy1 = __dadd_rn(-bxy, __dmul_rn(__dmul_rn(2.0, bxy), div_u(dp, iter, k, tr, 0)));
+            tz1 = __dadd_rn(-bz, __dmul_rn(__dmul_rn(2.0, bz), div_u(dp, iter, k, tr, 1)));
+            txy2 = __dadd_rn(-bxy, __dmul_rn(__dmul_rn(2.0, bxy), div_u(dp, iter, k, tr, 2)));
+            tz2 = __dadd_rn(-bz, __dmul_rn(__dmul_rn(2.0, bz), div_u(dp, iter, k, tr, 3)));
         }
         Geom a = m, b = m;
         rotate_daughter(m.nx, m.ny, m.nz, txy1, tz1, a.nx, a.ny, a.nz);
         rotate_daughter(m.nx, m.ny, m.nz, txy2, tz2, b.nx, b.ny, b.nz);
         // growth.hpp:311-348: lengths M (L - 2R), (1 - M)(L - 2R) and centres either side of
-        // the division point
-        double r = 0.5 + dp.daughter_length_std * std_normal(div_u(dp, iter, k, tr, 4), div_u(dp, iter, k, tr, 5));
+        // the division point (correctly rounded operations, as the CPU restatement)
+        double r = __dadd_rn(0.5, __dmul_rn(dp.daughter_length_std,
+                                            std_normal(div_u(dp, iter, k, tr, 4), div_u(dp, iter, k, tr, 5))));
         double M = r < 0 ? 0.0 : (r > 1 ? 1.0 : r);
-        double Ld = l - 2 * dp.R;
-        double L1 = M * Ld, L2 = (1 - M) * Ld;
-        double dv = -m.h + L1 + dp.R;
-        double del1 = L1 / 2 + dp.R, del2 = L2 / 2 + dp.R;
-        a.rx = m.rx + (dv - del1) * a.nx; a.ry = m.ry + (dv - del1) * a.ny; a.rz = m.rz + (dv - del1) * a.nz;
-        b.rx = m.rx + (dv + del2) * b.nx; b.ry = m.ry + (dv + del2) * b.ny; b.rz = m.rz + (dv + del2) * b.nz;
-        a.h = L1 / 2; b.h = L2 / 2;
+        double Ld = __dsub_rn(l, __dmul_rn(2.0, dp.R));
+        double L1 = __dmul_rn(M, Ld), L2 = __dmul_rn(__dsub_rn(1.0, M), Ld);
+        double dv = __dadd_rn(__dadd_rn(-m.h, L1), dp.R);
+        double del1 = __dadd_rn(__ddiv_rn(L1, 2.0), dp.R), del2 = __dadd_rn(__ddiv_rn(L2, 2.0), dp.R);
+        double f1 = __dsub_rn(dv, del1), f2 = __dadd_rn(dv, del2);
+        a.rx = __dadd_rn(m.rx, __dmul_rn(f1, a.nx)); a.ry = __dadd_rn(m.ry, __dmul_rn(f1, a.ny));
+        a.rz = __dadd_rn(m.rz, __dmul_rn(f1, a.nz));
+        b.rx = __dadd_rn(m.rx, __dmul_rn(f2, b.nx)); b.ry = __dadd_rn(m.ry, __dmul_rn(f2, b.ny));
+        b.rz = __dadd_rn(m.rz, __dmul_rn(f2, b.nz));
+        a.h = __ddiv_rn(L1, 2.0); b.h = __ddiv_rn(L2, 2.0);
         d1[k] = a; d2[k] = b;
         dlen[2 * k] = L1; dlen[2 * k + 1] = L2;
-        dgrowth[2 * k] = dp.growth_mean + dp.growth_std * std_normal(div_u(dp, iter, k, tr, 6), div_u(dp, iter, k, tr, 7));
-        dgrowth[2 * k + 1] = dp.growth_mean + dp.growth_std * std_normal(div_u(dp, iter, k, tr, 8), div_u(dp, iter, k, tr, 9));
+        dgrowth[2 * k] = __dadd_rn(dp.growth_mean, __dmul_rn(dp.growth_std,
+                                   std_normal(div_u(dp, iter, k, tr, 6), div_u(dp, iter, k, tr, 7))));
+        dgrowth[2 * k + 1] = __dadd_rn(dp.growth_mean, __dmul_rn(dp.growth_std,
+                                       std_normal(div_u(dp, iter, k, tr, 8), div_u(dp, iter, k, tr, 9))));
     }
 }
 

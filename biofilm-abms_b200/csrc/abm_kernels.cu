@@ -483,18 +483,21 @@ __device__ __forceinline__ double jkr_magnitude(double dist, double gamma, const
     return term1 - term2;
 }
 
-template <bool MIXED>
-__device__ __forceinline__ void pair_contribution(int cell, int o, const Geom& gc, const Geom& go,
-                                                  const ForceParams& fp, const double* td,
-                                                  const double* tr, double acc[6])
+// Force of one unordered pair (i > j, distance from cell i to cell j, as the
+// reference's j < i loop computes it): magnitude m along d, returned as
+// v = m d_hat with the body coordinates s (on i) and t (on j).  Cell i gains
+// (v, s v) in dE/dq and cell j gains (-v, -t v) (mechanics.hpp:1390-1659).
+struct PairOut { double vx, vy, vz, s, t; bool touch; };
+
+__device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& gj, const ForceParams& fp,
+                                                   const double* td, const double* tr)
 {
-    const bool first = cell > o;                 // cell is "cell 1" (row index i) of the pair
-    const Geom& gi = first ? gc : go;
-    const Geom& gj = first ? go : gc;
-    Dist d = MIXED ? dist_geom_mixed(gi, gj) : dist_geom(gi, gj);
+    PairOut out;
+    out.touch = false;
+    Dist d = dist_geom(gi, gj);
     double dist = xnorm(x3(d.dx, d.dy, d.dz));
     double overlap = 2 * fp.R - dist;
-    if (!(overlap > 0)) return;
+    if (!(overlap > 0)) return out;
     double ux = d.dx / dist, uy = d.dy / dist, uz = d.dz / dist;
     double m;
     double gamma = fp.adhesion ? fmin(gi.gamma, gj.gamma) : 0.0;
@@ -506,26 +509,65 @@ __device__ __forceinline__ void pair_contribution(int cell, int o, const Geom& g
         if (!fp.adhesion) m += fp.pf1 * pow15(overlap - fp.max_overlap);
     }
     if (fp.adhesion && overlap > fp.max_overlap) m += fp.pf1 * pow15(overlap - fp.max_overlap);
-    double vx = m * ux, vy = m * uy, vz = m * uz;
-    if (first)
+    out.vx = m * ux; out.vy = m * uy; out.vz = m * uz;
+    out.s = d.s; out.t = d.t; out.touch = true;
+    return out;
+}
+
+// FP32 variant: segment distance (FP64 near-parallel branch kept), overlap,
+// Hertz / JKR magnitude and direction in single precision
+__device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& gj, const ForceParams& fp,
+                                                   const double* td, const double* tr)
+{
+    PairOut out;
+    out.touch = false;
+    Dist d = dist_geom_mixed(gi, gj);
+    float dx = (float)d.dx, dy = (float)d.dy, dz = (float)d.dz;
+    float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float R = (float)fp.R, max_overlap = (float)fp.max_overlap;
+    float overlap = 2.f * R - dist;
+    if (!(overlap > 0.f)) return out;
+    float inv = 1.f / dist;
+    float m;
+    float gamma = fp.adhesion ? fminf((float)gi.gamma, (float)gj.gamma) : 0.f;
+    if (fp.adhesion && gamma > 0.f)
     {
-        acc[0] += vx; acc[1] += vy; acc[2] += vz;
-        acc[3] += d.s * vx; acc[4] += d.s * vy; acc[5] += d.s * vz;
+        float delta = overlap > max_overlap ? max_overlap : overlap;
+        const int nm = fp.jkr_n;
+        int k = (int)(delta / (float)fp.jkr_step);
+        k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
+        while (k > 0 && (float)td[k] > delta) --k;
+        while (k < nm - 2 && (float)td[k + 1] <= delta) ++k;
+        float d1 = (float)td[k], d2 = (float)td[k + 1], r1 = (float)tr[k], r2 = (float)tr[k + 1];
+        float radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
+        float a3 = radius * radius * radius;
+        float E0 = (float)fp.E0;
+        m = 4.f * E0 * a3 / (3.f * (R * 0.5f)) - 4.f * sqrtf(3.14159265f * a3 * gamma * E0);
     }
+    else if (overlap <= max_overlap) m = (float)fp.pf0 * overlap * sqrtf(overlap);
     else
     {
-        acc[0] -= vx; acc[1] -= vy; acc[2] -= vz;
-        acc[3] -= d.t * vx; acc[4] -= d.t * vy; acc[5] -= d.t * vz;
+        m = (float)fp.pf2;
+        if (!fp.adhesion) { float e = overlap - max_overlap; m += (float)fp.pf1 * e * sqrtf(e); }
     }
+    if (fp.adhesion && overlap > max_overlap) { float e = overlap - max_overlap; m += (float)fp.pf1 * e * sqrtf(e); }
+    out.vx = (double)(m * dx * inv); out.vy = (double)(m * dy * inv); out.vz = (double)(m * dz * inv);
+    out.s = d.s; out.t = d.t; out.touch = true;
+    return out;
 }
 
 const int PF_T = 256, JKR_MAX = 512;
 
+// Pass 1: G lanes per cell i walk the lower part of its sorted CSR row (j < i),
+// evaluate each unordered pair once, keep i's share and write j's share
+// (v, t) into the slot of i in row j (rev[k]).
 template <int G, bool MIXED>
 __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ geom, const int* __restrict__ row_ptr,
-                                                    const int* __restrict__ col, const Ctrl* ctrl, ForceParams fp,
+                                                    const int* __restrict__ lower_end, const int* __restrict__ col,
+                                                    const int* __restrict__ rev, const Ctrl* ctrl, ForceParams fp,
                                                     const double* __restrict__ jkr_delta,
-                                                    const double* __restrict__ jkr_radius, Gen6* fcc)
+                                                    const double* __restrict__ jkr_radius, Gen6* fcc,
+                                                    double4* __restrict__ jbuf)
 {
     __shared__ double td[JKR_MAX], tr[JKR_MAX];
     for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
@@ -539,12 +581,20 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
     {
         const Geom gc = load_geom(geom, cell);
         double acc[6] = {0, 0, 0, 0, 0, 0};
-        const int r0 = row_ptr[cell], r1 = row_ptr[cell + 1];
+        const int r0 = row_ptr[cell], r1 = lower_end[cell];
         for (int k = r0 + lane; k < r1; k += G)
         {
             const int o = col[k];
             const Geom go = load_geom(geom, o);
-            pair_contribution<MIXED>(cell, o, gc, go, fp, td, tr, acc);
+            PairOut p = MIXED ? pair_force_fp32(gc, go, fp, td, tr) : pair_force_fp64(gc, go, fp, td, tr);
+            double4 js = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (p.touch)
+            {
+                acc[0] += p.vx; acc[1] += p.vy; acc[2] += p.vz;
+                acc[3] += p.s * p.vx; acc[4] += p.s * p.vy; acc[5] += p.s * p.vz;
+                js = make_double4(p.vx, p.vy, p.vz, p.t);
+            }
+            jbuf[rev[k]] = js;
         }
 #pragma unroll
         for (int off = G / 2; off > 0; off >>= 1)
@@ -559,18 +609,80 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
     }
 }
 
-void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, const Ctrl* ctrl,
-                       ForceParams fp, const double* jkr_delta, const double* jkr_radius,
-                       Gen6* fcc, int lanes, int mixed, int cap_cells, cudaStream_t st)
+// Pass 2: each cell j adds the shares its higher-index neighbors left in the
+// upper part of its row: (-v, -t v).
+template <int G>
+__global__ void __launch_bounds__(PF_T) k_pair_gather(const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
+                                                     const Ctrl* ctrl, const double4* __restrict__ jbuf, Gen6* fcc)
+{
+    const int n = ctrl->n;
+    const int lane = threadIdx.x & (G - 1);
+    const unsigned gmask = (G == 32) ? 0xffffffffu
+                                     : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    const int groups_per_grid = gridDim.x * (blockDim.x / G);
+    for (int cell = (blockIdx.x * blockDim.x + threadIdx.x) / G; cell < n; cell += groups_per_grid)
+    {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = lower_end[cell] + lane; k < row_ptr[cell + 1]; k += G)
+        {
+            double4 js = jbuf[k];
+            acc[0] -= js.x; acc[1] -= js.y; acc[2] -= js.z;
+            acc[3] -= js.w * js.x; acc[4] -= js.w * js.y; acc[5] -= js.w * js.z;
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc[c] += __shfl_xor_sync(gmask, acc[c], off, G);
+        if (lane == 0)
+        {
+            Gen6 f = fcc[cell];
+            for (int c = 0; c < 6; ++c) f.f[c] += acc[c];
+            fcc[cell] = f;
+        }
+    }
+}
+
+void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
+                       const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st)
 {
     int blocks = max(cdiv((long long)cap_cells * lanes, PF_T), 1);
 #define PF_CASE(G) \
     if (lanes == G) { \
-        if (mixed) k_pair_force<G, true><<<blocks, PF_T, 0, st>>>(geom, row_ptr, col, ctrl, fp, jkr_delta, jkr_radius, fcc); \
-        else k_pair_force<G, false><<<blocks, PF_T, 0, st>>>(geom, row_ptr, col, ctrl, fp, jkr_delta, jkr_radius, fcc); \
+        if (mixed) k_pair_force<G, true><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
+        else k_pair_force<G, false><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
+        k_pair_gather<G><<<blocks, PF_T, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc); \
         return; }
     PF_CASE(4) PF_CASE(8) PF_CASE(16) PF_CASE(32)
 #undef PF_CASE
+}
+
+// Reverse slots and the end of the lower part of each sorted CSR row: for an
+// entry (i, j) with j < i, rev = position of i in row j.
+__global__ void k_csr_rev(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                          int* lower_end, int* rev)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
+        int lo = r0, hi = r1;
+        while (lo < hi) { int mid = (lo + hi) >> 1; if (col[mid] < i) lo = mid + 1; else hi = mid; }
+        lower_end[i] = lo;
+        for (int k = r0; k < lo; ++k)
+        {
+            const int j = col[k];
+            int a = row_ptr[j], b = row_ptr[j + 1];
+            while (a < b) { int mid = (a + b) >> 1; if (col[mid] < i) a = mid + 1; else b = mid; }
+            rev[k] = a;
+        }
+    }
+}
+
+void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
+                    int cap_cells, cudaStream_t st)
+{
+    k_csr_rev<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, lower_end, rev);
 }
 
 // ---------------------------------------------------------------------------

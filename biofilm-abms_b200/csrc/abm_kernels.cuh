@@ -103,9 +103,13 @@ void launch_csr_fill(const Ctrl* ctrl, const int* row_ptr, const int* scratch, i
 void launch_scan(const int* in, const int* len, int* out, int* block_sums, int cap, cudaStream_t st);
 size_t scan_block_sums_size(int cap);
 
-void launch_pair_force(const Geom* geom, const int* row_ptr, const int* col, const Ctrl* ctrl,
-                       ForceParams fp, const double* jkr_delta, const double* jkr_radius,
-                       Gen6* fcc, int lanes, int mixed, int cap_cells, cudaStream_t st);
+// two passes: each unordered pair once from the row of its larger index, then the
+// partner's share gathered from the reverse slots (jbuf, one double4 per CSR entry)
+void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
+                       const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st);
+void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
+                    int cap_cells, cudaStream_t st);
 
 // kind: MODE_TRIAL / MODE_RETRY / MODE_FINAL for the loop, 3 = evaluation for the API
 // (writes candidates and errors without touching the controller)

@@ -30,6 +30,7 @@
 #include <omp.h>
 #endif
 #include "philox.hpp"
+#include "detmath.hpp"
 
 namespace oracle {
 
@@ -958,17 +959,21 @@ inline double min_dist_to_cell(const Cells& cells, int i)
     return mindist;
 }
 
-// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms
+// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms, with
+// the deterministic log / cos of detmath.hpp
 inline double standard_normal(double u, double v)
 {
-    double c = std::sqrt(-2 * std::log(u));
-    return c * std::cos(TWO_PI * v);
+    double c = std::sqrt(-2 * det_log(u));
+    double sn, cs;
+    det_sincos(TWO_PI * v, sn, cs);
+    return c * cs;
 }
 
 // utils.hpp:791-801 (rotateXY)
 inline V3 rotate_xy(V3 n, double theta)
 {
-    double st = std::sin(theta), ct = std::cos(theta);
+    double st, ct;
+    det_sincos(theta, st, ct);
     return v3(ct * n.x + (-st) * n.y + 0 * n.z, st * n.x + ct * n.y + 0 * n.z, (0 * n.x + 0 * n.y) + 1 * n.z);
 }
 
@@ -978,7 +983,8 @@ inline V3 rotate_out_of_xy(V3 n, double theta)
     V3 v = v3(n.y * 1 - n.z * 0, n.z * 0 - n.x * 1, n.x * 0 - n.y * 0);   // n x z
     double nv = norm(v);
     v = v3(v.x / nv, v.y / nv, v.z / nv);
-    double st = std::sin(theta), ct = std::cos(theta);
+    double st, ct;
+    det_sincos(theta, st, ct);
     V3 w = v3(v.y * n.z - v.z * n.y, v.z * n.x - v.x * n.z, v.x * n.y - v.y * n.x);   // v x n
     return v3(n.x * ct + w.x * st, n.y * ct + w.y * st, n.z * ct + w.z * st);
 }

@@ -307,6 +307,10 @@ double oracle_rng_uniform(unsigned long long seed, unsigned purpose, unsigned a,
     return rng_uniform(seed, purpose, a, b, cc, d);
 }
 
+// deterministic log / sincos used by the division draws
+double oracle_det_log(double x) { return det_log(x); }
+void oracle_det_sincos(double x, double* s, double* c) { det_sincos(x, *s, *c); }
+
 // integrals.hpp:400-463
 void oracle_area_integrals(double rz, double nz, double R, double half_l, double* out)
 {

@@ -78,6 +78,8 @@ def _load():
         "oracle_rng_uniform": ([ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
                                 ctypes.c_uint, ctypes.c_uint], d),
         "oracle_area_integrals": ([d, d, d, d, dp], None),
+        "oracle_det_log": ([d], d),
+        "oracle_det_sincos": ([d, dp, dp], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -160,3 +160,15 @@ def test_oracle_velocity_identity():
         np.testing.assert_allclose(prod[:3], F[:3], atol=1e-9 * max(1, abs(F).max()))
         lam = (prod[5] - F[5]) / (2 * nz)
         np.testing.assert_allclose(prod[3:5], F[3:5] + 2 * lam * n[:2], atol=1e-9 * max(1, abs(F).max()))
+
+
+def test_deterministic_log_sincos_accuracy():
+    # the division draws use series log / sin / cos evaluated identically on both sides;
+    # they must still be accurate to a few ulp
+    rng = np.random.default_rng(0)
+    for u in np.concatenate([rng.random(2000), [2.2e-16, 1e-300, 0.5, 0.999999999999]]):
+        assert abs(orc.LIB.oracle_det_log(u) - math.log(u)) <= 4e-16 * max(1.0, abs(math.log(u)))
+    s, c = orc.ctypes.c_double(), orc.ctypes.c_double()
+    for x in np.concatenate([rng.uniform(-7, 7, 2000), rng.uniform(0, 2 * math.pi, 500)]):
+        orc.LIB.oracle_det_sincos(x, orc.ctypes.byref(s), orc.ctypes.byref(c))
+        assert abs(s.value - math.sin(x)) <= 4e-16 and abs(c.value - math.cos(x)) <= 4e-16

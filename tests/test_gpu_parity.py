@@ -276,6 +276,11 @@ def test_gpu_division_matches_oracle():
 
 @pytest.mark.parametrize("graphs", [1, 0])
 def test_gpu_growth_and_division_loop(graphs):
+    # Per-step parity from identical inputs: each iteration starts both sides from the
+    # oracle's state (cells, neighbor table, clock, lineage).  Free-running trajectories
+    # are not compared here: two daughters of one mother start exactly 2R apart, where
+    # the JKR force jumps at zero overlap (adhesion.hpp:282-370), so a one-ulp
+    # difference in an earlier step decides whether the siblings touch.
     cells = patch_state(400, 33)
     rng = np.random.default_rng(3)
     cells[:, 13] = rng.uniform(4.5, 5.55, size=len(cells))
@@ -286,18 +291,26 @@ def test_gpu_growth_and_division_loop(graphs):
     sim, o = make_pair(cells, cap_cells=3 * n, use_graphs=graphs, max_stepsize=1e-3, iter_update_neighbors=7,
                        **DIV_KW)
     parents = -np.ones(n, dtype=np.int32)
-    sim.set_parents(parents)
     o.set_parents(parents)
-    sim.get_cell_neighbors()
     o.loop_init()
-    for _ in range(4):
-        s = sim.iterate(10)
-        o.iterate(10)
+    divided = 0
+    for it in range(24):
+        sim.upload_cells(o.cells())
+        sim.set_neighbors(o.neighbors())
+        sim.set_clock(*o.clock())
+        sim.set_parents(o.parents())
+        n0 = o.cells().shape[0]
+        s = sim.iterate(1)
+        o.iterate(1)
         cg, co = sim.download_cells(), o.cells()
         assert cg.shape == co.shape
-        assert np.array_equal(cg[:, 0], co[:, 0])
-        assert np.array_equal(sim.parents(), o.parents())
-        assert colwise_relerr(cg, co) <= 1e-8
-        assert s["attempts"] == o.stats()["attempts"]
-        assert s["rebuilds"] == o.stats()["rebuilds"]
-    assert sim.num_cells() > n
+        divided += co.shape[0] - n0
+        assert np.array_equal(cg[:, 0], co[:, 0])                # IDs
+        assert np.array_equal(sim.parents(), o.parents())        # lineage
+        assert colwise_relerr(cg, co) <= 1e-9
+        t, dt, i = sim.clock()
+        to, dto, io = o.clock()
+        assert i == io and abs(dt - dto) <= 1e-10 * dto
+        if i % 7 == 0 or co.shape[0] != n0:                      # a rebuild happened
+            assert np.array_equal(sim.neighbors()[:, :2], o.neighbors()[:, :2])
+    assert divided > 0

@@ -485,27 +485,36 @@ static void enqueue_rebuild(abm_ctx* c)
 // one iteration of the loop body without division: stage-invariant pair
 // forces, then the trial attempt, up to max_tries retries and the accepted
 // final attempt (simulation.hpp:1677-1769), each an early exit when idle
-static void enqueue_pair_force(abm_ctx* c)
+static void enqueue_pair_force(abm_ctx* c, int with_gather)
 {
-    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
-                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta,
+                      c->jkr_radius, c->fcc, c->jbuf, c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED,
+                      c->cap, c->st, with_gather);
+}
+
+// the attempts of one iteration; the first one completes the pair-force sum
+static PairGather loop_gather(abm_ctx* c)
+{
+    PairGather pg = {1, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
+    return pg;
 }
 
 static void enqueue_attempts(abm_ctx* c)
 {
     cudaStream_t st = c->st;
+    PairGather pg = loop_gather(c);
     launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                   c->k0buf, 0.0, 0, c->cap, st);
+                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
     for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
         launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, st);
+                       c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                   c->k0buf, 0.0, 0, c->cap, st);
+                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
 }
 
 static void enqueue_iteration(abm_ctx* c)
 {
-    enqueue_pair_force(c);
+    enqueue_pair_force(c, 0);
     enqueue_attempts(c);
 }
 
@@ -610,10 +619,11 @@ static int build_iteration_graph(abm_ctx* c)
         rc = capture_into(c, body, bd, [&]() { enqueue_division_body_and_rebuild(c); });
         if (rc) return rc;
     }
+    PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
-        enqueue_pair_force(c);
+        enqueue_pair_force(c, 0);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0);
+                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg);
     });
     if (rc) return rc;
     if (retries)
@@ -624,13 +634,13 @@ static int build_iteration_graph(abm_ctx* c)
         std::vector<cudaGraphNode_t> bd;
         rc = capture_into(c, body, bd, [&]() {
             launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                           c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1);
+                           c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg);
         });
         if (rc) return rc;
     }
     rc = capture_into(c, G, deps, [&]() {
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st);
+                       c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg);
     });
     if (rc) return rc;
     cudaError_t inst = cudaGraphInstantiate(&c->g_iter, G, 0);
@@ -938,7 +948,7 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     {
         cudaEvent_t* e = &ev[(size_t)k * 4];
         CK(cudaEventRecord(e[0], st));
-        enqueue_pair_force(c);
+        enqueue_pair_force(c, 0);
         CK(cudaEventRecord(e[1], st));
         enqueue_attempts(c);
         CK(cudaEventRecord(e[2], st));

@@ -91,16 +91,13 @@ __device__ __forceinline__ void closest_params(X3 p1, X3 q1, X3 p2, X3 q2, doubl
 
 struct Dist { double dx, dy, dz, s, t; };
 
-// distances.hpp:206-357 (distBetweenCells): d runs from cell 1 to cell 2.
-__device__ __forceinline__ Dist dist_between_cells(X3 r1, X3 n1, double h1, X3 r2, X3 n2, double h2)
+// distances.hpp:227-337: the near-parallel branch (|n1 . n2| >= 0.9999), kept out
+// of line so the common skew path keeps its registers
+static __device__ __noinline__ Dist dist_near_parallel(X3 r1, X3 n1, double h1, X3 r2, X3 n2, double h2)
 {
-    Dist o;
-    double cos_theta = xdot(n1, n2);
     X3 p1 = xsub(r1, xscale(h1, n1)), q1 = xadd(r1, xscale(h1, n1));
     X3 p2 = xsub(r2, xscale(h2, n2)), q2 = xadd(r2, xscale(h2, n2));
     X3 d; double s, t;
-    if (cos_theta >= 0.9999 || cos_theta <= -0.9999)
-    {
         double s_p1 = nearest_body_coord(r2, n2, h2, p1);
         double s_q1 = nearest_body_coord(r2, n2, h2, q1);
         X3 d_p1 = xsub(xadd(r2, xscale(s_p1, n2)), p1);
@@ -148,15 +145,26 @@ __device__ __forceinline__ Dist dist_between_cells(X3 r1, X3 n1, double h1, X3 r
                 d = xsub(xsub(xadd(r2, xscale(t, n2)), r1), xscale(s, n1));
             }
         }
-    }
-    else
-    {
-        double x, y;
-        closest_params(p1, q1, p2, q2, x, y);
-        s = __dsub_rn(__dmul_rn(__dmul_rn(x, 2.0), h1), h1);
-        t = __dsub_rn(__dmul_rn(__dmul_rn(y, 2.0), h2), h2);
-        d = xsub(xsub(xadd(r2, xscale(t, n2)), r1), xscale(s, n1));
-    }
+    
+    Dist o;
+    o.dx = d.x; o.dy = d.y; o.dz = d.z; o.s = s; o.t = t;
+    return o;
+}
+
+// distances.hpp:206-357 (distBetweenCells): d runs from cell 1 to cell 2.
+__device__ __forceinline__ Dist dist_between_cells(X3 r1, X3 n1, double h1, X3 r2, X3 n2, double h2)
+{
+    double cos_theta = xdot(n1, n2);
+    if (cos_theta >= 0.9999 || cos_theta <= -0.9999) return dist_near_parallel(r1, n1, h1, r2, n2, h2);
+    // skew: CGAL's segment closest points (distances.hpp:338-345)
+    X3 p1 = xsub(r1, xscale(h1, n1)), q1 = xadd(r1, xscale(h1, n1));
+    X3 p2 = xsub(r2, xscale(h2, n2)), q2 = xadd(r2, xscale(h2, n2));
+    double x, y;
+    closest_params(p1, q1, p2, q2, x, y);
+    double s = __dsub_rn(__dmul_rn(__dmul_rn(x, 2.0), h1), h1);
+    double t = __dsub_rn(__dmul_rn(__dmul_rn(y, 2.0), h2), h2);
+    X3 d = xsub(xsub(xadd(r2, xscale(t, n2)), r1), xscale(s, n1));
+    Dist o;
     o.dx = d.x; o.dy = d.y; o.dz = d.z; o.s = s; o.t = t;
     return o;
 }
@@ -309,23 +317,24 @@ __device__ __forceinline__ double epw(const EndPow& w, int e, bool second)
     return second ? half_pow(w.q, w.sq, e) : half_pow(w.p, w.sp, e);
 }
 
-// integrals.hpp:116-140 (integral1) with gamma + 1 = e / 2
-__device__ __forceinline__ double integral1(const EndPow& w, double nz, double h, int e, double ss)
+// integrals.hpp:116-140 (integral1) with gamma + 1 = e / 2; the division by
+// nz (gamma + 1) is a multiplication by inz = 1 / nz and the constant 2 / e
+__device__ __forceinline__ double integral1(const EndPow& w, double inz, double h, int e, double ss)
 {
-    double g1 = 0.5 * e;
-    if (ss > h) return (epw(w, e, false) - epw(w, e, true)) / (nz * g1);
-    else if (ss > -h) return epw(w, e, false) / (nz * g1);
+    const double ig1 = 2.0 / e;
+    if (ss > h) return (epw(w, e, false) - epw(w, e, true)) * inz * ig1;
+    else if (ss > -h) return epw(w, e, false) * inz * ig1;
     return 0.0;
 }
 
 // integrals.hpp:159-184 (integral2) with gamma + 1 = e / 2
-__device__ __forceinline__ double integral2(const EndPow& w, double nz, double h, int e, double ss)
+__device__ __forceinline__ double integral2(const EndPow& w, double inz, double h, int e, double ss)
 {
-    double term1 = integral1(w, nz, h, e + 2, ss);
+    double term1 = integral1(w, inz, h, e + 2, ss);
     double term2 = 0.0;
     if (ss > h) term2 = -h * (epw(w, e, false) + epw(w, e, true));
     else if (ss > -h) term2 = -h * epw(w, e, false);
-    return (term1 + term2) / (nz * (0.5 * e));
+    return (term1 + term2) * inz * (2.0 / e);
 }
 
 // The end overlaps that integral1/2 and areaIntegrals read (integrals.hpp:56-60,
@@ -369,13 +378,14 @@ __device__ __forceinline__ void surface_dEdq(const MechParams& P, bool assume_2d
     }
     const double pf0 = 2 * E0, pf1 = (8. / 3.) * E0 * P.sqrtR, pf2 = 2 * E0 * P.sqrtR;
     double nz2 = nz * nz;
-    double int1 = integral1(w, nz, h, 4, ss);   // delta
-    double int2 = integral1(w, nz, h, 3, ss);   // sqrt(delta)
+    const double inz = 1.0 / nz;
+    double int1 = integral1(w, inz, h, 4, ss);   // delta
+    double int2 = integral1(w, inz, h, 3, ss);   // sqrt(delta)
     rep2 = -pf0 * ((1.0 - nz2) * int1 + P.sqrtR * nz2 * int2);
-    double int3 = integral1(w, nz, h, 6, ss);   // delta^2
-    double int4 = integral2(w, nz, h, 4, ss);   // s delta
-    double int5 = integral1(w, nz, h, 5, ss);   // delta^1.5
-    double int6 = integral2(w, nz, h, 3, ss);   // s sqrt(delta)
+    double int3 = integral1(w, inz, h, 6, ss);   // delta^2
+    double int4 = integral2(w, inz, h, 4, ss);   // s delta
+    double int5 = integral1(w, inz, h, 5, ss);   // delta^1.5
+    double int6 = integral2(w, inz, h, 3, ss);   // s sqrt(delta)
     double d5 = 0.0;
     d5 -= pf0 * nz * int3;
     d5 -= pf0 * (1 - nz2) * int4;
@@ -384,12 +394,12 @@ __device__ __forceinline__ void surface_dEdq(const MechParams& P, bool assume_2d
     rep5 = d5;
     // adhesion
     const double a0 = P.sqrtR / 2, a1 = 2 * M_PI * R, a2 = 2 * P.sqrtR;
-    double i1 = integral1(w, nz, h, 1, ss);     // delta^-1/2
+    double i1 = integral1(w, inz, h, 1, ss);     // delta^-1/2
     bool partial = fabs(ss) < h;
     double term2 = partial ? (a1 / 2) * nz : 0.0;
     adh2 = (a0 * (1 - nz2) * i1 + term2) * sigma0;
-    double i2 = integral1(w, nz, h, 3, ss);     // delta^1/2
-    double i3 = integral2(w, nz, h, 1, ss);     // s delta^-1/2
+    double i2 = integral1(w, inz, h, 3, ss);     // delta^1/2
+    double i3 = integral2(w, inz, h, 1, ss);     // s delta^-1/2
     double i4 = (ss > h) ? 2 * h : ((ss > -h) ? ss + h : 0.0);   // integral4
     double term4 = partial ? (a1 / 2) * (R - rz) : 0.0;
     double e5 = 0.0;
@@ -408,19 +418,20 @@ __device__ __forceinline__ void area_integrals(const MechParams& P, double nz, d
     double int4 = (ss > h) ? 2 * h : ((ss > -h) ? ss + h : 0.0);
     double int5 = (-h < ss && ss <= h) ? (ss * ss - h * h) / 2.0 : 0.0;
     double int6 = (ss > h) ? 2 * h * h * h / 3.0 : ((ss > -h) ? (ss * ss * ss + h * h * h) / 3.0 : 0.0);
-    double int1a = integral1(w, nz, h, 3, ss);
-    double int1b = integral1(w, nz, h, 5, ss);
-    double int1c = integral1(w, nz, h, 7, ss);
+    const double inz = 1.0 / nz;
+    double int1a = integral1(w, inz, h, 3, ss);
+    double int1b = integral1(w, inz, h, 5, ss);
+    double int1c = integral1(w, inz, h, 7, ss);
     double onz = 1 - nz * nz;
     double piRnz2 = M_PI * R * nz * nz;
     A1 = P.sqrtR * onz * int1a + piRnz2 * int4;
     const double p3 = epw(w, 3, false), q3 = epw(w, 3, true);
     double term2 = -h * (p3 + q3);
-    double int2a = (int1b + term2) / (1.5 * nz);
+    double int2a = (int1b + term2) * inz * (1.0 / 1.5);
     A2 = P.sqrtR * onz * int2a + piRnz2 * int5;
     term2 = -h * (epw(w, 5, false) + epw(w, 5, true));
-    double int2b = (int1c + term2) / (2.5 * nz);
-    double int3 = (2 * int2b + h * h * (p3 - q3)) / (1.5 * nz);
+    double int2b = (int1c + term2) * inz * (1.0 / 2.5);
+    double int3 = (2 * int2b + h * h * (p3 - q3)) * inz * (1.0 / 1.5);
     A3 = P.sqrtR * onz * int3 + piRnz2 * int6;
 }
 
@@ -486,8 +497,9 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
             double drxy = sqrt(d01.x * d01.x + d01.y * d01.y);
             double dnxy = sqrt(d23.y * d23.y + d45.x * d45.x);
             double friction_norm = (A1 * drxy + A2 * dnxy) * (eta1 / R);
-            double max_norm = (1 - nz * nz) * integral1(w, nz, h, 4, ss)
-                            + P.sqrtR * nz * nz * integral1(w, nz, h, 3, ss);
+            const double inz = 1.0 / nz;
+            double max_norm = (1 - nz * nz) * integral1(w, inz, h, 4, ss)
+                            + P.sqrtR * nz * nz * integral1(w, inz, h, 3, ss);
             max_norm *= (2 * E0 * coul);
             if (friction_norm > max_norm) eta1 = max_norm * R / (A1 * drxy + A2 * dnxy);
         }
@@ -496,19 +508,22 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         const double c4 = c2 * l * l / 12;
         const double c3 = c4 + (eta1 / R) * A3;
         const double c5 = (eta1 / R) * A2;
-        const double term1 = c3 - (c5 * c5 / c1);
-        const double w4 = f[3] - f[0] * (c5 / c1);
-        const double w5 = f[4] - f[1] * (c5 / c1);
-        const double nx2 = nx / term1, ny2 = ny / term1, nz2 = nz / c4;
+        const double ic1 = 1.0 / c1, ic4 = 1.0 / c4;
+        const double c5c1 = c5 * ic1;
+        const double term1 = c3 - c5 * c5c1;
+        const double it1 = 1.0 / term1;
+        const double w4 = f[3] - f[0] * c5c1;
+        const double w5 = f[4] - f[1] * c5c1;
+        const double nx2 = nx * it1, ny2 = ny * it1, nz2 = nz * ic4;
         const double alpha = 2 * ((nx * nx2 + ny * ny2) + nz * nz2);
         const double beta = -((w4 * nx2 + w5 * ny2) + f[5] * nz2);
         const double lambda = beta / alpha;
-        v[5] = (f[5] + 2 * nz * lambda) / c4;
-        v[4] = (w5 + 2 * ny * lambda) / term1;
-        v[3] = (w4 + 2 * nx * lambda) / term1;
+        v[5] = (f[5] + 2 * nz * lambda) * ic4;
+        v[4] = (w5 + 2 * ny * lambda) * it1;
+        v[3] = (w4 + 2 * nx * lambda) * it1;
         v[2] = f[2] / c2;
-        v[1] = (f[1] - c5 * v[4]) / c1;
-        v[0] = (f[0] - c5 * v[3]) / c1;
+        v[1] = (f[1] - c5 * v[4]) * ic1;
+        v[0] = (f[0] - c5 * v[3]) * ic1;
     }
 }
 

@@ -644,14 +644,15 @@ __global__ void __launch_bounds__(PF_T) k_pair_gather(const int* __restrict__ ro
 
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
                        const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
-                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st)
+                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
+                       int with_gather)
 {
     int blocks = max(cdiv((long long)cap_cells * lanes, PF_T), 1);
 #define PF_CASE(G) \
     if (lanes == G) { \
         if (mixed) k_pair_force<G, true><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
         else k_pair_force<G, false><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
-        k_pair_gather<G><<<blocks, PF_T, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc); \
+        if (with_gather) k_pair_gather<G><<<blocks, PF_T, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc); \
         return; }
     PF_CASE(4) PF_CASE(8) PF_CASE(16) PF_CASE(32)
 #undef PF_CASE
@@ -725,12 +726,11 @@ __device__ __forceinline__ void cell_velocity(const StepParams& sp, bool a2, con
 // -dE/dq of the pair forces (getConservativeForces, mechanics.hpp:1768) plus the
 // attempt's noise (mechanics.hpp:2489-2510, forces += noise at :2066)
 template <bool NOISE>
-__device__ __forceinline__ void base_force(const StepParams& sp, const Gen6* __restrict__ fcc, int iter,
-                                           int attempt, int i, double f0[6])
+__device__ __forceinline__ void base_force(const StepParams& sp, const Gen6& cc, int iter, int attempt, int i,
+                                           double f0[6])
 {
-    const double2* cp = reinterpret_cast<const double2*>(fcc + i);
-    double2 a = __ldg(cp), b = __ldg(cp + 1), c = __ldg(cp + 2);
-    f0[0] = -a.x; f0[1] = -a.y; f0[2] = -b.x; f0[3] = -b.y; f0[4] = -c.x; f0[5] = -c.y;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) f0[c] = -cc.f[c];
     if (NOISE)
     {
         for (int k = 0; k < 3; ++k)
@@ -742,6 +742,33 @@ __device__ __forceinline__ void base_force(const StepParams& sp, const Gen6* __r
             f0[2 * k + 1] += -sp.noise_max[2 * k + 1] + 2 * sp.noise_max[2 * k + 1] * u1;
         }
     }
+}
+
+__device__ __forceinline__ Gen6 load_gen6(const Gen6* __restrict__ g, int i)
+{
+    const double2* p = reinterpret_cast<const double2*>(g + i);
+    double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    Gen6 o;
+    o.f[0] = a.x; o.f[1] = a.y; o.f[2] = b.x; o.f[3] = b.y; o.f[4] = c.x; o.f[5] = c.y;
+    return o;
+}
+
+// dE/dq of cell i: the share of its lower neighbors (written by k_pair_force) plus
+// the shares its higher-index neighbors left in the upper part of its row
+__device__ __forceinline__ Gen6 gather_pair_force(const Gen6* fcc, const int* __restrict__ row_ptr,
+                                                  const int* __restrict__ lower_end,
+                                                  const double4* __restrict__ jbuf, int i)
+{
+    Gen6 f = fcc[i];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = lower_end[i]; k < row_ptr[i + 1]; ++k)
+    {
+        double4 js = jbuf[k];
+        acc[0] -= js.x; acc[1] -= js.y; acc[2] -= js.z;
+        acc[3] -= js.w * js.x; acc[4] -= js.w * js.y; acc[5] -= js.w * js.z;
+    }
+    for (int c = 0; c < 6; ++c) f.f[c] += acc[c];
+    return f;
 }
 
 // Step-size controller, run once per attempt by the last block
@@ -802,10 +829,10 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
 // iteration (y0 and the pair forces do not change), so the trial stores it in k0buf
 // and the retries and the final attempt read it back.
 template <int S, int KIND, bool NOISE>
-__global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* __restrict__ fcc,
+__global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
-                                                 unsigned long long cond, int use_cond)
+                                                 unsigned long long cond, int use_cond, PairGather pg)
 {
     __shared__ double sh_max[AT_T / 32];
     __shared__ bool last;
@@ -840,6 +867,9 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     }
     else { dt = eval_dt; attempt = eval_attempt; }
 
+    // the first attempt of an iteration completes the pair force (k_pair_force left
+    // only the lower-neighbor share); the trial writes the total back for the rest
+    const bool do_gather = pg.fused && (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran));
     double local_max = 0.0;
     bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -848,8 +878,15 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
         const double l = phys[i].l, eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
         const bool a2 = y0[5] < sp.mp.nz_threshold;
+        Gen6 cc;
+        if (do_gather)
+        {
+            cc = gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
+            if (KIND == MODE_TRIAL) pg.fcc_w[i] = cc;
+        }
+        else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);
         double f0[6];
-        base_force<NOISE>(sp, fcc, iter, attempt, i, f0);
+        base_force<NOISE>(sp, cc, iter, attempt, i, f0);
         double k[S][6];
         if (load_k0)
         {
@@ -966,9 +1003,9 @@ template <int S, bool NOISE>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
                              Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
-                             unsigned long long cond, int use_cond)
+                             unsigned long long cond, int use_cond, PairGather pg)
 {
-#define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond
+#define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg
     switch (kind)
     {
         case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
@@ -982,12 +1019,12 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
-                    unsigned long long cond, int use_cond)
+                    unsigned long long cond, int use_cond, PairGather pg)
 {
     int blocks = max(cdiv(cap_cells, AT_T), 1);
 #define AT_CASE(S) case S: \
-        if (sp.noise_on) launch_attempt_s<S, true>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond); \
-        else launch_attempt_s<S, false>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond); \
+        if (sp.noise_on) launch_attempt_s<S, true>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
+        else launch_attempt_s<S, false>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
         break;
     switch (sp.s)
     {
@@ -1008,7 +1045,7 @@ __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restric
         const double y[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
         const bool a2 = y[5] < sp.mp.nz_threshold;
         double f0[6];
-        base_force<false>(sp, fcc, 0, 0, i, f0);
+        base_force<false>(sp, load_gen6(fcc, i), 0, 0, i, f0);
         Gen6 out;
         const Phys ph = phys[i];
         cell_velocity(sp, a2, y, ph.l, g.h, ph.eta0, ph.eta1, ph.sigma0, vel + i, f0, out.f);

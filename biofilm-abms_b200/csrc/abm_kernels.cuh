@@ -79,6 +79,16 @@ struct BuildParams {
     int cap_per_cell;
 };
 
+// Where an attempt finds the upper half of the pair force when it completes the
+// sum itself (fused = 1, the loop); fused = 0 when fcc already holds the total.
+struct PairGather {
+    int fused;
+    const int* row_ptr;
+    const int* lower_end;
+    const double4* jbuf;
+    Gen6* fcc_w;
+};
+
 // ---- launch wrappers (abm_kernels.cu) ----
 void launch_cells_from_colmajor(const double* cm, int n, int ncols, int ld, int has_gamma,
                                 Geom* geom, Vel* vel, Phys* phys, cudaStream_t st);
@@ -107,7 +117,8 @@ size_t scan_block_sums_size(int cap);
 // partner's share gathered from the reverse slots (jbuf, one double4 per CSR entry)
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
                        const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
-                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st);
+                       Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
+                       int with_gather = 1);
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
                     int cap_cells, cudaStream_t st);
 
@@ -118,7 +129,7 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
-                    unsigned long long cond = 0, int use_cond = 0);
+                    unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0});
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
                        cudaStream_t st);

@@ -143,6 +143,8 @@ def _load():
         "abm_divide": ([vp, ip], i),
         "abm_last_division_tries": ([vp, ip], i),
         "abm_graph_info": ([vp], ctypes.c_char_p),
+        "abm_cell_cell_forces_noalloc": ([P(AbmParams), vp, i, i, i, vp, vp, i, dp, dp, i, vp, vp], i),
+        "abm_noalloc_last_error": ([], ctypes.c_char_p),
         "abm_iterate": ([vp, i, i, P(AbmStats)], i),
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
@@ -160,7 +162,8 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
-            "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info").split()
+            "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
+            "abm_cell_cell_forces_noalloc abm_noalloc_last_error").split()
 
 
 def _dptr(a):

@@ -162,6 +162,38 @@ const char* abm_graph_info(const abm_ctx* ctx);
  * (no reference counterpart; measurement only). */
 int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);
 
+/* ---------------------------------------------------------------------------
+ * Cell-cell forces without device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: their device memory is owned by
+ * another allocator (a framework's caching pool or a fixed budget), or they
+ * cannot take the device-wide synchronisation of cudaMalloc/cudaFree inside a
+ * step loop.  Same result as abm_cell_cell_forces (dE/dq, mechanics.hpp:
+ * 1209-1659) for a neighbor set given in CSR form: d_row_ptr[n + 1] and
+ * d_col[n_entries] list each cell's neighbors in both directions, each row
+ * sorted ascending.  d_cells (n x ncols, leading dimension ld), the CSR arrays
+ * and d_dEdq (n x 6, leading dimension n) are device buffers the caller owns;
+ * jkr_delta / jkr_radius are host arrays (ignored without adhesion).  Work is
+ * enqueued on `stream` (a cudaStream_t, 0 = legacy default stream); results are
+ * ready when the stream reaches that point.
+ *
+ * Scratch lives in one fixed __device__ array of about 21 MB that every GPU
+ * loading this library holds until the process exits.  Limits per call:
+ * n <= ABM_NOALLOC_MAX_CELLS, n_entries <= ABM_NOALLOC_MAX_ENTRIES; larger
+ * inputs return ABM_ERR_CAPACITY.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current: make it
+ * before any stream capture.  All calls share the array, so calls that overlap
+ * on the GPU race; serialise them.  The call allocates nothing.
+ * abm_noalloc_last_error() describes the last failure of this thread.
+ * ------------------------------------------------------------------------- */
+#define ABM_NOALLOC_MAX_CELLS 32768
+#define ABM_NOALLOC_MAX_ENTRIES 524288
+int abm_cell_cell_forces_noalloc(const abm_params* params, const double* d_cells, int n, int ncols, int ld,
+                                 const int* d_row_ptr, const int* d_col, int n_entries,
+                                 const double* jkr_delta, const double* jkr_radius, int jkr_n,
+                                 double* d_dEdq, void* stream);
+const char* abm_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark: accepted cell-steps/s of the 3-D mechanics step at 100k cells.
+"""Benchmark: accepted cell-steps/s of the 3-D mechanics step at 100k cells,
+chosen configuration vs the plain FP64 GPU path at equal RK tolerance.
 
 Workload (one "step" = one accepted iteration of the runSimulation loop body,
 ABM-3d/ABM-3d-cpp/include/simulation.hpp:1617-1864): 100,000 cells, centres
@@ -8,8 +9,14 @@ uniform in a 300 um disk with z in [R, 10] um, no growth or division, Heun-Euler
 isotropic JKR cell-cell adhesion (gamma = 100) and cell-surface Hertz + JKR.
 Inputs are seeded synthetic states (no dataset is involved).
 
-  value     device-resident throughput, CUDA events on the context stream, L2
-            flushed (256 MB write) between timed steps, max over ranks
+  chosen    mixed precision (segment distance and pair force in FP32, the rest
+            FP64) and the learned step-size controller (the network's proposal is
+            one RK attempt, accepted when its embedded error passes)
+  plain     FP64 everywhere with the reference controller (trial + final re-run)
+
+  value     chosen: device-resident throughput, CUDA events on the context stream,
+            L2 flushed (256 MB write) between timed steps, max over ranks;
+            `plain` holds the same figures for the plain path
   e2e       through the C ABI with pinned host buffers: upload cells -> one
             iteration -> download cells, every step
   roofline  the dominant kernel's algorithmic bytes per launch / its
@@ -51,7 +58,9 @@ def parse_args(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--tableau", type=int, default=1, help="1 HE21, 2 BS32, 3 RKF45, 4 DP54")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--variant", default="chosen", choices=["chosen", "plain"],
+                    help="headline configuration; the other one is timed beside it unless --only")
+    ap.add_argument("--only", action="store_true", help="time the headline variant only")
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -171,10 +180,24 @@ def workload(n, seed):
     return workloads.biofilm_3d(n=n, seed=seed, disk_radius=radius, p_contact=P_CONTACT)
 
 
-def sim_params(args, n):
-    return dict(cap_cells=n, integration_mode=args.tableau,
-                precision=1 if args.precision == "mixed" else 0, pair_lanes=args.lanes,
-                max_stepsize=1e-6, max_error_allowed=1e-8, iter_update_neighbors=100)
+VARIANTS = {"plain": dict(precision=0, controller=0), "chosen": dict(precision=1, controller=1)}
+
+
+def sim_params(args, n, variant="plain"):
+    d = dict(cap_cells=n, integration_mode=args.tableau, pair_lanes=args.lanes,
+             max_stepsize=1e-6, max_error_allowed=1e-8, iter_update_neighbors=100)
+    d.update(VARIANTS[variant])
+    return d
+
+
+def stepsize_weights():
+    """The shipped step-size network (trained on the GPU from reference-controller
+    logs, abm_b200/stepsize.py); trained here on the spot if it is missing."""
+    from abm_b200 import stepsize
+    if os.path.exists(stepsize.WEIGHTS_FILE):
+        return stepsize.load(), "shipped weights (%s)" % os.path.basename(stepsize.WEIGHTS_FILE)
+    w, info = stepsize.train_protocol(stepsize.default_runs(), n_iters=1500, epochs=150)
+    return w, "trained at start on the GPU: %s" % json.dumps(info)
 
 
 def config(args, info, extra=None):
@@ -182,7 +205,9 @@ def config(args, info, extra=None):
                      (args.n, {1: "HE21", 2: "BS32", 3: "RKF45", 4: "DP54"}[args.tableau]),
          "cells": args.n, "tableau": {1: "HE21", 2: "BS32", 3: "RKF45", 4: "DP54"}[args.tableau],
          "rk_tol": 1e-8, "max_stepsize_h": 1e-6, "iter_update_neighbors": 100,
-         "adhesion": "JKR isotropic gamma=100", "precision": args.precision,
+         "adhesion": "JKR isotropic gamma=100", "variant": args.variant,
+         "precision": "mixed (FP32 segment distance + pair force)" if args.variant == "chosen" else "fp64",
+         "controller": "learned (network proposal, error test)" if args.variant == "chosen" else "reference",
          "mean_contacts_per_cell": round(info["mean_contacts_per_cell"], 3),
          "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas"}
     if extra:
@@ -200,6 +225,11 @@ def attempt_bytes(n, final):
     # geometry 64 + stored velocity 48 + physical record 64 + pair force 48 read;
     # the accepted attempt also writes geometry 64 + velocity 48 + length 8
     return n * (224 + (120 if final else 0))
+
+
+def commit_bytes(n):
+    # candidate geometry 64 + velocity 48 read, state geometry 64 + velocity 48 + length 8 written
+    return n * (112 + 120)
 
 
 def load_traffic():
@@ -226,7 +256,7 @@ def cpu_reference_rate(cells, args, steps, n_threads):
     import abm_b200
     import oracle_ref as orc
     _, pd = abm_b200.make_params(**{k: v for k, v in sim_params(args, args.n).items()
-                                   if k not in ("cap_cells", "precision", "pair_lanes")})
+                                   if k not in ("cap_cells", "precision", "pair_lanes", "controller")})
     o = orc.Oracle(pd, jkr=orc.jkr_table(0.8, 0.5, 3900.0, 100.0, 100), n_threads=n_threads)
     o.set_cells(cells)
     t0 = time.perf_counter()
@@ -281,28 +311,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args):
-    import numpy as np
-    import torch
+def make_sim(args, variant, cells, weights):
     import abm_b200
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if world > 1:
-        dist_init("nccl")
-    cells, info = workload(args.n, SEED + rank)
-    sim = abm_b200.Simulation(**sim_params(args, args.n))
+    sim = abm_b200.Simulation(**sim_params(args, args.n, variant))
     sim.upload_cells(cells)
+    if VARIANTS[variant]["controller"] == 1:
+        sim.set_stepsize_weights(weights)
     pairs = sim.get_cell_neighbors()
-    stream = torch.cuda.ExternalStream(sim.stream, device=device)
-    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
+    return sim, pairs
 
-    # warm-up (untimed)
+
+def time_variant(sim, args, stream, flush, world, device, local):
+    """W untimed iterations, then K timed ones (CUDA events on the context stream,
+    L2 flushed before each), max over ranks."""
+    import torch
     sim.iterate(max(args.warmup, 0), stats=False)
     sim.synchronize()
     s0 = sim.stats()
-
-    # timed region: device-resident, L2 flushed between steps
     sampler = ClockSampler(local)
     sampler.start()
     barrier(world)
@@ -318,74 +343,167 @@ def run_b200(args):
     barrier(world)
     clocks = sampler.stop()
     sim.synchronize()
-    ms_total = sum(a.elapsed_time(b) for a, b in ev)
-    ms_total = reduce_max(ms_total, device, world)
+    ms_total = reduce_max(sum(a.elapsed_time(b) for a, b in ev), device, world)
     s1 = sim.stats()
-    iters = s1["iterations"] - s0["iterations"]
-    attempts = s1["attempts"] - s0["attempts"]
-    rebuilds = s1["rebuilds"] - s0["rebuilds"]
-    value = world * args.n * args.steps / (ms_total / 1000.0)
-    # per iteration: pair force, trial, max_tries retries (exit at once when idle), final;
-    # per rebuild: bbox, bin count, 3 scan passes, scatter, pair build, 3 scan passes, CSR fill, counter
-    launches_per_iter = 3 + sim.params.max_tries_update_stepsize
-    gpu_launches = args.steps * launches_per_iter + rebuilds * 12
+    d = {k: s1[k] - s0[k] for k in ("iterations", "attempts", "retries", "rejected", "rebuilds")}
+    d.update(ms_total=ms_total, clocks=clocks, t_sim_h=s1["t"] - s0["t"])
+    return d
 
-    # per-kernel event timing for the roofline (same iteration loop without the graph)
+
+def kernel_groups(sim, args, variant):
+    """Per-kernel-group event timing (the iteration without the graph) and algorithmic bytes."""
     prof = sim.profile_iterations(max(1, min(args.profile_steps, args.steps)))
     n_dir = 2 * sim.stats()["n_pairs"]
     pf_ms = prof["pair_force_ms"] / prof["pair_force_launches"]
     at_ms = prof["attempt_ms"] / prof["iterations"]
+    if VARIANTS[variant]["controller"] == 1:
+        # network proposal + one RK attempt + commit of the accepted candidate
+        at_name, at_bytes = "k_attempt(proposal+commit)", attempt_bytes(args.n, True)
+    else:
+        at_name, at_bytes = "k_attempt(trial+final)", attempt_bytes(args.n, False) + attempt_bytes(args.n, True)
+    kernels = {"k_pair_force": (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
+    return kernels, prof["rebuild_ms"] / max(prof["rebuild_launches"], 1)
+
+
+def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
     peak, peak_kind = measured_peak_hbm()
     traffic = load_traffic()
-    kernels = {
-        "k_pair_force": (pair_force_bytes(args.n, n_dir), pf_ms),
-        "k_attempt(trial+final)": (attempt_bytes(args.n, False) + attempt_bytes(args.n, True), at_ms),
-    }
     dom = max(kernels, key=lambda k: kernels[k][1])
     b, ms = kernels[dom]
     achieved = b / (ms / 1000.0) / 1e9
-    tr = traffic.get(dom, {}).get("bytes_per_launch")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": tr, "kernel": dom,
-                "algorithmic_bytes_per_launch": b, "ms_per_launch": ms, "peak_source": peak_kind,
-                "other_kernels": {k: {"ms_per_launch": v[1], "algorithmic_bytes_per_launch": v[0],
-                                      "achieved_gbs": v[0] / (v[1] / 1000.0) / 1e9}
-                                  for k, v in kernels.items() if k != dom},
-                "rebuild_ms_per_rebuild": prof["rebuild_ms"] / max(prof["rebuild_launches"], 1)}
+    tr = traffic.get(dom + traffic_key_suffix, {}).get("bytes_per_launch")
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": tr, "kernel": dom,
+            "algorithmic_bytes_per_launch": b, "ms_per_launch": ms, "peak_source": peak_kind,
+            "other_kernels": {k: {"ms_per_launch": v[1], "algorithmic_bytes_per_launch": v[0],
+                                  "achieved_gbs": v[0] / (v[1] / 1000.0) / 1e9}
+                              for k, v in kernels.items() if k != dom},
+            "rebuild_ms_per_rebuild": rebuild_ms}
 
-    # e2e through the C ABI with pinned host buffers
-    ncols = cells.shape[1]
-    host = torch.empty((ncols, args.n), dtype=torch.float64, pin_memory=True)
-    host_np = host.numpy()
-    host_np[:] = sim.download_cells().T
-    ptr = host.data_ptr()
-    e2e_steps = max(1, min(args.steps, 200))
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    barrier(world)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        sim.upload_cells_raw(ptr, args.n, ncols, args.n)
-        sim.iterate(1, stats=False)
-        sim.download_cells_raw(ptr, args.n)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = reduce_max(e0.elapsed_time(e1), device, world)
-    e2e_value = world * args.n * e2e_steps / (e2e_ms / 1000.0)
-    nbytes = args.n * ncols * 8
 
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+def launches(variant, t):
+    # per iteration: pair force (+ the network's proposal), every RK attempt, and
+    # (learned) the commit of an accepted proposal; 13 kernels per neighbor rebuild
+    if VARIANTS[variant]["controller"] == 1:
+        return 2 * t["iterations"] + t["attempts"] + (t["iterations"] - t["rejected"]) + 13 * t["rebuilds"]
+    return t["iterations"] + t["attempts"] + 13 * t["rebuilds"]
+
+
+def relerr(a, b):
+    """(max, rms) over columns of normwise relative errors |a - b| / |b|."""
+    import numpy as np
+    a, b = np.asarray(a), np.asarray(b)
+    mx, rms = 0.0, 0.0
+    for c in range(b.shape[1]):
+        sb = np.abs(b[:, c]).max()
+        if sb == 0:
+            continue
+        mx = max(mx, float(np.abs(a[:, c] - b[:, c]).max() / sb))
+        rms = max(rms, float(np.sqrt(np.mean((a[:, c] - b[:, c]) ** 2) / np.mean(b[:, c] ** 2))))
+    return {"max_rel": mx, "rms_rel": rms}
+
+
+def mixed_precision_errors(args, cells):
+    """Per-step error of the mixed-precision path against the FP64 path (which
+    matches the CPU oracle to <= 1e-10): pair forces dE/dq, velocities, and one RK
+    step's position/orientation increment."""
+    import abm_b200
+    out = {}
+    sims = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        sim = abm_b200.Simulation(cap_cells=args.n, integration_mode=args.tableau, precision=prec,
+                                  max_stepsize=1e-6, max_error_allowed=1e-8)
+        sim.upload_cells(cells)
+        sim.get_cell_neighbors()
+        f = sim.cell_cell_forces()
+        v = sim.get_velocities()
+        c1, _, e = sim.step_runge_kutta_adaptive(1e-6)
+        sims[name] = (f, v, c1[:, 1:7] - cells[:, 1:7], e)
+        sim.close()
+    f64, v64, d64, e64 = sims["fp64"]
+    f32, v32, d32, e32 = sims["mixed"]
+    out["pair_forces"] = relerr(f32, f64)
+    out["velocities"] = relerr(v32, v64)
+    out["step_increment_dt_1e-6"] = relerr(d32, d64)
+    out["scaled_error_norm"] = {"fp64": e64, "mixed": e32}
+    out["against"] = "FP64 path of this library (matches the CPU oracle to <= 1e-10)"
+    return out
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        dist_init("nccl")
+    cells, info = workload(args.n, SEED + rank)
+    weights, weights_note = stepsize_weights()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    head = args.variant
+    other = None if args.only else ("plain" if head == "chosen" else "chosen")
+    results = {}
+    for variant in [v for v in (other, head) if v]:
+        sim, pairs = make_sim(args, variant, cells, weights)
+        stream = torch.cuda.ExternalStream(sim.stream, device=device)
+        t = time_variant(sim, args, stream, flush, world, device, local)
+        t["pairs"] = pairs
+        t["value"] = world * args.n * args.steps / (t["ms_total"] / 1000.0)
+        t["kernels"], t["rebuild_ms"] = kernel_groups(sim, args, variant)
+        if variant == head:
+            # e2e through the C ABI with pinned host buffers
+            ncols = cells.shape[1]
+            host = torch.empty((ncols, args.n), dtype=torch.float64, pin_memory=True)
+            host.numpy()[:] = sim.download_cells().T
+            ptr = host.data_ptr()
+            e2e_steps = max(1, min(args.steps, 200))
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            barrier(world)
+            e0.record(stream)
+            for _ in range(e2e_steps):
+                sim.upload_cells_raw(ptr, args.n, ncols, args.n)
+                sim.iterate(1, stats=False)
+                sim.download_cells_raw(ptr, args.n)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = reduce_max(e0.elapsed_time(e1), device, world)
+            nbytes = args.n * ncols * 8
+            t["e2e"] = {"value": world * args.n * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
+                        "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": e2e_steps}
+        sim.close()
+        results[variant] = t
+
+    h = results[head]
+    line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": h["ms_total"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32" if head == "chosen" else "f64",
             "data": "synthetic (seeded biofilm state, p_contact=%g)" % P_CONTACT,
-            "config": config(args, info, {"pairs_per_cell": round(pairs / args.n, 3),
-                                          "rk_evals_per_step": round(attempts / max(iters, 1), 3),
-                                          "rebuilds_in_timed_region": rebuilds}),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
-            "gpu_launches": gpu_launches, "roofline": roofline,
-            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+            "config": config(args, info, {"pairs_per_cell": round(h["pairs"] / args.n, 3),
+                                          "rk_evals_per_step": round(h["attempts"] / max(h["iterations"], 1), 3),
+                                          "rejected_first_attempts": h["rejected"],
+                                          "rebuilds_in_timed_region": h["rebuilds"],
+                                          "simulated_h_in_timed_region": h["t_sim_h"],
+                                          "stepsize_network": weights_note if head == "chosen" else None}),
+            "e2e": h["e2e"], "gpu_launches": launches(head, h),
+            "roofline": roofline(h["kernels"], h["rebuild_ms"], "[mixed]" if head == "chosen" else ""),
+            "clocks": {k: h["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    if other:
+        o = results[other]
+        line[other] = {"value": o["value"], "ms_per_step": o["ms_total"] / args.steps,
+                       "rk_evals_per_step": round(o["attempts"] / max(o["iterations"], 1), 3),
+                       "rejected_first_attempts": o["rejected"], "simulated_h_in_timed_region": o["t_sim_h"],
+                       "kernels_ms_per_launch": {k: v[1] for k, v in o["kernels"].items()},
+                       "clocks": {k: o["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+        chosen, plain = results["chosen"], results["plain"]
+        line["chosen_over_plain"] = {"accepted_cell_steps": chosen["value"] / plain["value"],
+                                     "simulated_time_per_s": (chosen["t_sim_h"] / chosen["ms_total"]) /
+                                                             (plain["t_sim_h"] / plain["ms_total"])}
+    if rank == 0 and world == 1 and "chosen" in results:
+        line["mixed_precision_error"] = mixed_precision_errors(args, cells)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores, model = cpu_info()
         v, sample, extra = cpu_reference_rate(cells, args, args.cpu_steps, cores)
@@ -393,7 +511,6 @@ def run_b200(args):
                                 "sample": sample + " on " + model}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sim.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

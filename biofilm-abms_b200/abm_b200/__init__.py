@@ -56,6 +56,7 @@ class AbmParams(ctypes.Structure):
         ("precision", ctypes.c_int), ("cap_cells", ctypes.c_int),
         ("cap_neighbors_per_cell", ctypes.c_int), ("pair_lanes", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
+        ("controller", ctypes.c_int), ("stepsize_log_capacity", ctypes.c_int),
     ]
 
 
@@ -65,6 +66,7 @@ class AbmStats(ctypes.Structure):
         ("retries", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong),
         ("divisions", ctypes.c_longlong), ("t", ctypes.c_double), ("dt", ctypes.c_double),
         ("last_max_error", ctypes.c_double), ("n_cells", ctypes.c_int), ("n_pairs", ctypes.c_int),
+        ("rejected", ctypes.c_longlong), ("log_rows", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -93,7 +95,7 @@ DEFAULTS = dict(
     max_nxy_noise=0.0, max_nz_noise=0.0, cell_surface_coulomb_coeff=1.0, no_surface=0,
     growth_mean=0.0, growth_std=0.0, daughter_length_std=0.0, daughter_angle_xy_bound=0.0,
     daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
-    cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1,
+    cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
 )
 
 
@@ -116,7 +118,7 @@ def _load():
     lib = ctypes.CDLL(LIB_PATH)
     P = ctypes.POINTER
     d, i, vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
-    dp, ip = P(d), P(i)
+    dp, ip, fp = P(d), P(i), P(ctypes.c_float)
     sig = {
         "abm_create": ([P(AbmParams), P(vp)], i),
         "abm_destroy": ([vp], i),
@@ -148,6 +150,14 @@ def _load():
         "abm_iterate": ([vp, i, i, P(AbmStats)], i),
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
+        "abm_stepsize_set_weights": ([vp, fp, i], i),
+        "abm_stepsize_get_weights": ([vp, fp, i], i),
+        "abm_stepsize_get_log": ([vp, fp, i, ip], i),
+        "abm_stepsize_clear_log": ([vp], i),
+        "abm_mlp_forward": ([fp, fp, i, fp], i),
+        "abm_mlp_grad": ([fp, fp, fp, i, fp, fp], i),
+        "abm_mlp_train": ([fp, fp, fp, i, i, ctypes.c_float, ctypes.c_uint, fp], i),
+        "abm_mlp_last_error": ([], ctypes.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -163,7 +173,12 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
             "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
-            "abm_cell_cell_forces_noalloc abm_noalloc_last_error").split()
+            "abm_cell_cell_forces_noalloc abm_noalloc_last_error abm_stepsize_set_weights "
+            "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
+            "abm_mlp_grad abm_mlp_train abm_mlp_last_error").split()
+
+CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
+MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
 
 
 def _dptr(a):
@@ -372,3 +387,65 @@ class Simulation:
         s = AbmStats()
         self._check(LIB.abm_get_stats(self._ctx, ctypes.byref(s)), "abm_get_stats")
         return s.as_dict()
+
+    # ---- step-size network (no reference counterpart) ----
+    def set_stepsize_weights(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float32).ravel()
+        self._check(LIB.abm_stepsize_set_weights(self._ctx, _fptr(w), w.size), "abm_stepsize_set_weights")
+
+    def stepsize_weights(self):
+        w = np.zeros(MLP_NPARAM, dtype=np.float32)
+        self._check(LIB.abm_stepsize_get_weights(self._ctx, _fptr(w), w.size), "abm_stepsize_get_weights")
+        return w
+
+    def stepsize_log(self):
+        """Logged rows, oldest first: (n, 40) float32 (features, ln(dt_max/dt_first),
+        ln(dt_first/dt_prev), log10 E of the first attempt, passed, error-model baseline b)."""
+        cap = max(int(self.params.stepsize_log_capacity), 0)
+        rows = np.zeros((max(cap, 1), MLP_LOG_COLS), dtype=np.float32)
+        n = ctypes.c_int()
+        self._check(LIB.abm_stepsize_get_log(self._ctx, _fptr(rows), cap, ctypes.byref(n)), "abm_stepsize_get_log")
+        return rows[:n.value].copy()
+
+    def clear_stepsize_log(self):
+        self._check(LIB.abm_stepsize_clear_log(self._ctx), "abm_stepsize_clear_log")
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _mlp_check(rc, what):
+    if rc != 0:
+        raise RuntimeError("%s failed (%d): %s" % (what, rc, LIB.abm_mlp_last_error().decode()))
+
+
+def mlp_forward(weights, X):
+    """Network output ln(dt/dt_prev) for each row of X (n x 32), on the GPU."""
+    w = np.ascontiguousarray(weights, dtype=np.float32).ravel()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros(X.shape[0], dtype=np.float32)
+    _mlp_check(LIB.abm_mlp_forward(_fptr(w), _fptr(X), X.shape[0], _fptr(Y)), "abm_mlp_forward")
+    return Y
+
+
+def mlp_grad(weights, X, T):
+    """(gradient of 0.5 mean (y - t)^2, loss) from the GPU backward kernels."""
+    w = np.ascontiguousarray(weights, dtype=np.float32).ravel()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    G = np.zeros(MLP_NPARAM, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    _mlp_check(LIB.abm_mlp_grad(_fptr(w), _fptr(X), _fptr(T), X.shape[0], _fptr(G), _fptr(loss)), "abm_mlp_grad")
+    return G, float(loss[0])
+
+
+def mlp_train(weights, X, T, epochs=200, lr=1e-3, seed=0):
+    """Adam on the GPU; returns (trained weights, loss per epoch)."""
+    w = np.ascontiguousarray(weights, dtype=np.float32).ravel().copy()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    losses = np.zeros(max(epochs, 1), dtype=np.float32)
+    _mlp_check(LIB.abm_mlp_train(_fptr(w), _fptr(X), _fptr(T), X.shape[0], epochs, lr, seed, _fptr(losses)),
+               "abm_mlp_train")
+    return w, losses[:epochs]

@@ -50,6 +50,11 @@ struct abm_ctx {
     int *div_ok = nullptr, *parents_dev = nullptr;
     Geom *d1 = nullptr, *d2 = nullptr;
     double *dlen = nullptr, *dgrowth = nullptr;
+    // step-size network and its features
+    float* mlp_w = nullptr;          // ABM_MLP_NPARAM FP32 master weights
+    float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
+    double4* stat_part = nullptr;    // per-block feature partials of the final attempt
+    bool mlp_loaded = false;
     // parameters
     ForceParams fp; StepParams sp; BuildParams bp;
     // graphs
@@ -124,7 +129,7 @@ static void free_all(abm_ctx* c)
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
-                    c->dgrowth};
+                    c->dgrowth, c->mlp_w, c->log_buf, c->stat_part};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -306,6 +311,26 @@ int abm_create(const abm_params* q, abm_ctx** out)
     dp.seed = p.rng_seed; dp.cap_cells = c->cap;
     if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
         return fail(c, ABM_ERR_ARG, "adhesion_mode must be 0 (none) or 1 (isotropic JKR, fixed gamma)");
+    if (p.controller != ABM_CONTROLLER_REFERENCE && p.controller != ABM_CONTROLLER_LEARNED)
+        return fail(c, ABM_ERR_ARG, "controller must be ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED");
+    if (p.stepsize_log_capacity < 0) return fail(c, ABM_ERR_ARG, "stepsize_log_capacity must be >= 0");
+    // step-size network, its features and the feature log
+    sp.learned = p.controller == ABM_CONTROLLER_LEARNED;
+    sp.log_cap = p.stepsize_log_capacity;
+    sp.stats_on = sp.learned || sp.log_cap > 0;
+    sp.near_div_length = 0.9 * p.Ldiv;
+    fp.stats = sp.stats_on;
+    CK(cudaMalloc(&c->mlp_w, MLP_NPARAM * sizeof(float)));
+    CK(cudaMemset(c->mlp_w, 0, MLP_NPARAM * sizeof(float)));
+    CK(cudaMalloc(&c->stat_part, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
+    CK(cudaMemset(c->stat_part, 0, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
+    if (sp.log_cap > 0)
+    {
+        CK(cudaMalloc(&c->log_buf, (size_t)sp.log_cap * MLP_LOG_COLS * sizeof(float)));
+        CK(cudaMemset(c->log_buf, 0, (size_t)sp.log_cap * MLP_LOG_COLS * sizeof(float)));
+    }
+    sp.stat_part = c->stat_part;
+    sp.log_buf = c->log_buf;
     return ABM_OK;
 }
 
@@ -499,22 +524,29 @@ static PairGather loop_gather(abm_ctx* c)
     return pg;
 }
 
+// the step-size features of the iteration (and, learned, the proposed dt)
+static void enqueue_propose(abm_ctx* c)
+{
+    if (c->sp.stats_on) launch_mlp_propose(c->ctrl, c->sp, c->mlp_w, attempt_blocks(c->cap), c->st);
+}
+
 static void enqueue_attempts(abm_ctx* c)
 {
     cudaStream_t st = c->st;
     PairGather pg = loop_gather(c);
-    launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+    launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
     for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
-        launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+        launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
-    launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+    launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
 }
 
 static void enqueue_iteration(abm_ctx* c)
 {
     enqueue_pair_force(c, 0);
+    enqueue_propose(c);
     enqueue_attempts(c);
 }
 
@@ -622,7 +654,8 @@ static int build_iteration_graph(abm_ctx* c)
     PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
         enqueue_pair_force(c, 0);
-        launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+        enqueue_propose(c);
+        launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg);
     });
     if (rc) return rc;
@@ -633,13 +666,13 @@ static int build_iteration_graph(abm_ctx* c)
         if (rc) return rc;
         std::vector<cudaGraphNode_t> bd;
         rc = capture_into(c, body, bd, [&]() {
-            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
-                           c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg);
+            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c,
+                           nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg);
         });
         if (rc) return rc;
     }
     rc = capture_into(c, G, deps, [&]() {
-        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, nullptr, nullptr, nullptr,
+        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg);
     });
     if (rc) return rc;
@@ -874,6 +907,7 @@ int abm_get_stats(abm_ctx* c, abm_stats* s)
     s->rebuilds = h.rebuilds; s->divisions = h.divisions;
     s->t = h.t; s->dt = h.dt; s->last_max_error = h.last_max_error;
     s->n_cells = h.n; s->n_pairs = h.n_dir / 2;
+    s->rejected = h.rejected; s->log_rows = h.log_rows;
     return check_status(c);
 }
 
@@ -882,6 +916,8 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
     if (!c || n_iters < 0) return ABM_ERR_ARG;
     int rc = ready_for_forces(c);
     if (rc) return rc;
+    if (c->sp.learned && !c->mlp_loaded)
+        return fail(c, ABM_ERR_STATE, "the learned controller needs weights (abm_stepsize_set_weights)");
     if (!c->nbrs_valid)
     {
         enqueue_rebuild(c);
@@ -938,6 +974,8 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     if (!c || !prof || n_iters < 0) return ABM_ERR_ARG;
     int rc = ready_for_forces(c);
     if (rc) return rc;
+    if (c->sp.learned && !c->mlp_loaded)
+        return fail(c, ABM_ERR_STATE, "the learned controller needs weights (abm_stepsize_set_weights)");
     if (!c->nbrs_valid) { enqueue_rebuild(c); c->nbrs_valid = true; }
     memset(prof, 0, sizeof(*prof));
     std::vector<cudaEvent_t> ev((size_t)n_iters * 4);
@@ -950,6 +988,7 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
         CK(cudaEventRecord(e[0], st));
         enqueue_pair_force(c, 0);
         CK(cudaEventRecord(e[1], st));
+        enqueue_propose(c);
         enqueue_attempts(c);
         CK(cudaEventRecord(e[2], st));
         c->host_iter += 1;
@@ -973,6 +1012,59 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     prof->iterations = n_iters;
     for (auto& e : ev) cudaEventDestroy(e);
     return check_status(c);
+}
+
+int abm_stepsize_set_weights(abm_ctx* c, const float* w, int n)
+{
+    if (!c || !w || n != MLP_NPARAM) return fail(c, ABM_ERR_ARG, "weights must have ABM_MLP_NPARAM entries");
+    CK(cudaMemcpyAsync(c->mlp_w, w, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->mlp_loaded = true;
+    return ABM_OK;
+}
+
+int abm_stepsize_get_weights(abm_ctx* c, float* w, int n)
+{
+    if (!c || !w || n != MLP_NPARAM) return fail(c, ABM_ERR_ARG, "weights must have ABM_MLP_NPARAM entries");
+    CK(cudaMemcpyAsync(w, c->mlp_w, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
+int abm_stepsize_get_log(abm_ctx* c, float* rows, int cap_rows, int* n_rows)
+{
+    if (!c || !n_rows || cap_rows < 0 || (cap_rows > 0 && !rows)) return fail(c, ABM_ERR_ARG, "bad arguments");
+    *n_rows = 0;
+    if (c->sp.log_cap <= 0) return ABM_OK;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const long long total = h.log_rows;
+    const int cap = c->sp.log_cap;
+    const int have = (int)std::min<long long>(total, cap);
+    const int take = std::min(have, cap_rows);
+    // oldest first: ring positions (total - have) .. total - 1, the first `take` of them
+    std::vector<float> all((size_t)cap * MLP_LOG_COLS);
+    CK(cudaMemcpy(all.data(), c->log_buf, all.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < take; ++r)
+    {
+        const long long pos = (total - have + r) % cap;
+        memcpy(rows + (size_t)r * MLP_LOG_COLS, all.data() + (size_t)pos * MLP_LOG_COLS, MLP_LOG_COLS * sizeof(float));
+    }
+    *n_rows = take;
+    return ABM_OK;
+}
+
+int abm_stepsize_clear_log(abm_ctx* c)
+{
+    if (!c) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    h.log_rows = 0;
+    CK(cudaMemcpyAsync(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
 }
 
 }   // extern "C"

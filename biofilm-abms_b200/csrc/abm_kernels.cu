@@ -487,7 +487,7 @@ __device__ __forceinline__ double jkr_magnitude(double dist, double gamma, const
 // reference's j < i loop computes it): magnitude m along d, returned as
 // v = m d_hat with the body coordinates s (on i) and t (on j).  Cell i gains
 // (v, s v) in dE/dq and cell j gains (-v, -t v) (mechanics.hpp:1390-1659).
-struct PairOut { double vx, vy, vz, s, t; bool touch; };
+struct PairOut { double vx, vy, vz, s, t, ovl; bool touch; };
 
 __device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& gj, const ForceParams& fp,
                                                    const double* td, const double* tr)
@@ -510,7 +510,7 @@ __device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& g
     }
     if (fp.adhesion && overlap > fp.max_overlap) m += fp.pf1 * pow15(overlap - fp.max_overlap);
     out.vx = m * ux; out.vy = m * uy; out.vz = m * uz;
-    out.s = d.s; out.t = d.t; out.touch = true;
+    out.s = d.s; out.t = d.t; out.ovl = overlap; out.touch = true;
     return out;
 }
 
@@ -552,7 +552,7 @@ __device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& g
     }
     if (fp.adhesion && overlap > max_overlap) { float e = overlap - max_overlap; m += (float)fp.pf1 * e * sqrtf(e); }
     out.vx = (double)(m * dx * inv); out.vy = (double)(m * dy * inv); out.vz = (double)(m * dz * inv);
-    out.s = d.s; out.t = d.t; out.touch = true;
+    out.s = d.s; out.t = d.t; out.ovl = overlap; out.touch = true;
     return out;
 }
 
@@ -564,7 +564,7 @@ const int PF_T = 256, JKR_MAX = 512;
 template <int G, bool MIXED>
 __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ geom, const int* __restrict__ row_ptr,
                                                     const int* __restrict__ lower_end, const int* __restrict__ col,
-                                                    const int* __restrict__ rev, const Ctrl* ctrl, ForceParams fp,
+                                                    const int* __restrict__ rev, Ctrl* ctrl, ForceParams fp,
                                                     const double* __restrict__ jkr_delta,
                                                     const double* __restrict__ jkr_radius, Gen6* fcc,
                                                     double4* __restrict__ jbuf)
@@ -577,6 +577,7 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
     const unsigned gmask = (G == 32) ? 0xffffffffu
                                      : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
     const int groups_per_grid = gridDim.x * (blockDim.x / G);
+    double ovl_max = 0.0;
     for (int cell = (blockIdx.x * blockDim.x + threadIdx.x) / G; cell < n; cell += groups_per_grid)
     {
         const Geom gc = load_geom(geom, cell);
@@ -593,6 +594,7 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
                 acc[0] += p.vx; acc[1] += p.vy; acc[2] += p.vz;
                 acc[3] += p.s * p.vx; acc[4] += p.s * p.vy; acc[5] += p.s * p.vz;
                 js = make_double4(p.vx, p.vy, p.vz, p.t);
+                ovl_max = fmax(ovl_max, p.ovl);
             }
             jbuf[rev[k]] = js;
         }
@@ -606,6 +608,12 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
             for (int c = 0; c < 6; ++c) out.f[c] = acc[c];
             fcc[cell] = out;
         }
+    }
+    if (fp.stats)
+    {
+        ovl_max = warp_max(ovl_max);
+        if ((threadIdx.x & 31) == 0 && ovl_max > 0)
+            atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
     }
 }
 
@@ -643,7 +651,7 @@ __global__ void __launch_bounds__(PF_T) k_pair_gather(const int* __restrict__ ro
 }
 
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
-                       const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
                        int with_gather)
 {
@@ -773,13 +781,35 @@ __device__ __forceinline__ Gen6 gather_pair_force(const Gen6* fcc, const int* __
 
 // Step-size controller, run once per attempt by the last block
 // (simulation.hpp:1690-1769; the final re-run is accepted unconditionally).
-__device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, double E)
+// commit: the final step copies an accepted proposal (no RK evaluation of its own)
+__device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, double E, bool commit = false)
 {
-    c->attempts += 1;
+    if (!commit) c->attempts += 1;
     if (kind == MODE_TRIAL)
     {
         c->last_trial_error = E;
         bool exceeded = E > 1.0;
+        c->first_passed = !exceeded;
+        if (exceeded) c->rejected += 1;
+        if (sp.log_cap > 0)
+        {
+            // complete the feature row of this iteration: the log ratio of the largest
+            // dt the error model accepts, and of this attempt's dt, to the last accepted dt
+            float* row = sp.log_buf + (size_t)(c->log_rows % sp.log_cap) * MLP_LOG_COLS;
+            row[32] = (float)(-sp.inv_q1 * log(E));
+            row[33] = (float)log(c->dt / c->dt_prev);
+            row[34] = (float)log10(E);
+            row[35] = exceeded ? 0.f : 1.f;
+            c->log_rows += 1;
+        }
+        if (sp.learned && !exceeded)
+        {
+            // the proposal passed the error test: accept its candidate state as is
+            c->mode = MODE_COMMIT;
+            c->tries = 0;
+            c->attempt = 1;
+            return;
+        }
         double factor = 0.9 * pow(1.0 / E, sp.inv_q1);
         if (factor >= 10) factor = 10;
         else if (factor < 0.2) factor = 0.2;
@@ -804,9 +834,15 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
             if (exceeded && c->tries < sp.max_tries) { c->mode = MODE_RETRY; c->dt_try = c->dt * factor; return; }
         }
     }
-    else   // MODE_FINAL: accepted
+    else   // MODE_FINAL (or a committed proposal): accepted
     {
         c->last_max_error = E;
+        const int h = c->hist_pos;
+        c->hist_dt[h] = c->dt;
+        c->hist_err[h] = E;
+        c->hist_acc[h] = c->first_passed;
+        c->hist_pos = (h + 1) % HIST;
+        c->since_div = c->n_divide > 0 ? 0 : c->since_div + 1;
         c->t += c->dt;
         c->iter += 1;
         c->iterations += 1;
@@ -835,18 +871,23 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                                                  unsigned long long cond, int use_cond, PairGather pg)
 {
     __shared__ double sh_max[AT_T / 32];
+    __shared__ double4 sh_stat[AT_T / 32];
     __shared__ bool last;
     const int n = ctrl->n;
     const int mode = ctrl->mode;
     const int iter = ctrl->iter;
-    const bool trial_ran = (iter % sp.iter_update_stepsize == 0);
+    // the learned controller proposes (and tests) a step every iteration
+    const bool trial_ran = sp.learned || (iter % sp.iter_update_stepsize == 0);
+    // k0 is shared across attempts only under the reference controller: a passing
+    // proposal needs no second attempt, so it does not store k0 or the total pair force
+    const bool share_k0 = !NOISE && !sp.learned;
     double dt;
     int attempt;
     bool load_k0 = false, store_k0 = false;
     if (KIND == MODE_TRIAL)
     {
         if (!trial_ran) return;   // no step-size update this iteration: FINAL runs at dt
-        dt = ctrl->dt; attempt = 0; store_k0 = !NOISE;
+        dt = ctrl->dt; attempt = 0; store_k0 = share_k0;
     }
     else if (KIND == MODE_RETRY)
     {
@@ -857,23 +898,47 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                 cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
             return;
         }
-        dt = ctrl->dt_try; attempt = ctrl->attempt; load_k0 = !NOISE;
+        dt = ctrl->dt_try; attempt = ctrl->attempt; load_k0 = share_k0;
     }
     else if (KIND == MODE_FINAL)
     {
         dt = (mode == MODE_FINAL) ? ctrl->dt_try : ctrl->dt;
         attempt = (mode == MODE_FINAL) ? ctrl->attempt : 0;
-        load_k0 = !NOISE && trial_ran;
+        load_k0 = share_k0 && trial_ran;
     }
     else { dt = eval_dt; attempt = eval_attempt; }
+    const bool commit = (KIND == MODE_FINAL) && mode == MODE_COMMIT;
+    // the learned trial writes its candidate state for a commit
+    const bool write_candidate = (KIND == MODE_TRIAL) && sp.learned;
 
     // the first attempt of an iteration completes the pair force (k_pair_force left
-    // only the lower-neighbor share); the trial writes the total back for the rest
-    const bool do_gather = pg.fused && (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran));
+    // only the lower-neighbor share); under the reference controller the trial writes
+    // the total back for the rest, under the learned one every attempt gathers
+    const bool do_gather = pg.fused && !commit &&
+                           (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran) || sp.learned);
     double local_max = 0.0;
     bool bad = false;
+    double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
+        if (commit)
+        {
+            // committed proposal: candidate -> state (growth already applied)
+            const Geom gc = geom_c[i];
+            const Vel vc = vel_c[i];
+            geom[i] = gc;
+            vel[i] = vc;
+            phys[i].l = 2 * gc.h;
+            if (sp.stats_on)
+            {
+                const double v2 = vc.v[0] * vc.v[0] + vc.v[1] * vc.v[1] + vc.v[2] * vc.v[2];
+                st_vmax = fmax(st_vmax, sqrt(v2));
+                st_v2 += v2;
+                st_g += phys[i].growth;
+                st_near += (2 * gc.h > sp.near_div_length) ? 1.0 : 0.0;
+            }
+            continue;
+        }
         const Geom g = load_geom(geom, i);
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
         const double l = phys[i].l, eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
@@ -882,7 +947,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         if (do_gather)
         {
             cc = gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
-            if (KIND == MODE_TRIAL) pg.fcc_w[i] = cc;
+            if (KIND == MODE_TRIAL && !sp.learned) pg.fcc_w[i] = cc;
         }
         else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);
         double f0[6];
@@ -935,7 +1000,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             local_max = fmax(local_max, scaled);
             if (KIND == 3 && err_out) err_out[i].f[c] = err;
         }
-        if (KIND == MODE_FINAL || KIND == 3)
+        if (KIND == MODE_FINAL || KIND == 3 || write_candidate)
         {
             double y1[6];
 #pragma unroll
@@ -946,20 +1011,61 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             Vel vo;
 #pragma unroll
             for (int c = 0; c < 6; ++c) vo.v[c] = vf1[c];
-            if (KIND == MODE_FINAL)
+            if (KIND == MODE_FINAL || write_candidate)
             {
                 // growCells (growth.hpp:51-57) fused with the accepted step
-                double lg = l + phys[i].growth * (4 * sp.mp.R / 3 + l) * dt;
+                const double g_rate = phys[i].growth;
+                double lg = l + g_rate * (4 * sp.mp.R / 3 + l) * dt;
                 go.h = lg / 2;
-                phys[i].l = lg;
-                geom[i] = go;
-                vel[i] = vo;
+                if (KIND == MODE_FINAL)
+                {
+                    phys[i].l = lg;
+                    geom[i] = go;
+                    vel[i] = vo;
+                    if (sp.stats_on)
+                    {
+                        const double v2 = vf1[0] * vf1[0] + vf1[1] * vf1[1] + vf1[2] * vf1[2];
+                        st_vmax = fmax(st_vmax, sqrt(v2));
+                        st_v2 += v2;
+                        st_g += g_rate;
+                        st_near += (lg > sp.near_div_length) ? 1.0 : 0.0;
+                    }
+                }
+                else
+                {
+                    geom_c[i] = go;
+                    vel_c[i] = vo;
+                }
             }
             else
             {
                 geom_c[i] = go;
                 vel_c[i] = vo;
             }
+        }
+    }
+    if (KIND == MODE_FINAL && sp.stats_on)
+    {
+        // per-block partials of the step-size features, summed in block order later
+        st_vmax = warp_max(st_vmax);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            st_v2 += __shfl_xor_sync(0xffffffffu, st_v2, off);
+            st_g += __shfl_xor_sync(0xffffffffu, st_g, off);
+            st_near += __shfl_xor_sync(0xffffffffu, st_near, off);
+        }
+        if ((threadIdx.x & 31) == 0) sh_stat[threadIdx.x >> 5] = make_double4(st_vmax, st_v2, st_g, st_near);
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double4 a = sh_stat[0];
+            for (int w = 1; w < AT_T / 32; ++w)
+            {
+                const double4 b = sh_stat[w];
+                a.x = fmax(a.x, b.x); a.y += b.y; a.z += b.z; a.w += b.w;
+            }
+            sp.stat_part[blockIdx.x] = a;
         }
     }
     // block max of the scaled error, floored at min_error (simulation.hpp:1703)
@@ -989,9 +1095,10 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         __threadfence();
         double E = __longlong_as_double((long long)atomicAdd(&ctrl->err_bits, 0ull));
         E = fmax(E, sp.min_error);
+        if (commit) E = ctrl->last_trial_error;
         ctrl->err_bits = 0ull;
         ctrl->blocks_done = 0u;
-        controller_finish(ctrl, sp, KIND, E);
+        controller_finish(ctrl, sp, KIND, E, commit);
         // another retry?  (bounded: the controller schedules at most max_tries of them)
         if (use_cond && (KIND == MODE_TRIAL || KIND == MODE_RETRY))
             cudaGraphSetConditional((cudaGraphConditionalHandle)cond,
@@ -1016,12 +1123,14 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 #undef AT_ARGS
 }
 
+int attempt_blocks(int cap_cells) { return max(cdiv(cap_cells, AT_T), 1); }
+
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
                     unsigned long long cond, int use_cond, PairGather pg)
 {
-    int blocks = max(cdiv(cap_cells, AT_T), 1);
+    int blocks = attempt_blocks(cap_cells);
 #define AT_CASE(S) case S: \
         if (sp.noise_on) launch_attempt_s<S, true>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
         else launch_attempt_s<S, false>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \

@@ -9,7 +9,19 @@ namespace abm {
 const int MAX_STAGES = 7;
 
 // Controller modes of one iteration (simulation.hpp:1690-1769)
-enum CtrlMode { MODE_TRIAL = 0, MODE_RETRY = 1, MODE_FINAL = 2 };
+// MODE_COMMIT: the learned controller's proposal passed the error test; the final
+// attempt copies its candidate state instead of re-running the step.
+enum CtrlMode { MODE_TRIAL = 0, MODE_RETRY = 1, MODE_FINAL = 2, MODE_COMMIT = 3 };
+
+// Step-size network: 32 features -> 64 -> 64 -> 1 (log dt ratio)
+const int MLP_IN = 32, MLP_H = 64;
+const int MLP_OFF_W1 = 0, MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_IN, MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;
+const int MLP_OFF_B2 = MLP_OFF_W2 + MLP_H * MLP_H, MLP_OFF_W3 = MLP_OFF_B2 + MLP_H, MLP_OFF_B3 = MLP_OFF_W3 + MLP_H;
+const int MLP_NPARAM = MLP_OFF_B3 + 1;
+// log row: 32 features, ln(dt_max / dt_first), ln(dt_first / dt_prev), log10 E, passed,
+// the proposal's error-model baseline, 3 spare columns
+const int MLP_LOG_COLS = 40;
+const int HIST = 8;
 
 // Status bits raised on the device and turned into ABM_ERR_* by the host.
 enum StatusBits {
@@ -44,6 +56,19 @@ struct Ctrl {
     int div_done, div_tries, last_div_tries;
     int n_parents;              // length of the lineage vector
     long long div_events;       // iterations in which cells divided
+    // step-size features (filled when StepParams::stats_on)
+    unsigned long long st_vmax_bits;    // max |v_r| of the last accepted step (ordered bits)
+    unsigned long long st_ovl_bits;     // max overlap of the last pair-force pass
+    double st_v2sum, st_gsum;           // sum |v_r|^2 and sum of growth rates over cells
+    int st_near_div;                    // cells with l > 0.9 Ldiv
+    int since_div;                      // iterations since cells last divided
+    double hist_dt[HIST], hist_err[HIST];   // accepted dt and its scaled error, newest at hist_pos - 1
+    int hist_acc[HIST];                 // 1 if that iteration's first attempt passed the error test
+    int hist_pos;
+    int first_passed;                   // the running iteration's first attempt passed
+    double dt_prev;                     // accepted dt before the running iteration
+    long long rejected;                 // iterations whose first attempt failed the error test
+    long long log_rows;                 // feature rows written (ring position = log_rows % capacity)
 };
 
 struct Grid {
@@ -62,6 +87,13 @@ struct StepParams {
     double noise_max[6];
     int noise_on;
     uint64_t seed;
+    // step-size control
+    int learned;                // 1: the network proposes dt, a passing proposal is accepted as is
+    int stats_on;               // accumulate the network's features (learned or logging)
+    double near_div_length;     // 0.9 Ldiv
+    double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
+    float* log_buf;             // MLP_LOG_COLS floats per row, log_cap rows (ring)
+    int log_cap;
 };
 
 struct ForceParams {
@@ -71,6 +103,7 @@ struct ForceParams {
     int adhesion;
     int jkr_n;
     double jkr_step;            // spacing of the overlap mesh
+    int stats;                  // record the max overlap (step-size features)
 };
 
 struct BuildParams {
@@ -116,7 +149,7 @@ size_t scan_block_sums_size(int cap);
 // two passes: each unordered pair once from the row of its larger index, then the
 // partner's share gathered from the reverse slots (jbuf, one double4 per CSR entry)
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
-                       const Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
+                       Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
                        int with_gather = 1);
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
@@ -140,6 +173,17 @@ void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, in
                         int cap_cells, cudaStream_t st);
 void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
                        const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st);
+
+// step-size network (abm_mlp.cu); weights are the flat FP32 master copy
+void launch_mlp_forward(const float* master, const float* X, int n, float* Y, cudaStream_t st);
+void launch_mlp_grad(const float* master, const float* X, const float* T, int n, float* G, float* loss,
+                     cudaStream_t st);
+void launch_mlp_train(float* master, float* m1, float* m2, float* G, const float* X, const float* T, int n,
+                      int epochs, float lr, unsigned seed, float* loss_out, cudaStream_t st);
+// features of the running iteration -> log row; with sp.learned also the dt of the first attempt.
+// stat_blocks = blocks of the attempt kernels (entries of sp.stat_part)
+void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* master, int stat_blocks, cudaStream_t st);
+int attempt_blocks(int cap_cells);
 
 // division (growth.hpp:66-426), abm_divide.cu
 struct DivideParams {

@@ -34,7 +34,7 @@ const int NA_MAX_JKR = 512;
 
 // byte offsets inside the scratch array, each 256-byte aligned
 const size_t OFF_CTRL = 0;
-const size_t OFF_GEOM = 256;
+const size_t OFF_GEOM = (sizeof(Ctrl) + 255) / 256 * 256;
 const size_t OFF_FCC = OFF_GEOM + (size_t)NA_MAX_CELLS * sizeof(Geom);
 const size_t OFF_LOWER = OFF_FCC + (size_t)NA_MAX_CELLS * sizeof(Gen6);
 const size_t OFF_REV = OFF_LOWER + (size_t)NA_MAX_CELLS * sizeof(int);
@@ -138,6 +138,7 @@ extern "C" int abm_cell_cell_forces_noalloc(const abm_params* p, const double* d
     fp.pf2 = (4. / 3.) * p->E0 * std::sqrt(p->R / 2) * std::pow(2 * (p->R - p->Rcell), 1.5);
     fp.max_overlap = 2 * (p->R - p->Rcell);
     fp.adhesion = p->adhesion_mode != 0;
+    fp.stats = 0;
     fp.jkr_n = fp.adhesion ? jkr_n : 0;
     fp.jkr_step = fp.adhesion ? (jkr_delta[jkr_n - 1] - jkr_delta[0]) / double(jkr_n - 1) : 1.0;
     if (fp.adhesion)

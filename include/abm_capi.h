@@ -37,6 +37,27 @@ extern "C" {
 #define ABM_DORMAND_PRINCE 4
 
 /* Pair-force precision */
+/* Step-size controllers.  REFERENCE: the rule of simulation.hpp:1688-1769 (trial, up to
+ * max_tries retries, a final re-run accepted unconditionally).  LEARNED: the step-size
+ * network proposes dt from 32 features; the proposal is one RK attempt, accepted as is
+ * when its embedded error passes (E <= 1), otherwise the REFERENCE rule continues from
+ * that attempt (its retries and final re-run). */
+#define ABM_CONTROLLER_REFERENCE 0
+#define ABM_CONTROLLER_LEARNED 1
+
+/* Step-size network: 32 features -> 64 -> 64 -> 1 (ReLU), output ln(dt / dt_prev).
+ * Flat FP32 parameter layout: W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3. */
+#define ABM_MLP_FEATURES 32
+#define ABM_MLP_HIDDEN 64
+#define ABM_MLP_NPARAM 6337
+/* The proposal is ln(dt / dt_prev) = clamp(b + y, ln 0.2, ln 10): y the network output,
+ * b = ln 0.9 - ln(E_last)/(q+1) the error-model baseline (E_last: scaled error of the last
+ * accepted step, q: error order of the tableau).
+ * Log row: 32 features, ln(dt_max / dt_first) with dt_max = dt_first E^(-1/(q+1)),
+ * ln(dt_first / dt_prev), log10 E of the first attempt, 1 if it passed (E <= 1), b, and
+ * three spare columns. */
+#define ABM_MLP_LOG_COLS 40
+
 #define ABM_PRECISION_FP64 0    /* everything in FP64 */
 #define ABM_PRECISION_MIXED 1   /* segment distance + pair force in FP32; near-parallel branch,
                                    positions, orientations, stage sums and error norm in FP64 */
@@ -66,6 +87,9 @@ typedef struct abm_params {
     int cap_neighbors_per_cell;  /* directed neighbor slots per cell (0 = default 64) */
     int pair_lanes;              /* lanes per cell in the pair-force kernel: 4, 8, 16 or 32 (0 = 8) */
     int use_graphs;              /* 1 = capture the iteration in a CUDA graph */
+    /* step-size control (no reference counterpart beyond ABM_CONTROLLER_REFERENCE) */
+    int controller;              /* ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED */
+    int stepsize_log_capacity;   /* rows of step-size features logged per context (0 = off) */
 } abm_params;
 
 typedef struct abm_stats {
@@ -77,6 +101,8 @@ typedef struct abm_stats {
     double t, dt;                /* simulated time and current step size */
     double last_max_error;       /* scaled max error of the accepted attempt */
     int n_cells, n_pairs;        /* current population and neighbor pairs (unordered) */
+    long long rejected;          /* iterations whose first attempt failed the error test */
+    long long log_rows;          /* step-size feature rows written so far */
 } abm_stats;
 
 /* Device time per kernel group, from CUDA events on the context stream. */
@@ -161,6 +187,29 @@ const char* abm_graph_info(const abm_ctx* ctx);
 /* Same as abm_iterate without graphs, with CUDA events around each kernel group
  * (no reference counterpart; measurement only). */
 int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);
+
+/* ---------------------------------------------------------------------------
+ * Step-size network (no reference counterpart).  The weights are the flat FP32
+ * layout above; every kernel rounds them to BF16 and accumulates in FP32 on the
+ * tensor cores.
+ * ------------------------------------------------------------------------- */
+/* Install / read the weights the context's learned controller uses. */
+int abm_stepsize_set_weights(abm_ctx* ctx, const float* weights, int n_param);
+int abm_stepsize_get_weights(abm_ctx* ctx, float* weights, int n_param);
+/* Copy the logged rows (ABM_MLP_LOG_COLS floats each, oldest first, at most
+ * stepsize_log_capacity) into rows[cap_rows][ABM_MLP_LOG_COLS]; n_rows = rows copied. */
+int abm_stepsize_get_log(abm_ctx* ctx, float* rows, int cap_rows, int* n_rows);
+int abm_stepsize_clear_log(abm_ctx* ctx);
+/* Host-buffer entry points on the current device (they allocate device memory).
+ * X is n x 32 row-major; Y and T have n entries. */
+int abm_mlp_forward(const float* weights, const float* X, int n, float* Y);
+/* Gradient of L = 0.5/n sum (y - t)^2 with respect to the weights, and L. */
+int abm_mlp_grad(const float* weights, const float* X, const float* T, int n, float* grad, float* loss);
+/* Mini-batch Adam (batches of 64, seeded order) on the GPU; weights in/out;
+ * loss_per_epoch (epochs entries, may be NULL) gets each epoch's mean loss. */
+int abm_mlp_train(float* weights, const float* X, const float* T, int n, int epochs, float lr,
+                  unsigned seed, float* loss_per_epoch);
+const char* abm_mlp_last_error(void);
 
 /* ---------------------------------------------------------------------------
  * Cell-cell forces without device allocation.  No counterpart in the reference.

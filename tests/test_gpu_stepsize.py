@@ -1,0 +1,172 @@
+"""Step-size network on the GPU: forward and gradient against the CPU
+restatement (oracle/mlp_ref.py), training, the in-loop proposal, and the
+learned controller's accepted step against the oracle's RK step."""
+import numpy as np
+import pytest
+
+import abm_b200
+from abm_b200 import stepsize, workloads
+import mlp_ref
+import oracle_ref as orc
+
+pytestmark = pytest.mark.gpu
+
+JKR = orc.jkr_table(0.8, 0.5, 3900.0, 100.0, 100)
+
+
+def problem(n, seed):
+    rng = np.random.default_rng(seed)
+    w = stepsize.init_weights(seed, out_bias=0.2)
+    w[mlp_ref.OFF_B1:mlp_ref.OFF_W2] = rng.normal(0, 0.1, 64)
+    w[mlp_ref.OFF_B2:mlp_ref.OFF_W3] = rng.normal(0, 0.1, 64)
+    X = rng.normal(0, 1, (n, 32)).astype(np.float32)
+    T = (np.tanh(X[:, :4].sum(1) / 2) + 0.1 * X[:, 5]).astype(np.float32)
+    return w, X, T
+
+
+def test_mlp_forward_matches_cpu_restatement():
+    w, X, _ = problem(1003, 1)                 # not a multiple of the 16-row tile
+    y = abm_b200.mlp_forward(w, X)
+    yo, _, _ = mlp_ref.forward(w, X)
+    # same BF16 operands on both sides; FP32 vs FP64 accumulation can move a hidden
+    # activation across a BF16 rounding boundary (one BF16 ulp, 2^-8 relative)
+    assert np.abs(y - yo).max() <= 2e-3 * (1 + np.abs(yo).max())
+    assert np.median(np.abs(y - yo)) <= 1e-5 * (1 + np.abs(yo).max())
+
+
+def test_mlp_gradient_matches_cpu_restatement():
+    w, X, T = problem(1003, 2)
+    g, loss = abm_b200.mlp_grad(w, X, T)
+    go, losso = mlp_ref.grad(w, X, T)
+    assert abs(loss - losso) <= 1e-4 * losso
+    assert np.linalg.norm(g - go) <= 2e-3 * np.linalg.norm(go)
+    blocks = [(mlp_ref.OFF_W1, mlp_ref.OFF_B1), (mlp_ref.OFF_B1, mlp_ref.OFF_W2), (mlp_ref.OFF_W2, mlp_ref.OFF_B2),
+              (mlp_ref.OFF_B2, mlp_ref.OFF_W3), (mlp_ref.OFF_W3, mlp_ref.OFF_B3), (mlp_ref.OFF_B3, mlp_ref.NPARAM)]
+    for a, b in blocks:
+        assert np.linalg.norm(g[a:b] - go[a:b]) <= 5e-3 * np.linalg.norm(go[a:b]) + 1e-7, (a, b)
+    # and the rounded network's gradient is close to the exact FP64 gradient
+    g64, _ = mlp_ref.grad_fp64(w, X, T)
+    assert np.linalg.norm(g - g64) <= 3e-2 * np.linalg.norm(g64)
+
+
+def test_mlp_training_reduces_the_loss():
+    w, X, T = problem(4096, 3)
+    _, loss0 = abm_b200.mlp_grad(w, X, T)
+    w1, losses = abm_b200.mlp_train(w, X, T, epochs=60, lr=2e-3, seed=5)
+    _, loss1 = abm_b200.mlp_grad(w1, X, T)
+    assert loss1 < 0.1 * loss0, (loss0, loss1)
+    assert losses[-1] < losses[0]
+    # the gradient sums use FP32 atomics, so a second run differs in rounding only
+    w2, _ = abm_b200.mlp_train(w, X, T, epochs=60, lr=2e-3, seed=5)
+    _, loss2 = abm_b200.mlp_grad(w2, X, T)
+    assert loss2 < 0.1 * loss0
+
+
+def colony(n, seed, growth=1.5):
+    cells, _ = workloads.biofilm_3d(n=n, seed=seed, disk_radius=300.0 * np.sqrt(n / 1e5), p_contact=0.9)
+    cells[:, 16] = growth
+    return cells
+
+
+def test_in_loop_proposal_is_the_network_output():
+    cells = colony(1500, 31, growth=0.0)
+    sim = abm_b200.Simulation(cap_cells=1600, jkr_table=JKR, controller=1, stepsize_log_capacity=64,
+                              max_stepsize=1.0, min_stepsize=1e-15)
+    sim.upload_cells(cells)
+    w = stepsize.init_weights(7, out_bias=float(np.log(0.7)))
+    sim.set_stepsize_weights(w)
+    np.testing.assert_array_equal(sim.stepsize_weights(), w)
+    sim.set_clock(0.0, 1e-6, 0)
+    sim.get_cell_neighbors()
+    sim.iterate(6)
+    rows = sim.stepsize_log()
+    assert rows.shape == (6, abm_b200.MLP_LOG_COLS)
+    y = abm_b200.mlp_forward(w, rows[:, :32])
+    # baseline b = ln 0.9 - ln(E_last)/(q+1), HE21: q = 1
+    b = np.log(0.9) - 0.5 * np.float32(2.302585093) * np.float32(10.0) * rows[:, 12]
+    np.testing.assert_allclose(rows[:, 36], b, rtol=1e-5, atol=1e-5)
+    r = np.clip(rows[:, 36].astype(np.float64) + y, np.log(0.2), np.log(10.0))
+    np.testing.assert_allclose(rows[:, 33], r, atol=2e-6)
+    sim.close()
+
+
+def test_learned_step_equals_the_oracle_rk_step():
+    """A proposal that passes the error test is committed as is: the state equals
+    the oracle's RK step at the proposed dt followed by growth (growth.hpp:51-57)."""
+    cells = colony(3000, 32, growth=1.5)
+    cells[:, 13] = np.minimum(cells[:, 13], 4.0)
+    cells[:, 14] = cells[:, 13] / 2
+    sim = abm_b200.Simulation(cap_cells=3100, jkr_table=JKR, controller=1, max_stepsize=1e-4)
+    sim.upload_cells(cells)
+    w = np.zeros(abm_b200.MLP_NPARAM, dtype=np.float32)
+    # first iteration: no history, E_last = 1, baseline ln 0.9; output ln(0.5/0.9)
+    w[-1] = np.log(0.5) - np.log(0.9)
+    sim.set_stepsize_weights(w)
+    sim.set_clock(0.0, 1e-6, 0)
+    sim.get_cell_neighbors()
+    s = sim.iterate(1)
+    assert s["attempts"] == 1 and s["rejected"] == 0 and s["iterations"] == 1
+    t, dt, it = sim.clock()
+    assert it == 1 and abs(t - 1e-6 * 0.5) <= 1e-6 * 1e-6
+    got = sim.download_cells()
+    o = orc.Oracle(sim.pdict, jkr=JKR)
+    o.set_cells(cells)
+    o.build_neighbors()
+    co, _, mo = o.rk_attempt(t)
+    assert mo <= 1.0
+    for c in range(1, 13):                    # r, n, then the stored velocities
+        scale = np.abs(co[:, c]).max()
+        assert np.abs(got[:, c] - co[:, c]).max() <= 1e-10 * max(scale, 1e-300), c
+    l = cells[:, 13]
+    lg = l + cells[:, 16] * (4 * 0.8 / 3 + l) * t
+    np.testing.assert_allclose(got[:, 13], lg, rtol=1e-14, atol=0)
+    np.testing.assert_allclose(got[:, 14], lg / 2, rtol=1e-14, atol=0)
+    sim.close()
+
+
+def test_rejected_proposal_falls_back_to_the_reference_rule():
+    """A proposal far too large fails the error test; the reference rule then
+    retries from that attempt and re-runs the final step, as simulation.hpp:1688-1769."""
+    cells = colony(2000, 33, growth=0.0)
+    sim = abm_b200.Simulation(cap_cells=2100, jkr_table=JKR, controller=1, max_stepsize=1.0)
+    sim.upload_cells(cells)
+    w = np.zeros(abm_b200.MLP_NPARAM, dtype=np.float32)
+    w[-1] = 50.0                              # always ask for the largest step (10x)
+    sim.set_stepsize_weights(w)
+    sim.set_clock(0.0, 1e-3, 0)
+    sim.get_cell_neighbors()
+    s = sim.iterate(3)
+    assert s["iterations"] == 3
+    assert s["rejected"] >= 1
+    assert s["attempts"] > s["iterations"]      # fallback iterations take more than one attempt
+    assert np.isfinite(sim.download_cells()).all()
+    sim.close()
+
+
+def test_learned_controller_gain_over_the_reference_controller():
+    """What the trained network gains over the method without it (the reference
+    controller, simulation.hpp:1688-1769) at equal RK tolerance on a growing,
+    dividing colony: simulated time per RK evaluation.  Also reported: the
+    same proposal loop with the network zeroed (error-model baseline only)."""
+    runs = [(stepsize.growing_colony(1500, 41), dict(max_stepsize=1e-4)),
+            (stepsize.growing_colony(3000, 42), dict(max_stepsize=1e-4))]
+    w, info = stepsize.train_protocol(runs, n_iters=1500, epochs=150)
+    cells = stepsize.growing_colony(2500, 43)
+    _, ref = stepsize.logged_run(cells, 2000, controller=0)
+    _, zero = stepsize.logged_run(cells, 2000, controller=1, weights=np.zeros(abm_b200.MLP_NPARAM, np.float32))
+    rows, lrn = stepsize.logged_run(cells, 2000, controller=1, weights=w)
+    per_eval = {k: s["t"] / s["attempts"] for k, s in (("reference", ref), ("zeroed", zero), ("learned", lrn))}
+    print("\nstep-size controllers on a 2500-cell growing colony, 2000 steps, tol 1e-8:")
+    for k, s in (("reference", ref), ("zeroed", zero), ("learned", lrn)):
+        print("  %-9s evals/step %.3f  rejected %d  divisions %d  t %.5f h  sim-time/eval %.3e h" % (
+            k, s["attempts"] / s["iterations"], s["rejected"], s["divisions"], s["t"], per_eval[k]))
+    # reference rule: trial + final every step, plus its retries
+    assert ref["attempts"] == 2 * ref["iterations"] + ref["retries"]
+    # learned: a passing proposal is the only attempt of its step; a failing one continues
+    # with the reference rule (its retries and the final re-run)
+    assert lrn["attempts"] == lrn["iterations"] + lrn["rejected"] + lrn["retries"]
+    assert (rows[:, 35] < 0.5).sum() == lrn["rejected"]
+    assert lrn["rejected"] <= 0.02 * lrn["iterations"]
+    assert lrn["t"] >= 0.75 * ref["t"]                       # comparable step sizes
+    assert per_eval["learned"] >= 1.6 * per_eval["reference"]
+    assert per_eval["learned"] >= 0.9 * per_eval["zeroed"]

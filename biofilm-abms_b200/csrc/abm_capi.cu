@@ -53,7 +53,6 @@ struct abm_ctx {
     // step-size network and its features
     float* mlp_w = nullptr;          // ABM_MLP_NPARAM FP32 master weights
     float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
-    double4* stat_part = nullptr;    // per-block feature partials of the final attempt
     bool mlp_loaded = false;
     // parameters
     ForceParams fp; StepParams sp; BuildParams bp;
@@ -129,7 +128,7 @@ static void free_all(abm_ctx* c)
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
-                    c->dgrowth, c->mlp_w, c->log_buf, c->stat_part};
+                    c->dgrowth, c->mlp_w, c->log_buf};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -322,14 +321,11 @@ int abm_create(const abm_params* q, abm_ctx** out)
     fp.stats = sp.stats_on;
     CK(cudaMalloc(&c->mlp_w, MLP_NPARAM * sizeof(float)));
     CK(cudaMemset(c->mlp_w, 0, MLP_NPARAM * sizeof(float)));
-    CK(cudaMalloc(&c->stat_part, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
-    CK(cudaMemset(c->stat_part, 0, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
     if (sp.log_cap > 0)
     {
         CK(cudaMalloc(&c->log_buf, (size_t)sp.log_cap * MLP_LOG_COLS * sizeof(float)));
         CK(cudaMemset(c->log_buf, 0, (size_t)sp.log_cap * MLP_LOG_COLS * sizeof(float)));
     }
-    sp.stat_part = c->stat_part;
     sp.log_buf = c->log_buf;
     return ABM_OK;
 }
@@ -527,7 +523,7 @@ static PairGather loop_gather(abm_ctx* c)
 // the step-size features of the iteration (and, learned, the proposed dt)
 static void enqueue_propose(abm_ctx* c)
 {
-    if (c->sp.stats_on) launch_mlp_propose(c->ctrl, c->sp, c->mlp_w, attempt_blocks(c->cap), c->st);
+    if (c->sp.stats_on) launch_mlp_propose(c->ctrl, c->sp, c->mlp_w, c->st);
 }
 
 static void enqueue_attempts(abm_ctx* c)

@@ -1065,7 +1065,11 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                 const double4 b = sh_stat[w];
                 a.x = fmax(a.x, b.x); a.y += b.y; a.z += b.z; a.w += b.w;
             }
-            sp.stat_part[blockIdx.x] = a;
+            // block sums in fixed point: integer atomics add up the same in any order
+            if (a.x > 0) atomicMax(&ctrl->st_vmax_bits, (unsigned long long)__double_as_longlong(a.x));
+            atomicAdd(&ctrl->st_v2_fx, (unsigned long long)llrint(ldexp(a.y, STAT_V2_SHIFT)));
+            atomicAdd(&ctrl->st_g_fx, (unsigned long long)llrint(ldexp(fmax(a.z, 0.0), STAT_G_SHIFT)));
+            atomicAdd(&ctrl->st_near_div, (unsigned long long)a.w);
         }
     }
     // block max of the scaled error, floored at min_error (simulation.hpp:1703)

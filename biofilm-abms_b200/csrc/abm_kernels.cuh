@@ -22,6 +22,7 @@ const int MLP_NPARAM = MLP_OFF_B3 + 1;
 // the proposal's error-model baseline, 3 spare columns
 const int MLP_LOG_COLS = 40;
 const int HIST = 8;
+const int STAT_V2_SHIFT = 20, STAT_G_SHIFT = 32;
 
 // Status bits raised on the device and turned into ABM_ERR_* by the host.
 enum StatusBits {
@@ -57,10 +58,12 @@ struct Ctrl {
     int n_parents;              // length of the lineage vector
     long long div_events;       // iterations in which cells divided
     // step-size features (filled when StepParams::stats_on)
+    // sums in fixed point so that their value does not depend on the order of the atomics
     unsigned long long st_vmax_bits;    // max |v_r| of the last accepted step (ordered bits)
     unsigned long long st_ovl_bits;     // max overlap of the last pair-force pass
-    double st_v2sum, st_gsum;           // sum |v_r|^2 and sum of growth rates over cells
-    int st_near_div;                    // cells with l > 0.9 Ldiv
+    unsigned long long st_v2_fx;        // sum |v_r|^2 * 2^STAT_V2_SHIFT
+    unsigned long long st_g_fx;         // sum of growth rates * 2^STAT_G_SHIFT
+    unsigned long long st_near_div;     // cells with l > 0.9 Ldiv
     int since_div;                      // iterations since cells last divided
     double hist_dt[HIST], hist_err[HIST];   // accepted dt and its scaled error, newest at hist_pos - 1
     int hist_acc[HIST];                 // 1 if that iteration's first attempt passed the error test
@@ -91,7 +94,6 @@ struct StepParams {
     int learned;                // 1: the network proposes dt, a passing proposal is accepted as is
     int stats_on;               // accumulate the network's features (learned or logging)
     double near_div_length;     // 0.9 Ldiv
-    double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
     float* log_buf;             // MLP_LOG_COLS floats per row, log_cap rows (ring)
     int log_cap;
 };
@@ -180,9 +182,8 @@ void launch_mlp_grad(const float* master, const float* X, const float* T, int n,
                      cudaStream_t st);
 void launch_mlp_train(float* master, float* m1, float* m2, float* G, const float* X, const float* T, int n,
                       int epochs, float lr, unsigned seed, float* loss_out, cudaStream_t st);
-// features of the running iteration -> log row; with sp.learned also the dt of the first attempt.
-// stat_blocks = blocks of the attempt kernels (entries of sp.stat_part)
-void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* master, int stat_blocks, cudaStream_t st);
+// features of the running iteration -> log row; with sp.learned also the dt of the first attempt
+void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* master, cudaStream_t st);
 int attempt_blocks(int cap_cells);
 
 // division (growth.hpp:66-426), abm_divide.cu

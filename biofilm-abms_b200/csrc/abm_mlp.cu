@@ -7,8 +7,8 @@
 //   k_mlp_forward    batch inference, 16-row tiles per warp
 //   k_mlp_grad       loss and gradient of a batch (checked against a CPU restatement)
 //   k_mlp_train      mini-batch Adam on a logged data set, one block of 4 warps
-//   k_mlp_propose    inside the loop, one warp per iteration: the features of the
-//                    iteration -> log row, and (learned controller) the network's dt
+//   k_mlp_propose    inside the loop, one block of 8 warps per iteration: the features
+//                    of the iteration -> log row, and (learned controller) the network's dt
 //
 // Forward arithmetic is identical in all of them: the same MMA sequence over the
 // same BF16 operands, then bias and ReLU in FP32.
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(128) k_mlp_train(float* W, float* m1, float* m
 }
 
 // ---------------------------------------------------------------------------
-// Inside the loop (one warp, after the pair force, before the first attempt).
+// Inside the loop (after the pair force, before the first attempt).
 // Features, in order:
 //   0       ln(n) / 10
 //   1       log10(max |v_r| + 1e-12) / 4     (velocities of the last accepted step)
@@ -353,32 +353,50 @@ __global__ void __launch_bounds__(128) k_mlp_train(float* W, float* m1, float* m
 // the proposal is the classical one-step controller, which keeps dt stable.
 // After a failed first attempt among the last 8 steps the correction is capped at 0.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(32) k_mlp_propose(Ctrl* ctrl, StepParams sp, const float* __restrict__ W,
-                                                    int stat_blocks)
+// One 8-unit tile of a hidden layer for row 0 (the other 15 rows of the MMA are
+// zero): warp `j` computes units 8j..8j+7 from the layer input in shared memory,
+// with the same MMA sequence (k-steps in order) as mlp_tile_forward_regs.
+template <int K>
+__device__ __forceinline__ void row0_tile(const float* __restrict__ W, int w_off, int b_off, const float* in,
+                                          float* out, int j)
 {
-    __shared__ float feat[MLP_IN];
-    const int lane = threadIdx.x;
-    // block-order sums of the last final attempt's partials (deterministic)
-    double vmax = 0.0, v2 = 0.0, gs = 0.0, near = 0.0;
-    if (ctrl->iterations > 0)
-        for (int b = lane; b < stat_blocks; b += 32)
-        {
-            const double4 p = sp.stat_part[b];
-            vmax = fmax(vmax, p.x); v2 += p.y; gs += p.z; near += p.w;
-        }
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    const float* wr = W + w_off + (8 * j + g) * K;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
+    for (int kk = 0; kk < K / 16; ++kk)
     {
-        vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
-        v2 += __shfl_xor_sync(0xffffffffu, v2, off);
-        gs += __shfl_xor_sync(0xffffffffu, gs, off);
-        near += __shfl_xor_sync(0xffffffffu, near, off);
+        const int k0 = 16 * kk + 2 * t;
+        const uint32_t a0 = g == 0 ? pack_bf16(in[k0], in[k0 + 1]) : 0u;
+        const uint32_t a2 = g == 0 ? pack_bf16(in[k0 + 8], in[k0 + 9]) : 0u;
+        mma_bf16(c, a0, 0u, a2, 0u, pack_bf16(wr[k0], wr[k0 + 1]), pack_bf16(wr[k0 + 8], wr[k0 + 9]));
     }
+    if (g == 0)
+    {
+        out[8 * j + 2 * t] = fmaxf(c[0] + W[b_off + 8 * j + 2 * t], 0.f);
+        out[8 * j + 2 * t + 1] = fmaxf(c[1] + W[b_off + 8 * j + 2 * t + 1], 0.f);
+    }
+}
+
+// 8 warps: features, then layer 1 and layer 2 one 8-unit tile per warp, then the
+// output unit on warp 0 (bit-identical to mlp_tile_forward_regs for row 0)
+__global__ void __launch_bounds__(256) k_mlp_propose(Ctrl* ctrl, StepParams sp, const float* __restrict__ W)
+{
+    __shared__ float feat[MLP_IN], h1[MLP_H], h2[MLP_H];
+    __shared__ float sh_base;
+    __shared__ int sh_fail;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = ctrl->n;
     const double inv_n = 1.0 / (double)max(n, 1);
-    if (lane == 0)
+    if (tid == 0)
     {
+        // sums of the last accepted step (final attempt or commit), then reset
+        const double vmax = __longlong_as_double((long long)ctrl->st_vmax_bits);
+        const double v2 = ldexp((double)ctrl->st_v2_fx, -STAT_V2_SHIFT);
+        const double gs = ldexp((double)ctrl->st_g_fx, -STAT_G_SHIFT);
+        const double near = (double)ctrl->st_near_div;
         const double ovl = __longlong_as_double((long long)ctrl->st_ovl_bits);
+        ctrl->st_vmax_bits = 0ull; ctrl->st_v2_fx = 0ull; ctrl->st_g_fx = 0ull; ctrl->st_near_div = 0ull;
         ctrl->st_ovl_bits = 0ull;
         feat[0] = (float)(log((double)max(n, 1)) / 10.0);
         feat[1] = (float)(log10(vmax + 1e-12) / 4.0);
@@ -389,48 +407,69 @@ __global__ void __launch_bounds__(32) k_mlp_propose(Ctrl* ctrl, StepParams sp, c
         feat[30] = (float)log10(1.0 + (double)ctrl->n_divide);
         feat[31] = (float)(log1p((double)ctrl->since_div) / 5.0);
     }
-    if (lane < HIST)
+    if (tid >= 32 && tid < 32 + HIST)
     {
-        const int slot = (ctrl->hist_pos - 1 - lane + 2 * HIST) % HIST;
+        const int k = tid - 32;
+        const int slot = (ctrl->hist_pos - 1 - k + 2 * HIST) % HIST;
         const bool have = ctrl->hist_dt[slot] > 0;
         const double hd = have ? ctrl->hist_dt[slot] : ctrl->dt;
         const double he = have ? ctrl->hist_err[slot] : 1.0;
-        feat[4 + lane] = (float)log10(hd / sp.max_stepsize);
-        feat[12 + lane] = (float)(log10(fmax(he, 1e-30)) / 10.0);
-        feat[20 + lane] = have ? (float)ctrl->hist_acc[slot] : 1.f;
+        feat[4 + k] = (float)log10(hd / sp.max_stepsize);
+        feat[12 + k] = (float)(log10(fmax(he, 1e-30)) / 10.0);
+        feat[20 + k] = have ? (float)ctrl->hist_acc[slot] : 1.f;
     }
-    __syncwarp();
-    // ln E_last = ln(10) * 10 * feature 12
-    const float base = (float)(log(0.9) - sp.inv_q1 * (double)(2.302585093f * 10.f * feat[12]));
-    if (sp.log_cap > 0)
+    __syncthreads();
+    if (tid == 0)
+    {
+        // ln E_last = ln(10) * 10 * feature 12
+        sh_base = (float)(log(0.9) - sp.inv_q1 * (double)(2.302585093f * 10.f * feat[12]));
+        int fail = 0;
+        for (int k = 0; k < HIST; ++k) fail |= feat[20 + k] < 0.5f;
+        sh_fail = fail;
+    }
+    __syncthreads();
+    if (sp.log_cap > 0 && wid == 0)
     {
         float* row = sp.log_buf + (size_t)(ctrl->log_rows % sp.log_cap) * MLP_LOG_COLS;
         row[lane] = feat[lane];
-        if (lane == 0) { row[36] = base; row[37] = 0.f; row[38] = 0.f; row[39] = 0.f; }
+        if (lane == 0) { row[36] = sh_base; row[37] = 0.f; row[38] = 0.f; row[39] = 0.f; }
     }
     const double dt_prev = ctrl->dt;
-    double dt_next = dt_prev;
-    if (sp.learned)
+    if (!sp.learned)
     {
-        auto x = [&](int r, int k) { return r == 0 ? feat[k] : 0.f; };
-        const float2 y = mlp_tile_forward_regs(W, x);
-        float y0 = __shfl_sync(0xffffffffu, y.x, 0);
+        if (tid == 0) ctrl->dt_prev = dt_prev;
+        return;
+    }
+    row0_tile<MLP_IN>(W, MLP_OFF_W1, MLP_OFF_B1, feat, h1, wid);
+    __syncthreads();
+    row0_tile<MLP_H>(W, MLP_OFF_W2, MLP_OFF_B2, h1, h2, wid);
+    __syncthreads();
+    if (wid != 0) return;
+    const int g = lane >> 2, t = lane & 3;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    const float* w3 = W + MLP_OFF_W3;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+    {
+        const int k0 = 16 * kk + 2 * t;
+        const uint32_t a0 = g == 0 ? pack_bf16(h2[k0], h2[k0 + 1]) : 0u;
+        const uint32_t a2 = g == 0 ? pack_bf16(h2[k0 + 8], h2[k0 + 9]) : 0u;
+        const uint32_t b0 = g == 0 ? pack_bf16(w3[k0], w3[k0 + 1]) : 0u;
+        const uint32_t b1 = g == 0 ? pack_bf16(w3[k0 + 8], w3[k0 + 9]) : 0u;
+        mma_bf16(c, a0, 0u, a2, 0u, b0, b1);
+    }
+    if (lane == 0)
+    {
+        float y0 = c[0] + W[MLP_OFF_B3];
         // after a failed first attempt among the last 8 steps the network may only
         // shrink the step: a network that keeps asking for too much cannot make
         // every proposal fail
-        bool recent_fail = false;
-        for (int k = 0; k < HIST; ++k) recent_fail |= feat[20 + k] < 0.5f;
-        if (recent_fail) y0 = fminf(y0, 0.f);
+        if (sh_fail) y0 = fminf(y0, 0.f);
         // ln ratio within the reference controller's factor bounds [0.2, 10]
         // (simulation.hpp:1710-1713), then the step-size bounds (:1752-1757)
-        const double r = fmin(fmax((double)(base + y0), log(0.2)), log(10.0));
-        dt_next = fmin(fmax(dt_prev * exp(r), sp.min_stepsize), sp.max_stepsize);
-    }
-    __syncwarp();
-    if (lane == 0)
-    {
+        const double r = fmin(fmax((double)(sh_base + y0), log(0.2)), log(10.0));
         ctrl->dt_prev = dt_prev;
-        ctrl->dt = dt_next;
+        ctrl->dt = fmin(fmax(dt_prev * exp(r), sp.min_stepsize), sp.max_stepsize);
     }
 }
 
@@ -459,9 +498,9 @@ void launch_mlp_train(float* W, float* m1, float* m2, float* G, const float* X, 
     k_mlp_train<<<1, 32 * MLP_WARPS, sm, st>>>(W, m1, m2, G, X, T, n, epochs, lr, seed, loss_out);
 }
 
-void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* W, int stat_blocks, cudaStream_t st)
+void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* W, cudaStream_t st)
 {
-    k_mlp_propose<<<1, 32, 0, st>>>(ctrl, sp, W, stat_blocks);
+    k_mlp_propose<<<1, 256, 0, st>>>(ctrl, sp, W);
 }
 
 }   // namespace abm

@@ -57,6 +57,8 @@ class AbmParams(ctypes.Structure):
         ("cap_neighbors_per_cell", ctypes.c_int), ("pair_lanes", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
         ("controller", ctypes.c_int), ("stepsize_log_capacity", ctypes.c_int),
+        ("dims", ctypes.c_int), ("sigma0", ctypes.c_double), ("adhesion_strength", ctypes.c_double),
+        ("adhesion_mindist", ctypes.c_double), ("max_noise", ctypes.c_double),
     ]
 
 
@@ -96,7 +98,13 @@ DEFAULTS = dict(
     growth_mean=0.0, growth_std=0.0, daughter_length_std=0.0, daughter_angle_xy_bound=0.0,
     daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
     cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
+    dims=3, sigma0=100.0, adhesion_strength=0.0, adhesion_mindist=0.0, max_noise=0.0,
 )
+
+# The 2-D driver (ABM-2d/ABM-2d-cpp/include/simulation.hpp:163-237): Bogacki-Shampine 3(2),
+# Hertz E0 = 3900 and Ecell = 3.9e6, sigma0 = 100 for the contact density, JKR-Lagrange
+# adhesion off unless requested.
+DEFAULTS_2D = dict(dims=2, integration_mode=BOGACKI_SHAMPINE, adhesion_mode=0)
 
 
 def make_params(**kw):
@@ -150,6 +158,8 @@ def _load():
         "abm_iterate": ([vp, i, i, P(AbmStats)], i),
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
+        "abm_get_adhesion_flags": ([vp, ip, i, ip], i),
+        "abm_set_adhesion_flags": ([vp, ip, i], i),
         "abm_stepsize_set_weights": ([vp, fp, i], i),
         "abm_stepsize_get_weights": ([vp, fp, i], i),
         "abm_stepsize_get_log": ([vp, fp, i, ip], i),
@@ -175,7 +185,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
             "abm_cell_cell_forces_noalloc abm_noalloc_last_error abm_stepsize_set_weights "
             "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
-            "abm_mlp_grad abm_mlp_train abm_mlp_last_error").split()
+            "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
@@ -220,7 +230,9 @@ class Simulation:
             self._ctx = None
             raise RuntimeError("abm_create failed (%s): %s" % (ERRORS.get(rc, rc), msg))
         self.ncols = None
-        if self.params.adhesion_mode:
+        self.dims = 2 if self.params.dims == 2 else 3
+        self.nq = 4 if self.dims == 2 else 6          # generalized coordinates per cell
+        if self.params.adhesion_mode and self.dims == 3:
             if jkr_table is None:
                 jkr_table = jkr_radius_table(self.params.R, self.params.Rcell, self.params.E0, gamma,
                                              n_mesh_overlap)
@@ -316,10 +328,10 @@ class Simulation:
         return m.value
 
     def neighbors(self):
-        """(m, 7) table in the reference's row order with current distances."""
+        """(m, 7) table (2-D: (m, 6)) in the reference's row order with current distances."""
         m = ctypes.c_int()
         self._check(LIB.abm_download_neighbors(self._ctx, None, 0, 0, ctypes.byref(m)), "abm_download_neighbors")
-        out = np.zeros((m.value, 7), dtype=np.float64, order="F")
+        out = np.zeros((m.value, 6 if self.dims == 2 else 7), dtype=np.float64, order="F")
         ld = max(m.value, 1)
         self._check(LIB.abm_download_neighbors(self._ctx, _dptr(out), ld, m.value, ctypes.byref(m)),
                     "abm_download_neighbors")
@@ -332,13 +344,13 @@ class Simulation:
 
     def cell_cell_forces(self):
         n = self.num_cells()
-        out = np.zeros((n, 6), dtype=np.float64, order="F")
+        out = np.zeros((n, self.nq), dtype=np.float64, order="F")
         self._check(LIB.abm_cell_cell_forces(self._ctx, _dptr(out)), "abm_cell_cell_forces")
         return out
 
     def get_velocities(self):
         n = self.num_cells()
-        out = np.zeros((n, 6), dtype=np.float64, order="F")
+        out = np.zeros((n, self.nq), dtype=np.float64, order="F")
         self._check(LIB.abm_get_velocities(self._ctx, _dptr(out)), "abm_get_velocities")
         return out
 
@@ -346,7 +358,7 @@ class Simulation:
         """One RK attempt at dt (not accepted): (new cells, errors, scaled max error)."""
         n = self.num_cells()
         cells = np.zeros((n, self.ncols), dtype=np.float64, order="F")
-        errors = np.zeros((n, 6), dtype=np.float64, order="F")
+        errors = np.zeros((n, self.nq), dtype=np.float64, order="F")
         e = ctypes.c_double()
         self._check(LIB.abm_rk_attempt(self._ctx, dt, attempt, _dptr(cells), _dptr(errors), ctypes.byref(e)),
                     "abm_rk_attempt")
@@ -387,6 +399,20 @@ class Simulation:
         s = AbmStats()
         self._check(LIB.abm_get_stats(self._ctx, ctypes.byref(s)), "abm_get_stats")
         return s.as_dict()
+
+    # ---- 2-D adhesion flags (to_adhere, 2D/include/simulation.hpp:242-258) ----
+    def adhesion_flags(self):
+        m = ctypes.c_int()
+        self._check(LIB.abm_get_adhesion_flags(self._ctx, None, 0, ctypes.byref(m)), "abm_get_adhesion_flags")
+        a = np.zeros(max(m.value, 1), dtype=np.int32)
+        self._check(LIB.abm_get_adhesion_flags(self._ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), m.value,
+                                               ctypes.byref(m)), "abm_get_adhesion_flags")
+        return a[:m.value]
+
+    def set_adhesion_flags(self, flags):
+        a = np.ascontiguousarray(flags, dtype=np.int32)
+        self._check(LIB.abm_set_adhesion_flags(self._ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)),
+                    "abm_set_adhesion_flags")
 
     # ---- step-size network (no reference counterpart) ----
     def set_stepsize_weights(self, weights):

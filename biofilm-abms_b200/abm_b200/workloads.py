@@ -15,6 +15,7 @@ import ctypes
 import numpy as np
 
 NCOLS_3D = 22   # indices.hpp:17-47 plus gamma (column 21)
+NCOLS_2D = 17   # ABM-2d/ABM-2d-cpp/include/indices.hpp:17-41
 
 
 def _generate(n, seed, disk_radius, z_lo, z_hi, lmin, lmax, min_gap, contact_dist, p_contact,
@@ -88,4 +89,53 @@ def two_cell_3d(r1, n1, r2, n2, half_l=0.5, eta0=100.0, eta1=720.0, sigma0=100.0
         cells[k, 19] = sigma0
         cells[k, 20] = 1
         cells[k, 21] = gamma
+    return cells
+
+
+def biofilm_2d(n, seed=1, disk_radius=None, lmin=2.0, lmax=4.4, R=0.8, Rcell=0.5, eta0=100.0, eta1=100.0,
+               growth=0.0, min_gap=None, p_contact=0.9, density=0.1):
+    """A seeded 2-D colony in the 17-column layout of ABM-2d/ABM-2d-cpp/include/indices.hpp:
+    centres uniform in a disk (radius from `density` cells per um^2 unless given),
+    orientations uniform in the plane, lengths uniform on [lmin, lmax], contacts
+    inside the EPS shell as in biofilm_3d."""
+    from . import LIB
+    gap = 2 * Rcell + 0.1 if min_gap is None else min_gap
+    if disk_radius is None:
+        disk_radius = float(np.sqrt(n / (np.pi * density)))
+    LIB.abm_generate_biofilm_2d.argtypes = [
+        ctypes.c_int, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+        ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.POINTER(ctypes.c_int)]
+    LIB.abm_generate_biofilm_2d.restype = ctypes.c_int
+    r = np.zeros((n, 3))
+    nv = np.zeros((n, 3))
+    l = np.zeros(n)
+    placed = ctypes.c_int()
+    rc = LIB.abm_generate_biofilm_2d(n, seed, disk_radius, lmin, lmax, gap, 2 * R, p_contact, 10000,
+                                     r.ctypes.data, nv.ctypes.data, l.ctypes.data, ctypes.byref(placed))
+    if rc:
+        raise RuntimeError("could only place %d of %d cells" % (placed.value, n))
+    cells = np.zeros((n, NCOLS_2D), dtype=np.float64, order="F")
+    cells[:, 0] = np.arange(n)
+    cells[:, 1:3] = r[:, :2]
+    cells[:, 3:5] = nv[:, :2]
+    cells[:, 9] = l
+    cells[:, 10] = l / 2
+    cells[:, 12] = growth
+    cells[:, 13] = eta0
+    cells[:, 14] = eta1
+    cells[:, 15] = eta1
+    return cells
+
+
+def founder_2d(L0=2.0, growth=1.5, eta0=100.0, eta1=100.0):
+    """One cell at the origin along (1, 0) with centreline length L0 (the 2-D driver's start)."""
+    cells = np.zeros((1, NCOLS_2D), dtype=np.float64, order="F")
+    cells[0, 3] = 1.0
+    cells[0, 9] = L0
+    cells[0, 10] = L0 / 2
+    cells[0, 12] = growth
+    cells[0, 13] = eta0
+    cells[0, 14] = eta1
+    cells[0, 15] = eta1
     return cells

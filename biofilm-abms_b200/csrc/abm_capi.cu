@@ -54,6 +54,9 @@ struct abm_ctx {
     float* mlp_w = nullptr;          // ABM_MLP_NPARAM FP32 master weights
     float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
     bool mlp_loaded = false;
+    // 2-D model
+    int dims = 3;
+    unsigned char* adhere = nullptr;  // to_adhere per CSR entry
     // parameters
     ForceParams fp; StepParams sp; BuildParams bp;
     // graphs
@@ -128,7 +131,7 @@ static void free_all(abm_ctx* c)
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
-                    c->dgrowth, c->mlp_w, c->log_buf};
+                    c->dgrowth, c->mlp_w, c->log_buf, c->adhere};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -310,6 +313,29 @@ int abm_create(const abm_params* q, abm_ctx** out)
     dp.seed = p.rng_seed; dp.cap_cells = c->cap;
     if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
         return fail(c, ABM_ERR_ARG, "adhesion_mode must be 0 (none) or 1 (isotropic JKR, fixed gamma)");
+    // 2-D model
+    c->dims = (p.dims == 0) ? 3 : p.dims;
+    if (c->dims != 2 && c->dims != 3) return fail(c, ABM_ERR_ARG, "dims must be 2 or 3");
+    if (c->dims == 2)
+    {
+        if (p.integration_mode != ABM_HEUN_EULER && p.integration_mode != ABM_BOGACKI_SHAMPINE)
+            return fail(c, ABM_ERR_ARG, "the 2-D model integrates with ABM_BOGACKI_SHAMPINE or ABM_HEUN_EULER");
+        if (p.daughter_angle_z_bound != 0) return fail(c, ABM_ERR_ARG, "2-D daughters have no out-of-plane angle");
+        if (p.precision != ABM_PRECISION_FP64) return fail(c, ABM_ERR_ARG, "the 2-D model runs in FP64");
+        // 2D/include/simulation.hpp:232-237
+        fp.pf2d[0] = 2.5 * p.E0 * std::sqrt(p.R);
+        fp.pf2d[1] = 2.5 * p.E0 * std::sqrt(p.R) * std::pow(2 * (p.R - p.Rcell), 2.5);
+        fp.pf2d[2] = 2.5 * p.Ecell * std::sqrt(p.Rcell);
+        fp.adh_strength = p.adhesion_strength;
+        fp.adh_mindist = p.adhesion_mindist;
+        sp.rho_c = std::pow(p.sigma0 * p.R * p.R / (4 * p.E0), 1. / 3.);
+        sp.max_noise_2d = p.max_noise;
+        sp.noise_on = p.max_noise > 0;
+        dp.angle_z_bound = 0.0;
+        CK(cudaMalloc(&c->adhere, cap * c->cap_nbr));
+        CK(cudaMemset(c->adhere, 0, cap * c->cap_nbr));
+        fp.adhere = c->adhere;
+    }
     if (p.controller != ABM_CONTROLLER_REFERENCE && p.controller != ABM_CONTROLLER_LEARNED)
         return fail(c, ABM_ERR_ARG, "controller must be ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED");
     if (p.stepsize_log_capacity < 0) return fail(c, ABM_ERR_ARG, "stepsize_log_capacity must be >= 0");
@@ -387,15 +413,19 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
 {
     if (!c || !cm || n < 0 || ld < n) return fail(c, ABM_ERR_ARG, "bad cell array");
     if (n > c->cap) return fail(c, ABM_ERR_CAPACITY, "more cells than cap_cells");
-    if (ncols < 21 || ncols > STAGING_COLS) return fail(c, ABM_ERR_ARG, "cell arrays need 21..32 columns");
-    if (c->p.adhesion_mode != 0 && ncols < 22) return fail(c, ABM_ERR_ARG, "adhesion needs the gamma column (21)");
+    const bool two_d = c->dims == 2;
+    if (two_d && (ncols < 17 || ncols > STAGING_COLS)) return fail(c, ABM_ERR_ARG, "2-D cell arrays need 17..32 columns");
+    if (!two_d && (ncols < 21 || ncols > STAGING_COLS)) return fail(c, ABM_ERR_ARG, "cell arrays need 21..32 columns");
+    if (!two_d && c->p.adhesion_mode != 0 && ncols < 22)
+        return fail(c, ABM_ERR_ARG, "adhesion needs the gamma column (21)");
     c->ncols = ncols;
-    c->has_gamma = (c->p.adhesion_mode != 0);
+    c->has_gamma = !two_d && (c->p.adhesion_mode != 0);
     if (n > 0)
     {
         CK(cudaMemcpy2DAsync(c->staging, (size_t)n * sizeof(double), cm, (size_t)ld * sizeof(double),
                              (size_t)n * sizeof(double), ncols, cudaMemcpyHostToDevice, c->st));
-        launch_cells_from_colmajor(c->staging, n, ncols, n, c->has_gamma, c->geom, c->vel, c->phys, c->st);
+        if (two_d) launch_cells_from_colmajor_2d(c->staging, n, ncols, n, c->geom, c->vel, c->phys, c->st);
+        else launch_cells_from_colmajor(c->staging, n, ncols, n, c->has_gamma, c->geom, c->vel, c->phys, c->st);
     }
     k_set_n<<<1, 1, 0, c->st>>>(c->ctrl, n);
     CK(cudaGetLastError());
@@ -404,8 +434,9 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     c->cells_loaded = true;
     // division is possible when a cell already exceeds Ldiv or any cell can grow
     bool grows = (c->p.growth_mean != 0 || c->p.growth_std != 0);
+    const int col_growth = two_d ? 12 : 16, col_l = two_d ? 9 : 13;
     for (int i = 0; i < n && !grows; ++i)
-        grows = cm[(size_t)16 * ld + i] != 0 || cm[(size_t)13 * ld + i] > c->p.Ldiv;
+        grows = cm[(size_t)col_growth * ld + i] != 0 || cm[(size_t)col_l * ld + i] > c->p.Ldiv;
     if (grows != c->div_enabled && c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
     c->div_enabled = grows;
     return ABM_OK;
@@ -423,7 +454,8 @@ int abm_download_cells(abm_ctx* c, double* cm, int ld)
     if (ld < n) return fail(c, ABM_ERR_ARG, "ld smaller than the cell count");
     if (n > 0)
     {
-        launch_cells_to_colmajor(c->geom, c->vel, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        if (c->dims == 2) launch_cells_to_colmajor_2d(c->geom, c->vel, c->phys, n, c->ncols, n, c->staging, c->st);
+        else launch_cells_to_colmajor(c->geom, c->vel, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
         CK(cudaMemcpy2DAsync(cm, (size_t)ld * sizeof(double), c->staging, (size_t)n * sizeof(double),
                              (size_t)n * sizeof(double), c->ncols, cudaMemcpyDeviceToHost, c->st));
     }
@@ -500,6 +532,8 @@ static void enqueue_rebuild(abm_ctx* c)
     launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
     launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
     launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st);
+    if (c->dims == 2 && c->p.adhesion_mode != 0)
+        launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, st);
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
 }
 
@@ -510,7 +544,7 @@ static void enqueue_pair_force(abm_ctx* c, int with_gather)
 {
     launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta,
                       c->jkr_radius, c->fcc, c->jbuf, c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED,
-                      c->cap, c->st, with_gather);
+                      c->cap, c->st, with_gather, c->dims);
 }
 
 // the attempts of one iteration; the first one completes the pair-force sum
@@ -531,12 +565,12 @@ static void enqueue_attempts(abm_ctx* c)
     cudaStream_t st = c->st;
     PairGather pg = loop_gather(c);
     launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
+                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
     for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
         launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
+                       c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg);
+                   c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
 }
 
 static void enqueue_iteration(abm_ctx* c)
@@ -652,7 +686,7 @@ static int build_iteration_graph(abm_ctx* c)
         enqueue_pair_force(c, 0);
         enqueue_propose(c);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg);
+                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg, c->dims);
     });
     if (rc) return rc;
     if (retries)
@@ -663,13 +697,13 @@ static int build_iteration_graph(abm_ctx* c)
         std::vector<cudaGraphNode_t> bd;
         rc = capture_into(c, body, bd, [&]() {
             launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c,
-                           nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg);
+                           nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg, c->dims);
         });
         if (rc) return rc;
     }
     rc = capture_into(c, G, deps, [&]() {
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg);
+                       c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
     });
     if (rc) return rc;
     cudaError_t inst = cudaGraphInstantiate(&c->g_iter, G, 0);
@@ -700,7 +734,7 @@ static int divide_now(abm_ctx* c, bool rebuild, int* n_divided)
 static int ready_for_forces(abm_ctx* c)
 {
     if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
-    if (c->p.adhesion_mode != 0 && c->jkr_n < 2) return fail(c, ABM_ERR_STATE, "JKR table not set");
+    if (c->dims == 3 && c->p.adhesion_mode != 0 && c->jkr_n < 2) return fail(c, ABM_ERR_STATE, "JKR table not set");
     return ABM_OK;
 }
 
@@ -735,12 +769,13 @@ int abm_download_neighbors(abm_ctx* c, double* rows, int ld, int cap, int* m)
     if (cap < mm || ld < mm) return fail(c, ABM_ERR_CAPACITY, "row buffer too small");
     launch_count_lower(c->ctrl, c->row_ptr, c->col, c->nbr_count, c->cap, c->st);
     launch_scan(c->nbr_count, &c->ctrl->n, c->key, c->scan_sums, c->cap, c->st);
+    const int ncol = c->dims == 2 ? 6 : 7;
     double* d_rows = nullptr;
-    CK(cudaMallocAsync(&d_rows, (size_t)std::max(mm, 1) * 7 * sizeof(double), c->st));
-    launch_table_rows(c->ctrl, c->row_ptr, c->col, c->key, c->geom, d_rows, std::max(mm, 1), c->cap, c->st);
+    CK(cudaMallocAsync(&d_rows, (size_t)std::max(mm, 1) * ncol * sizeof(double), c->st));
+    launch_table_rows(c->ctrl, c->row_ptr, c->col, c->key, c->geom, d_rows, std::max(mm, 1), c->cap, c->st, c->dims);
     if (mm > 0)
         CK(cudaMemcpy2DAsync(rows, (size_t)ld * sizeof(double), d_rows, (size_t)mm * sizeof(double),
-                             (size_t)mm * sizeof(double), 7, cudaMemcpyDeviceToHost, c->st));
+                             (size_t)mm * sizeof(double), ncol, cudaMemcpyDeviceToHost, c->st));
     CK(cudaFreeAsync(d_rows, c->st));
     CK(cudaStreamSynchronize(c->st));
     return ABM_OK;
@@ -774,17 +809,28 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
     h.n_dir = (int)cl.size();
     CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
     launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st);
+    if (c->dims == 2 && c->p.adhesion_mode != 0)
+        launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, c->st);
     CK(cudaGetLastError());
     c->nbrs_valid = true;
     return ABM_OK;
 }
 
+// n x 6 (3-D) or the (x, y, nx, ny) columns n x 4 (2-D)
 static int download_gen6(abm_ctx* c, const Gen6* src, double* out)
 {
     int n = c->n_host;
     if (n == 0) return ABM_OK;
     launch_gen6_to_colmajor(src, n, c->staging, c->st);
-    CK(cudaMemcpyAsync(out, c->staging, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    if (c->dims == 2)
+    {
+        const int cols[4] = {0, 1, 3, 4};
+        for (int k = 0; k < 4; ++k)
+            CK(cudaMemcpyAsync(out + (size_t)k * n, c->staging + (size_t)cols[k] * n, (size_t)n * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->st));
+    }
+    else
+        CK(cudaMemcpyAsync(out, c->staging, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return ABM_OK;
 }
@@ -795,9 +841,18 @@ int abm_cell_cell_forces(abm_ctx* c, double* out)
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
-                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    enqueue_pair_force(c, 1);
     CK(cudaGetLastError());
+    if (c->dims == 2)
+    {
+        // the reference's 2-D dE/dq projects each pair's torque with the current n
+        const int n = c->n_host;
+        if (n == 0) return ABM_OK;
+        launch_pair_dEdq_2d(c->geom, c->fcc, c->ctrl, c->staging, c->cap, c->st);
+        CK(cudaMemcpyAsync(out, c->staging, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return ABM_OK;
+    }
     return download_gen6(c, c->fcc, out);
 }
 
@@ -807,9 +862,8 @@ int abm_get_velocities(abm_ctx* c, double* out)
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
-                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
-    launch_velocities(c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->gen_tmp, c->cap, c->st);
+    enqueue_pair_force(c, 1);
+    launch_velocities(c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->gen_tmp, c->cap, c->st, c->dims);
     CK(cudaGetLastError());
     rc = download_gen6(c, c->gen_tmp, out);
     if (rc) return rc;
@@ -825,16 +879,16 @@ int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
-    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf,
-                      c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED, c->cap, c->st);
+    enqueue_pair_force(c, 1);
     k_clear_eval<<<1, 1, 0, c->st>>>(c->ctrl);
     launch_attempt(3, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->gen_tmp,
-                   c->k0buf, dt, attempt, c->cap, c->st);
+                   c->k0buf, dt, attempt, c->cap, c->st, 0, 0, PairGather{0, 0, 0, 0, 0}, c->dims);
     CK(cudaGetLastError());
     const int n = c->n_host;
     if (cells_out && n > 0)
     {
-        launch_cells_to_colmajor(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        if (c->dims == 2) launch_cells_to_colmajor_2d(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->staging, c->st);
+        else launch_cells_to_colmajor(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
         CK(cudaMemcpyAsync(cells_out, c->staging, (size_t)n * c->ncols * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     }
     if (errors_out)
@@ -1008,6 +1062,55 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     prof->iterations = n_iters;
     for (auto& e : ev) cudaEventDestroy(e);
     return check_status(c);
+}
+
+// lower CSR entry of every neighbor row (i ascending, j < i ascending), on the host
+static int row_entries(abm_ctx* c, std::vector<int>& entries)
+{
+    const int n = c->n_host;
+    std::vector<int> rp(n + 1), cl;
+    CK(cudaMemcpyAsync(rp.data(), c->row_ptr, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    cl.resize(rp[n]);
+    if (rp[n] > 0) CK(cudaMemcpy(cl.data(), c->col, rp[n] * sizeof(int), cudaMemcpyDeviceToHost));
+    entries.clear();
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (cl[k] < i) entries.push_back(k);
+    return ABM_OK;
+}
+
+int abm_get_adhesion_flags(abm_ctx* c, int* flags, int cap, int* m)
+{
+    if (!c || !m) return ABM_ERR_ARG;
+    if (c->dims != 2) return fail(c, ABM_ERR_STATE, "adhesion flags belong to the 2-D model");
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    std::vector<int> e;
+    int rc = row_entries(c, e);
+    if (rc) return rc;
+    *m = (int)e.size();
+    if (!flags) return ABM_OK;
+    if (cap < (int)e.size()) return fail(c, ABM_ERR_CAPACITY, "flag buffer too small");
+    std::vector<unsigned char> a(std::max<size_t>(1, (size_t)c->cap * c->cap_nbr));
+    if (!e.empty()) CK(cudaMemcpy(a.data(), c->adhere, (size_t)(e.back() + 1), cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < e.size(); ++r) flags[r] = a[e[r]];
+    return ABM_OK;
+}
+
+int abm_set_adhesion_flags(abm_ctx* c, const int* flags, int m)
+{
+    if (!c || (m > 0 && !flags)) return ABM_ERR_ARG;
+    if (c->dims != 2) return fail(c, ABM_ERR_STATE, "adhesion flags belong to the 2-D model");
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    std::vector<int> e;
+    int rc = row_entries(c, e);
+    if (rc) return rc;
+    if ((int)e.size() != m) return fail(c, ABM_ERR_ARG, "one flag per neighbor row");
+    if (m == 0) return ABM_OK;
+    std::vector<unsigned char> a((size_t)e.back() + 1, 0);
+    for (int r = 0; r < m; ++r) a[e[r]] = flags[r] ? 1 : 0;
+    CK(cudaMemcpy(c->adhere, a.data(), a.size(), cudaMemcpyHostToDevice));
+    return ABM_OK;
 }
 
 int abm_stepsize_set_weights(abm_ctx* c, const float* w, int n)

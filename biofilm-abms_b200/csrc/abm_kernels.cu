@@ -76,6 +76,55 @@ __global__ void k_gen6_to_colmajor(const Gen6* __restrict__ g, int n, double* cm
     for (int k = 0; k < 6; ++k) cm[(size_t)k * n + i] = v.f[k];
 }
 
+// 2-D layout (ABM-2d/ABM-2d-cpp/include/indices.hpp:17-41): id, r(2), n(2), dr(2), dn(2),
+// l, half_l, t0, growth, eta0, eta1, maxeta1, group; the records hold z = nz = 0 and
+// maxeta1 in the sigma0 slot
+__global__ void k_cells_from_colmajor_2d(const double* __restrict__ cm, int n, int ld, Geom* geom, Vel* vel,
+                                         Phys* phys)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto c = [&](int col) { return cm[(size_t)col * ld + i]; };
+    Geom g;
+    g.rx = c(1); g.ry = c(2); g.rz = 0.0; g.h = c(10);
+    g.nx = c(3); g.ny = c(4); g.nz = 0.0; g.gamma = 0.0;
+    geom[i] = g;
+    Vel v;
+    v.v[0] = c(5); v.v[1] = c(6); v.v[2] = 0.0; v.v[3] = c(7); v.v[4] = c(8); v.v[5] = 0.0;
+    vel[i] = v;
+    Phys p;
+    p.l = c(9); p.t0 = c(11); p.growth = c(12); p.eta0 = c(13); p.eta1 = c(14); p.sigma0 = c(15);
+    p.id = c(0); p.group = c(16);
+    phys[i] = p;
+}
+
+__global__ void k_cells_to_colmajor_2d(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
+                                       const Phys* __restrict__ phys, int n, int ld, double* cm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Geom g = geom[i]; Vel v = vel[i]; Phys p = phys[i];
+    auto w = [&](int col, double x) { cm[(size_t)col * ld + i] = x; };
+    w(0, p.id); w(1, g.rx); w(2, g.ry); w(3, g.nx); w(4, g.ny);
+    w(5, v.v[0]); w(6, v.v[1]); w(7, v.v[3]); w(8, v.v[4]);
+    w(9, p.l); w(10, g.h); w(11, p.t0); w(12, p.growth); w(13, p.eta0); w(14, p.eta1); w(15, p.sigma0);
+    w(16, p.group);
+}
+
+void launch_cells_from_colmajor_2d(const double* cm, int n, int ncols, int ld, Geom* geom, Vel* vel, Phys* phys,
+                                   cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_cells_from_colmajor_2d<<<cdiv(n, 256), 256, 0, st>>>(cm, n, ld, geom, vel, phys);
+}
+
+void launch_cells_to_colmajor_2d(const Geom* geom, const Vel* vel, const Phys* phys, int n, int ncols, int ld,
+                                 double* cm, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_cells_to_colmajor_2d<<<cdiv(n, 256), 256, 0, st>>>(geom, vel, phys, n, ld, cm);
+}
+
 void launch_cells_from_colmajor(const double* cm, int n, int ncols, int ld, int has_gamma,
                                 Geom* geom, Vel* vel, Phys* phys, cudaStream_t st)
 {
@@ -556,12 +605,42 @@ __device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& g
     return out;
 }
 
+// 2-D pair (2D/include/mechanics.hpp:448-547 and :572-670 with
+// 2D/include/adhesion.hpp:403-448).  Returns p = cell i's translational dE/dq of the
+// pair (Hertz v_ij minus strength * the JKR vector); i's torque share is s p and
+// j's is (-p, -t p), projected per RK stage with the stage orientation.
+__device__ __forceinline__ PairOut pair_force_2d(const Geom& gi, const Geom& gj, const ForceParams& fp,
+                                                 bool adhere)
+{
+    PairOut out;
+    out.touch = false;
+    Dist d = dist_geom(gi, gj);
+    const double mag = xnorm(x3(d.dx, d.dy, d.dz));
+    const double overlap = 2 * fp.R - mag;
+    if (!(overlap > 0)) return out;
+    const double dirx = d.dx / mag, diry = d.dy / mag;
+    double prefactor;
+    if (overlap < fp.max_overlap) prefactor = fp.pf2d[0] * pow15(overlap);
+    else prefactor = fp.pf2d[1] + fp.pf2d[2] * pow15(overlap - fp.max_overlap);
+    double px = prefactor * dirx, py = prefactor * diry;
+    if (adhere)
+    {
+        // overlap > 0 implies dist <= 2R
+        const double term = M_PI * fp.R * (2 * fp.R - (mag <= fp.adh_mindist ? fp.adh_mindist : mag));
+        px -= fp.adh_strength * (term * dirx);
+        py -= fp.adh_strength * (term * diry);
+    }
+    out.vx = px; out.vy = py; out.vz = 0.0;
+    out.s = d.s; out.t = d.t; out.ovl = overlap; out.touch = true;
+    return out;
+}
+
 const int PF_T = 256, JKR_MAX = 512;
 
 // Pass 1: G lanes per cell i walk the lower part of its sorted CSR row (j < i),
 // evaluate each unordered pair once, keep i's share and write j's share
 // (v, t) into the slot of i in row j (rev[k]).
-template <int G, bool MIXED>
+template <int G, bool MIXED, int DIM>
 __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ geom, const int* __restrict__ row_ptr,
                                                     const int* __restrict__ lower_end, const int* __restrict__ col,
                                                     const int* __restrict__ rev, Ctrl* ctrl, ForceParams fp,
@@ -587,7 +666,9 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
         {
             const int o = col[k];
             const Geom go = load_geom(geom, o);
-            PairOut p = MIXED ? pair_force_fp32(gc, go, fp, td, tr) : pair_force_fp64(gc, go, fp, td, tr);
+            PairOut p;
+            if (DIM == 2) p = pair_force_2d(gc, go, fp, fp.adhere[k] != 0);
+            else p = MIXED ? pair_force_fp32(gc, go, fp, td, tr) : pair_force_fp64(gc, go, fp, td, tr);
             double4 js = make_double4(0.0, 0.0, 0.0, 0.0);
             if (p.touch)
             {
@@ -653,13 +734,14 @@ __global__ void __launch_bounds__(PF_T) k_pair_gather(const int* __restrict__ ro
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
                        Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
-                       int with_gather)
+                       int with_gather, int dims)
 {
     int blocks = max(cdiv((long long)cap_cells * lanes, PF_T), 1);
 #define PF_CASE(G) \
     if (lanes == G) { \
-        if (mixed) k_pair_force<G, true><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
-        else k_pair_force<G, false><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
+        if (dims == 2) k_pair_force<G, false, 2><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
+        else if (mixed) k_pair_force<G, true, 3><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
+        else k_pair_force<G, false, 3><<<blocks, PF_T, 0, st>>>(geom, row_ptr, lower_end, col, rev, ctrl, fp, jkr_delta, jkr_radius, fcc, jbuf); \
         if (with_gather) k_pair_gather<G><<<blocks, PF_T, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc); \
         return; }
     PF_CASE(4) PF_CASE(8) PF_CASE(16) PF_CASE(32)
@@ -692,6 +774,60 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
                     int cap_cells, cudaStream_t st)
 {
     k_csr_rev<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, lower_end, rev);
+}
+
+// to_adhere (2D/include/simulation.hpp:242-258, one group in the adhesion map):
+// for each lower entry (i, j < i), dist of the (i, j) row > R + Rcell and < 2R
+__global__ void k_adhere_flags(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                               const Geom* __restrict__ geom, double R, double Rcell, unsigned char* adhere)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom gi = load_geom(geom, i);
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+        {
+            const int j = col[k];
+            unsigned char a = 0;
+            if (j < i)
+            {
+                Dist d = dist_geom(gi, load_geom(geom, j));
+                const double dist = xnorm(x3(d.dx, d.dy, d.dz));
+                a = (dist > R + Rcell && dist < 2 * R) ? 1 : 0;
+            }
+            adhere[k] = a;
+        }
+    }
+}
+
+void launch_adhere_flags(const Ctrl* ctrl, const int* row_ptr, const int* col, const Geom* geom, double R,
+                         double Rcell, unsigned char* adhere, int cap_cells, cudaStream_t st)
+{
+    k_adhere_flags<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, geom, R, Rcell, adhere);
+}
+
+// the reference's 2-D dE/dq (cellCellRepulsiveForces + cellCellAdhesiveForces) from the
+// pair sums F = sum p and S = sum s p: torque S - (n . S) n at the current orientation
+__global__ void k_pair_dEdq_2d(const Geom* __restrict__ geom, const Gen6* __restrict__ fcc, const Ctrl* ctrl,
+                               double* cm)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom g = load_geom(geom, i);
+        const Gen6 f = fcc[i];
+        const double w = g.nx * f.f[3] + g.ny * f.f[4];
+        cm[i] = f.f[0];
+        cm[(size_t)n + i] = f.f[1];
+        cm[(size_t)2 * n + i] = f.f[3] - w * g.nx;
+        cm[(size_t)3 * n + i] = f.f[4] - w * g.ny;
+    }
+}
+
+void launch_pair_dEdq_2d(const Geom* geom, const Gen6* fcc, const Ctrl* ctrl, double* cm, int cap_cells,
+                         cudaStream_t st)
+{
+    k_pair_dEdq_2d<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(geom, fcc, ctrl, cm);
 }
 
 // ---------------------------------------------------------------------------
@@ -750,6 +886,38 @@ __device__ __forceinline__ void base_force(const StepParams& sp, const Gen6& cc,
             f0[2 * k + 1] += -sp.noise_max[2 * k + 1] + 2 * sp.noise_max[2 * k + 1] * u1;
         }
     }
+}
+
+// 2-D noise of one attempt (2D/include/mechanics.hpp:1760-1771): uniform on
+// [-max, max] for (rx, ry, nx, ny), from the 3-D counter slots 0, 1, 3, 4
+__device__ __forceinline__ void noise_2d(const StepParams& sp, int iter, int attempt, int i, double nz[4])
+{
+    double u[6];
+    for (int k = 0; k < 3; ++k)
+    {
+        uint32_t x[4] = {(uint32_t)iter, (uint32_t)attempt, (uint32_t)i, (uint32_t)k};
+        philox4x32_10(x, (uint32_t)sp.seed, (uint32_t)(sp.seed >> 32) ^ RNG_PURPOSE_NOISE);
+        u[2 * k] = philox_u01(x[0], x[1]);
+        u[2 * k + 1] = philox_u01(x[2], x[3]);
+    }
+    const double m = sp.max_noise_2d;
+    nz[0] = -m + 2 * m * u[0]; nz[1] = -m + 2 * m * u[1];
+    nz[2] = -m + 2 * m * u[3]; nz[3] = -m + 2 * m * u[4];
+}
+
+// 2-D getVelocities (2D/include/mechanics.hpp:1503-1667) at stage orientation (y3, y4):
+// dE/dq = (F, S - (n . S) n) + noise from the pair sums cc = (F, S); v = -dE/dq / (K, L)
+// with K = l (eta0 + eta1 rho_c / R), L = l^3 (...) / 12 (:264-279)
+__device__ __forceinline__ void velocity_2d(const StepParams& sp, const double y[6], double l, double eta0,
+                                            double eta1, const Gen6& cc, const double nz[4], double v[6])
+{
+    const double drag = eta0 + eta1 * sp.rho_c / sp.mp.R;
+    const double K = l * drag, L = l * l * l * drag / 12;
+    const double w = y[3] * cc.f[3] + y[4] * cc.f[4];
+    const double d0 = cc.f[0] + nz[0], d1 = cc.f[1] + nz[1];
+    const double d2 = (cc.f[3] - w * y[3]) + nz[2], d3 = (cc.f[4] - w * y[4]) + nz[3];
+    v[0] = -d0 / K; v[1] = -d1 / K; v[2] = 0.0;
+    v[3] = -d2 / L; v[4] = -d3 / L; v[5] = 0.0;
 }
 
 __device__ __forceinline__ Gen6 load_gen6(const Gen6* __restrict__ g, int i)
@@ -864,7 +1032,7 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
 // Without noise the stage-0 velocity k0 = f(y0) is the same for every attempt of an
 // iteration (y0 and the pair forces do not change), so the trial stores it in k0buf
 // and the retries and the final attempt read it back.
-template <int S, int KIND, bool NOISE>
+template <int S, int KIND, bool NOISE, int DIM>
 __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
@@ -951,7 +1119,12 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         }
         else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);
         double f0[6];
-        base_force<NOISE>(sp, cc, iter, attempt, i, f0);
+        double nz2[4] = {0.0, 0.0, 0.0, 0.0};
+        if constexpr (DIM == 2)
+        {
+            if (NOISE) noise_2d(sp, iter, attempt, i, nz2);
+        }
+        else base_force<NOISE>(sp, cc, iter, attempt, i, f0);
         double k[S][6];
         if (load_k0)
         {
@@ -961,7 +1134,8 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         }
         else
         {
-            cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[0]);
+            if constexpr (DIM == 2) velocity_2d(sp, y0, l, eta0, eta1, cc, nz2, k[0]);
+            else cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[0]);
             if (store_k0)
             {
                 double2* kp = reinterpret_cast<double2*>(k0buf + i);
@@ -983,7 +1157,8 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                 y[c] = y0[c] + m * dt;
             }
             normalize_n(y);
-            cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[st]);
+            if constexpr (DIM == 2) velocity_2d(sp, y, l, eta0, eta1, cc, nz2, k[st]);
+            else cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[st]);
         }
         double vf1[6], d1[6];
 #pragma unroll
@@ -1110,7 +1285,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     }
 }
 
-template <int S, bool NOISE>
+template <int S, bool NOISE, int DIM>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
                              Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
@@ -1119,10 +1294,10 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 #define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg
     switch (kind)
     {
-        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        default: k_attempt<S, 3, NOISE><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        default: k_attempt<S, 3, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
     }
 #undef AT_ARGS
 }
@@ -1132,19 +1307,46 @@ int attempt_blocks(int cap_cells) { return max(cdiv(cap_cells, AT_T), 1); }
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
-                    unsigned long long cond, int use_cond, PairGather pg)
+                    unsigned long long cond, int use_cond, PairGather pg, int dims)
 {
     int blocks = attempt_blocks(cap_cells);
-#define AT_CASE(S) case S: \
-        if (sp.noise_on) launch_attempt_s<S, true>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
-        else launch_attempt_s<S, false>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
+#define AT_CASE(S, D) case S: \
+        if (sp.noise_on) launch_attempt_s<S, true, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
+        else launch_attempt_s<S, false, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
         break;
+    if (dims == 2)
+    {
+        // the 2-D driver integrates with Bogacki-Shampine 3(2) (2D/include/simulation.hpp:217-228);
+        // Heun-Euler is kept for comparison runs
+        switch (sp.s)
+        {
+            AT_CASE(2, 2) AT_CASE(4, 2)
+            default: break;
+        }
+        return;
+    }
     switch (sp.s)
     {
-        AT_CASE(2) AT_CASE(4) AT_CASE(6) AT_CASE(7)
+        AT_CASE(2, 3) AT_CASE(4, 3) AT_CASE(6, 3) AT_CASE(7, 3)
         default: break;
     }
 #undef AT_CASE
+}
+
+__global__ void k_velocities_2d(const Geom* __restrict__ geom, const Phys* __restrict__ phys,
+                                const Gen6* __restrict__ fcc, const Ctrl* ctrl, StepParams sp, Gen6* v_out)
+{
+    const int n = ctrl->n;
+    const double nz[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom g = load_geom(geom, i);
+        const double y[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
+        const Phys ph = phys[i];
+        Gen6 out;
+        velocity_2d(sp, y, ph.l, ph.eta0, ph.eta1, load_gen6(fcc, i), nz, out.f);
+        v_out[i] = out;
+    }
 }
 
 __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
@@ -1168,8 +1370,13 @@ __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restric
 
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
-                       cudaStream_t st)
+                       cudaStream_t st, int dims)
 {
+    if (dims == 2)
+    {
+        k_velocities_2d<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(geom, phys, fcc, ctrl, sp, v_out);
+        return;
+    }
     k_velocities<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, v_out);
 }
 
@@ -1212,8 +1419,9 @@ void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, in
     k_count_lower<<<max(cdiv(cap_cells, 256), 1), 256, 0, st>>>(ctrl, row_ptr, col, cnt);
 }
 
+// 3-D rows (i, j, dx, dy, dz, si, sj); 2-D rows (i, j, dx, dy, si, sj)
 __global__ void k_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
-                             const Geom* __restrict__ geom, double* out, int ld)
+                             const Geom* __restrict__ geom, double* out, int ld, int dims)
 {
     const int n = ctrl->n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -1226,17 +1434,25 @@ __global__ void k_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* co
             if (j >= i) continue;
             Dist d = dist_geom(gi, load_geom(geom, j));
             out[p] = i; out[(size_t)ld + p] = j;
-            out[(size_t)2 * ld + p] = d.dx; out[(size_t)3 * ld + p] = d.dy; out[(size_t)4 * ld + p] = d.dz;
-            out[(size_t)5 * ld + p] = d.s; out[(size_t)6 * ld + p] = d.t;
+            out[(size_t)2 * ld + p] = d.dx; out[(size_t)3 * ld + p] = d.dy;
+            if (dims == 2)
+            {
+                out[(size_t)4 * ld + p] = d.s; out[(size_t)5 * ld + p] = d.t;
+            }
+            else
+            {
+                out[(size_t)4 * ld + p] = d.dz;
+                out[(size_t)5 * ld + p] = d.s; out[(size_t)6 * ld + p] = d.t;
+            }
             ++p;
         }
     }
 }
 
 void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
-                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st)
+                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st, int dims)
 {
-    k_table_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, pos, geom, out, ld);
+    k_table_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, pos, geom, out, ld, dims);
 }
 
 }   // namespace abm

@@ -90,6 +90,9 @@ struct StepParams {
     double noise_max[6];
     int noise_on;
     uint64_t seed;
+    // 2-D model: composite drag eta0 + eta1 rho_c / R (2D/include/mechanics.hpp:264-279)
+    double rho_c;
+    double max_noise_2d;
     // step-size control
     int learned;                // 1: the network proposes dt, a passing proposal is accepted as is
     int stats_on;               // accumulate the network's features (learned or logging)
@@ -106,6 +109,11 @@ struct ForceParams {
     int jkr_n;
     double jkr_step;            // spacing of the overlap mesh
     int stats;                  // record the max overlap (step-size features)
+    // 2-D model (ABM-2d): Hertz prefactors of 2D/include/simulation.hpp:232-235 and
+    // the JKR-Lagrange adhesion of 2D/include/adhesion.hpp:403-448
+    double pf2d[3];
+    double adh_strength, adh_mindist;
+    const unsigned char* adhere;    // per CSR entry: to_adhere at the last rebuild
 };
 
 struct BuildParams {
@@ -129,6 +137,17 @@ void launch_cells_from_colmajor(const double* cm, int n, int ncols, int ld, int 
                                 Geom* geom, Vel* vel, Phys* phys, cudaStream_t st);
 void launch_cells_to_colmajor(const Geom* geom, const Vel* vel, const Phys* phys, int n, int ncols,
                               int ld, int has_gamma, double* cm, cudaStream_t st);
+// 2-D layout (ABM-2d/ABM-2d-cpp/include/indices.hpp) <-> records with z = 0
+void launch_cells_from_colmajor_2d(const double* cm, int n, int ncols, int ld, Geom* geom, Vel* vel, Phys* phys,
+                                   cudaStream_t st);
+void launch_cells_to_colmajor_2d(const Geom* geom, const Vel* vel, const Phys* phys, int n, int ncols, int ld,
+                                 double* cm, cudaStream_t st);
+// 2-D dE/dq (n x 4) from the pair sums (F, S): torques projected with the current n
+void launch_pair_dEdq_2d(const Geom* geom, const Gen6* fcc, const Ctrl* ctrl, double* cm, int cap_cells,
+                         cudaStream_t st);
+// to_adhere of every CSR entry (2D/include/simulation.hpp:242-258)
+void launch_adhere_flags(const Ctrl* ctrl, const int* row_ptr, const int* col, const Geom* geom, double R,
+                         double Rcell, unsigned char* adhere, int cap_cells, cudaStream_t st);
 void launch_gen6_to_colmajor(const Gen6* g, int n, double* cm, cudaStream_t st);
 
 void launch_bbox(const Geom* geom, Ctrl* ctrl, Grid* grid, unsigned long long* scratch8,
@@ -153,7 +172,7 @@ size_t scan_block_sums_size(int cap);
 void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
                        Ctrl* ctrl, ForceParams fp, const double* jkr_delta, const double* jkr_radius,
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
-                       int with_gather = 1);
+                       int with_gather = 1, int dims = 3);
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
                     int cap_cells, cudaStream_t st);
 
@@ -164,17 +183,18 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
-                    unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0});
+                    unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0},
+                    int dims = 3);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
-                       cudaStream_t st);
+                       cudaStream_t st, int dims = 3);
 void launch_grow(Geom* geom, Phys* phys, const Ctrl* ctrl, double R, double dt, int cap_cells,
                  cudaStream_t st);
 
 void launch_count_lower(const Ctrl* ctrl, const int* row_ptr, const int* col, int* cnt,
                         int cap_cells, cudaStream_t st);
 void launch_table_rows(const Ctrl* ctrl, const int* row_ptr, const int* col, const int* pos,
-                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st);
+                       const Geom* geom, double* out, int ld, int cap_cells, cudaStream_t st, int dims = 3);
 
 // step-size network (abm_mlp.cu); weights are the flat FP32 master copy
 void launch_mlp_forward(const float* master, const float* X, int n, float* Y, cudaStream_t st);

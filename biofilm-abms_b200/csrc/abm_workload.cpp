@@ -65,10 +65,11 @@ struct Grid3 {
 
 }   // namespace
 
-extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double disk_radius, double z_lo,
-                                       double z_hi, double lmin, double lmax, double min_gap,
-                                       double contact_dist, double p_contact, int max_tries,
-                                       double* out_r, double* out_n, double* out_l, int* placed)
+// planar: every cell in the plane z = 0 with an in-plane orientation (the 2-D model);
+// the draws are the same as in 3-D, with the out-of-plane components set to zero
+static int generate(int n, unsigned long long seed, double disk_radius, double z_lo, double z_hi, double lmin,
+                    double lmax, double min_gap, double contact_dist, double p_contact, int max_tries,
+                    bool planar, double* out_r, double* out_n, double* out_l, int* placed)
 {
     if (n <= 0 || !out_r || !out_n || !out_l) return -1;
     SplitMix64 rng = {seed * 0x2545F4914F6CDD1Dull + 1};
@@ -89,7 +90,8 @@ extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double di
         for (int tr = 0; tr < max_tries && !ok; ++tr)
         {
             double az = 2 * pi * rng.u01(), pol = 0.5 * pi * rng.u01();
-            C3 nv = c3(std::cos(pol) * std::cos(az), std::cos(pol) * std::sin(az), std::sin(pol));
+            if (planar) pol = 0.0;
+            C3 nv = c3(std::cos(pol) * std::cos(az), std::cos(pol) * std::sin(az), planar ? 0.0 : std::sin(pol));
             double l = lmin + (lmax - lmin) * rng.u01();
             double h = l / 2;
             C3 rv;
@@ -98,6 +100,7 @@ extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double di
                 int j = (int)(rng.u01() * count);
                 double sj = (2 * rng.u01() - 1) * H[j];
                 C3 u = c3(2 * rng.u01() - 1, 2 * rng.u01() - 1, 2 * rng.u01() - 1);
+                if (planar) u.z = 0.0;
                 u = sub(u, mul(dot(u, N[j]), N[j]));
                 double un = std::sqrt(dot(u, u));
                 if (un < 1e-9) continue;
@@ -113,6 +116,7 @@ extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double di
             {
                 double rad = disk_radius * std::sqrt(rng.u01()), ang = 2 * pi * rng.u01();
                 rv = c3(rad * std::cos(ang), rad * std::sin(ang), z_lo + (z_hi - z_lo) * rng.u01());
+                if (planar) rv.z = 0.0;
             }
             int k = g.key(rv.x, rv.y, rv.z);
             int iz = k / (g.nx * g.ny), iy = (k / g.nx) % g.ny, ix = k % g.nx;
@@ -138,6 +142,24 @@ extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double di
     }
     if (placed) *placed = count;
     return count == n ? 0 : -3;
+}
+
+extern "C" int abm_generate_biofilm_3d(int n, unsigned long long seed, double disk_radius, double z_lo,
+                                       double z_hi, double lmin, double lmax, double min_gap,
+                                       double contact_dist, double p_contact, int max_tries,
+                                       double* out_r, double* out_n, double* out_l, int* placed)
+{
+    return generate(n, seed, disk_radius, z_lo, z_hi, lmin, lmax, min_gap, contact_dist, p_contact, max_tries,
+                    false, out_r, out_n, out_l, placed);
+}
+
+// 2-D colonies: centres uniform in a disk in the plane, orientations uniform in the plane
+extern "C" int abm_generate_biofilm_2d(int n, unsigned long long seed, double disk_radius, double lmin,
+                                       double lmax, double min_gap, double contact_dist, double p_contact,
+                                       int max_tries, double* out_r, double* out_n, double* out_l, int* placed)
+{
+    return generate(n, seed, disk_radius, 0.0, 0.0, lmin, lmax, min_gap, contact_dist, p_contact, max_tries,
+                    true, out_r, out_n, out_l, placed);
 }
 
 // Number of pairs closer than `dist` (segment distance), on the same grid.

@@ -90,6 +90,18 @@ typedef struct abm_params {
     /* step-size control (no reference counterpart beyond ABM_CONTROLLER_REFERENCE) */
     int controller;              /* ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED */
     int stepsize_log_capacity;   /* rows of step-size features logged per context (0 = off) */
+    /* model dimension: 3 (ABM-3d, default when 0) or 2 (ABM-2d).  The 2-D model uses the
+     * 17-column cell layout of ABM-2d/ABM-2d-cpp/include/indices.hpp, neighbor rows
+     * (i, j, dx, dy, si, sj), n x 4 forces / velocities / errors, Hertz prefactors of
+     * 2D/include/simulation.hpp:232-235, adhesion_mode 1 = JKR-Lagrange
+     * (2D/include/adhesion.hpp:403-448, strength and mindist below), composite drag with
+     * rho_c = (sigma0 R^2 / 4 E0)^(1/3), uniform noise max_noise on (r, n), and
+     * daughter_angle_xy_bound as its daughter angle bound (daughter_angle_z_bound must be 0).
+     * integration_mode ABM_BOGACKI_SHAMPINE (the 2-D driver's) or ABM_HEUN_EULER. */
+    int dims;
+    double sigma0;
+    double adhesion_strength, adhesion_mindist;
+    double max_noise;
 } abm_params;
 
 typedef struct abm_stats {
@@ -187,6 +199,12 @@ const char* abm_graph_info(const abm_ctx* ctx);
 /* Same as abm_iterate without graphs, with CUDA events around each kernel group
  * (no reference counterpart; measurement only). */
 int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);
+
+/* 2-D adhesion flags (the to_adhere array of 2D/include/simulation.hpp:242-258), one per
+ * neighbor row in the order of abm_download_neighbors.  abm_build_neighbors and every
+ * rebuild set them from the distances at that time, as the reference does. */
+int abm_get_adhesion_flags(abm_ctx* ctx, int* flags, int cap, int* m);
+int abm_set_adhesion_flags(abm_ctx* ctx, const int* flags, int m);
 
 /* ---------------------------------------------------------------------------
  * Step-size network (no reference counterpart).  The weights are the flat FP32

@@ -230,3 +230,173 @@ class Oracle:
 
     def min_dist_to_cell(self, i):
         return LIB.oracle_min_dist_to_cell(self._c, i)
+
+
+# ---------------------------------------------------------------------------
+# 2-D restatement (oracle/abm2d.hpp, oracle/capi2d.cpp)
+# ---------------------------------------------------------------------------
+class Oracle2DParams(ctypes.Structure):
+    _fields_ = [
+        ("R", ctypes.c_double), ("Rcell", ctypes.c_double), ("E0", ctypes.c_double),
+        ("Ecell", ctypes.c_double), ("sigma0", ctypes.c_double), ("Ldiv", ctypes.c_double),
+        ("neighbor_threshold", ctypes.c_double), ("adhesion_mode", ctypes.c_int),
+        ("adhesion_strength", ctypes.c_double), ("adhesion_mindist", ctypes.c_double),
+        ("integration_mode", ctypes.c_int), ("max_stepsize", ctypes.c_double),
+        ("min_stepsize", ctypes.c_double), ("max_error_allowed", ctypes.c_double),
+        ("min_error", ctypes.c_double), ("max_tries_update_stepsize", ctypes.c_int),
+        ("iter_update_stepsize", ctypes.c_int), ("iter_update_neighbors", ctypes.c_int),
+        ("max_noise", ctypes.c_double), ("growth_mean", ctypes.c_double), ("growth_std", ctypes.c_double),
+        ("daughter_length_std", ctypes.c_double), ("daughter_angle_bound", ctypes.c_double),
+        ("rng_seed", ctypes.c_ulonglong), ("use_pf", ctypes.c_int), ("pf", ctypes.c_double * 3),
+    ]
+
+
+def _load2d(lib):
+    P = ctypes.POINTER
+    d, i, vp, dp, ip = ctypes.c_double, ctypes.c_int, ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int)
+    ll = P(ctypes.c_longlong)
+    sig = {
+        "oracle2d_create": ([P(Oracle2DParams), P(vp)], i),
+        "oracle2d_destroy": ([vp], None),
+        "oracle2d_set_cells": ([vp, dp, i, i, i], i),
+        "oracle2d_get_num_cells": ([vp], i),
+        "oracle2d_get_cells": ([vp, dp, i], i),
+        "oracle2d_set_parents": ([vp, ip, i], i),
+        "oracle2d_get_parents": ([vp, ip, i], i),
+        "oracle2d_set_clock": ([vp, d, d, i], None),
+        "oracle2d_get_clock": ([vp, dp, dp, ip], None),
+        "oracle2d_build_neighbors": ([vp], i),
+        "oracle2d_num_neighbors": ([vp], i),
+        "oracle2d_get_neighbors": ([vp, dp, i, ip], i),
+        "oracle2d_cell_cell_forces": ([vp, dp], i),
+        "oracle2d_get_velocities": ([vp, dp], i),
+        "oracle2d_rk_attempt": ([vp, d, i, i, dp, dp, dp], i),
+        "oracle2d_loop_init": ([vp], i),
+        "oracle2d_iterate": ([vp, i, i], i),
+        "oracle2d_get_stats": ([vp, ll, ll, ll, dp], None),
+        "oracle2d_divide": ([vp, d, i, ip], i),
+        "oracle2d_grow": ([vp, d], i),
+        "oracle2d_jkr_lagrange_pair": ([dp, dp, dp, d, d, d, d, dp], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+
+
+_load2d(LIB)
+
+
+def jkr_lagrange_pair(n1, n2, d12, R, s, t, dmin):
+    """forcesJKRLagrange (2D/include/adhesion.hpp:403-448) with the constraint: 2 x 4 dE/dq."""
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (n1, n2, d12)]
+    out = np.zeros(8)
+    LIB.oracle2d_jkr_lagrange_pair(_dp(a[0]), _dp(a[1]), _dp(a[2]), R, s, t, dmin, _dp(out))
+    return out.reshape(2, 4)
+
+
+class Oracle2D:
+    """The 2-D oracle; parameter names as abm_b200.DEFAULTS (max_noise, sigma0, adhesion_*)."""
+
+    def __init__(self, pdict, pf=None):
+        import abm_b200
+        full = dict(abm_b200.DEFAULTS)
+        full.update(abm_b200.DEFAULTS_2D)
+        full.update(pdict)
+        pdict = full
+        p = Oracle2DParams()
+        for name, _ in Oracle2DParams._fields_:
+            if name in pdict and name not in ("pf", "use_pf"):
+                setattr(p, name, pdict[name])
+        p.daughter_angle_bound = pdict.get("daughter_angle_xy_bound", 0.0)
+        if pf is not None:
+            p.use_pf = 1
+            for k in range(3):
+                p.pf[k] = pf[k]
+        self._c = ctypes.c_void_p()
+        LIB.oracle2d_create(ctypes.byref(p), ctypes.byref(self._c))
+        self.ncols = None
+
+    def __del__(self):
+        if getattr(self, "_c", None):
+            LIB.oracle2d_destroy(self._c)
+            self._c = None
+
+    def set_cells(self, cells):
+        a = np.asfortranarray(cells, dtype=np.float64)
+        self.ncols = a.shape[1]
+        LIB.oracle2d_set_cells(self._c, _dp(a), a.shape[0], a.shape[1], max(a.shape[0], 1))
+
+    def cells(self):
+        n = LIB.oracle2d_get_num_cells(self._c)
+        out = np.zeros((n, self.ncols), order="F")
+        LIB.oracle2d_get_cells(self._c, _dp(out), max(n, 1))
+        return out
+
+    def set_parents(self, parents):
+        a = np.ascontiguousarray(parents, dtype=np.int32)
+        LIB.oracle2d_set_parents(self._c, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a))
+
+    def parents(self):
+        n = LIB.oracle2d_get_parents(self._c, None, 0)
+        a = np.zeros(n, dtype=np.int32)
+        LIB.oracle2d_get_parents(self._c, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+        return a
+
+    def set_clock(self, t, dt, iteration):
+        LIB.oracle2d_set_clock(self._c, t, dt, iteration)
+
+    def clock(self):
+        t, dt, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        LIB.oracle2d_get_clock(self._c, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it))
+        return t.value, dt.value, it.value
+
+    def build_neighbors(self):
+        return LIB.oracle2d_build_neighbors(self._c)
+
+    def neighbors(self, with_adhere=False):
+        m = LIB.oracle2d_num_neighbors(self._c)
+        out = np.zeros((m, 6), order="F")
+        adh = np.zeros(max(m, 1), dtype=np.int32)
+        LIB.oracle2d_get_neighbors(self._c, _dp(out), max(m, 1), adh.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return (out, adh[:m]) if with_adhere else out
+
+    def _n4(self, fn):
+        n = LIB.oracle2d_get_num_cells(self._c)
+        out = np.zeros((n, 4), order="F")
+        fn(self._c, _dp(out))
+        return out
+
+    def cell_cell_forces(self):
+        return self._n4(LIB.oracle2d_cell_cell_forces)
+
+    def get_velocities(self):
+        return self._n4(LIB.oracle2d_get_velocities)
+
+    def rk_attempt(self, dt, iteration=0, attempt=0):
+        n = LIB.oracle2d_get_num_cells(self._c)
+        cells = np.zeros((n, self.ncols), order="F")
+        errors = np.zeros((n, 4), order="F")
+        e = ctypes.c_double()
+        LIB.oracle2d_rk_attempt(self._c, dt, iteration, attempt, _dp(cells), _dp(errors), ctypes.byref(e))
+        return cells, errors, e.value
+
+    def loop_init(self):
+        return LIB.oracle2d_loop_init(self._c)
+
+    def iterate(self, n_iters, n_cells=0):
+        return LIB.oracle2d_iterate(self._c, n_iters, n_cells)
+
+    def stats(self):
+        a, r, dv = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        e = ctypes.c_double()
+        LIB.oracle2d_get_stats(self._c, ctypes.byref(a), ctypes.byref(r), ctypes.byref(dv), ctypes.byref(e))
+        return dict(attempts=a.value, rebuilds=r.value, divisions=dv.value, last_max_error=e.value)
+
+    def divide(self, t, iteration):
+        tr = ctypes.c_int()
+        nd = LIB.oracle2d_divide(self._c, t, iteration, ctypes.byref(tr))
+        return nd, tr.value
+
+    def grow(self, dt):
+        LIB.oracle2d_grow(self._c, dt)

@@ -68,7 +68,7 @@ class AbmStats(ctypes.Structure):
         ("retries", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong),
         ("divisions", ctypes.c_longlong), ("t", ctypes.c_double), ("dt", ctypes.c_double),
         ("last_max_error", ctypes.c_double), ("n_cells", ctypes.c_int), ("n_pairs", ctypes.c_int),
-        ("rejected", ctypes.c_longlong), ("log_rows", ctypes.c_longlong),
+        ("rejected", ctypes.c_longlong), ("log_rows", ctypes.c_longlong), ("cell_steps", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -159,6 +159,14 @@ def _load():
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
         "abm_get_adhesion_flags": ([vp, ip, i, ip], i),
+        "abm_set_cell_limit": ([vp, i], i),
+        "abm_batch_create": ([P(vp), i, P(vp)], i),
+        "abm_batch_iterate": ([vp, i], i),
+        "abm_batch_synchronize": ([vp], i),
+        "abm_batch_get_stream": ([vp, P(vp)], i),
+        "abm_batch_destroy": ([vp], i),
+        "abm_batch_last_error": ([], ctypes.c_char_p),
+        "abm_autotune_pair_lanes": ([P(AbmParams), dp, i, i, i, dp, dp, i, i, ip, fp], i),
         "abm_set_adhesion_flags": ([vp, ip, i], i),
         "abm_stepsize_set_weights": ([vp, fp, i], i),
         "abm_stepsize_get_weights": ([vp, fp, i], i),
@@ -185,7 +193,9 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
             "abm_cell_cell_forces_noalloc abm_noalloc_last_error abm_stepsize_set_weights "
             "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
-            "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags").split()
+            "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags "
+            "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "
+            "abm_batch_destroy abm_batch_last_error abm_autotune_pair_lanes").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
@@ -400,6 +410,10 @@ class Simulation:
         self._check(LIB.abm_get_stats(self._ctx, ctypes.byref(s)), "abm_get_stats")
         return s.as_dict()
 
+    def set_cell_limit(self, n_max):
+        """Stop on the device once the population reaches n_max (terminate(), simulation.hpp:1600-1615)."""
+        self._check(LIB.abm_set_cell_limit(self._ctx, int(n_max)), "abm_set_cell_limit")
+
     # ---- 2-D adhesion flags (to_adhere, 2D/include/simulation.hpp:242-258) ----
     def adhesion_flags(self):
         m = ctypes.c_int()
@@ -475,3 +489,61 @@ def mlp_train(weights, X, T, epochs=200, lr=1e-3, seed=0):
     _mlp_check(LIB.abm_mlp_train(_fptr(w), _fptr(X), _fptr(T), X.shape[0], epochs, lr, seed, _fptr(losses)),
                "abm_mlp_train")
     return w, losses[:epochs]
+
+
+def _batch_check(rc, what):
+    if rc != 0:
+        raise RuntimeError("%s failed (%s): %s" % (what, ERRORS.get(rc, rc), LIB.abm_batch_last_error().decode()))
+
+
+class Batch:
+    """Independent simulations (replicate biofilms) advanced by one CUDA graph launch
+    per iteration; each keeps its own clock, step size and controller."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s._ctx.value for s in self.sims])
+        self._b = ctypes.c_void_p()
+        _batch_check(LIB.abm_batch_create(arr, len(self.sims), ctypes.byref(self._b)), "abm_batch_create")
+
+    def iterate(self, n_iters):
+        _batch_check(LIB.abm_batch_iterate(self._b, int(n_iters)), "abm_batch_iterate")
+
+    def synchronize(self):
+        _batch_check(LIB.abm_batch_synchronize(self._b), "abm_batch_synchronize")
+
+    @property
+    def stream(self):
+        s = ctypes.c_void_p()
+        _batch_check(LIB.abm_batch_get_stream(self._b, ctypes.byref(s)), "abm_batch_get_stream")
+        return s.value
+
+    def close(self):
+        if self._b:
+            LIB.abm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_pair_lanes(cells, launches=20, jkr_table=None, gamma=100.0, **params):
+    """Time the pair-force kernel at 4, 8, 16 and 32 lanes per cell on `cells`;
+    returns (best lanes, {lanes: ms per launch})."""
+    p, d = make_params(**params)
+    a = np.asfortranarray(cells, dtype=np.float64)
+    if p.cap_cells <= 0:
+        p.cap_cells = a.shape[0]
+    if jkr_table is None and p.adhesion_mode and p.dims != 2:
+        jkr_table = jkr_radius_table(p.R, p.Rcell, p.E0, gamma)
+    jd = np.ascontiguousarray(jkr_table[0] if jkr_table is not None else np.zeros(2))
+    jr = np.ascontiguousarray(jkr_table[1] if jkr_table is not None else np.zeros(2))
+    best = ctypes.c_int()
+    ms = np.zeros(4, dtype=np.float32)
+    _batch_check(LIB.abm_autotune_pair_lanes(ctypes.byref(p), _dptr(a), a.shape[0], a.shape[1], a.shape[0],
+                                             _dptr(jd), _dptr(jr), len(jd), launches, ctypes.byref(best),
+                                             _fptr(ms)), "abm_autotune_pair_lanes")
+    return best.value, dict(zip((4, 8, 16, 32), ms.tolist()))

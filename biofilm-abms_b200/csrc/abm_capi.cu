@@ -183,7 +183,8 @@ static void fill_tableau(StepParams& sp, int mode, bool& ok)
     sp.inv_q1 = 1.0 / (q + 1);
 }
 
-__global__ void k_set_n(Ctrl* c, int n) { c->n = n; }
+__global__ void k_set_n(Ctrl* c, int n) { c->n = n; c->halted = 0; }
+__global__ void k_set_halt(Ctrl* c, int n_max) { c->halt_n = n_max; c->halted = 0; }
 __global__ void k_set_clock(Ctrl* c, double t, double dt, int iter)
 {
     c->t = t; c->dt = dt; c->iter = iter; c->mode = MODE_TRIAL; c->tries = 0; c->attempt = 0;
@@ -656,18 +657,16 @@ static int add_conditional(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphN
     return ABM_OK;
 }
 
-// One loop iteration as a graph with conditional nodes:
+// One loop iteration as a graph with conditional nodes, appended to G after `deps`
+// (empty: root nodes); `deps` becomes the iteration's leaf set:
 //   [division count] -> IF(n_divide > 0){division + rebuild}
-//   -> pair force -> trial -> WHILE(retry requested){retry} -> final
-static int build_iteration_graph(abm_ctx* c)
+//   -> pair force -> [proposal] -> trial -> WHILE(retry requested){retry} -> final
+static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode_t>& deps)
 {
-    cudaGraph_t G;
-    CK(cudaGraphCreate(&G, 0));
     // every handle must belong to a conditional node of this graph, or instantiation fails
     cudaGraphConditionalHandle h_div = 0, h_retry = 0;
     const bool retries = c->p.max_tries_update_stepsize > 0;
     if (retries) CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
-    std::vector<cudaGraphNode_t> deps;
     int rc;
     if (c->div_enabled)
     {
@@ -705,7 +704,16 @@ static int build_iteration_graph(abm_ctx* c)
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
     });
-    if (rc) return rc;
+    return rc;
+}
+
+static int build_iteration_graph(abm_ctx* c)
+{
+    cudaGraph_t G;
+    CK(cudaGraphCreate(&G, 0));
+    std::vector<cudaGraphNode_t> deps;
+    int rc = append_iteration(c, G, deps);
+    if (rc) { cudaGraphDestroy(G); return rc; }
     cudaError_t inst = cudaGraphInstantiate(&c->g_iter, G, 0);
     cudaGraphDestroy(G);
     CK(inst);
@@ -957,7 +965,7 @@ int abm_get_stats(abm_ctx* c, abm_stats* s)
     s->rebuilds = h.rebuilds; s->divisions = h.divisions;
     s->t = h.t; s->dt = h.dt; s->last_max_error = h.last_max_error;
     s->n_cells = h.n; s->n_pairs = h.n_dir / 2;
-    s->rejected = h.rejected; s->log_rows = h.log_rows;
+    s->rejected = h.rejected; s->log_rows = h.log_rows; s->cell_steps = h.cell_steps;
     return check_status(c);
 }
 
@@ -1113,6 +1121,14 @@ int abm_set_adhesion_flags(abm_ctx* c, const int* flags, int m)
     return ABM_OK;
 }
 
+int abm_set_cell_limit(abm_ctx* c, int n_max)
+{
+    if (!c || n_max < 0) return ABM_ERR_ARG;
+    k_set_halt<<<1, 1, 0, c->st>>>(c->ctrl, n_max);
+    CK(cudaGetLastError());
+    return ABM_OK;
+}
+
 int abm_stepsize_set_weights(abm_ctx* c, const float* w, int n)
 {
     if (!c || !w || n != MLP_NPARAM) return fail(c, ABM_ERR_ARG, "weights must have ABM_MLP_NPARAM entries");
@@ -1163,6 +1179,215 @@ int abm_stepsize_clear_log(abm_ctx* c)
     h.log_rows = 0;
     CK(cudaMemcpyAsync(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
+}   // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches of contexts (independent replicate biofilms) advanced by one graph
+// ---------------------------------------------------------------------------
+struct abm_batch {
+    std::vector<abm_ctx*> ctxs;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t g_iter = nullptr, g_rebuild = nullptr;
+    int k_rebuild = 100;
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t done = nullptr;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_batch_err;
+
+int batch_fail(abm_batch* b, int code, const std::string& msg)
+{
+    if (b) b->err = msg;
+    g_batch_err = msg;
+    return code;
+}
+
+#define BK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+    return batch_fail(b, ABM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
+
+void batch_free(abm_batch* b)
+{
+    if (b->g_iter) cudaGraphExecDestroy(b->g_iter);
+    if (b->g_rebuild) cudaGraphExecDestroy(b->g_rebuild);
+    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->st) cudaStreamDestroy(b->st);
+}
+}   // namespace
+
+extern "C" {
+
+const char* abm_batch_last_error(void) { return g_batch_err.c_str(); }
+
+int abm_batch_create(abm_ctx* const* ctxs, int n, abm_batch** out)
+{
+    g_batch_err.clear();
+    if (!ctxs || n <= 0 || !out) return batch_fail(nullptr, ABM_ERR_ARG, "bad arguments");
+    *out = nullptr;
+    abm_batch* b = new abm_batch();
+    b->ctxs.assign(ctxs, ctxs + n);
+    b->k_rebuild = ctxs[0]->p.iter_update_neighbors;
+    int dev = ctxs[0]->dev;
+    for (abm_ctx* c : b->ctxs)
+    {
+        if (!c || !c->cells_loaded) { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "every context needs cells"); }
+        if (c->dev != dev) { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts on different devices"); }
+        if (c->p.iter_update_neighbors != b->k_rebuild)
+        { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts must share iter_update_neighbors"); }
+        if (c->sp.learned && !c->mlp_loaded)
+        { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "a learned controller needs weights"); }
+        if (c->dims == 3 && c->p.adhesion_mode != 0 && c->jkr_n < 2)
+        { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "JKR table not set"); }
+        if (c->host_iter % b->k_rebuild != ctxs[0]->host_iter % b->k_rebuild)
+        { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "contexts must be in phase of the rebuild cadence"); }
+        if (!c->nbrs_valid) { enqueue_rebuild(c); c->nbrs_valid = true; }
+    }
+    int rc = ABM_OK;
+    cudaGraph_t G = nullptr, GR = nullptr;
+    do {
+        if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        { rc = batch_fail(b, ABM_ERR_CUDA, "stream or event creation failed"); break; }
+        b->ev.resize(n);
+        for (int k = 0; k < n && !rc; ++k)
+            if (cudaEventCreateWithFlags(&b->ev[k], cudaEventDisableTiming) != cudaSuccess)
+                rc = batch_fail(b, ABM_ERR_CUDA, "event creation failed");
+        if (rc) break;
+        // one graph: every context's iteration as an independent branch
+        if (cudaGraphCreate(&G, 0) != cudaSuccess || cudaGraphCreate(&GR, 0) != cudaSuccess)
+        { rc = batch_fail(b, ABM_ERR_CUDA, "graph creation failed"); break; }
+        for (abm_ctx* c : b->ctxs)
+        {
+            std::vector<cudaGraphNode_t> deps;
+            rc = append_iteration(c, G, deps);
+            if (rc) { rc = batch_fail(b, rc, "iteration graph of a context: " + c->err); break; }
+            std::vector<cudaGraphNode_t> rdeps;
+            rc = capture_into(c, GR, rdeps, [&]() { enqueue_rebuild(c); });
+            if (rc) { rc = batch_fail(b, rc, "rebuild graph of a context: " + c->err); break; }
+        }
+        if (rc) break;
+        if (cudaGraphInstantiate(&b->g_iter, G, 0) != cudaSuccess ||
+            cudaGraphInstantiate(&b->g_rebuild, GR, 0) != cudaSuccess)
+        { rc = batch_fail(b, ABM_ERR_CUDA, "graph instantiation failed"); break; }
+    } while (0);
+    if (G) cudaGraphDestroy(G);
+    if (GR) cudaGraphDestroy(GR);
+    if (rc) { batch_free(b); delete b; return rc; }
+    *out = b;
+    return ABM_OK;
+}
+
+// n_iters iterations of every context: one graph launch per iteration, the joint
+// neighbor rebuild every iter_update_neighbors iterations (all contexts take their
+// steps in lockstep, so their cadences coincide).  Work already queued on the
+// contexts' streams runs first; their streams wait for the batch at the end.
+int abm_batch_iterate(abm_batch* b, int n_iters)
+{
+    if (!b || n_iters < 0) return batch_fail(b, ABM_ERR_ARG, "bad arguments");
+    const int n = (int)b->ctxs.size();
+    for (int k = 0; k < n; ++k)
+    {
+        BK(cudaEventRecord(b->ev[k], b->ctxs[k]->st));
+        BK(cudaStreamWaitEvent(b->st, b->ev[k], 0));
+    }
+    for (int it = 0; it < n_iters; ++it)
+    {
+        BK(cudaGraphLaunch(b->g_iter, b->st));
+        bool rebuild = false;
+        for (abm_ctx* c : b->ctxs)
+        {
+            c->host_iter += 1;
+            rebuild = (c->host_iter % b->k_rebuild == 0);
+        }
+        if (rebuild) BK(cudaGraphLaunch(b->g_rebuild, b->st));
+    }
+    BK(cudaEventRecord(b->done, b->st));
+    for (abm_ctx* c : b->ctxs) BK(cudaStreamWaitEvent(c->st, b->done, 0));
+    BK(cudaGetLastError());
+    return ABM_OK;
+}
+
+int abm_batch_synchronize(abm_batch* b)
+{
+    if (!b) return ABM_ERR_ARG;
+    BK(cudaStreamSynchronize(b->st));
+    for (abm_ctx* c : b->ctxs)
+    {
+        int rc = check_status(c);
+        if (rc) return batch_fail(b, rc, c->err);
+    }
+    return ABM_OK;
+}
+
+int abm_batch_get_stream(abm_batch* b, void** stream)
+{
+    if (!b || !stream) return ABM_ERR_ARG;
+    *stream = (void*)b->st;
+    return ABM_OK;
+}
+
+int abm_batch_destroy(abm_batch* b)
+{
+    if (!b) return ABM_ERR_ARG;
+    cudaStreamSynchronize(b->st);
+    batch_free(b);
+    delete b;
+    return ABM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the pair-force tile: lanes per cell of the pair kernel (4, 8, 16
+// or 32), timed on a scratch context holding the caller's state; the fastest
+// candidate by CUDA events over `launches` launches wins.  No reference counterpart.
+// ---------------------------------------------------------------------------
+int abm_autotune_pair_lanes(const abm_params* p, const double* cells, int n, int ncols, int ld,
+                            const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
+                            int* best_lanes, float* ms_per_launch)
+{
+    g_batch_err.clear();
+    if (!p || !cells || n <= 0 || !best_lanes || launches <= 0) return batch_fail(nullptr, ABM_ERR_ARG, "bad arguments");
+    const int cand[4] = {4, 8, 16, 32};
+    float best = 0;
+    *best_lanes = 0;
+    for (int k = 0; k < 4; ++k)
+    {
+        abm_params q = *p;
+        q.pair_lanes = cand[k];
+        q.cap_cells = std::max(q.cap_cells, n);
+        q.controller = ABM_CONTROLLER_REFERENCE;
+        q.stepsize_log_capacity = 0;
+        abm_ctx* c = nullptr;
+        int rc = abm_create(&q, &c);
+        if (rc == ABM_OK && q.adhesion_mode != 0 && (q.dims == 0 || q.dims == 3))
+            rc = abm_set_jkr_table(c, jkr_delta, jkr_radius, jkr_n);
+        if (rc == ABM_OK) rc = abm_upload_cells(c, cells, n, ncols, ld);
+        int m = 0;
+        if (rc == ABM_OK) rc = abm_build_neighbors(c, &m);
+        float ms = 0;
+        if (rc == ABM_OK)
+        {
+            cudaEvent_t e0, e1;
+            cudaEventCreate(&e0); cudaEventCreate(&e1);
+            enqueue_pair_force(c, 1);                       // warm-up
+            cudaEventRecord(e0, c->st);
+            for (int r = 0; r < launches; ++r) enqueue_pair_force(c, 1);
+            cudaEventRecord(e1, c->st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = ABM_ERR_CUDA;
+            else cudaEventElapsedTime(&ms, e0, e1);
+            cudaEventDestroy(e0); cudaEventDestroy(e1);
+            ms /= launches;
+        }
+        std::string why = c ? c->err : std::string("abm_create failed");
+        if (c) abm_destroy(c);
+        if (rc) return batch_fail(nullptr, rc, "autotune candidate: " + why);
+        if (ms_per_launch) ms_per_launch[k] = ms;
+        if (*best_lanes == 0 || ms < best) { best = ms; *best_lanes = cand[k]; }
+    }
     return ABM_OK;
 }
 

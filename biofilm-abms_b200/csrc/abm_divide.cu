@@ -31,8 +31,10 @@ __global__ void k_div_count(const Phys* __restrict__ phys, Ctrl* ctrl, DividePar
     if (threadIdx.x == 0) sh_cnt = 0;
     __syncthreads();
     const int n = ctrl->n;
+    // terminate() at the top of the loop: no division and no step once n reaches the limit
+    const bool halt = ctrl->halt_n > 0 && n >= ctrl->halt_n;
     int cnt = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n && !halt; i += gridDim.x * blockDim.x)
     {
         int f = phys[i].l > dp.Ldiv;          // divideMaxLength, growth.hpp:66-71
         flags[i] = f;
@@ -59,6 +61,7 @@ __global__ void k_div_count(const Phys* __restrict__ phys, Ctrl* ctrl, DividePar
             total = 0;
         }
         ctrl->n_divide = total;
+        ctrl->halted = halt ? 1 : 0;
         ctrl->div_done = (total == 0);
         ctrl->div_tries = 0;
         if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, total > 0 ? 1u : 0u);

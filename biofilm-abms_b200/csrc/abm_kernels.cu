@@ -649,6 +649,7 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
                                                     double4* __restrict__ jbuf)
 {
     __shared__ double td[JKR_MAX], tr[JKR_MAX];
+    if (ctrl->halted) return;
     for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
     __syncthreads();
     const int n = ctrl->n;
@@ -1011,6 +1012,7 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
         c->hist_acc[h] = c->first_passed;
         c->hist_pos = (h + 1) % HIST;
         c->since_div = c->n_divide > 0 ? 0 : c->since_div + 1;
+        c->cell_steps += c->n;
         c->t += c->dt;
         c->iter += 1;
         c->iterations += 1;
@@ -1041,6 +1043,13 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     __shared__ double sh_max[AT_T / 32];
     __shared__ double4 sh_stat[AT_T / 32];
     __shared__ bool last;
+    if (KIND != 3 && ctrl->halted)
+    {
+        // a halted context takes no step: stop an enclosing WHILE node
+        if (use_cond && (KIND == MODE_TRIAL || KIND == MODE_RETRY) && blockIdx.x == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
+        return;
+    }
     const int n = ctrl->n;
     const int mode = ctrl->mode;
     const int iter = ctrl->iter;

@@ -72,6 +72,11 @@ struct Ctrl {
     double dt_prev;                     // accepted dt before the running iteration
     long long rejected;                 // iterations whose first attempt failed the error test
     long long log_rows;                 // feature rows written (ring position = log_rows % capacity)
+    // cell-count stop on the device (terminate(), simulation.hpp:1600-1615): decided at the
+    // start of each iteration by the division count; a halted context skips its iterations
+    int halt_n;                         // 0 = no limit
+    int halted;
+    long long cell_steps;               // sum of the population over accepted steps
 };
 
 struct Grid {

@@ -385,6 +385,7 @@ __global__ void __launch_bounds__(256) k_mlp_propose(Ctrl* ctrl, StepParams sp, 
     __shared__ float feat[MLP_IN], h1[MLP_H], h2[MLP_H];
     __shared__ float sh_base;
     __shared__ int sh_fail;
+    if (ctrl->halted) return;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = ctrl->n;
     const double inv_n = 1.0 / (double)max(n, 1);

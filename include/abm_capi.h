@@ -115,6 +115,7 @@ typedef struct abm_stats {
     int n_cells, n_pairs;        /* current population and neighbor pairs (unordered) */
     long long rejected;          /* iterations whose first attempt failed the error test */
     long long log_rows;          /* step-size feature rows written so far */
+    long long cell_steps;        /* sum of the population over accepted steps */
 } abm_stats;
 
 /* Device time per kernel group, from CUDA events on the context stream. */
@@ -205,6 +206,34 @@ int abm_profile_iterations(abm_ctx* ctx, int n_iters, abm_profile* profile);
  * rebuild set them from the distances at that time, as the reference does. */
 int abm_get_adhesion_flags(abm_ctx* ctx, int* flags, int cap, int* m);
 int abm_set_adhesion_flags(abm_ctx* ctx, const int* flags, int m);
+
+/* Stop on the device once the population reaches n_max cells (0 = no limit): the
+ * terminate() test at the top of the loop (simulation.hpp:1600-1615); a context at its
+ * limit takes no further division or step.  Used by batches, where the host does not
+ * poll each context. */
+int abm_set_cell_limit(abm_ctx* ctx, int n_max);
+
+/* ---------------------------------------------------------------------------
+ * Batches (no reference counterpart: the reference runs replicates as separate jobs).
+ * A batch advances independent contexts (replicate biofilms of any sizes, each with
+ * its own clock, step size and controller) by one CUDA graph launch per iteration:
+ * every context's iteration graph is a branch of one graph, so a context's results
+ * are bit-identical to advancing it alone.  Contexts must share a device and
+ * iter_update_neighbors.  Batch calls report errors through abm_batch_last_error().
+ * ------------------------------------------------------------------------- */
+typedef struct abm_batch abm_batch;
+int abm_batch_create(abm_ctx* const* ctxs, int n, abm_batch** batch);
+int abm_batch_iterate(abm_batch* batch, int n_iters);
+int abm_batch_synchronize(abm_batch* batch);
+int abm_batch_get_stream(abm_batch* batch, void** stream);
+int abm_batch_destroy(abm_batch* batch);
+const char* abm_batch_last_error(void);
+/* Autotuner: times the pair-force kernel with 4, 8, 16 and 32 lanes per cell on a
+ * scratch context holding `cells` and returns the fastest in best_lanes;
+ * ms_per_launch (4 entries, may be NULL) receives each candidate's time. */
+int abm_autotune_pair_lanes(const abm_params* params, const double* cells, int n, int ncols, int ld,
+                            const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
+                            int* best_lanes, float* ms_per_launch);
 
 /* ---------------------------------------------------------------------------
  * Step-size network (no reference counterpart).  The weights are the flat FP32

@@ -61,6 +61,9 @@ def parse_args(argv=None):
     ap.add_argument("--variant", default="chosen", choices=["chosen", "plain"],
                     help="headline configuration; the other one is timed beside it unless --only")
     ap.add_argument("--only", action="store_true", help="time the headline variant only")
+    ap.add_argument("--workload", default="3d", choices=["3d", "replicates"],
+                    help="3d: the 100k-cell headline; replicates: batched 2-D replicate biofilms")
+    ap.add_argument("--replicates", type=int, default=256)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -516,10 +519,76 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_replicates(args):
+    """Batched 2-D replicates: args.replicates colonies with log-uniform target sizes in
+    [500, 50000], each started from its own seeded colony at 90 % of its target and
+    grown with config-0 growth and division (BS32, tol 1e-8) until its target; one
+    graph launch per iteration advances all of them.  Pair-kernel lanes per size
+    decade come from the autotuner."""
+    import torch
+    from abm_b200 import replicates
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        dist_init("nccl")
+    targets = replicates.target_sizes(args.replicates, 500, 50000, seed=rank)
+    lanes = replicates.lanes_by_bucket(targets, replicates.CONFIG0)
+    bt, sims = replicates.make_batch(targets, seed=1000 * rank + 1, start_fraction=0.9, lanes=lanes)
+    bt.iterate(max(args.warmup, 0))
+    bt.synchronize()
+    s0 = [s.stats() for s in sims]
+    stream = torch.cuda.ExternalStream(bt.stream, device=device)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bt.iterate(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bt.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = reduce_max(e0.elapsed_time(e1), device, world)
+    s1 = [s.stats() for s in sims]
+    d = {k: sum(b[k] - a[k] for a, b in zip(s0, s1)) for k in ("cell_steps", "iterations", "attempts",
+                                                                "rejected", "retries", "divisions")}
+    cells_now = sum(s.num_cells() for s in sims)
+    halted = sum(1 for s, t in zip(sims, targets) if s.num_cells() >= t)
+    value = world * d["cell_steps"] / (ms / 1000.0)
+    line = {"metric": "accepted cell-steps/s, batched 2D replicates", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 2-D colonies)",
+            "config": {"workload": "2d_replicates_%d_loguniform500-50000_BS32_tol1e-8" % args.replicates,
+                       "replicates": args.replicates, "cells_at_end": cells_now,
+                       "target_cells_total": int(targets.sum()), "replicates_at_target": halted,
+                       "rejected_step_fraction": d["rejected"] / max(d["iterations"], 1),
+                       "rk_evals_per_step": d["attempts"] / max(d["iterations"], 1),
+                       "divisions": d["divisions"], "l2": "state larger than L2 (no flush needed)",
+                       "pair_lanes_by_size_decade": {str(10 ** b): v[0] for b, v in lanes.items()},
+                       "parallelism": "replicas"},
+            "gpu_launches": None,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bt.close()
+    for s in sims:
+        s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "replicates":
+        run_replicates(args)
     else:
         run_b200(args)
 

@@ -500,7 +500,18 @@ __global__ void k_set_n_parents(Ctrl* c, int n) { c->n_parents = n; }
 int abm_set_parents(abm_ctx* c, const int* parents, int n)
 {
     if (!c || (n > 0 && !parents) || n < 0) return ABM_ERR_ARG;
-    if (n > c->cap_parents - 2 * c->cap) return fail(c, ABM_ERR_CAPACITY, "lineage longer than capacity");
+    // room for the given lineage plus two entries per division up to cap_cells cells
+    if ((long long)n + 2LL * c->cap > (long long)c->cap_parents)
+    {
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaFree(c->parents_dev));
+        c->parents_dev = nullptr;
+        c->cap_parents = n + 2 * c->cap + 1024;
+        CK(cudaMalloc(&c->parents_dev, (size_t)c->cap_parents * sizeof(int)));
+        // captured graphs hold the old buffer
+        if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+        if (c->g_rebuild) { cudaGraphExecDestroy(c->g_rebuild); c->g_rebuild = nullptr; }
+    }
     if (n > 0) CK(cudaMemcpyAsync(c->parents_dev, parents, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->st));
     k_set_n_parents<<<1, 1, 0, c->st>>>(c->ctrl, n);
     CK(cudaStreamSynchronize(c->st));

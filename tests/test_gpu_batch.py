@@ -35,6 +35,9 @@ def states():
     a = replicates.start_state(300, 1)
     b = replicates.start_state(700, 2)
     c = replicates.start_state(1500, 3)
+    for x in (a, b, c):
+        x[:25, 9] = 4.4 - 1e-4          # about to reach Ldiv: divisions within the run
+        x[:25, 10] = x[:25, 9] / 2
     d, _ = workloads.biofilm_3d(n=1200, seed=4, disk_radius=300.0 * np.sqrt(1200 / 1e5), p_contact=0.9)
     return a, b, c, d
 

@@ -65,6 +65,8 @@ def parse_args(argv=None):
                     help="3d: the 100k-cell headline; replicates: batched 2-D replicate biofilms")
     ap.add_argument("--replicates", type=int, default=256)
     ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--tile", type=int, default=0, help="screened pair pass: CSR entries per block tile")
+    ap.add_argument("--bpsm", type=int, default=0, help="screened pair pass: blocks per SM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--profile-steps", type=int, default=200)
@@ -187,7 +189,8 @@ VARIANTS = {"plain": dict(precision=0, controller=0), "chosen": dict(precision=1
 
 
 def sim_params(args, n, variant="plain"):
-    d = dict(cap_cells=n, integration_mode=args.tableau, pair_lanes=args.lanes,
+    d = dict(cap_cells=n, integration_mode=args.tableau, pair_lanes=args.lanes, pair_tile=args.tile,
+             pair_blocks_per_sm=args.bpsm,
              max_stepsize=1e-6, max_error_allowed=1e-8, iter_update_neighbors=100)
     d.update(VARIANTS[variant])
     return d
@@ -364,7 +367,7 @@ def kernel_groups(sim, args, variant):
         at_name, at_bytes = "k_attempt(proposal+commit)", attempt_bytes(args.n, True)
     else:
         at_name, at_bytes = "k_attempt(trial+final)", attempt_bytes(args.n, False) + attempt_bytes(args.n, True)
-    kernels = {"k_pair_force": (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
+    kernels = {"k_pair_screened": (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
     return kernels, prof["rebuild_ms"] / max(prof["rebuild_launches"], 1)
 
 
@@ -533,8 +536,8 @@ def run_replicates(args):
     if world > 1:
         dist_init("nccl")
     targets = replicates.target_sizes(args.replicates, 500, 50000, seed=rank)
-    lanes = replicates.lanes_by_bucket(targets, replicates.CONFIG0)
-    bt, sims = replicates.make_batch(targets, seed=1000 * rank + 1, start_fraction=0.9, lanes=lanes)
+    tiles = replicates.tiles_by_bucket(targets, replicates.CONFIG0)
+    bt, sims = replicates.make_batch(targets, seed=1000 * rank + 1, start_fraction=0.9, tiles=tiles)
     bt.iterate(max(args.warmup, 0))
     bt.synchronize()
     s0 = [s.stats() for s in sims]
@@ -569,7 +572,7 @@ def run_replicates(args):
                        "rejected_step_fraction": d["rejected"] / max(d["iterations"], 1),
                        "rk_evals_per_step": d["attempts"] / max(d["iterations"], 1),
                        "divisions": d["divisions"], "l2": "state larger than L2 (no flush needed)",
-                       "pair_lanes_by_size_decade": {str(10 ** b): v[0] for b, v in lanes.items()},
+                       "pair_tile_by_size_decade": {str(10 ** b): list(v[0]) for b, v in tiles.items()},
                        "parallelism": "replicas"},
             "gpu_launches": None,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}

@@ -59,6 +59,7 @@ class AbmParams(ctypes.Structure):
         ("controller", ctypes.c_int), ("stepsize_log_capacity", ctypes.c_int),
         ("dims", ctypes.c_int), ("sigma0", ctypes.c_double), ("adhesion_strength", ctypes.c_double),
         ("adhesion_mindist", ctypes.c_double), ("max_noise", ctypes.c_double),
+        ("pair_tile", ctypes.c_int), ("pair_blocks_per_sm", ctypes.c_int),
     ]
 
 
@@ -99,6 +100,7 @@ DEFAULTS = dict(
     daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
     cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
     dims=3, sigma0=100.0, adhesion_strength=0.0, adhesion_mindist=0.0, max_noise=0.0,
+    pair_tile=0, pair_blocks_per_sm=0,
 )
 
 # The 2-D driver (ABM-2d/ABM-2d-cpp/include/simulation.hpp:163-237): Bogacki-Shampine 3(2),
@@ -166,7 +168,7 @@ def _load():
         "abm_batch_get_stream": ([vp, P(vp)], i),
         "abm_batch_destroy": ([vp], i),
         "abm_batch_last_error": ([], ctypes.c_char_p),
-        "abm_autotune_pair_lanes": ([P(AbmParams), dp, i, i, i, dp, dp, i, i, ip, fp], i),
+        "abm_autotune_pair_tile": ([P(AbmParams), dp, i, i, i, dp, dp, i, i, ip, ip, fp], i),
         "abm_set_adhesion_flags": ([vp, ip, i], i),
         "abm_stepsize_set_weights": ([vp, fp, i], i),
         "abm_stepsize_get_weights": ([vp, fp, i], i),
@@ -195,7 +197,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
             "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags "
             "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "
-            "abm_batch_destroy abm_batch_last_error abm_autotune_pair_lanes").split()
+            "abm_batch_destroy abm_batch_last_error abm_autotune_pair_tile").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
@@ -530,9 +532,9 @@ class Batch:
             pass
 
 
-def autotune_pair_lanes(cells, launches=20, jkr_table=None, gamma=100.0, **params):
-    """Time the pair-force kernel at 4, 8, 16 and 32 lanes per cell on `cells`;
-    returns (best lanes, {lanes: ms per launch})."""
+def autotune_pair_tile(cells, launches=20, jkr_table=None, gamma=100.0, **params):
+    """Time the screened pair pass on `cells` with tiles of 512, 1024, 2048 CSR entries
+    and 4, 8, 16 blocks per SM; returns ((tile, blocks_per_sm), {(tile, bpsm): ms})."""
     p, d = make_params(**params)
     a = np.asfortranarray(cells, dtype=np.float64)
     if p.cap_cells <= 0:
@@ -541,9 +543,10 @@ def autotune_pair_lanes(cells, launches=20, jkr_table=None, gamma=100.0, **param
         jkr_table = jkr_radius_table(p.R, p.Rcell, p.E0, gamma)
     jd = np.ascontiguousarray(jkr_table[0] if jkr_table is not None else np.zeros(2))
     jr = np.ascontiguousarray(jkr_table[1] if jkr_table is not None else np.zeros(2))
-    best = ctypes.c_int()
-    ms = np.zeros(4, dtype=np.float32)
-    _batch_check(LIB.abm_autotune_pair_lanes(ctypes.byref(p), _dptr(a), a.shape[0], a.shape[1], a.shape[0],
-                                             _dptr(jd), _dptr(jr), len(jd), launches, ctypes.byref(best),
-                                             _fptr(ms)), "abm_autotune_pair_lanes")
-    return best.value, dict(zip((4, 8, 16, 32), ms.tolist()))
+    bt, bb = ctypes.c_int(), ctypes.c_int()
+    ms = np.zeros(9, dtype=np.float32)
+    _batch_check(LIB.abm_autotune_pair_tile(ctypes.byref(p), _dptr(a), a.shape[0], a.shape[1], a.shape[0],
+                                            _dptr(jd), _dptr(jr), len(jd), launches, ctypes.byref(bt),
+                                            ctypes.byref(bb), _fptr(ms)), "abm_autotune_pair_tile")
+    keys = [(t, g) for t in (512, 1024, 2048) for g in (4, 8, 16)]
+    return (bt.value, bb.value), dict(zip(keys, ms.tolist()))

@@ -3,12 +3,13 @@ advanced together, each with its own seed, clock and adaptive step).
 
 The 2-D driver (ABM-2d/ABM-2d-cpp/include/simulation.hpp:163-237) runs one colony
 per job; here every replicate is a context of its own and a Batch advances all of
-them with one CUDA graph launch per iteration.  Pair-kernel lanes per cell are
-picked per replicate-size bucket by the autotuner (abm_autotune_pair_lanes).
+them with one CUDA graph launch per iteration.  The screened pair pass's tile and
+grid shape are picked per replicate-size decade by the autotuner
+(abm_autotune_pair_tile).
 """
 import numpy as np
 
-from . import DEFAULTS_2D, Batch, Simulation, autotune_pair_lanes, workloads
+from . import DEFAULTS_2D, Batch, Simulation, autotune_pair_tile, workloads
 
 # config-0 mechanics and growth: R 0.8, Hertz E0 3900, Ldiv 4.4, growth N(1.5, 0.1^2),
 # daughter fraction N(0.5, 0.01^2), BS32 at tol 1e-8
@@ -33,19 +34,19 @@ def start_state(n, seed, growth_mean=1.5, growth_std=0.1, Ldiv=4.4):
     return cells
 
 
-def lanes_by_bucket(sizes, params, seed=0, launches=10):
-    """Autotune the pair kernel's lanes per cell once per decade of replicate size."""
+def tiles_by_bucket(sizes, params, seed=0, launches=10):
+    """Autotune the screened pair pass's (tile, blocks per SM) once per decade of replicate size."""
     buckets = sorted(set(int(np.floor(np.log10(max(s, 1)))) for s in sizes))
     out = {}
     for b in buckets:
         n = int(min(max(3 * 10 ** b, 200), 30000))
-        best, times = autotune_pair_lanes(start_state(n, seed + b), launches=launches, cap_cells=n,
-                                          **{k: v for k, v in params.items() if k != "cap_cells"})
+        best, times = autotune_pair_tile(start_state(n, seed + b), launches=launches, cap_cells=n,
+                                         **{k: v for k, v in params.items() if k != "cap_cells"})
         out[b] = (best, times)
     return out
 
 
-def make_batch(targets, seed=0, start_fraction=0.9, lanes=None, founders=False, **overrides):
+def make_batch(targets, seed=0, start_fraction=0.9, tiles=None, founders=False, **overrides):
     """Replicate r: a colony of start_fraction * targets[r] cells (or one founder cell)
     with seed seed + r, stopping at targets[r] cells.  Returns (Batch, [Simulation])."""
     params = dict(CONFIG0)
@@ -56,9 +57,10 @@ def make_batch(targets, seed=0, start_fraction=0.9, lanes=None, founders=False, 
         p = dict(params)
         p["cap_cells"] = int(2 * tgt + 64)
         p["rng_seed"] = seed + r
-        if lanes is not None:
+        if tiles is not None:
             b = int(np.floor(np.log10(max(tgt, 1))))
-            p["pair_lanes"] = lanes[b][0] if b in lanes else 8
+            if b in tiles:
+                p["pair_tile"], p["pair_blocks_per_sm"] = tiles[b][0]
         sim = Simulation(**p)
         sim.upload_cells(cells)
         sim.set_parents(-np.ones(cells.shape[0], dtype=np.int32))

@@ -36,7 +36,7 @@ struct abm_ctx {
     int *bin_count = nullptr, *bin_start = nullptr, *key = nullptr, *slot = nullptr, *sorted_cell = nullptr;
     Geom* sorted_geom = nullptr;
     int *scratch = nullptr, *nbr_count = nullptr, *row_ptr = nullptr, *col = nullptr;
-    int *lower_end = nullptr, *rev = nullptr;
+    int *lower_end = nullptr, *rev = nullptr, *row_of = nullptr;
     double4* jbuf = nullptr;
     int* scan_sums = nullptr;
     double *jkr_delta = nullptr, *jkr_radius = nullptr;
@@ -128,7 +128,7 @@ static void free_all(abm_ctx* c)
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
-                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->jbuf,
+                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->row_of, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere};
@@ -255,6 +255,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     CK(cudaMalloc(&c->col, cap * c->cap_nbr * sizeof(int)));
     CK(cudaMalloc(&c->lower_end, cap * sizeof(int)));
     CK(cudaMalloc(&c->rev, cap * c->cap_nbr * sizeof(int)));
+    CK(cudaMalloc(&c->row_of, cap * c->cap_nbr * sizeof(int)));
     CK(cudaMalloc(&c->jbuf, cap * c->cap_nbr * sizeof(double4)));
     CK(cudaMemset(c->lower_end, 0, cap * sizeof(int)));
     size_t ns = std::max(scan_block_sums_size((int)cap + 1), scan_block_sums_size(c->cap_bins + 1)) + 1;
@@ -543,7 +544,7 @@ static void enqueue_rebuild(abm_ctx* c)
                       c->nbr_count, c->cap_bins, c->num_sms, st);
     launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
     launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
-    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st);
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st, c->row_of);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, st);
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
@@ -552,17 +553,20 @@ static void enqueue_rebuild(abm_ctx* c)
 // one iteration of the loop body without division: stage-invariant pair
 // forces, then the trial attempt, up to max_tries retries and the accepted
 // final attempt (simulation.hpp:1677-1769), each an early exit when idle
+// the screened pass writes both shares of every pair; with_gather also sums them
+// per cell into fcc (the API paths; the loop's first attempt sums them itself)
 static void enqueue_pair_force(abm_ctx* c, int with_gather)
 {
-    launch_pair_force(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp, c->jkr_delta,
-                      c->jkr_radius, c->fcc, c->jbuf, c->p.pair_lanes, c->p.precision == ABM_PRECISION_MIXED,
-                      c->cap, c->st, with_gather, c->dims);
+    launch_pair_screened(c->geom, c->row_ptr, c->lower_end, c->row_of, c->col, c->rev, c->ctrl, c->fp,
+                         c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf, c->p.precision == ABM_PRECISION_MIXED,
+                         c->cap * c->cap_nbr, c->cap, c->num_sms, c->st, with_gather, c->dims, c->p.pair_tile,
+                         c->p.pair_blocks_per_sm);
 }
 
 // the attempts of one iteration; the first one completes the pair-force sum
 static PairGather loop_gather(abm_ctx* c)
 {
-    PairGather pg = {1, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
+    PairGather pg = {2, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
     return pg;
 }
 
@@ -827,7 +831,7 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
     CK(cudaStreamSynchronize(c->st));
     h.n_dir = (int)cl.size();
     CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
-    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st);
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st, c->row_of);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, c->st);
     CK(cudaGetLastError());
@@ -1352,53 +1356,55 @@ int abm_batch_destroy(abm_batch* b)
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner of the pair-force tile: lanes per cell of the pair kernel (4, 8, 16
-// or 32), timed on a scratch context holding the caller's state; the fastest
-// candidate by CUDA events over `launches` launches wins.  No reference counterpart.
+// Autotuner of the screened pair pass: tile of CSR entries per block and grid
+// blocks per SM, timed on a scratch context holding the caller's state; the
+// fastest candidate by CUDA events over `launches` launches wins.  No reference
+// counterpart.
 // ---------------------------------------------------------------------------
-int abm_autotune_pair_lanes(const abm_params* p, const double* cells, int n, int ncols, int ld,
-                            const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
-                            int* best_lanes, float* ms_per_launch)
+int abm_autotune_pair_tile(const abm_params* p, const double* cells, int n, int ncols, int ld,
+                           const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
+                           int* best_tile, int* best_bpsm, float* ms_per_launch)
 {
     g_batch_err.clear();
-    if (!p || !cells || n <= 0 || !best_lanes || launches <= 0) return batch_fail(nullptr, ABM_ERR_ARG, "bad arguments");
-    const int cand[4] = {4, 8, 16, 32};
+    if (!p || !cells || n <= 0 || !best_tile || !best_bpsm || launches <= 0)
+        return batch_fail(nullptr, ABM_ERR_ARG, "bad arguments");
+    abm_params q = *p;
+    q.cap_cells = std::max(q.cap_cells, n);
+    q.controller = ABM_CONTROLLER_REFERENCE;
+    q.stepsize_log_capacity = 0;
+    abm_ctx* c = nullptr;
+    int rc = abm_create(&q, &c);
+    if (rc == ABM_OK && q.adhesion_mode != 0 && (q.dims == 0 || q.dims == 3))
+        rc = abm_set_jkr_table(c, jkr_delta, jkr_radius, jkr_n);
+    if (rc == ABM_OK) rc = abm_upload_cells(c, cells, n, ncols, ld);
+    int m = 0;
+    if (rc == ABM_OK) rc = abm_build_neighbors(c, &m);
+    const int tiles[3] = {512, 1024, 2048}, grids[3] = {4, 8, 16};
     float best = 0;
-    *best_lanes = 0;
-    for (int k = 0; k < 4; ++k)
-    {
-        abm_params q = *p;
-        q.pair_lanes = cand[k];
-        q.cap_cells = std::max(q.cap_cells, n);
-        q.controller = ABM_CONTROLLER_REFERENCE;
-        q.stepsize_log_capacity = 0;
-        abm_ctx* c = nullptr;
-        int rc = abm_create(&q, &c);
-        if (rc == ABM_OK && q.adhesion_mode != 0 && (q.dims == 0 || q.dims == 3))
-            rc = abm_set_jkr_table(c, jkr_delta, jkr_radius, jkr_n);
-        if (rc == ABM_OK) rc = abm_upload_cells(c, cells, n, ncols, ld);
-        int m = 0;
-        if (rc == ABM_OK) rc = abm_build_neighbors(c, &m);
-        float ms = 0;
-        if (rc == ABM_OK)
+    *best_tile = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == ABM_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = ABM_ERR_CUDA;
+    for (int a = 0; a < 3 && rc == ABM_OK; ++a)
+        for (int b = 0; b < 3 && rc == ABM_OK; ++b)
         {
-            cudaEvent_t e0, e1;
-            cudaEventCreate(&e0); cudaEventCreate(&e1);
-            enqueue_pair_force(c, 1);                       // warm-up
+            c->p.pair_tile = tiles[a];
+            c->p.pair_blocks_per_sm = grids[b];
+            enqueue_pair_force(c, 0);                       // warm-up
             cudaEventRecord(e0, c->st);
-            for (int r = 0; r < launches; ++r) enqueue_pair_force(c, 1);
+            for (int r = 0; r < launches; ++r) enqueue_pair_force(c, 0);
             cudaEventRecord(e1, c->st);
-            if (cudaEventSynchronize(e1) != cudaSuccess) rc = ABM_ERR_CUDA;
-            else cudaEventElapsedTime(&ms, e0, e1);
-            cudaEventDestroy(e0); cudaEventDestroy(e1);
+            float ms = 0;
+            if (cudaEventSynchronize(e1) != cudaSuccess) { rc = ABM_ERR_CUDA; break; }
+            cudaEventElapsedTime(&ms, e0, e1);
             ms /= launches;
+            if (ms_per_launch) ms_per_launch[3 * a + b] = ms;
+            if (*best_tile == 0 || ms < best) { best = ms; *best_tile = tiles[a]; *best_bpsm = grids[b]; }
         }
-        std::string why = c ? c->err : std::string("abm_create failed");
-        if (c) abm_destroy(c);
-        if (rc) return batch_fail(nullptr, rc, "autotune candidate: " + why);
-        if (ms_per_launch) ms_per_launch[k] = ms;
-        if (*best_lanes == 0 || ms < best) { best = ms; *best_lanes = cand[k]; }
-    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    std::string why = c ? c->err : std::string("abm_create failed");
+    if (c) abm_destroy(c);
+    if (rc) return batch_fail(nullptr, rc, "autotune: " + why);
     return ABM_OK;
 }
 

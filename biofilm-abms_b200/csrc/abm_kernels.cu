@@ -752,12 +752,14 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_en
 // Reverse slots and the end of the lower part of each sorted CSR row: for an
 // entry (i, j) with j < i, rev = position of i in row j.
 __global__ void k_csr_rev(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ col,
-                          int* lower_end, int* rev)
+                          int* lower_end, int* rev, int* row_of)
 {
     const int n = ctrl->n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
+        if (row_of)
+            for (int k = r0; k < r1; ++k) row_of[k] = i;
         int lo = r0, hi = r1;
         while (lo < hi) { int mid = (lo + hi) >> 1; if (col[mid] < i) lo = mid + 1; else hi = mid; }
         lower_end[i] = lo;
@@ -772,9 +774,135 @@ __global__ void k_csr_rev(const Ctrl* ctrl, const int* __restrict__ row_ptr, con
 }
 
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
-                    int cap_cells, cudaStream_t st)
+                    int cap_cells, cudaStream_t st, int* row_of)
 {
-    k_csr_rev<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, lower_end, rev);
+    k_csr_rev<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, lower_end, rev, row_of);
+}
+
+// ---------------------------------------------------------------------------
+// Screened pair pass.  A block takes tiles of `tile` directed CSR entries.
+// Phase 1 visits each unordered pair once (from its lower entry, larger index
+// as cell 1) and tests a lower bound on the centreline distance: for any unit
+// vector a, the gap between the projections of the two segments on a,
+//     a . (c_j - c_i) - h_i |a . n_i| - h_j |a . n_j|,
+// bounds their distance from below.  a is the closest-point direction of a
+// single-precision estimate, so the bound is nearly tight, and it is evaluated
+// in FP64, so it is rigorous: a pair whose bound exceeds 2R (+1e-9) cannot
+// overlap and contributes exactly zero in every force law of the reference
+// (all need overlap > 0).  Its two slots are zeroed.  Phase 2 runs the exact
+// pair force on the compacted survivors of the tile with every lane busy and
+// writes the pair's two shares: (v, s) into the lower entry and (v, t) into the
+// partner's entry (rev).  The first attempt sums a cell's whole row in CSR order.
+// ---------------------------------------------------------------------------
+const int PS_T = 256, PS_TILE_MAX = 2048;
+
+__device__ __forceinline__ bool may_touch(const Geom& a, const Geom& b, double limit)
+{
+    const double wx = b.rx - a.rx, wy = b.ry - a.ry, wz = b.rz - a.rz;
+    // single-precision closest points (clamped, one refinement): only a direction
+    const float fwx = (float)wx, fwy = (float)wy, fwz = (float)wz;
+    const float ax = (float)a.nx, ay = (float)a.ny, az = (float)a.nz;
+    const float bx = (float)b.nx, by = (float)b.ny, bz = (float)b.nz;
+    const float ha = (float)a.h, hb = (float)b.h;
+    const float B = ax * bx + ay * by + az * bz;
+    const float D = ax * fwx + ay * fwy + az * fwz, E = bx * fwx + by * fwy + bz * fwz;
+    const float den = 1.f - B * B;
+    float s = den > 1e-6f ? (D - B * E) / den : 0.f;
+    s = fminf(fmaxf(s, -ha), ha);
+    float t = fminf(fmaxf(B * s - E, -hb), hb);
+    s = fminf(fmaxf(B * t + D, -ha), ha);
+    const double dx = wx + (double)t * b.nx - (double)s * a.nx;
+    const double dy = wy + (double)t * b.ny - (double)s * a.ny;
+    const double dz = wz + (double)t * b.nz - (double)s * a.nz;
+    const double dn = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(dn > 1e-6)) return true;
+    const double ux = dx / dn, uy = dy / dn, uz = dz / dn;
+    const double gap = (ux * wx + uy * wy + uz * wz) - a.h * fabs(ux * a.nx + uy * a.ny + uz * a.nz)
+                       - b.h * fabs(ux * b.nx + uy * b.ny + uz * b.nz);
+    return !(gap > limit + 1e-9);
+}
+
+template <bool MIXED, int DIM>
+__global__ void __launch_bounds__(PS_T) k_pair_screened(const Geom* __restrict__ geom, const int* __restrict__ row_of,
+                                                       const int* __restrict__ col, const int* __restrict__ rev,
+                                                       Ctrl* ctrl, ForceParams fp,
+                                                       const double* __restrict__ jkr_delta,
+                                                       const double* __restrict__ jkr_radius,
+                                                       double4* __restrict__ jbuf, int tile)
+{
+    __shared__ double td[JKR_MAX], tr[JKR_MAX];
+    __shared__ int list[PS_TILE_MAX];
+    __shared__ int cnt;
+    if (ctrl->halted) return;
+    for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
+    const int n_dir = ctrl->n_dir;
+    const double limit = 2 * fp.R;
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    double ovl_max = 0.0;
+    for (int base = blockIdx.x * tile; base < n_dir; base += gridDim.x * tile)
+    {
+        if (threadIdx.x == 0) cnt = 0;
+        __syncthreads();
+        for (int q = threadIdx.x; q < tile; q += PS_T)
+        {
+            const int k = base + q;
+            if (k >= n_dir) break;
+            const int i = row_of[k], j = col[k];
+            if (j >= i) continue;                    // taken from the pair's lower entry
+            if (may_touch(load_geom(geom, i), load_geom(geom, j), limit)) list[atomicAdd(&cnt, 1)] = k;
+            else { jbuf[k] = zero; jbuf[rev[k]] = zero; }
+        }
+        __syncthreads();
+        const int m = cnt;
+        for (int q = threadIdx.x; q < m; q += PS_T)
+        {
+            const int k = list[q];
+            const int i = row_of[k], j = col[k];
+            const Geom gi = load_geom(geom, i), gj = load_geom(geom, j);
+            PairOut p;
+            if (DIM == 2) p = pair_force_2d(gi, gj, fp, fp.adhere[k] != 0);
+            else p = MIXED ? pair_force_fp32(gi, gj, fp, td, tr) : pair_force_fp64(gi, gj, fp, td, tr);
+            double4 own = zero, other = zero;
+            if (p.touch)
+            {
+                own = make_double4(p.vx, p.vy, p.vz, p.s);
+                other = make_double4(p.vx, p.vy, p.vz, p.t);
+                ovl_max = fmax(ovl_max, p.ovl);
+            }
+            jbuf[k] = own;
+            jbuf[rev[k]] = other;
+        }
+        __syncthreads();
+    }
+    if (fp.stats)
+    {
+        ovl_max = warp_max(ovl_max);
+        if ((threadIdx.x & 31) == 0 && ovl_max > 0)
+            atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
+    }
+}
+
+// total dE/dq of each cell from the two shares of every pair (the API paths;
+// the loop's first attempt does the same sum itself)
+__global__ void k_pair_sum_rows(const int* __restrict__ row_ptr, const int* __restrict__ lower_end, const Ctrl* ctrl,
+                                const double4* __restrict__ jbuf, Gen6* fcc);
+
+void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* row_of,
+                          const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
+                          const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
+                          int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
+                          int blocks_per_sm)
+{
+    tile = tile <= 0 ? 1024 : min(tile, PS_TILE_MAX);
+    blocks_per_sm = blocks_per_sm <= 0 ? 8 : blocks_per_sm;
+    const int blocks = max(1, min(cdiv(max_entries, tile), num_sms * blocks_per_sm));
+#define PS_ARGS geom, row_of, col, rev, ctrl, fp, jkr_delta, jkr_radius, jbuf, tile
+    if (dims == 2) k_pair_screened<false, 2><<<blocks, PS_T, 0, st>>>(PS_ARGS);
+    else if (mixed) k_pair_screened<true, 3><<<blocks, PS_T, 0, st>>>(PS_ARGS);
+    else k_pair_screened<false, 3><<<blocks, PS_T, 0, st>>>(PS_ARGS);
+#undef PS_ARGS
+    if (with_sum)
+        k_pair_sum_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc);
 }
 
 // to_adhere (2D/include/simulation.hpp:242-258, one group in the adhesion map):
@@ -946,6 +1074,38 @@ __device__ __forceinline__ Gen6 gather_pair_force(const Gen6* fcc, const int* __
     }
     for (int c = 0; c < 6; ++c) f.f[c] += acc[c];
     return f;
+}
+
+// dE/dq of cell i from both shares of every pair in its row: (v, s v) from its lower
+// entries, (-v, -t v) from the partners' entries, in CSR order
+__device__ __forceinline__ Gen6 sum_row_shares(const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
+                                               const double4* __restrict__ jbuf, int i)
+{
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int le = lower_end[i], r1 = row_ptr[i + 1];
+    for (int k = row_ptr[i]; k < le; ++k)
+    {
+        const double4 js = jbuf[k];
+        acc[0] += js.x; acc[1] += js.y; acc[2] += js.z;
+        acc[3] += js.w * js.x; acc[4] += js.w * js.y; acc[5] += js.w * js.z;
+    }
+    for (int k = le; k < r1; ++k)
+    {
+        const double4 js = jbuf[k];
+        acc[0] -= js.x; acc[1] -= js.y; acc[2] -= js.z;
+        acc[3] -= js.w * js.x; acc[4] -= js.w * js.y; acc[5] -= js.w * js.z;
+    }
+    Gen6 f;
+    for (int c = 0; c < 6; ++c) f.f[c] = acc[c];
+    return f;
+}
+
+__global__ void k_pair_sum_rows(const int* __restrict__ row_ptr, const int* __restrict__ lower_end, const Ctrl* ctrl,
+                                const double4* __restrict__ jbuf, Gen6* fcc)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        fcc[i] = sum_row_shares(row_ptr, lower_end, jbuf, i);
 }
 
 // Step-size controller, run once per attempt by the last block
@@ -1123,7 +1283,8 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         Gen6 cc;
         if (do_gather)
         {
-            cc = gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
+            cc = pg.fused == 2 ? sum_row_shares(pg.row_ptr, pg.lower_end, pg.jbuf, i)
+                               : gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
             if (KIND == MODE_TRIAL && !sp.learned) pg.fcc_w[i] = cc;
         }
         else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);

@@ -127,8 +127,10 @@ struct BuildParams {
     int cap_per_cell;
 };
 
-// Where an attempt finds the upper half of the pair force when it completes the
-// sum itself (fused = 1, the loop); fused = 0 when fcc already holds the total.
+// Where an attempt finds the pair force when it completes the sum itself:
+// fused = 1: fcc holds the lower-neighbor share, jbuf the partners' shares;
+// fused = 2: jbuf holds both shares of every pair (screened pass);
+// fused = 0: fcc already holds the total.
 struct PairGather {
     int fused;
     const int* row_ptr;
@@ -179,7 +181,14 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_en
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
                        int with_gather = 1, int dims = 3);
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
-                    int cap_cells, cudaStream_t st);
+                    int cap_cells, cudaStream_t st, int* row_of = nullptr);
+// screened pass over every unordered pair (both shares into jbuf); with_sum also
+// writes each cell's total into fcc.  row_of[k] = row of CSR entry k.
+void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* row_of,
+                          const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
+                          const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
+                          int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
+                          int blocks_per_sm);
 
 // kind: MODE_TRIAL / MODE_RETRY / MODE_FINAL for the loop, 3 = evaluation for the API
 // (writes candidates and errors without touching the controller)

@@ -102,6 +102,9 @@ typedef struct abm_params {
     double sigma0;
     double adhesion_strength, adhesion_mindist;
     double max_noise;
+    /* shape of the screened pair pass: CSR entries per block tile (512..2048, 0 = 1024)
+     * and resident blocks per SM of its grid (0 = 8); abm_autotune_pair_tile picks them */
+    int pair_tile, pair_blocks_per_sm;
 } abm_params;
 
 typedef struct abm_stats {
@@ -228,12 +231,13 @@ int abm_batch_synchronize(abm_batch* batch);
 int abm_batch_get_stream(abm_batch* batch, void** stream);
 int abm_batch_destroy(abm_batch* batch);
 const char* abm_batch_last_error(void);
-/* Autotuner: times the pair-force kernel with 4, 8, 16 and 32 lanes per cell on a
- * scratch context holding `cells` and returns the fastest in best_lanes;
- * ms_per_launch (4 entries, may be NULL) receives each candidate's time. */
-int abm_autotune_pair_lanes(const abm_params* params, const double* cells, int n, int ncols, int ld,
-                            const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
-                            int* best_lanes, float* ms_per_launch);
+/* Autotuner of the screened pair pass: times tiles of 512, 1024 and 2048 CSR entries
+ * with 4, 8 and 16 blocks per SM (9 candidates, candidate c = 3 * tile index + grid
+ * index) on a scratch context holding `cells`, over `launches` launches each, and
+ * returns the fastest shape; ms_per_launch (9 entries, may be NULL) receives each time. */
+int abm_autotune_pair_tile(const abm_params* params, const double* cells, int n, int ncols, int ld,
+                           const double* jkr_delta, const double* jkr_radius, int jkr_n, int launches,
+                           int* best_tile, int* best_blocks_per_sm, float* ms_per_launch);
 
 /* ---------------------------------------------------------------------------
  * Step-size network (no reference counterpart).  The weights are the flat FP32

@@ -101,7 +101,21 @@ def test_batch_cell_limit_stops_each_replicate():
 
 def test_autotuner_picks_a_pair_tile():
     cells = replicates.start_state(5000, 9)
-    best, times = abm_b200.autotune_pair_lanes(cells, launches=5, **{k: v for k, v in replicates.CONFIG0.items()})
-    assert best in (4, 8, 16, 32)
-    assert all(t > 0 for t in times.values())
+    best, times = abm_b200.autotune_pair_tile(cells, launches=5, **{k: v for k, v in replicates.CONFIG0.items()})
+    assert best[0] in (512, 1024, 2048) and best[1] in (4, 8, 16)
+    assert len(times) == 9 and all(t > 0 for t in times.values())
     assert times[best] == min(times.values())
+
+
+def test_pair_tile_shapes_give_the_same_forces():
+    cells = replicates.start_state(3000, 10)
+    out = []
+    for tile, bpsm in ((512, 4), (1024, 8), (2048, 16)):
+        s = abm_b200.Simulation(cap_cells=3100, pair_tile=tile, pair_blocks_per_sm=bpsm,
+                                **{k: v for k, v in replicates.CONFIG0.items()})
+        s.upload_cells(cells)
+        s.get_cell_neighbors()
+        out.append(s.cell_cell_forces())
+        s.close()
+    # each cell's sum runs over its CSR row in a fixed order: the tile shape changes nothing
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[1], out[2])

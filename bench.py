@@ -388,11 +388,12 @@ def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
 
 
 def launches(variant, t):
-    # per iteration: pair force (+ the network's proposal), every RK attempt, and
-    # (learned) the commit of an accepted proposal; 13 kernels per neighbor rebuild
-    if VARIANTS[variant]["controller"] == 1:
-        return 2 * t["iterations"] + t["attempts"] + (t["iterations"] - t["rejected"]) + 13 * t["rebuilds"]
-    return t["iterations"] + t["attempts"] + 13 * t["rebuilds"]
+    # per iteration: the screened pair pass (screen + exact), the trial, its retries and
+    # the final attempt (an early exit after an accepted proposal), plus, with the
+    # learned controller, the network's proposal and the commit kernel; 18 kernels per
+    # neighbor rebuild
+    learned = VARIANTS[variant]["controller"] == 1
+    return t["iterations"] * (4 + (2 if learned else 0)) + t["retries"] + 18 * t["rebuilds"]
 
 
 def relerr(a, b):

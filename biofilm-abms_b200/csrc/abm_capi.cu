@@ -37,6 +37,8 @@ struct abm_ctx {
     Geom* sorted_geom = nullptr;
     int *scratch = nullptr, *nbr_count = nullptr, *row_ptr = nullptr, *col = nullptr;
     int *lower_end = nullptr, *rev = nullptr, *row_of = nullptr;
+    int4* pairs = nullptr;                                           // screened pair pass
+    int *pair_start = nullptr, *surv = nullptr;
     double4* jbuf = nullptr;
     int* scan_sums = nullptr;
     double *jkr_delta = nullptr, *jkr_radius = nullptr;
@@ -53,6 +55,7 @@ struct abm_ctx {
     // step-size network and its features
     float* mlp_w = nullptr;          // ABM_MLP_NPARAM FP32 master weights
     float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
+    double4* stat_part = nullptr;    // per-block feature partials of the final attempt
     bool mlp_loaded = false;
     // 2-D model
     int dims = 3;
@@ -128,10 +131,10 @@ static void free_all(abm_ctx* c)
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
-                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->row_of, c->jbuf,
+                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->row_of, c->pairs, c->pair_start, c->surv, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
-                    c->dgrowth, c->mlp_w, c->log_buf, c->adhere};
+                    c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -183,7 +186,8 @@ static void fill_tableau(StepParams& sp, int mode, bool& ok)
     sp.inv_q1 = 1.0 / (q + 1);
 }
 
-__global__ void k_set_n(Ctrl* c, int n) { c->n = n; c->halted = 0; }
+__global__ void k_set_n(Ctrl* c, int n) { c->n = n; c->halted = 0; c->screen_valid = 0; }
+__global__ void k_screen_stale(Ctrl* c) { c->screen_valid = 0; }
 __global__ void k_set_halt(Ctrl* c, int n_max) { c->halt_n = n_max; c->halted = 0; }
 __global__ void k_set_clock(Ctrl* c, double t, double dt, int iter)
 {
@@ -256,6 +260,9 @@ int abm_create(const abm_params* q, abm_ctx** out)
     CK(cudaMalloc(&c->lower_end, cap * sizeof(int)));
     CK(cudaMalloc(&c->rev, cap * c->cap_nbr * sizeof(int)));
     CK(cudaMalloc(&c->row_of, cap * c->cap_nbr * sizeof(int)));
+    CK(cudaMalloc(&c->pairs, cap * c->cap_nbr / 2 * sizeof(int4) + sizeof(int4)));
+    CK(cudaMalloc(&c->surv, cap * c->cap_nbr / 2 * sizeof(int) + sizeof(int)));
+    CK(cudaMalloc(&c->pair_start, (cap + 1) * sizeof(int)));
     CK(cudaMalloc(&c->jbuf, cap * c->cap_nbr * sizeof(double4)));
     CK(cudaMemset(c->lower_end, 0, cap * sizeof(int)));
     size_t ns = std::max(scan_block_sums_size((int)cap + 1), scan_block_sums_size(c->cap_bins + 1)) + 1;
@@ -304,6 +311,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     fp.max_overlap = 2 * (p.R - p.Rcell);
     fp.adhesion = p.adhesion_mode != 0;
     fp.jkr_n = 0; fp.jkr_step = 1.0;
+    fp.skin = p.pair_skin == 0 ? 0.3 : std::max(p.pair_skin, 0.0);
     c->bp.threshold = p.neighbor_threshold;
     c->bp.prefilter = p.neighbor_threshold + p.Ldiv + 2 * p.R;
     c->bp.cap_per_cell = c->cap_nbr;
@@ -355,6 +363,8 @@ int abm_create(const abm_params* q, abm_ctx** out)
         CK(cudaMemset(c->log_buf, 0, (size_t)sp.log_cap * MLP_LOG_COLS * sizeof(float)));
     }
     sp.log_buf = c->log_buf;
+    CK(cudaMalloc(&c->stat_part, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
+    sp.stat_part = c->stat_part;
     return ABM_OK;
 }
 
@@ -545,6 +555,9 @@ static void enqueue_rebuild(abm_ctx* c)
     launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
     launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
     launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st, c->row_of);
+    // pairs in the bin order of the sort just made (sorted_cell)
+    launch_pair_list(c->ctrl, c->row_ptr, c->lower_end, c->col, c->rev, c->nbr_count, c->pair_start, c->scan_sums,
+                     c->pairs, c->cap, st, c->sorted_cell);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, st);
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
@@ -560,13 +573,14 @@ static void enqueue_pair_force(abm_ctx* c, int with_gather)
     launch_pair_screened(c->geom, c->row_ptr, c->lower_end, c->row_of, c->col, c->rev, c->ctrl, c->fp,
                          c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf, c->p.precision == ABM_PRECISION_MIXED,
                          c->cap * c->cap_nbr, c->cap, c->num_sms, c->st, with_gather, c->dims, c->p.pair_tile,
-                         c->p.pair_blocks_per_sm);
+                         c->p.pair_blocks_per_sm, c->pairs, c->surv);
 }
 
 // the attempts of one iteration; the first one completes the pair-force sum
 static PairGather loop_gather(abm_ctx* c)
 {
-    PairGather pg = {2, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
+    const bool f32 = c->p.precision == ABM_PRECISION_MIXED && c->dims == 3;
+    PairGather pg = {f32 ? 3 : 2, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
     return pg;
 }
 
@@ -587,6 +601,7 @@ static void enqueue_attempts(abm_ctx* c)
                        c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
+    if (c->sp.learned) launch_commit(c->geom, c->vel, c->phys, c->ctrl, c->sp, c->geom_c, c->vel_c, c->cap, st);
 }
 
 static void enqueue_iteration(abm_ctx* c)
@@ -718,6 +733,8 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
     rc = capture_into(c, G, deps, [&]() {
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
+        if (c->sp.learned)
+            launch_commit(c->geom, c->vel, c->phys, c->ctrl, c->sp, c->geom_c, c->vel_c, c->cap, c->st);
     });
     return rc;
 }
@@ -832,6 +849,8 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
     h.n_dir = (int)cl.size();
     CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
     launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st, c->row_of);
+    launch_pair_list(c->ctrl, c->row_ptr, c->lower_end, c->col, c->rev, c->nbr_count, c->pair_start, c->scan_sums,
+                     c->pairs, c->cap, c->st);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, c->st);
     CK(cudaGetLastError());
@@ -936,6 +955,7 @@ int abm_grow(abm_ctx* c, double dt)
     if (!c) return ABM_ERR_ARG;
     if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
     launch_grow(c->geom, c->phys, c->ctrl, c->p.R, dt, c->cap, c->st);
+    k_screen_stale<<<1, 1, 0, c->st>>>(c->ctrl);
     CK(cudaGetLastError());
     return ABM_OK;
 }

@@ -311,6 +311,7 @@ __global__ void k_div_finish(Ctrl* ctrl)
     ctrl->div_events += 1;
     ctrl->last_div_tries = ctrl->div_tries;
     ctrl->n_divide = 0;
+    ctrl->screen_valid = 0;            // new cells: the active pair list is stale
 }
 
 void launch_div_count(const Phys* phys, Ctrl* ctrl, const DivideParams& dp, int* flags,

@@ -780,19 +780,21 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
 }
 
 // ---------------------------------------------------------------------------
-// Screened pair pass.  A block takes tiles of `tile` directed CSR entries.
-// Phase 1 visits each unordered pair once (from its lower entry, larger index
-// as cell 1) and tests a lower bound on the centreline distance: for any unit
+// Screened pair pass.  Phase 1 (k_pair_screen) visits each unordered pair once
+// (from its lower entry, larger index as cell 1; pair_k lists them) and tests a
+// lower bound on the centreline distance: for any unit
 // vector a, the gap between the projections of the two segments on a,
 //     a . (c_j - c_i) - h_i |a . n_i| - h_j |a . n_j|,
 // bounds their distance from below.  a is the closest-point direction of a
 // single-precision estimate, so the bound is nearly tight, and it is evaluated
 // in FP64, so it is rigorous: a pair whose bound exceeds 2R (+1e-9) cannot
 // overlap and contributes exactly zero in every force law of the reference
-// (all need overlap > 0).  Its two slots are zeroed.  Phase 2 runs the exact
-// pair force on the compacted survivors of the tile with every lane busy and
-// writes the pair's two shares: (v, s) into the lower entry and (v, t) into the
-// partner's entry (rev).  The first attempt sums a cell's whole row in CSR order.
+// (all need overlap > 0).  Its two slots are zeroed; the others are appended to a
+// survivor list.  Phase 2 (k_pair_exact) runs the exact pair force on the
+// survivors with every lane busy and writes the pair's two shares: (v, s) into
+// the lower entry and (v, t) into the partner's entry (rev).  Every slot is
+// written by exactly one pair, so the order of the survivor list changes no
+// result.  The first attempt sums a cell's whole row in CSR order.
 // ---------------------------------------------------------------------------
 const int PS_T = 256, PS_TILE_MAX = 2048;
 
@@ -822,47 +824,103 @@ __device__ __forceinline__ bool may_touch(const Geom& a, const Geom& b, double l
     return !(gap > limit + 1e-9);
 }
 
+// Phase 1: one thread per unordered pair (its lower entry k, listed in pair_k).
+// Few registers, so many warps hide the latency of the scattered loads.
+template <bool MIXED>
+__device__ __forceinline__ void zero_shares(double4* jbuf, int k, int r)
+{
+    if (MIXED)
+    {
+        float4* fb = reinterpret_cast<float4*>(jbuf);
+        fb[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        fb[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    else
+    {
+        jbuf[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+        jbuf[r] = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+}
+
+// Refresh of the active list, when it is stale: after a rebuild, an upload or a
+// division, or once the cells may have moved by half the skin since the last
+// refresh (2 * drift >= skin).  Otherwise the kernel returns at once.  A pair
+// whose bound exceeds 2R + skin stays inactive (its shares are zeroed here and
+// stay zero) until the next refresh: in the meantime its distance can fall by at
+// most 2 * drift < skin, so it still exceeds 2R and its force is exactly zero.
+template <bool MIXED>
+__global__ void __launch_bounds__(PS_T) k_pair_screen(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
+                                                     Ctrl* ctrl, double R, double skin, double4* __restrict__ jbuf,
+                                                     int* __restrict__ surv)
+{
+    if (ctrl->halted) return;
+    if (ctrl->screen_valid && 2.0 * ctrl->drift * (1.0 + 1e-6) + 1e-9 < skin) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->refreshing = 1;
+    const int n_pairs = ctrl->n_dir >> 1;
+    const double limit = 2 * R + skin;
+    const int lane = threadIdx.x & 31;
+    // warp-uniform rounds, so that every ballot covers all 32 lanes
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n_pairs; base += stride)
+    {
+        const int p = base + lane;
+        bool keep = false;
+        if (p < n_pairs)
+        {
+            const int4 pr = pairs[p];             // (i, j, lower entry k, partner entry)
+            keep = may_touch(load_geom(geom, pr.x), load_geom(geom, pr.y), limit);
+            if (!keep) zero_shares<MIXED>(jbuf, pr.z, pr.w);
+        }
+        // warp-aggregated append of the active pairs
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        int pos = 0;
+        if (lane == 0 && mask) pos = atomicAdd(&ctrl->n_surv_next, __popc(mask));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (keep) surv[pos + __popc(mask & ((1u << lane) - 1u))] = p;
+    }
+}
+
+// Phase 2: the exact pair force of every active pair, its two shares into jbuf;
+// after a refresh the last block installs the new list and clears the drift.
 template <bool MIXED, int DIM>
-__global__ void __launch_bounds__(PS_T) k_pair_screened(const Geom* __restrict__ geom, const int* __restrict__ row_of,
-                                                       const int* __restrict__ col, const int* __restrict__ rev,
-                                                       Ctrl* ctrl, ForceParams fp,
-                                                       const double* __restrict__ jkr_delta,
-                                                       const double* __restrict__ jkr_radius,
-                                                       double4* __restrict__ jbuf, int tile)
+__global__ void __launch_bounds__(PS_T) k_pair_exact(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
+                                                    Ctrl* ctrl, ForceParams fp, const double* __restrict__ jkr_delta,
+                                                    const double* __restrict__ jkr_radius,
+                                                    double4* __restrict__ jbuf, const int* __restrict__ surv)
 {
     __shared__ double td[JKR_MAX], tr[JKR_MAX];
-    __shared__ int list[PS_TILE_MAX];
-    __shared__ int cnt;
+    __shared__ bool last;
     if (ctrl->halted) return;
     for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
-    const int n_dir = ctrl->n_dir;
-    const double limit = 2 * fp.R;
-    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    __syncthreads();
+    const bool refreshed = ctrl->refreshing != 0;
+    const int m = refreshed ? ctrl->n_surv_next : ctrl->n_surv;
     double ovl_max = 0.0;
-    for (int base = blockIdx.x * tile; base < n_dir; base += gridDim.x * tile)
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
     {
-        if (threadIdx.x == 0) cnt = 0;
-        __syncthreads();
-        for (int q = threadIdx.x; q < tile; q += PS_T)
+        const int4 pr = pairs[surv[q]];
+        const int k = pr.z, r = pr.w;
+        const Geom gi = load_geom(geom, pr.x), gj = load_geom(geom, pr.y);
+        PairOut p;
+        if (DIM == 2) p = pair_force_2d(gi, gj, fp, fp.adhere[k] != 0);
+        else p = MIXED ? pair_force_fp32(gi, gj, fp, td, tr) : pair_force_fp64(gi, gj, fp, td, tr);
+        if (MIXED)
         {
-            const int k = base + q;
-            if (k >= n_dir) break;
-            const int i = row_of[k], j = col[k];
-            if (j >= i) continue;                    // taken from the pair's lower entry
-            if (may_touch(load_geom(geom, i), load_geom(geom, j), limit)) list[atomicAdd(&cnt, 1)] = k;
-            else { jbuf[k] = zero; jbuf[rev[k]] = zero; }
+            // mixed precision: the shares are single-precision forces, stored as such
+            float4* fb = reinterpret_cast<float4*>(jbuf);
+            float4 own = make_float4(0.f, 0.f, 0.f, 0.f), other = own;
+            if (p.touch)
+            {
+                own = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.s);
+                other = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.t);
+                ovl_max = fmax(ovl_max, p.ovl);
+            }
+            fb[k] = own;
+            fb[r] = other;
         }
-        __syncthreads();
-        const int m = cnt;
-        for (int q = threadIdx.x; q < m; q += PS_T)
+        else
         {
-            const int k = list[q];
-            const int i = row_of[k], j = col[k];
-            const Geom gi = load_geom(geom, i), gj = load_geom(geom, j);
-            PairOut p;
-            if (DIM == 2) p = pair_force_2d(gi, gj, fp, fp.adhere[k] != 0);
-            else p = MIXED ? pair_force_fp32(gi, gj, fp, td, tr) : pair_force_fp64(gi, gj, fp, td, tr);
-            double4 own = zero, other = zero;
+            double4 own = make_double4(0.0, 0.0, 0.0, 0.0), other = own;
             if (p.touch)
             {
                 own = make_double4(p.vx, p.vy, p.vz, p.s);
@@ -870,9 +928,8 @@ __global__ void __launch_bounds__(PS_T) k_pair_screened(const Geom* __restrict__
                 ovl_max = fmax(ovl_max, p.ovl);
             }
             jbuf[k] = own;
-            jbuf[rev[k]] = other;
+            jbuf[r] = other;
         }
-        __syncthreads();
     }
     if (fp.stats)
     {
@@ -880,29 +937,96 @@ __global__ void __launch_bounds__(PS_T) k_pair_screened(const Geom* __restrict__
         if ((threadIdx.x & 31) == 0 && ovl_max > 0)
             atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
     }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        last = atomicAdd(&ctrl->surv_blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        if (refreshed)
+        {
+            ctrl->n_surv = ctrl->n_surv_next;
+            ctrl->n_surv_next = 0;
+            ctrl->refreshing = 0;
+            ctrl->screen_valid = 1;
+            ctrl->drift = 0.0;
+        }
+        ctrl->surv_blocks = 0u;
+    }
+}
+
+// The pair list visits cells in `order` (the cell list's bin order after a rebuild,
+// else index order): pairs of one region of space are screened together, so each
+// cell's record is fetched once and reused from the caches by its neighbours' pairs.
+// a new pair list (or new cells) makes the active list stale
+__global__ void k_invalidate_screen(Ctrl* ctrl) { ctrl->screen_valid = 0; }
+
+__global__ void k_lower_counts(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
+                               const int* __restrict__ order, int* count)
+{
+    const int n = ctrl->n;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    {
+        const int i = order ? order[q] : q;
+        count[q] = lower_end[i] - row_ptr[i];
+    }
+}
+
+__global__ void k_pair_list_fill(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
+                                 const int* __restrict__ col, const int* __restrict__ rev,
+                                 const int* __restrict__ order, const int* __restrict__ start, int4* pairs)
+{
+    const int n = ctrl->n;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    {
+        const int i = order ? order[q] : q;
+        const int r0 = row_ptr[i], p0 = start[q];
+        for (int k = r0; k < lower_end[i]; ++k) pairs[p0 + (k - r0)] = make_int4(i, col[k], k, rev[k]);
+    }
+}
+
+void launch_pair_list(const Ctrl* ctrl, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
+                      int* count, int* start, int* block_sums, int4* pairs, int cap_cells, cudaStream_t st,
+                      const int* order)
+{
+    const int blocks = max(cdiv(cap_cells, 256), 1);
+    k_lower_counts<<<blocks, 256, 0, st>>>(ctrl, row_ptr, lower_end, order, count);
+    launch_scan(count, &ctrl->n, start, block_sums, cap_cells, st);
+    k_pair_list_fill<<<blocks, 256, 0, st>>>(ctrl, row_ptr, lower_end, col, rev, order, start, pairs);
+    k_invalidate_screen<<<1, 1, 0, st>>>(const_cast<Ctrl*>(ctrl));
 }
 
 // total dE/dq of each cell from the two shares of every pair (the API paths;
 // the loop's first attempt does the same sum itself)
 __global__ void k_pair_sum_rows(const int* __restrict__ row_ptr, const int* __restrict__ lower_end, const Ctrl* ctrl,
-                                const double4* __restrict__ jbuf, Gen6* fcc);
+                                const double4* __restrict__ jbuf, Gen6* fcc, int f32);
 
 void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* row_of,
                           const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
-                          int blocks_per_sm)
+                          int blocks_per_sm, const int4* pairs, int* surv)
 {
+    // tile: pairs per screening block over the capacity (sets the screening grid);
+    // blocks_per_sm: resident blocks per SM of the exact pass's grid
     tile = tile <= 0 ? 1024 : min(tile, PS_TILE_MAX);
     blocks_per_sm = blocks_per_sm <= 0 ? 8 : blocks_per_sm;
-    const int blocks = max(1, min(cdiv(max_entries, tile), num_sms * blocks_per_sm));
-#define PS_ARGS geom, row_of, col, rev, ctrl, fp, jkr_delta, jkr_radius, jbuf, tile
-    if (dims == 2) k_pair_screened<false, 2><<<blocks, PS_T, 0, st>>>(PS_ARGS);
-    else if (mixed) k_pair_screened<true, 3><<<blocks, PS_T, 0, st>>>(PS_ARGS);
-    else k_pair_screened<false, 3><<<blocks, PS_T, 0, st>>>(PS_ARGS);
-#undef PS_ARGS
+    const int max_pairs = max(max_entries / 2, 1);
+    const int b1 = max(1, min(cdiv(max_pairs, tile), num_sms * 32));
+    const int b2 = max(1, min(cdiv(max_pairs, PS_T), num_sms * blocks_per_sm));
+    const bool f32 = mixed && dims != 2;
+    if (f32) k_pair_screen<true><<<b1, PS_T, 0, st>>>(geom, pairs, ctrl, fp.R, fp.skin, jbuf, surv);
+    else k_pair_screen<false><<<b1, PS_T, 0, st>>>(geom, pairs, ctrl, fp.R, fp.skin, jbuf, surv);
+#define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv
+    if (dims == 2) k_pair_exact<false, 2><<<b2, PS_T, 0, st>>>(PX_ARGS);
+    else if (mixed) k_pair_exact<true, 3><<<b2, PS_T, 0, st>>>(PX_ARGS);
+    else k_pair_exact<false, 3><<<b2, PS_T, 0, st>>>(PX_ARGS);
+#undef PX_ARGS
     if (with_sum)
-        k_pair_sum_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc);
+        k_pair_sum_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc, f32);
 }
 
 // to_adhere (2D/include/simulation.hpp:242-258, one group in the adhesion map):
@@ -1076,22 +1200,30 @@ __device__ __forceinline__ Gen6 gather_pair_force(const Gen6* fcc, const int* __
     return f;
 }
 
+__device__ __forceinline__ double4 widen(const double4& v) { return v; }
+__device__ __forceinline__ double4 widen(const float4& v)
+{
+    return make_double4((double)v.x, (double)v.y, (double)v.z, (double)v.w);
+}
+
 // dE/dq of cell i from both shares of every pair in its row: (v, s v) from its lower
-// entries, (-v, -t v) from the partners' entries, in CSR order
+// entries, (-v, -t v) from the partners' entries, in CSR order.  Shares are stored
+// as double4, or as float4 (mixed precision), summed in FP64 either way.
+template <class SHARE>
 __device__ __forceinline__ Gen6 sum_row_shares(const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
-                                               const double4* __restrict__ jbuf, int i)
+                                               const SHARE* __restrict__ jbuf, int i)
 {
     double acc[6] = {0, 0, 0, 0, 0, 0};
     const int le = lower_end[i], r1 = row_ptr[i + 1];
     for (int k = row_ptr[i]; k < le; ++k)
     {
-        const double4 js = jbuf[k];
+        const double4 js = widen(jbuf[k]);
         acc[0] += js.x; acc[1] += js.y; acc[2] += js.z;
         acc[3] += js.w * js.x; acc[4] += js.w * js.y; acc[5] += js.w * js.z;
     }
     for (int k = le; k < r1; ++k)
     {
-        const double4 js = jbuf[k];
+        const double4 js = widen(jbuf[k]);
         acc[0] -= js.x; acc[1] -= js.y; acc[2] -= js.z;
         acc[3] -= js.w * js.x; acc[4] -= js.w * js.y; acc[5] -= js.w * js.z;
     }
@@ -1101,11 +1233,12 @@ __device__ __forceinline__ Gen6 sum_row_shares(const int* __restrict__ row_ptr, 
 }
 
 __global__ void k_pair_sum_rows(const int* __restrict__ row_ptr, const int* __restrict__ lower_end, const Ctrl* ctrl,
-                                const double4* __restrict__ jbuf, Gen6* fcc)
+                                const double4* __restrict__ jbuf, Gen6* fcc, int f32)
 {
     const int n = ctrl->n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        fcc[i] = sum_row_shares(row_ptr, lower_end, jbuf, i);
+        fcc[i] = f32 ? sum_row_shares(row_ptr, lower_end, reinterpret_cast<const float4*>(jbuf), i)
+                     : sum_row_shares(row_ptr, lower_end, jbuf, i);
 }
 
 // Step-size controller, run once per attempt by the last block
@@ -1200,7 +1333,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
                                                  unsigned long long cond, int use_cond, PairGather pg)
 {
-    __shared__ double sh_max[AT_T / 32];
+    __shared__ double sh_max[AT_T / 32], sh_drift[AT_T / 32];
     __shared__ double4 sh_stat[AT_T / 32];
     __shared__ bool last;
     if (KIND != 3 && ctrl->halted)
@@ -1244,7 +1377,9 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         load_k0 = share_k0 && trial_ran;
     }
     else { dt = eval_dt; attempt = eval_attempt; }
-    const bool commit = (KIND == MODE_FINAL) && mode == MODE_COMMIT;
+    // an accepted proposal is committed by k_commit, which follows this kernel
+    if (KIND == MODE_FINAL && mode == MODE_COMMIT) return;
+    const bool commit = false;
     // the learned trial writes its candidate state for a commit
     const bool write_candidate = (KIND == MODE_TRIAL) && sp.learned;
 
@@ -1256,26 +1391,10 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     double local_max = 0.0;
     bool bad = false;
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
+    // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
+    double local_drift = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        if (commit)
-        {
-            // committed proposal: candidate -> state (growth already applied)
-            const Geom gc = geom_c[i];
-            const Vel vc = vel_c[i];
-            geom[i] = gc;
-            vel[i] = vc;
-            phys[i].l = 2 * gc.h;
-            if (sp.stats_on)
-            {
-                const double v2 = vc.v[0] * vc.v[0] + vc.v[1] * vc.v[1] + vc.v[2] * vc.v[2];
-                st_vmax = fmax(st_vmax, sqrt(v2));
-                st_v2 += v2;
-                st_g += phys[i].growth;
-                st_near += (2 * gc.h > sp.near_div_length) ? 1.0 : 0.0;
-            }
-            continue;
-        }
         const Geom g = load_geom(geom, i);
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
         const double l = phys[i].l, eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
@@ -1283,7 +1402,8 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         Gen6 cc;
         if (do_gather)
         {
-            cc = pg.fused == 2 ? sum_row_shares(pg.row_ptr, pg.lower_end, pg.jbuf, i)
+            cc = pg.fused == 3 ? sum_row_shares(pg.row_ptr, pg.lower_end, reinterpret_cast<const float4*>(pg.jbuf), i)
+               : pg.fused == 2 ? sum_row_shares(pg.row_ptr, pg.lower_end, pg.jbuf, i)
                                : gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
             if (KIND == MODE_TRIAL && !sp.learned) pg.fcc_w[i] = cc;
         }
@@ -1362,6 +1482,13 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                 const double g_rate = phys[i].growth;
                 double lg = l + g_rate * (4 * sp.mp.R / 3 + l) * dt;
                 go.h = lg / 2;
+                {
+                    const double ax = go.rx - g.rx, ay = go.ry - g.ry, az = go.rz - g.rz;
+                    const double bx = go.nx - g.nx, by = go.ny - g.ny, bz = go.nz - g.nz;
+                    local_drift = fmax(local_drift, sqrt(ax * ax + ay * ay + az * az)
+                                                        + go.h * sqrt(bx * bx + by * by + bz * bz)
+                                                        + fabs(go.h - g.h));
+                }
                 if (KIND == MODE_FINAL)
                 {
                     phys[i].l = lg;
@@ -1410,12 +1537,14 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                 const double4 b = sh_stat[w];
                 a.x = fmax(a.x, b.x); a.y += b.y; a.z += b.z; a.w += b.w;
             }
-            // block sums in fixed point: integer atomics add up the same in any order
-            if (a.x > 0) atomicMax(&ctrl->st_vmax_bits, (unsigned long long)__double_as_longlong(a.x));
-            atomicAdd(&ctrl->st_v2_fx, (unsigned long long)llrint(ldexp(a.y, STAT_V2_SHIFT)));
-            atomicAdd(&ctrl->st_g_fx, (unsigned long long)llrint(ldexp(fmax(a.z, 0.0), STAT_G_SHIFT)));
-            atomicAdd(&ctrl->st_near_div, (unsigned long long)a.w);
+            // the last block sums the partials in block order (no contended atomics)
+            sp.stat_part[blockIdx.x] = a;
         }
+    }
+    if (KIND == MODE_FINAL || write_candidate)
+    {
+        local_drift = warp_max(local_drift);
+        if ((threadIdx.x & 31) == 0) sh_drift[threadIdx.x >> 5] = local_drift;
     }
     // block max of the scaled error, floored at min_error (simulation.hpp:1703)
     local_max = fmax(local_max, sp.min_error);
@@ -1429,6 +1558,12 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         for (int w = 1; w < AT_T / 32; ++w) m = fmax(m, sh_max[w]);
         unsigned long long bits = (unsigned long long)__double_as_longlong(m);
         if (bad) atomicOr(&ctrl->status, (int)ST_NAN);
+        if (KIND == MODE_FINAL || write_candidate)
+        {
+            double dm = sh_drift[0];
+            for (int w = 1; w < AT_T / 32; ++w) dm = fmax(dm, sh_drift[w]);
+            if (dm > 0) atomicMax(&ctrl->drift_bits, (unsigned long long)__double_as_longlong(dm));
+        }
         if (KIND == 3) { atomicMax(&ctrl->eval_err_bits, bits); last = false; }
         else
         {
@@ -1439,12 +1574,53 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         }
     }
     __syncthreads();
+    if (KIND == MODE_FINAL && sp.stats_on && last)
+    {
+        // step-size features of the accepted step: every block's partial, in block order
+        __threadfence();
+        double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int b = threadIdx.x; b < gridDim.x; b += AT_T)
+        {
+            const double2* q = reinterpret_cast<const double2*>(sp.stat_part + b);
+            const double2 p0 = __ldcg(q), p1 = __ldcg(q + 1);
+            a.x = fmax(a.x, p0.x); a.y += p0.y; a.z += p1.x; a.w += p1.y;
+        }
+        a.x = warp_max(a.x);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
+            a.z += __shfl_xor_sync(0xffffffffu, a.z, off);
+            a.w += __shfl_xor_sync(0xffffffffu, a.w, off);
+        }
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) sh_stat[threadIdx.x >> 5] = a;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double4 t = sh_stat[0];
+            for (int w = 1; w < AT_T / 32; ++w)
+            {
+                const double4 b = sh_stat[w];
+                t.x = fmax(t.x, b.x); t.y += b.y; t.z += b.z; t.w += b.w;
+            }
+            ctrl->st_vmax_bits = (unsigned long long)__double_as_longlong(t.x);
+            ctrl->st_v2_fx = (unsigned long long)llrint(ldexp(t.y, STAT_V2_SHIFT));
+            ctrl->st_g_fx = (unsigned long long)llrint(ldexp(fmax(t.z, 0.0), STAT_G_SHIFT));
+            ctrl->st_near_div = (unsigned long long)t.w;
+        }
+    }
     if (KIND != 3 && last && threadIdx.x == 0)
     {
         __threadfence();
         double E = __longlong_as_double((long long)atomicAdd(&ctrl->err_bits, 0ull));
         E = fmax(E, sp.min_error);
         if (commit) E = ctrl->last_trial_error;
+        // motion of the new state: counted now for a final step, at the commit for a proposal
+        const double dm = __longlong_as_double((long long)atomicAdd(&ctrl->drift_bits, 0ull));
+        if (KIND == MODE_FINAL) ctrl->drift += dm;
+        else if (write_candidate) ctrl->drift_cand = dm;
+        ctrl->drift_bits = 0ull;
         ctrl->err_bits = 0ull;
         ctrl->blocks_done = 0u;
         controller_finish(ctrl, sp, KIND, E, commit);
@@ -1473,6 +1649,106 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 }
 
 int attempt_blocks(int cap_cells) { return max(cdiv(cap_cells, AT_T), 1); }
+
+// Commit of an accepted proposal (learned controller): candidate -> state, growth
+// already applied by the proposal; per-block feature partials for the next
+// proposal; the last block sums them in block order and closes the step.  A light
+// kernel (copies and sums only), so it runs at full occupancy.  Returns at once
+// when the iteration has no accepted proposal.
+__global__ void __launch_bounds__(AT_T) k_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, StepParams sp,
+                                                 const Geom* __restrict__ geom_c, const Vel* __restrict__ vel_c)
+{
+    __shared__ double4 sh[AT_T / 32];
+    __shared__ bool last;
+    if (ctrl->halted || ctrl->mode != MODE_COMMIT) return;
+    const int n = ctrl->n;
+    double vmax = 0.0, v2s = 0.0, gs = 0.0, near = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom gc = geom_c[i];
+        const Vel vc = vel_c[i];
+        geom[i] = gc;
+        vel[i] = vc;
+        phys[i].l = 2 * gc.h;
+        if (sp.stats_on)
+        {
+            const double v2 = vc.v[0] * vc.v[0] + vc.v[1] * vc.v[1] + vc.v[2] * vc.v[2];
+            vmax = fmax(vmax, sqrt(v2));
+            v2s += v2;
+            gs += phys[i].growth;
+            near += (2 * gc.h > sp.near_div_length) ? 1.0 : 0.0;
+        }
+    }
+    // block partial in a fixed reduction order
+    vmax = warp_max(vmax);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        v2s += __shfl_xor_sync(0xffffffffu, v2s, off);
+        gs += __shfl_xor_sync(0xffffffffu, gs, off);
+        near += __shfl_xor_sync(0xffffffffu, near, off);
+    }
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = make_double4(vmax, v2s, gs, near);
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double4 a = sh[0];
+        for (int w = 1; w < AT_T / 32; ++w)
+        {
+            const double4 b = sh[w];
+            a.x = fmax(a.x, b.x); a.y += b.y; a.z += b.z; a.w += b.w;
+        }
+        sp.stat_part[blockIdx.x] = a;
+        __threadfence();
+        last = atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int b = threadIdx.x; b < gridDim.x; b += AT_T)
+    {
+        const double2* q = reinterpret_cast<const double2*>(sp.stat_part + b);
+        const double2 p0 = __ldcg(q), p1 = __ldcg(q + 1);
+        a.x = fmax(a.x, p0.x); a.y += p0.y; a.z += p1.x; a.w += p1.y;
+    }
+    a.x = warp_max(a.x);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
+        a.z += __shfl_xor_sync(0xffffffffu, a.z, off);
+        a.w += __shfl_xor_sync(0xffffffffu, a.w, off);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double4 t = sh[0];
+        for (int w = 1; w < AT_T / 32; ++w)
+        {
+            const double4 b = sh[w];
+            t.x = fmax(t.x, b.x); t.y += b.y; t.z += b.z; t.w += b.w;
+        }
+        if (sp.stats_on)
+        {
+            ctrl->st_vmax_bits = (unsigned long long)__double_as_longlong(t.x);
+            ctrl->st_v2_fx = (unsigned long long)llrint(ldexp(t.y, STAT_V2_SHIFT));
+            ctrl->st_g_fx = (unsigned long long)llrint(ldexp(fmax(t.z, 0.0), STAT_G_SHIFT));
+            ctrl->st_near_div = (unsigned long long)t.w;
+        }
+        ctrl->blocks_done = 0u;
+        ctrl->drift += ctrl->drift_cand;
+        controller_finish(ctrl, sp, MODE_FINAL, ctrl->last_trial_error, true);
+    }
+}
+
+void launch_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const StepParams& sp, const Geom* geom_c,
+                   const Vel* vel_c, int cap_cells, cudaStream_t st)
+{
+    k_commit<<<attempt_blocks(cap_cells), AT_T, 0, st>>>(geom, vel, phys, ctrl, sp, geom_c, vel_c);
+}
 
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,

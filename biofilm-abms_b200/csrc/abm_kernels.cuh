@@ -77,6 +77,16 @@ struct Ctrl {
     int halt_n;                         // 0 = no limit
     int halted;
     long long cell_steps;               // sum of the population over accepted steps
+    // screened pair pass: the active list (pairs that passed the bound test with the
+    // skin at the last refresh) and the motion since then
+    int n_surv;                         // active pairs
+    int n_surv_next;                    // pairs appended by a refresh in progress
+    int refreshing;                     // the screening pass of this iteration refreshed
+    int screen_valid;                   // 0 after a rebuild, an upload or a division
+    unsigned int surv_blocks;           // last-block counter of the exact pass
+    double drift;                       // sum over accepted steps of the max segment motion
+    double drift_cand;                  // max segment motion of the learned proposal's candidate
+    unsigned long long drift_bits;      // block maxima of the running attempt (ordered bits)
 };
 
 struct Grid {
@@ -102,6 +112,7 @@ struct StepParams {
     int learned;                // 1: the network proposes dt, a passing proposal is accepted as is
     int stats_on;               // accumulate the network's features (learned or logging)
     double near_div_length;     // 0.9 Ldiv
+    double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
     float* log_buf;             // MLP_LOG_COLS floats per row, log_cap rows (ring)
     int log_cap;
 };
@@ -114,6 +125,7 @@ struct ForceParams {
     int jkr_n;
     double jkr_step;            // spacing of the overlap mesh
     int stats;                  // record the max overlap (step-size features)
+    double skin;                // screened pair pass: margin of the active list (um)
     // 2-D model (ABM-2d): Hertz prefactors of 2D/include/simulation.hpp:232-235 and
     // the JKR-Lagrange adhesion of 2D/include/adhesion.hpp:403-448
     double pf2d[3];
@@ -129,7 +141,8 @@ struct BuildParams {
 
 // Where an attempt finds the pair force when it completes the sum itself:
 // fused = 1: fcc holds the lower-neighbor share, jbuf the partners' shares;
-// fused = 2: jbuf holds both shares of every pair (screened pass);
+// fused = 2: jbuf holds both shares of every pair (screened pass), as double4;
+// fused = 3: the same as float4 (mixed precision);
 // fused = 0: fcc already holds the total.
 struct PairGather {
     int fused;
@@ -188,7 +201,13 @@ void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower
                           const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
-                          int blocks_per_sm);
+                          int blocks_per_sm, const int4* pairs, int* surv);
+// the list of unordered pairs (i, j < i, lower entry k, partner entry rev[k]) after
+// k_csr_rev, cells in `order` (null: index order): counts -> scan -> fill; uses
+// `count` and `start` (cap_cells + 1) as scratch
+void launch_pair_list(const Ctrl* ctrl, const int* row_ptr, const int* lower_end, const int* col, const int* rev,
+                      int* count, int* start, int* block_sums, int4* pairs, int cap_cells, cudaStream_t st,
+                      const int* order = nullptr);
 
 // kind: MODE_TRIAL / MODE_RETRY / MODE_FINAL for the loop, 3 = evaluation for the API
 // (writes candidates and errors without touching the controller)
@@ -199,6 +218,9 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
                     unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0},
                     int dims = 3);
+// accepted proposal of the learned controller: candidate -> state (no-op otherwise)
+void launch_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const StepParams& sp, const Geom* geom_c,
+                   const Vel* vel_c, int cap_cells, cudaStream_t st);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
                        cudaStream_t st, int dims = 3);

@@ -102,9 +102,13 @@ typedef struct abm_params {
     double sigma0;
     double adhesion_strength, adhesion_mindist;
     double max_noise;
-    /* shape of the screened pair pass: CSR entries per block tile (512..2048, 0 = 1024)
-     * and resident blocks per SM of its grid (0 = 8); abm_autotune_pair_tile picks them */
+    /* shape of the screened pair pass: pairs per block of the screening grid (512..2048,
+     * 0 = 1024) and blocks per SM of the exact pass's grid (0 = 8);
+     * abm_autotune_pair_tile picks them */
     int pair_tile, pair_blocks_per_sm;
+    /* skin of the active pair list in um (0 = 0.3, negative = none): pairs farther than
+     * 2R + skin at a refresh are skipped until the cells may have moved by half the skin */
+    double pair_skin;
 } abm_params;
 
 typedef struct abm_stats {
@@ -231,8 +235,8 @@ int abm_batch_synchronize(abm_batch* batch);
 int abm_batch_get_stream(abm_batch* batch, void** stream);
 int abm_batch_destroy(abm_batch* batch);
 const char* abm_batch_last_error(void);
-/* Autotuner of the screened pair pass: times tiles of 512, 1024 and 2048 CSR entries
- * with 4, 8 and 16 blocks per SM (9 candidates, candidate c = 3 * tile index + grid
+/* Autotuner of the screened pair pass: times screening tiles of 512, 1024 and 2048 pairs
+ * with exact-pass grids of 4, 8 and 16 blocks per SM (9 candidates, c = 3 * tile index + grid
  * index) on a scratch context holding `cells`, over `launches` launches each, and
  * returns the fastest shape; ms_per_launch (9 entries, may be NULL) receives each time. */
 int abm_autotune_pair_tile(const abm_params* params, const double* cells, int n, int ncols, int ld,

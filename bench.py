@@ -67,6 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--tile", type=int, default=0, help="screened pair pass: CSR entries per block tile")
     ap.add_argument("--bpsm", type=int, default=0, help="screened pair pass: blocks per SM")
+    ap.add_argument("--pair-sum", type=int, default=0, help="1: shares summed in the first attempt, 2: separately")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--profile-steps", type=int, default=200)
@@ -190,7 +191,7 @@ VARIANTS = {"plain": dict(precision=0, controller=0), "chosen": dict(precision=1
 
 def sim_params(args, n, variant="plain"):
     d = dict(cap_cells=n, integration_mode=args.tableau, pair_lanes=args.lanes, pair_tile=args.tile,
-             pair_blocks_per_sm=args.bpsm,
+             pair_blocks_per_sm=args.bpsm, pair_sum=args.pair_sum,
              max_stepsize=1e-6, max_error_allowed=1e-8, iter_update_neighbors=100)
     d.update(VARIANTS[variant])
     return d

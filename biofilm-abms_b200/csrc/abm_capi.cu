@@ -576,11 +576,18 @@ static void enqueue_pair_force(abm_ctx* c, int with_gather)
                          c->p.pair_blocks_per_sm, c->pairs, c->surv);
 }
 
-// the attempts of one iteration; the first one completes the pair-force sum
+// pair_sum 1 (default): the first attempt sums each cell's shares itself; 2: a
+// separate light kernel sums them into fcc before the attempts
+static bool sum_in_attempt(abm_ctx* c) { return c->p.pair_sum != 2; }
+
+// the loop's pair pass: the shares, plus their per-cell sums unless the first attempt makes them
+static void enqueue_loop_pair_force(abm_ctx* c) { enqueue_pair_force(c, sum_in_attempt(c) ? 0 : 1); }
+
+// where the attempts of one iteration find the pair force
 static PairGather loop_gather(abm_ctx* c)
 {
     const bool f32 = c->p.precision == ABM_PRECISION_MIXED && c->dims == 3;
-    PairGather pg = {f32 ? 3 : 2, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
+    PairGather pg = {sum_in_attempt(c) ? (f32 ? 3 : 2) : 0, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
     return pg;
 }
 
@@ -606,7 +613,7 @@ static void enqueue_attempts(abm_ctx* c)
 
 static void enqueue_iteration(abm_ctx* c)
 {
-    enqueue_pair_force(c, 0);
+    enqueue_loop_pair_force(c);
     enqueue_propose(c);
     enqueue_attempts(c);
 }
@@ -712,7 +719,7 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
     }
     PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
-        enqueue_pair_force(c, 0);
+        enqueue_loop_pair_force(c);
         enqueue_propose(c);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg, c->dims);
@@ -1079,7 +1086,7 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     {
         cudaEvent_t* e = &ev[(size_t)k * 4];
         CK(cudaEventRecord(e[0], st));
-        enqueue_pair_force(c, 0);
+        enqueue_loop_pair_force(c);
         CK(cudaEventRecord(e[1], st));
         enqueue_propose(c);
         enqueue_attempts(c);

@@ -109,6 +109,9 @@ typedef struct abm_params {
     /* skin of the active pair list in um (0 = 0.3, negative = none): pairs farther than
      * 2R + skin at a refresh are skipped until the cells may have moved by half the skin */
     double pair_skin;
+    /* where each cell's pair shares are summed: 1 = inside the first RK attempt,
+     * 2 = a separate light kernel before it (0 = 1, the faster on B200) */
+    int pair_sum;
 } abm_params;
 
 typedef struct abm_stats {

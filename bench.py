@@ -311,7 +311,9 @@ def run_reference(args):
             "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded biofilm state)",
             "impl": "reference",
-            "config": config(args, info, {"cpu_model": model, "requested_steps": args.steps}),
+            "config": config(args, info, {"cpu_model": model, "requested_steps": args.steps,
+                                          "variant": "reference CPU path", "precision": "fp64",
+                                          "controller": "reference"}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

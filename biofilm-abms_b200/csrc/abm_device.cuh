@@ -38,6 +38,39 @@ __device__ __forceinline__ Geom load_geom(const Geom* __restrict__ g, int i)
     return o;
 }
 
+// Rigorous lower bound test on the distance of two segments: false only when the
+// gap between their projections on the single-precision closest-point direction a,
+//     a . (c_b - c_a) - h_a |a . n_a| - h_b |a . n_b|   (FP64),
+// exceeds limit + 1e-9.  For any unit a that gap bounds the distance from below,
+// and the reference's distance (CGAL's minimiser, or the near-parallel branch's
+// feasible pair of points) is never below the true minimum, so a pair that fails
+// the test is farther than `limit` in the reference too.
+__device__ __forceinline__ bool may_touch(const Geom& a, const Geom& b, double limit)
+{
+    const double wx = b.rx - a.rx, wy = b.ry - a.ry, wz = b.rz - a.rz;
+    // single-precision closest points (clamped, one refinement): only a direction
+    const float fwx = (float)wx, fwy = (float)wy, fwz = (float)wz;
+    const float ax = (float)a.nx, ay = (float)a.ny, az = (float)a.nz;
+    const float bx = (float)b.nx, by = (float)b.ny, bz = (float)b.nz;
+    const float ha = (float)a.h, hb = (float)b.h;
+    const float B = ax * bx + ay * by + az * bz;
+    const float D = ax * fwx + ay * fwy + az * fwz, E = bx * fwx + by * fwy + bz * fwz;
+    const float den = 1.f - B * B;
+    float s = den > 1e-6f ? (D - B * E) / den : 0.f;
+    s = fminf(fmaxf(s, -ha), ha);
+    float t = fminf(fmaxf(B * s - E, -hb), hb);
+    s = fminf(fmaxf(B * t + D, -ha), ha);
+    const double dx = wx + (double)t * b.nx - (double)s * a.nx;
+    const double dy = wy + (double)t * b.ny - (double)s * a.ny;
+    const double dz = wz + (double)t * b.nz - (double)s * a.nz;
+    const double dn = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(dn > 1e-6)) return true;
+    const double ux = dx / dn, uy = dy / dn, uz = dz / dn;
+    const double gap = (ux * wx + uy * wy + uz * wz) - a.h * fabs(ux * a.nx + uy * a.ny + uz * a.nz)
+                       - b.h * fabs(ux * b.nx + uy * b.ny + uz * b.nz);
+    return !(gap > limit + 1e-9);
+}
+
 // ---------------------------------------------------------------------------
 // Exact-rounding vector arithmetic.  The neighbor decision |d| < threshold
 // must come out identically on the GPU and in the CPU restatement, so the

@@ -798,31 +798,6 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
 // ---------------------------------------------------------------------------
 const int PS_T = 256, PS_TILE_MAX = 2048;
 
-__device__ __forceinline__ bool may_touch(const Geom& a, const Geom& b, double limit)
-{
-    const double wx = b.rx - a.rx, wy = b.ry - a.ry, wz = b.rz - a.rz;
-    // single-precision closest points (clamped, one refinement): only a direction
-    const float fwx = (float)wx, fwy = (float)wy, fwz = (float)wz;
-    const float ax = (float)a.nx, ay = (float)a.ny, az = (float)a.nz;
-    const float bx = (float)b.nx, by = (float)b.ny, bz = (float)b.nz;
-    const float ha = (float)a.h, hb = (float)b.h;
-    const float B = ax * bx + ay * by + az * bz;
-    const float D = ax * fwx + ay * fwy + az * fwz, E = bx * fwx + by * fwy + bz * fwz;
-    const float den = 1.f - B * B;
-    float s = den > 1e-6f ? (D - B * E) / den : 0.f;
-    s = fminf(fmaxf(s, -ha), ha);
-    float t = fminf(fmaxf(B * s - E, -hb), hb);
-    s = fminf(fmaxf(B * t + D, -ha), ha);
-    const double dx = wx + (double)t * b.nx - (double)s * a.nx;
-    const double dy = wy + (double)t * b.ny - (double)s * a.ny;
-    const double dz = wz + (double)t * b.nz - (double)s * a.nz;
-    const double dn = sqrt(dx * dx + dy * dy + dz * dz);
-    if (!(dn > 1e-6)) return true;
-    const double ux = dx / dn, uy = dy / dn, uz = dz / dn;
-    const double gap = (ux * wx + uy * wy + uz * wz) - a.h * fabs(ux * a.nx + uy * a.ny + uz * a.nz)
-                       - b.h * fabs(ux * b.nx + uy * b.ny + uz * b.nz);
-    return !(gap > limit + 1e-9);
-}
 
 // Phase 1: one thread per unordered pair (its lower entry k, listed in pair_k).
 // Few registers, so many warps hide the latency of the scattered loads.

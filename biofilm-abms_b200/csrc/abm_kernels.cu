@@ -378,89 +378,160 @@ void launch_scan(const int* in, const int* len, int* out, int* block_sums, int c
 }
 
 // ---------------------------------------------------------------------------
-// Pair build: one block per bin (grid-stride over bins).  Candidate cells of
-// the 27 surrounding bins are staged through shared memory in chunks; each
-// thread owns one cell of the bin and keeps the candidates that pass the
-// reference's two tests: centre distance < threshold + Ldiv + 2R and
-// segment distance < threshold (mechanics.hpp:548-577).  The segment distance
-// is always evaluated with the larger index as cell 1, as the reference's
-// j < i loop does, so both cells of a pair reach the same decision.
+// Pair build: one block per bin (grid-stride over bins), the bin's cells in
+// groups of up to PB_G.  The block's threads sweep the flattened (own cell,
+// candidate) products of the 27 surrounding bins with a cheap rejection test;
+// the survivors go to a per-warp queue and are evaluated 32 at a time, so the
+// exact FP64 distance runs on full warps instead of once per candidate for
+// whichever lane needs it.  A survivor is kept when it passes the reference's
+// two tests: centre distance < threshold + Ldiv + 2R and segment distance <
+// threshold (mechanics.hpp:548-577).  The segment distance is always evaluated
+// with the larger index as cell 1, as the reference's j < i loop does, so both
+// cells of a pair reach the same decision.  Rows are filled in any order
+// (shared-memory counters) and sorted by k_csr_fill.
+//
+// The rejection test is rigorous: every branch of dist_between_cells returns
+// points r1 + s n1, r2 + t n2 with |s| <= h1, |t| <= h2, so the computed |d|
+// is at least |r2 - r1| - h1 |n1| - h2 |n2| up to rounding (~1e-12 um at
+// these coordinates).  A candidate is dropped only when, in FP32 with a
+// 1e-4 um margin, |r2 - r1| > threshold + h1 max(1, |n1|^2) + h2 max(1, |n2|^2),
+// i.e. when its |d| is certainly >= threshold.
 // ---------------------------------------------------------------------------
-const int PB_T = 128, PB_CHUNK = 128;
+const int PB_T = 128, PB_G = 128, PB_WARPS = PB_T / 32, PB_SLICE = 1 << 20;
+
+struct PbShared {
+    double rx[PB_G], ry[PB_G], rz[PB_G];
+    float reach[PB_G];                  // h max(1, |n|^2)
+    int cnt[PB_G];
+    int q_own[PB_WARPS][64], q_pos[PB_WARPS][64];
+};
+
+__device__ __forceinline__ float pb_reach(double h, double nx, double ny, double nz)
+{
+    const float n2 = (float)(nx * nx + ny * ny + nz * nz);
+    return (float)h * fmaxf(1.f, n2 * 1.000001f);
+}
+
+// exact tests for one queued (own, candidate) product
+__device__ __forceinline__ void pb_exact(const Geom* __restrict__ sorted_geom, const int* __restrict__ sorted_cell,
+                                         int base, int own, int pos, const BuildParams& bp, PbShared& sh,
+                                         int* scratch)
+{
+    const Geom gm = sorted_geom[base + own], go = sorted_geom[pos];
+    const int cm = sorted_cell[base + own], o = sorted_cell[pos];
+    const Geom& gi = (cm > o) ? gm : go;
+    const Geom& gj = (cm > o) ? go : gm;
+    double cd = xnorm(xsub(x3(gi.rx, gi.ry, gi.rz), x3(gj.rx, gj.ry, gj.rz)));
+    if (!(cd < bp.prefilter)) return;
+    Dist d = dist_geom(gi, gj);
+    if (xnorm(x3(d.dx, d.dy, d.dz)) < bp.threshold)
+    {
+        const int slot = atomicAdd(&sh.cnt[own], 1);
+        if (slot < bp.cap_per_cell) scratch[(size_t)cm * bp.cap_per_cell + slot] = o;
+    }
+}
 
 __global__ void __launch_bounds__(PB_T) k_pair_build(const Grid* grid, const int* __restrict__ bin_start,
                                                     const int* __restrict__ sorted_cell,
                                                     const Geom* __restrict__ sorted_geom, const Ctrl* ctrl,
                                                     BuildParams bp, int* scratch, int* count)
 {
-    __shared__ Geom sg[PB_CHUNK];
-    __shared__ int sc[PB_CHUNK];
+    __shared__ PbShared sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     const Grid g = *grid;
     const int cap = bp.cap_per_cell;
+    const float thr = (float)bp.threshold + 1e-4f;
     for (int bin = blockIdx.x; bin < g.nbins; bin += gridDim.x)
     {
         const int s0 = bin_start[bin], s1 = bin_start[bin + 1];
         if (s0 == s1) continue;
         const int bx = bin % g.nx, by = (bin / g.nx) % g.ny, bz = bin / (g.nx * g.ny);
-        for (int base = s0; base < s1; base += PB_T)
+        for (int base = s0; base < s1; base += PB_G)
         {
-            const int my = base + threadIdx.x;
-            const bool act = my < s1;
-            Geom gm;
-            int cm = -1, cnt = 0;
-            if (act) { gm = sorted_geom[my]; cm = sorted_cell[my]; }
+            const int G = min(PB_G, s1 - base);
+            __syncthreads();                                   // the previous group is done with sh
+            for (int q = threadIdx.x; q < G; q += PB_T)
+            {
+                const Geom x = sorted_geom[base + q];
+                sh.rx[q] = x.rx; sh.ry[q] = x.ry; sh.rz[q] = x.rz;
+                sh.reach[q] = pb_reach(x.h, x.nx, x.ny, x.nz);
+                sh.cnt[q] = 0;
+            }
+            __syncthreads();
+            int qn = 0;                                        // this warp's queue length (warp-uniform)
             for (int dz = -1; dz <= 1; ++dz)
             {
-                int zz = bz + dz;
+                const int zz = bz + dz;
                 if (zz < 0 || zz >= g.nz) continue;
                 for (int dy = -1; dy <= 1; ++dy)
                 {
-                    int yy = by + dy;
+                    const int yy = by + dy;
                     if (yy < 0 || yy >= g.ny) continue;
                     for (int dx = -1; dx <= 1; ++dx)
                     {
-                        int xx = bx + dx;
+                        const int xx = bx + dx;
                         if (xx < 0 || xx >= g.nx) continue;
-                        int nbin = (zz * g.ny + yy) * g.nx + xx;
+                        const int nbin = (zz * g.ny + yy) * g.nx + xx;
                         if (nbin >= g.nbins) continue;
-                        const int c0 = bin_start[nbin], c1 = bin_start[nbin + 1];
-                        for (int ch = c0; ch < c1; ch += PB_CHUNK)
+                        const int nb0 = bin_start[nbin], nb1 = bin_start[nbin + 1];
+                        // candidates in slices of PB_SLICE so G * len stays far from INT_MAX
+                        for (int c0 = nb0; c0 < nb1; c0 += PB_SLICE)
                         {
-                            const int len = min(PB_CHUNK, c1 - ch);
-                            __syncthreads();
-                            for (int q = threadIdx.x; q < len; q += PB_T)
+                        const int total = G * min(PB_SLICE, nb1 - c0);
+                        // warps take consecutive 32-product slices; every lane of a
+                        // warp runs the same number of rounds
+                        for (int w0 = warp * 32; w0 < total; w0 += PB_T)
+                        {
+                            const int idx = w0 + lane;
+                            bool pass = false;
+                            int own = 0, pos = 0;
+                            if (idx < total)
                             {
-                                sg[q] = sorted_geom[ch + q];
-                                sc[q] = sorted_cell[ch + q];
-                            }
-                            __syncthreads();
-                            if (act)
-                            {
-                                for (int q = 0; q < len; ++q)
+                                own = idx % G;
+                                pos = c0 + idx / G;
+                                if (pos != base + own)
                                 {
-                                    const int o = sc[q];
-                                    if (o == cm) continue;
-                                    const Geom go = sg[q];
-                                    const Geom& gi = (cm > o) ? gm : go;
-                                    const Geom& gj = (cm > o) ? go : gm;
-                                    double cd = xnorm(xsub(x3(gi.rx, gi.ry, gi.rz), x3(gj.rx, gj.ry, gj.rz)));
-                                    if (!(cd < bp.prefilter)) continue;
-                                    Dist d = dist_geom(gi, gj);
-                                    if (xnorm(x3(d.dx, d.dy, d.dz)) < bp.threshold)
-                                    {
-                                        if (cnt < cap) scratch[(size_t)cm * cap + cnt] = o;
-                                        ++cnt;
-                                    }
+                                    const Geom& c = sorted_geom[pos];
+                                    const double cx = __ldg(&c.rx), cy = __ldg(&c.ry), cz = __ldg(&c.rz);
+                                    const float fx = (float)(cx - sh.rx[own]);
+                                    const float fy = (float)(cy - sh.ry[own]);
+                                    const float fz = (float)(cz - sh.rz[own]);
+                                    const float L = thr + sh.reach[own]
+                                                    + pb_reach(__ldg(&c.h), __ldg(&c.nx), __ldg(&c.ny), __ldg(&c.nz));
+                                    pass = !(fx * fx + fy * fy + fz * fz > L * L);
                                 }
                             }
+                            const unsigned m = __ballot_sync(0xffffffffu, pass);
+                            if (pass)
+                            {
+                                const int r = qn + __popc(m & lt);
+                                sh.q_own[warp][r] = own;
+                                sh.q_pos[warp][r] = pos;
+                            }
+                            qn += __popc(m);
+                            if (qn >= 32)
+                            {
+                                qn -= 32;
+                                __syncwarp();
+                                const int eo = sh.q_own[warp][qn + lane], ep = sh.q_pos[warp][qn + lane];
+                                __syncwarp();
+                                pb_exact(sorted_geom, sorted_cell, base, eo, ep, bp, sh, scratch);
+                            }
+                        }
                         }
                     }
                 }
             }
-            if (act)
+            __syncwarp();
+            if (lane < qn) pb_exact(sorted_geom, sorted_cell, base, sh.q_own[warp][lane], sh.q_pos[warp][lane], bp, sh,
+                                    scratch);
+            __syncthreads();                                   // every count of the group is final
+            for (int q = threadIdx.x; q < G; q += PB_T)
             {
+                int cnt = sh.cnt[q];
                 if (cnt > cap) { atomicOr((int*)&ctrl->status, (int)ST_NBR_OVERFLOW); cnt = cap; }
-                count[cm] = cnt;
+                count[sorted_cell[base + q]] = cnt;
             }
         }
     }

@@ -61,8 +61,13 @@ def parse_args(argv=None):
     ap.add_argument("--variant", default="chosen", choices=["chosen", "plain"],
                     help="headline configuration; the other one is timed beside it unless --only")
     ap.add_argument("--only", action="store_true", help="time the headline variant only")
-    ap.add_argument("--workload", default="3d", choices=["3d", "replicates"],
-                    help="3d: the 100k-cell headline; replicates: batched 2-D replicate biofilms")
+    ap.add_argument("--workload", default="3d", choices=["3d", "replicates", "growth"],
+                    help="3d: the 100k-cell headline; replicates: batched 2-D replicate biofilms; "
+                         "growth: 3-D growth from one founder cell, plain vs chosen")
+    ap.add_argument("--growth-target", type=int, default=200_000)
+    ap.add_argument("--growth-max-dt", type=float, default=1e-4, help="max_stepsize of the growth run (h)")
+    ap.add_argument("--growth-max-seconds", type=float, default=600.0,
+                    help="stop an arm of the growth run after this much device time")
     ap.add_argument("--replicates", type=int, default=256)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--tile", type=int, default=0, help="screened pair pass: CSR entries per block tile")
@@ -234,11 +239,6 @@ def attempt_bytes(n, final):
     return n * (224 + (120 if final else 0))
 
 
-def commit_bytes(n):
-    # candidate geometry 64 + velocity 48 read, state geometry 64 + velocity 48 + length 8 written
-    return n * (112 + 120)
-
-
 def load_traffic():
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(p):
@@ -366,8 +366,8 @@ def kernel_groups(sim, args, variant):
     pf_ms = prof["pair_force_ms"] / prof["pair_force_launches"]
     at_ms = prof["attempt_ms"] / prof["iterations"]
     if VARIANTS[variant]["controller"] == 1:
-        # network proposal + one RK attempt + commit of the accepted candidate
-        at_name, at_bytes = "k_attempt(proposal+commit)", attempt_bytes(args.n, True)
+        # network proposal + one RK attempt that advances the state in place
+        at_name, at_bytes = "k_attempt(proposal)", attempt_bytes(args.n, True)
     else:
         at_name, at_bytes = "k_attempt(trial+final)", attempt_bytes(args.n, False) + attempt_bytes(args.n, True)
     kernels = {"k_pair_screened": (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
@@ -391,12 +391,14 @@ def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
 
 
 def launches(variant, t):
-    # per iteration: the screened pair pass (screen + exact), the trial, its retries and
-    # the final attempt (an early exit after an accepted proposal), plus, with the
-    # learned controller, the network's proposal and the commit kernel; 18 kernels per
-    # neighbor rebuild
+    # per iteration: the screened pair pass (screen + exact) and the trial, then its
+    # retries; the reference controller adds the final attempt every iteration, the
+    # learned one adds the network's proposal and runs the final attempt only after
+    # a failed proposal (an IF node skips it otherwise); 18 kernels per neighbor rebuild
     learned = VARIANTS[variant]["controller"] == 1
-    return t["iterations"] * (4 + (2 if learned else 0)) + t["retries"] + 18 * t["rebuilds"]
+    per_iter = 4
+    extra = t["retries"] + (t["rejected"] if learned else 0)
+    return t["iterations"] * per_iter + extra + 18 * t["rebuilds"]
 
 
 def relerr(a, b):
@@ -590,12 +592,103 @@ def run_replicates(args):
         dist.destroy_process_group()
 
 
+def grow_arm(args, variant, weights, device, seed):
+    """One arm of the growth run: founder -> args.growth_target cells on the device."""
+    import torch
+    import abm_b200
+    from abm_b200 import stepsize, workloads
+    kw = dict(stepsize.GROWTH_KW, daughter_length_std=0.01)
+    target = args.growth_target
+    sim = abm_b200.Simulation(cap_cells=int(1.05 * target) + 4096, integration_mode=args.tableau,
+                              max_stepsize=args.growth_max_dt, max_error_allowed=1e-8, iter_update_neighbors=100,
+                              rng_seed=seed, **dict(kw, **VARIANTS[variant]))
+    try:
+        sim.upload_cells(workloads.founder_3d())
+        if VARIANTS[variant]["controller"] == 1:
+            sim.set_stepsize_weights(weights)
+        sim.set_parents([-1])
+        sim.set_clock(0.0, 1e-6, 0)          # dt0 = 1e-6 h
+        sim.set_cell_limit(target)
+        sim.get_cell_neighbors()
+        stream = torch.cuda.ExternalStream(sim.stream, device=device)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ms, chunk, error, n = 0.0, 512, None, 1
+        st = dict.fromkeys(("iterations", "attempts", "rejected", "retries", "divisions", "t", "cell_steps"), 0)
+        while True:
+            try:
+                st = sim.iterate(chunk)          # raises on a device-side error status
+            except RuntimeError as e:
+                error = str(e)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            n = sim.num_cells()
+            if error or n >= target or ms > 1000.0 * args.growth_max_seconds:
+                break
+    finally:
+        sim.close()
+    return {"cells": n, "reached_target": n >= target, "error": error, "device_s": ms / 1000.0,
+            "accepted_steps": st["iterations"], "rk_evals": st["attempts"],
+            "rk_evals_per_step": st["attempts"] / max(st["iterations"], 1),
+            "rejected_first_attempts": st["rejected"], "retries": st["retries"],
+            "divisions": st["divisions"], "simulated_h": st["t"], "cell_steps": st["cell_steps"],
+            "accepted_cell_steps_per_s": st["cell_steps"] / max(ms / 1000.0, 1e-9)}
+
+
+def run_growth(args):
+    """3-D growth from one founder cell to args.growth_target cells: growth rates
+    ~ N(1.5, 0.1^2)/h, division at Ldiv = 2 L0 + 2R = 5.6 um into daughters split at a
+    fraction ~ N(0.5, 0.01^2), Heun-Euler 2(1), RK tolerance 1e-8, dt0 = 1e-6 h, dt capped
+    at args.growth_max_dt; plain (FP64, reference controller) then chosen (mixed
+    precision, learned step size).  Each arm's device time runs from the founder to
+    the target (CUDA events on the context stream); the colony stops on the device when
+    it reaches the target."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        dist_init("nccl")
+    weights, weights_desc = stepsize_weights()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    arms = {v: grow_arm(args, v, weights, device, seed=7 + rank) for v in ("plain", "chosen")}
+    clocks = sampler.stop()
+    ms = {v: reduce_max(1000.0 * a["device_s"], device, world) for v, a in arms.items()}
+    ch = arms["chosen"]
+    value = world * ch["cell_steps"] / (ms["chosen"] / 1000.0)
+    line = {"metric": "3D growth founder -> %d cells: accepted cell-steps/s" % args.growth_target,
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": ch["accepted_steps"], "warmup": 0,
+            "ms_per_step": ms["chosen"] / max(ch["accepted_steps"], 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (one founder cell)",
+            "config": {"workload": "3d_growth_founder_to_%d_HE21_tol1e-8_maxdt%g" % (args.growth_target,
+                                                                                   args.growth_max_dt),
+                       "variant": "chosen", "parallelism": "replicas", "stepsize_network": weights_desc,
+                       "l2": "state larger than L2 after ~30k cells (no flush)"},
+            "arms": arms,
+            "chosen_over_plain": {"device_time": ms["plain"] / max(ms["chosen"], 1e-9),
+                                  "rk_evals": arms["plain"]["rk_evals"] / max(ch["rk_evals"], 1)},
+            "gpu_launches": None,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "replicates":
         run_replicates(args)
+    elif args.workload == "growth":
+        run_growth(args)
     else:
         run_b200(args)
 

@@ -99,7 +99,7 @@ DEFAULTS = dict(
     max_nxy_noise=0.0, max_nz_noise=0.0, cell_surface_coulomb_coeff=1.0, no_surface=0,
     growth_mean=0.0, growth_std=0.0, daughter_length_std=0.0, daughter_angle_xy_bound=0.0,
     daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
-    cap_neighbors_per_cell=64, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
+    cap_neighbors_per_cell=0, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
     dims=3, sigma0=100.0, adhesion_strength=0.0, adhesion_mindist=0.0, max_noise=0.0,
     pair_tile=0, pair_blocks_per_sm=0, pair_skin=0.0, pair_sum=0,
 )
@@ -534,8 +534,8 @@ class Batch:
 
 
 def autotune_pair_tile(cells, launches=20, jkr_table=None, gamma=100.0, **params):
-    """Time the screened pair pass on `cells` with tiles of 512, 1024, 2048 CSR entries
-    and 4, 8, 16 blocks per SM; returns ((tile, blocks_per_sm), {(tile, bpsm): ms})."""
+    """Time the screened pair pass on `cells` with at least 512, 1024, 2048 pairs per block
+    and at most 1, 2, 4 blocks per SM; returns ((tile, blocks_per_sm), {(tile, bpsm): ms})."""
     p, d = make_params(**params)
     a = np.asfortranarray(cells, dtype=np.float64)
     if p.cap_cells <= 0:
@@ -549,5 +549,5 @@ def autotune_pair_tile(cells, launches=20, jkr_table=None, gamma=100.0, **params
     _batch_check(LIB.abm_autotune_pair_tile(ctypes.byref(p), _dptr(a), a.shape[0], a.shape[1], a.shape[0],
                                             _dptr(jd), _dptr(jr), len(jd), launches, ctypes.byref(bt),
                                             ctypes.byref(bb), _fptr(ms)), "abm_autotune_pair_tile")
-    keys = [(t, g) for t in (512, 1024, 2048) for g in (4, 8, 16)]
+    keys = [(t, g) for t in (512, 1024, 2048) for g in (1, 2, 4)]
     return (bt.value, bb.value), dict(zip(keys, ms.tolist()))

@@ -92,6 +92,24 @@ def two_cell_3d(r1, n1, r2, n2, half_l=0.5, eta0=100.0, eta1=720.0, sigma0=100.0
     return cells
 
 
+def founder_3d(L0=2.0, R=0.8, E0=3900.0, sigma0=100.0, growth=1.5, eta0=100.0, eta1=720.0, gamma=100.0):
+    """One cell at the origin along (1, 0, 0) resting on the surface at the height
+    rz = R - (sigma0 sqrt(R) / (4 E0))^(2/3), with centreline length L0 and the mean
+    growth rate (the 3-D driver's start, abmConstAdhesion.cpp:414-431)."""
+    cells = np.zeros((1, NCOLS_3D), dtype=np.float64, order="F")
+    cells[0, 3] = R - (sigma0 * np.sqrt(R) / (4 * E0)) ** (2.0 / 3.0)
+    cells[0, 4] = 1.0
+    cells[0, 13] = L0
+    cells[0, 14] = L0 / 2
+    cells[0, 16] = growth
+    cells[0, 17] = eta0
+    cells[0, 18] = eta1
+    cells[0, 19] = sigma0
+    cells[0, 20] = 1
+    cells[0, 21] = gamma
+    return cells
+
+
 def biofilm_2d(n, seed=1, disk_radius=None, lmin=2.0, lmax=4.4, R=0.8, Rcell=0.5, eta0=100.0, eta1=100.0,
                growth=0.0, min_gap=None, p_contact=0.9, density=0.1):
     """A seeded 2-D colony in the 17-column layout of ABM-2d/ABM-2d-cpp/include/indices.hpp:

@@ -36,7 +36,7 @@ struct abm_ctx {
     int *bin_count = nullptr, *bin_start = nullptr, *key = nullptr, *slot = nullptr, *sorted_cell = nullptr;
     Geom* sorted_geom = nullptr;
     int *scratch = nullptr, *nbr_count = nullptr, *row_ptr = nullptr, *col = nullptr;
-    int *lower_end = nullptr, *rev = nullptr, *row_of = nullptr;
+    int *lower_end = nullptr, *rev = nullptr;
     int4* pairs = nullptr;                                           // screened pair pass
     int *pair_start = nullptr, *surv = nullptr;
     double4* jbuf = nullptr;
@@ -131,7 +131,7 @@ static void free_all(abm_ctx* c)
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
-                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->row_of, c->pairs, c->pair_start, c->surv, c->jbuf,
+                    c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->pairs, c->pair_start, c->surv, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part};
@@ -227,7 +227,9 @@ int abm_create(const abm_params* q, abm_ctx** out)
         c->err = "pair_lanes must be 4, 8, 16 or 32"; *out = c; return ABM_ERR_ARG;
     }
     c->cap = p.cap_cells;
-    c->cap_nbr = p.cap_neighbors_per_cell > 0 ? p.cap_neighbors_per_cell : 64;
+    // a compact 3-D colony reaches ~60 neighbors within the threshold (a 2-D monolayer ~30);
+    // the defaults leave room above that, and overflow is reported, never truncated silently
+    c->cap_nbr = p.cap_neighbors_per_cell > 0 ? p.cap_neighbors_per_cell : (p.dims == 2 ? 64 : 192);
     *out = c;
     CK(cudaGetDevice(&c->dev));
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev));
@@ -259,7 +261,6 @@ int abm_create(const abm_params* q, abm_ctx** out)
     CK(cudaMalloc(&c->col, cap * c->cap_nbr * sizeof(int)));
     CK(cudaMalloc(&c->lower_end, cap * sizeof(int)));
     CK(cudaMalloc(&c->rev, cap * c->cap_nbr * sizeof(int)));
-    CK(cudaMalloc(&c->row_of, cap * c->cap_nbr * sizeof(int)));
     CK(cudaMalloc(&c->pairs, cap * c->cap_nbr / 2 * sizeof(int4) + sizeof(int4)));
     CK(cudaMalloc(&c->surv, cap * c->cap_nbr / 2 * sizeof(int) + sizeof(int)));
     CK(cudaMalloc(&c->pair_start, (cap + 1) * sizeof(int)));
@@ -554,7 +555,7 @@ static void enqueue_rebuild(abm_ctx* c)
                       c->nbr_count, c->cap_bins, c->num_sms, st);
     launch_scan(c->nbr_count, &c->ctrl->n, c->row_ptr, c->scan_sums, c->cap, st);
     launch_csr_fill(c->ctrl, c->row_ptr, c->scratch, c->cap_nbr, c->col, c->ctrl, c->cap, st);
-    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st, c->row_of);
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, st);
     // pairs in the bin order of the sort just made (sorted_cell)
     launch_pair_list(c->ctrl, c->row_ptr, c->lower_end, c->col, c->rev, c->nbr_count, c->pair_start, c->scan_sums,
                      c->pairs, c->cap, st, c->sorted_cell);
@@ -570,7 +571,7 @@ static void enqueue_rebuild(abm_ctx* c)
 // per cell into fcc (the API paths; the loop's first attempt sums them itself)
 static void enqueue_pair_force(abm_ctx* c, int with_gather)
 {
-    launch_pair_screened(c->geom, c->row_ptr, c->lower_end, c->row_of, c->col, c->rev, c->ctrl, c->fp,
+    launch_pair_screened(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp,
                          c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf, c->p.precision == ABM_PRECISION_MIXED,
                          c->cap * c->cap_nbr, c->cap, c->num_sms, c->st, with_gather, c->dims, c->p.pair_tile,
                          c->p.pair_blocks_per_sm, c->pairs, c->surv);
@@ -608,7 +609,6 @@ static void enqueue_attempts(abm_ctx* c)
                        c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
-    if (c->sp.learned) launch_commit(c->geom, c->vel, c->phys, c->ctrl, c->sp, c->geom_c, c->vel_c, c->cap, st);
 }
 
 static void enqueue_iteration(abm_ctx* c)
@@ -697,13 +697,16 @@ static int add_conditional(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphN
 // One loop iteration as a graph with conditional nodes, appended to G after `deps`
 // (empty: root nodes); `deps` becomes the iteration's leaf set:
 //   [division count] -> IF(n_divide > 0){division + rebuild}
-//   -> pair force -> [proposal] -> trial -> WHILE(retry requested){retry} -> final
+//   -> pair force -> [proposal] -> trial -> WHILE(retry requested){retry}
+//   -> final (learned controller: IF(proposal failed){final})
 static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode_t>& deps)
 {
     // every handle must belong to a conditional node of this graph, or instantiation fails
-    cudaGraphConditionalHandle h_div = 0, h_retry = 0;
+    cudaGraphConditionalHandle h_div = 0, h_retry = 0, h_run = 0;
     const bool retries = c->p.max_tries_update_stepsize > 0;
+    const bool branch = c->sp.learned != 0;
     if (retries) CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
+    if (branch) CK(cudaGraphConditionalHandleCreate(&h_run, G, 0, cudaGraphCondAssignDefault));
     int rc;
     if (c->div_enabled)
     {
@@ -722,7 +725,8 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
         enqueue_loop_pair_force(c);
         enqueue_propose(c);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, retries ? 1 : 0, pg, c->dims);
+                       c->k0buf, 0.0, 0, c->cap, c->st, h_retry, (retries ? 1 : 0) | (branch ? 2 : 0), pg, c->dims,
+                       h_run);
     });
     if (rc) return rc;
     if (retries)
@@ -737,13 +741,17 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
         });
         if (rc) return rc;
     }
-    rc = capture_into(c, G, deps, [&]() {
+    auto final_attempt = [&]() {
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
-        if (c->sp.learned)
-            launch_commit(c->geom, c->vel, c->phys, c->ctrl, c->sp, c->geom_c, c->vel_c, c->cap, c->st);
-    });
-    return rc;
+    };
+    if (!branch) return capture_into(c, G, deps, final_attempt);
+    // a proposal that passed closed the step in the trial: skip the final launch
+    cudaGraph_t body;
+    rc = add_conditional(c, G, deps, h_run, cudaGraphCondTypeIf, &body);
+    if (rc) return rc;
+    std::vector<cudaGraphNode_t> bd;
+    return capture_into(c, body, bd, final_attempt);
 }
 
 static int build_iteration_graph(abm_ctx* c)
@@ -855,7 +863,7 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
     CK(cudaStreamSynchronize(c->st));
     h.n_dir = (int)cl.size();
     CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
-    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st, c->row_of);
+    launch_csr_rev(c->ctrl, c->row_ptr, c->col, c->lower_end, c->rev, c->cap, c->st);
     launch_pair_list(c->ctrl, c->row_ptr, c->lower_end, c->col, c->rev, c->nbr_count, c->pair_start, c->scan_sums,
                      c->pairs, c->cap, c->st);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
@@ -1406,7 +1414,7 @@ int abm_autotune_pair_tile(const abm_params* p, const double* cells, int n, int 
     if (rc == ABM_OK) rc = abm_upload_cells(c, cells, n, ncols, ld);
     int m = 0;
     if (rc == ABM_OK) rc = abm_build_neighbors(c, &m);
-    const int tiles[3] = {512, 1024, 2048}, grids[3] = {4, 8, 16};
+    const int tiles[3] = {512, 1024, 2048}, grids[3] = {1, 2, 4};
     float best = 0;
     *best_tile = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

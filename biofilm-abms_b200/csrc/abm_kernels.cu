@@ -546,32 +546,44 @@ void launch_pair_build(const Grid* grid, const int* bin_start, const int* sorted
                                                   scratch, count);
 }
 
-// CSR rows: copy the per-cell lists and sort each ascending (deterministic
-// order for the force reduction; the reference's table is i-major, j ascending).
-__global__ void k_csr_fill(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ scratch,
-                           int cap, int* col, Ctrl* ctrl_w)
+// CSR rows: copy each cell's list and sort it ascending (deterministic order for
+// the force reduction; the reference's table is i-major, j ascending).  One warp
+// per row: an entry's rank is the number of smaller entries in the row (entries
+// are distinct cell indices), counted with shuffles, and the entry lands at
+// row_ptr[i] + rank.
+const int CF_T = 256;
+
+__global__ void __launch_bounds__(CF_T) k_csr_fill(const Ctrl* ctrl, const int* __restrict__ row_ptr,
+                                                  const int* __restrict__ scratch, int cap, int* col, Ctrl* ctrl_w)
 {
     const int n = ctrl->n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (CF_T / 32);
+    for (int i = (blockIdx.x * CF_T + threadIdx.x) >> 5; i < n; i += nwarps)
     {
-        const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
+        const int r0 = row_ptr[i], len = row_ptr[i + 1] - r0;
         const int* src = scratch + (size_t)i * cap;
-        for (int k = 0; k < r1 - r0; ++k)
+        for (int a = 0; a < len; a += 32)
         {
-            int v = src[k];
-            int j = r0 + k - 1;
-            while (j >= r0 && col[j] > v) { col[j + 1] = col[j]; --j; }
-            col[j + 1] = v;
+            const int v = (a + lane < len) ? src[a + lane] : INT_MAX;
+            int rank = 0;
+            for (int b = 0; b < len; b += 32)
+            {
+                const int w = (b + lane < len) ? src[b + lane] : INT_MAX;
+#pragma unroll 8
+                for (int q = 0; q < 32; ++q) rank += (__shfl_sync(0xffffffffu, w, q) < v) ? 1 : 0;
+            }
+            if (a + lane < len) col[r0 + rank] = v;
         }
-        if (i == n - 1) ctrl_w->n_dir = r1;
+        if (i == n - 1 && lane == 0) ctrl_w->n_dir = r0 + len;
     }
     if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) ctrl_w->n_dir = 0;
 }
 
-void launch_csr_fill(const Ctrl* ctrl, const int* row_ptr, const int* scratch, int cap_per_cell,
-                     int* col, Ctrl* ctrl_w, int cap_cells, cudaStream_t st)
+void launch_csr_fill(const Ctrl* ctrl, const int* row_ptr, const int* scratch, int cap, int* col, Ctrl* ctrl_w,
+                     int cap_cells, cudaStream_t st)
 {
-    k_csr_fill<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, scratch, cap_per_cell, col, ctrl_w);
+    k_csr_fill<<<max(cdiv(cap_cells, CF_T / 32), 1), CF_T, 0, st>>>(ctrl, row_ptr, scratch, cap, col, ctrl_w);
 }
 
 // ---------------------------------------------------------------------------
@@ -822,56 +834,57 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_en
 
 // Reverse slots and the end of the lower part of each sorted CSR row: for an
 // entry (i, j) with j < i, rev = position of i in row j.
-__global__ void k_csr_rev(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ col,
-                          int* lower_end, int* rev, int* row_of)
+// Reverse indices and the lower part of each row, one warp per row: lower_end[i]
+// is the first entry with j >= i (rows are sorted), and every lower entry (i, j)
+// finds the position of i in row j by binary search.
+__global__ void __launch_bounds__(CF_T) k_csr_rev(const Ctrl* ctrl, const int* __restrict__ row_ptr,
+                                                 const int* __restrict__ col, int* lower_end, int* rev)
 {
     const int n = ctrl->n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (CF_T / 32);
+    for (int i = (blockIdx.x * CF_T + threadIdx.x) >> 5; i < n; i += nwarps)
     {
         const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
-        if (row_of)
-            for (int k = r0; k < r1; ++k) row_of[k] = i;
-        int lo = r0, hi = r1;
-        while (lo < hi) { int mid = (lo + hi) >> 1; if (col[mid] < i) lo = mid + 1; else hi = mid; }
-        lower_end[i] = lo;
-        for (int k = r0; k < lo; ++k)
+        int lower = 0;
+        for (int k0 = r0; k0 < r1; k0 += 32)
         {
-            const int j = col[k];
-            int a = row_ptr[j], b = row_ptr[j + 1];
-            while (a < b) { int mid = (a + b) >> 1; if (col[mid] < i) a = mid + 1; else b = mid; }
-            rev[k] = a;
+            const int k = k0 + lane;
+            const int j = k < r1 ? col[k] : INT_MAX;
+            const bool lo = j < i;
+            lower += __popc(__ballot_sync(0xffffffffu, lo));
+            if (lo)
+            {
+                int a = row_ptr[j], b = row_ptr[j + 1];
+                while (a < b) { const int mid = (a + b) >> 1; if (col[mid] < i) a = mid + 1; else b = mid; }
+                rev[k] = a;
+            }
         }
+        if (lane == 0) lower_end[i] = r0 + lower;
     }
 }
 
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
-                    int cap_cells, cudaStream_t st, int* row_of)
+                    int cap_cells, cudaStream_t st)
 {
-    k_csr_rev<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(ctrl, row_ptr, col, lower_end, rev, row_of);
+    k_csr_rev<<<max(cdiv(cap_cells, CF_T / 32), 1), CF_T, 0, st>>>(ctrl, row_ptr, col, lower_end, rev);
 }
 
 // ---------------------------------------------------------------------------
-// Screened pair pass.  Phase 1 (k_pair_screen) visits each unordered pair once
-// (from its lower entry, larger index as cell 1; pair_k lists them) and tests a
-// lower bound on the centreline distance: for any unit
-// vector a, the gap between the projections of the two segments on a,
+// Screened pair pass over the pair records (one per unordered pair: cell i, its
+// partner j < i, the lower CSR entry k and the partner's entry rev[k]; the larger
+// index is cell 1, as in the reference's j < i loop).  The screen is a lower
+// bound on the centreline distance: for any unit vector a, the gap between the
+// projections of the two segments on a,
 //     a . (c_j - c_i) - h_i |a . n_i| - h_j |a . n_j|,
 // bounds their distance from below.  a is the closest-point direction of a
 // single-precision estimate, so the bound is nearly tight, and it is evaluated
-// in FP64, so it is rigorous: a pair whose bound exceeds 2R (+1e-9) cannot
-// overlap and contributes exactly zero in every force law of the reference
-// (all need overlap > 0).  Its two slots are zeroed; the others are appended to a
-// survivor list.  Phase 2 (k_pair_exact) runs the exact pair force on the
-// survivors with every lane busy and writes the pair's two shares: (v, s) into
-// the lower entry and (v, t) into the partner's entry (rev).  Every slot is
-// written by exactly one pair, so the order of the survivor list changes no
-// result.  The first attempt sums a cell's whole row in CSR order.
+// in FP64, so it is rigorous (may_touch).  The exact pair force writes the pair's
+// two shares: (v, s) into the lower entry and (v, t) into the partner's entry.
+// The first attempt sums a cell's whole row in CSR order.
 // ---------------------------------------------------------------------------
 const int PS_T = 256, PS_TILE_MAX = 2048;
 
-
-// Phase 1: one thread per unordered pair (its lower entry k, listed in pair_k).
-// Few registers, so many warps hide the latency of the scattered loads.
 template <bool MIXED>
 __device__ __forceinline__ void zero_shares(double4* jbuf, int k, int r)
 {
@@ -888,99 +901,110 @@ __device__ __forceinline__ void zero_shares(double4* jbuf, int k, int r)
     }
 }
 
-// Refresh of the active list, when it is stale: after a rebuild, an upload or a
-// division, or once the cells may have moved by half the skin since the last
-// refresh (2 * drift >= skin).  Otherwise the kernel returns at once.  A pair
-// whose bound exceeds 2R + skin stays inactive (its shares are zeroed here and
-// stay zero) until the next refresh: in the meantime its distance can fall by at
-// most 2 * drift < skin, so it still exceeds 2R and its force is exactly zero.
-template <bool MIXED>
-__global__ void __launch_bounds__(PS_T) k_pair_screen(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
-                                                     Ctrl* ctrl, double R, double skin, double4* __restrict__ jbuf,
-                                                     int* __restrict__ surv)
+// One pass per iteration over the pair records.  A refresh iteration (the active
+// list is stale: after a rebuild, an upload or a division, or once the cells may
+// have moved by half the skin since the last refresh, 2 * drift >= skin) screens
+// every pair with the rigorous bound of may_touch, zeroes the shares of the pairs
+// beyond 2R + skin, computes the others and lists them as the new active pairs;
+// the other iterations compute the active pairs only.  A pair left out stays
+// beyond 2R until the next refresh (its distance can fall by at most
+// 2 * drift < skin), so its force is exactly zero in every force law of the
+// reference (all need overlap > 0).  Every share slot is written by exactly one
+// pair, so the order of the active list changes no result.  The last block
+// installs a new list and clears the drift.
+template <bool MIXED, int DIM>
+__device__ __forceinline__ void pair_shares(const Geom& gi, const Geom& gj, const int4& pr, const ForceParams& fp,
+                                            const double* __restrict__ td, const double* __restrict__ tr,
+                                            double4* __restrict__ jbuf, double& ovl_max)
 {
-    if (ctrl->halted) return;
-    if (ctrl->screen_valid && 2.0 * ctrl->drift * (1.0 + 1e-6) + 1e-9 < skin) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->refreshing = 1;
-    const int n_pairs = ctrl->n_dir >> 1;
-    const double limit = 2 * R + skin;
-    const int lane = threadIdx.x & 31;
-    // warp-uniform rounds, so that every ballot covers all 32 lanes
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n_pairs; base += stride)
+    const int k = pr.z, r = pr.w;
+    PairOut p;
+    if (DIM == 2) p = pair_force_2d(gi, gj, fp, fp.adhere[k] != 0);
+    else p = MIXED ? pair_force_fp32(gi, gj, fp, td, tr) : pair_force_fp64(gi, gj, fp, td, tr);
+    if (MIXED)
     {
-        const int p = base + lane;
-        bool keep = false;
-        if (p < n_pairs)
+        // mixed precision: the shares are single-precision forces, stored as such
+        float4* fb = reinterpret_cast<float4*>(jbuf);
+        float4 own = make_float4(0.f, 0.f, 0.f, 0.f), other = own;
+        if (p.touch)
         {
-            const int4 pr = pairs[p];             // (i, j, lower entry k, partner entry)
-            keep = may_touch(load_geom(geom, pr.x), load_geom(geom, pr.y), limit);
-            if (!keep) zero_shares<MIXED>(jbuf, pr.z, pr.w);
+            own = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.s);
+            other = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.t);
+            ovl_max = fmax(ovl_max, p.ovl);
         }
-        // warp-aggregated append of the active pairs
-        const unsigned mask = __ballot_sync(0xffffffffu, keep);
-        int pos = 0;
-        if (lane == 0 && mask) pos = atomicAdd(&ctrl->n_surv_next, __popc(mask));
-        pos = __shfl_sync(0xffffffffu, pos, 0);
-        if (keep) surv[pos + __popc(mask & ((1u << lane) - 1u))] = p;
+        fb[k] = own;
+        fb[r] = other;
+    }
+    else
+    {
+        double4 own = make_double4(0.0, 0.0, 0.0, 0.0), other = own;
+        if (p.touch)
+        {
+            own = make_double4(p.vx, p.vy, p.vz, p.s);
+            other = make_double4(p.vx, p.vy, p.vz, p.t);
+            ovl_max = fmax(ovl_max, p.ovl);
+        }
+        jbuf[k] = own;
+        jbuf[r] = other;
     }
 }
 
-// Phase 2: the exact pair force of every active pair, its two shares into jbuf;
-// after a refresh the last block installs the new list and clears the drift.
 template <bool MIXED, int DIM>
-__global__ void __launch_bounds__(PS_T) k_pair_exact(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
-                                                    Ctrl* ctrl, ForceParams fp, const double* __restrict__ jkr_delta,
-                                                    const double* __restrict__ jkr_radius,
-                                                    double4* __restrict__ jbuf, const int* __restrict__ surv)
+__global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
+                                                   Ctrl* ctrl, ForceParams fp, const double* __restrict__ td,
+                                                   const double* __restrict__ tr, double4* __restrict__ jbuf,
+                                                   int* __restrict__ surv)
 {
-    __shared__ double td[JKR_MAX], tr[JKR_MAX];
     __shared__ bool last;
     if (ctrl->halted) return;
-    for (int k = threadIdx.x; k < fp.jkr_n; k += blockDim.x) { td[k] = jkr_delta[k]; tr[k] = jkr_radius[k]; }
-    __syncthreads();
-    const bool refreshed = ctrl->refreshing != 0;
-    const int m = refreshed ? ctrl->n_surv_next : ctrl->n_surv;
+    const bool refresh = !ctrl->screen_valid || !(2.0 * ctrl->drift * (1.0 + 1e-6) + 1e-9 < fp.skin);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
     double ovl_max = 0.0;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    if (refresh)
     {
-        const int4 pr = pairs[surv[q]];
-        const int k = pr.z, r = pr.w;
-        const Geom gi = load_geom(geom, pr.x), gj = load_geom(geom, pr.y);
-        PairOut p;
-        if (DIM == 2) p = pair_force_2d(gi, gj, fp, fp.adhere[k] != 0);
-        else p = MIXED ? pair_force_fp32(gi, gj, fp, td, tr) : pair_force_fp64(gi, gj, fp, td, tr);
-        if (MIXED)
+        const int n_pairs = ctrl->n_dir >> 1;
+        const double limit = 2 * fp.R + fp.skin;
+        // warp-uniform rounds, so that every ballot covers all 32 lanes
+        for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n_pairs; base += stride)
         {
-            // mixed precision: the shares are single-precision forces, stored as such
-            float4* fb = reinterpret_cast<float4*>(jbuf);
-            float4 own = make_float4(0.f, 0.f, 0.f, 0.f), other = own;
-            if (p.touch)
+            const int p = base + lane;
+            bool keep = false;
+            int4 pr = make_int4(0, 0, 0, 0);
+            Geom gi, gj;
+            if (p < n_pairs)
             {
-                own = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.s);
-                other = make_float4((float)p.vx, (float)p.vy, (float)p.vz, (float)p.t);
-                ovl_max = fmax(ovl_max, p.ovl);
+                pr = pairs[p];                      // (i, j, lower entry k, partner entry)
+                gi = load_geom(geom, pr.x);
+                gj = load_geom(geom, pr.y);
+                keep = may_touch(gi, gj, limit);
+                if (!keep) zero_shares<MIXED>(jbuf, pr.z, pr.w);
             }
-            fb[k] = own;
-            fb[r] = other;
+            // warp-aggregated append of the active pairs
+            const unsigned mask = __ballot_sync(0xffffffffu, keep);
+            int pos = 0;
+            if (lane == 0 && mask) pos = atomicAdd(&ctrl->n_surv_next, __popc(mask));
+            pos = __shfl_sync(0xffffffffu, pos, 0);
+            if (keep)
+            {
+                surv[pos + __popc(mask & ((1u << lane) - 1u))] = p;
+                pair_shares<MIXED, DIM>(gi, gj, pr, fp, td, tr, jbuf, ovl_max);
+            }
         }
-        else
+    }
+    else
+    {
+        const int m = ctrl->n_surv;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride)
         {
-            double4 own = make_double4(0.0, 0.0, 0.0, 0.0), other = own;
-            if (p.touch)
-            {
-                own = make_double4(p.vx, p.vy, p.vz, p.s);
-                other = make_double4(p.vx, p.vy, p.vz, p.t);
-                ovl_max = fmax(ovl_max, p.ovl);
-            }
-            jbuf[k] = own;
-            jbuf[r] = other;
+            const int4 pr = pairs[surv[q]];
+            pair_shares<MIXED, DIM>(load_geom(geom, pr.x), load_geom(geom, pr.y), pr, fp, td, tr, jbuf, ovl_max);
         }
     }
     if (fp.stats)
     {
         ovl_max = warp_max(ovl_max);
-        if ((threadIdx.x & 31) == 0 && ovl_max > 0)
+        if (lane == 0 && ovl_max > 0)
             atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
     }
     __syncthreads();
@@ -992,11 +1016,11 @@ __global__ void __launch_bounds__(PS_T) k_pair_exact(const Geom* __restrict__ ge
     __syncthreads();
     if (last && threadIdx.x == 0)
     {
-        if (refreshed)
+        if (refresh)
         {
-            ctrl->n_surv = ctrl->n_surv_next;
+            __threadfence();
+            ctrl->n_surv = atomicAdd(&ctrl->n_surv_next, 0);
             ctrl->n_surv_next = 0;
-            ctrl->refreshing = 0;
             ctrl->screen_valid = 1;
             ctrl->drift = 0.0;
         }
@@ -1050,26 +1074,35 @@ void launch_pair_list(const Ctrl* ctrl, const int* row_ptr, const int* lower_end
 __global__ void k_pair_sum_rows(const int* __restrict__ row_ptr, const int* __restrict__ lower_end, const Ctrl* ctrl,
                                 const double4* __restrict__ jbuf, Gen6* fcc, int f32);
 
-void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* row_of,
-                          const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
+void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col,
+                          const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
                           int blocks_per_sm, const int4* pairs, int* surv)
 {
-    // tile: pairs per screening block over the capacity (sets the screening grid);
-    // blocks_per_sm: resident blocks per SM of the exact pass's grid
+    // grid: at least `tile` pairs per block, at most the blocks that are resident at
+    // once (blocks_per_sm caps them per SM); the blocks stride over the pairs
     tile = tile <= 0 ? 1024 : min(tile, PS_TILE_MAX);
-    blocks_per_sm = blocks_per_sm <= 0 ? 8 : blocks_per_sm;
     const int max_pairs = max(max_entries / 2, 1);
-    const int b1 = max(1, min(cdiv(max_pairs, tile), num_sms * 32));
-    const int b2 = max(1, min(cdiv(max_pairs, PS_T), num_sms * blocks_per_sm));
     const bool f32 = mixed && dims != 2;
-    if (f32) k_pair_screen<true><<<b1, PS_T, 0, st>>>(geom, pairs, ctrl, fp.R, fp.skin, jbuf, surv);
-    else k_pair_screen<false><<<b1, PS_T, 0, st>>>(geom, pairs, ctrl, fp.R, fp.skin, jbuf, surv);
+    auto grid = [&](const void* fn, int& occ_cache) {
+        if (occ_cache == 0)
+        {
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, PS_T, 0);
+            occ_cache = max(occ, 1);
+        }
+        const int per_sm = blocks_per_sm > 0 ? min(blocks_per_sm, occ_cache) : occ_cache;
+        return max(1, min(cdiv(max_pairs, tile), num_sms * per_sm));
+    };
+    static int occ2 = 0, occ3m = 0, occ3 = 0;
 #define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv
-    if (dims == 2) k_pair_exact<false, 2><<<b2, PS_T, 0, st>>>(PX_ARGS);
-    else if (mixed) k_pair_exact<true, 3><<<b2, PS_T, 0, st>>>(PX_ARGS);
-    else k_pair_exact<false, 3><<<b2, PS_T, 0, st>>>(PX_ARGS);
+    if (dims == 2)
+        k_pair_pass<false, 2><<<grid((const void*)k_pair_pass<false, 2>, occ2), PS_T, 0, st>>>(PX_ARGS);
+    else if (f32)
+        k_pair_pass<true, 3><<<grid((const void*)k_pair_pass<true, 3>, occ3m), PS_T, 0, st>>>(PX_ARGS);
+    else
+        k_pair_pass<false, 3><<<grid((const void*)k_pair_pass<false, 3>, occ3), PS_T, 0, st>>>(PX_ARGS);
 #undef PX_ARGS
     if (with_sum)
         k_pair_sum_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc, f32);
@@ -1373,11 +1406,19 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
 // Without noise the stage-0 velocity k0 = f(y0) is the same for every attempt of an
 // iteration (y0 and the pair forces do not change), so the trial stores it in k0buf
 // and the retries and the final attempt read it back.
+// Learned controller: the trial (the network's proposal) writes its state in place
+// and first copies y0 (with l in the gamma slot) and the stored velocity to
+// geom_c / vel_c; a proposal that passes the error test closes the step in the
+// trial's last block, one that fails continues with retries and a final attempt
+// that read y0 back from that copy.
+// use_cond bit 0: `cond` is the retry WHILE node's handle; bit 1: `cond_run` is the
+// handle of the IF node around the final attempt (0 after a committed proposal).
 template <int S, int KIND, bool NOISE, int DIM>
 __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
-                                                 unsigned long long cond, int use_cond, PairGather pg)
+                                                 unsigned long long cond, int use_cond, PairGather pg,
+                                                 unsigned long long cond_run)
 {
     __shared__ double sh_max[AT_T / 32], sh_drift[AT_T / 32];
     __shared__ double4 sh_stat[AT_T / 32];
@@ -1385,8 +1426,10 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     if (KIND != 3 && ctrl->halted)
     {
         // a halted context takes no step: stop an enclosing WHILE node
-        if (use_cond && (KIND == MODE_TRIAL || KIND == MODE_RETRY) && blockIdx.x == 0 && threadIdx.x == 0)
+        if ((use_cond & 1) && (KIND == MODE_TRIAL || KIND == MODE_RETRY) && blockIdx.x == 0 && threadIdx.x == 0)
             cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
+        if ((use_cond & 2) && KIND == MODE_TRIAL && blockIdx.x == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond_run, 0u);
         return;
     }
     const int n = ctrl->n;
@@ -1410,7 +1453,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         if (mode != MODE_RETRY)
         {
             // no retry pending: make sure an enclosing WHILE node stops
-            if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
+            if ((use_cond & 1) && blockIdx.x == 0 && threadIdx.x == 0)
                 cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
             return;
         }
@@ -1423,11 +1466,13 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         load_k0 = share_k0 && trial_ran;
     }
     else { dt = eval_dt; attempt = eval_attempt; }
-    // an accepted proposal is committed by k_commit, which follows this kernel
+    // the step was closed by a proposal that passed the error test
     if (KIND == MODE_FINAL && mode == MODE_COMMIT) return;
     const bool commit = false;
-    // the learned trial writes its candidate state for a commit
-    const bool write_candidate = (KIND == MODE_TRIAL) && sp.learned;
+    // the learned trial advances the state in place; the attempts after a failed
+    // proposal start from the copy of y0 it kept
+    const bool in_place = (KIND == MODE_TRIAL) && sp.learned;
+    const bool from_backup = (KIND == MODE_RETRY || KIND == MODE_FINAL) && sp.learned;
 
     // the first attempt of an iteration completes the pair force (k_pair_force left
     // only the lower-neighbor share); under the reference controller the trial writes
@@ -1439,11 +1484,22 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
     double local_drift = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    // one cell per thread: the grid covers the capacity (attempt_blocks)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
     {
-        const Geom g = load_geom(geom, i);
+        const Geom g = load_geom(from_backup ? geom_c : geom, i);
+        const Vel* vprev = (from_backup ? vel_c : vel) + i;
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
-        const double l = phys[i].l, eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
+        const double l = from_backup ? g.gamma : phys[i].l;
+        const double eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
+        if (in_place)
+        {
+            Geom b = g;
+            b.gamma = l;
+            geom_c[i] = b;
+            vel_c[i] = vel[i];
+        }
         const bool a2 = y0[5] < sp.mp.nz_threshold;
         Gen6 cc;
         if (do_gather)
@@ -1471,7 +1527,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         else
         {
             if constexpr (DIM == 2) velocity_2d(sp, y0, l, eta0, eta1, cc, nz2, k[0]);
-            else cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[0]);
+            else cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vprev, f0, k[0]);
             if (store_k0)
             {
                 double2* kp = reinterpret_cast<double2*>(k0buf + i);
@@ -1494,7 +1550,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             }
             normalize_n(y);
             if constexpr (DIM == 2) velocity_2d(sp, y, l, eta0, eta1, cc, nz2, k[st]);
-            else cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vel + i, f0, k[st]);
+            else cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, f0, k[st]);
         }
         double vf1[6], d1[6];
 #pragma unroll
@@ -1511,7 +1567,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             local_max = fmax(local_max, scaled);
             if (KIND == 3 && err_out) err_out[i].f[c] = err;
         }
-        if (KIND == MODE_FINAL || KIND == 3 || write_candidate)
+        if (KIND == MODE_FINAL || KIND == 3 || in_place)
         {
             double y1[6];
 #pragma unroll
@@ -1522,7 +1578,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             Vel vo;
 #pragma unroll
             for (int c = 0; c < 6; ++c) vo.v[c] = vf1[c];
-            if (KIND == MODE_FINAL || write_candidate)
+            if (KIND == MODE_FINAL || in_place)
             {
                 // growCells (growth.hpp:51-57) fused with the accepted step
                 const double g_rate = phys[i].growth;
@@ -1535,24 +1591,17 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
                                                         + go.h * sqrt(bx * bx + by * by + bz * bz)
                                                         + fabs(go.h - g.h));
                 }
-                if (KIND == MODE_FINAL)
+                if (from_backup) go.gamma = geom[i].gamma;   // the copy holds l in that slot
+                phys[i].l = lg;
+                geom[i] = go;
+                vel[i] = vo;
+                if (sp.stats_on)
                 {
-                    phys[i].l = lg;
-                    geom[i] = go;
-                    vel[i] = vo;
-                    if (sp.stats_on)
-                    {
-                        const double v2 = vf1[0] * vf1[0] + vf1[1] * vf1[1] + vf1[2] * vf1[2];
-                        st_vmax = fmax(st_vmax, sqrt(v2));
-                        st_v2 += v2;
-                        st_g += g_rate;
-                        st_near += (lg > sp.near_div_length) ? 1.0 : 0.0;
-                    }
-                }
-                else
-                {
-                    geom_c[i] = go;
-                    vel_c[i] = vo;
+                    const double v2 = vf1[0] * vf1[0] + vf1[1] * vf1[1] + vf1[2] * vf1[2];
+                    st_vmax = fmax(st_vmax, sqrt(v2));
+                    st_v2 += v2;
+                    st_g += g_rate;
+                    st_near += (lg > sp.near_div_length) ? 1.0 : 0.0;
                 }
             }
             else
@@ -1562,7 +1611,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             }
         }
     }
-    if (KIND == MODE_FINAL && sp.stats_on)
+    if ((KIND == MODE_FINAL || in_place) && sp.stats_on)
     {
         // per-block partials of the step-size features, summed in block order later
         st_vmax = warp_max(st_vmax);
@@ -1587,7 +1636,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             sp.stat_part[blockIdx.x] = a;
         }
     }
-    if (KIND == MODE_FINAL || write_candidate)
+    if (KIND == MODE_FINAL || in_place)
     {
         local_drift = warp_max(local_drift);
         if ((threadIdx.x & 31) == 0) sh_drift[threadIdx.x >> 5] = local_drift;
@@ -1604,7 +1653,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         for (int w = 1; w < AT_T / 32; ++w) m = fmax(m, sh_max[w]);
         unsigned long long bits = (unsigned long long)__double_as_longlong(m);
         if (bad) atomicOr(&ctrl->status, (int)ST_NAN);
-        if (KIND == MODE_FINAL || write_candidate)
+        if (KIND == MODE_FINAL || in_place)
         {
             double dm = sh_drift[0];
             for (int w = 1; w < AT_T / 32; ++w) dm = fmax(dm, sh_drift[w]);
@@ -1620,9 +1669,10 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         }
     }
     __syncthreads();
-    if (KIND == MODE_FINAL && sp.stats_on && last)
+    if ((KIND == MODE_FINAL || in_place) && sp.stats_on && last)
     {
-        // step-size features of the accepted step: every block's partial, in block order
+        // step-size features of the accepted step (a failed proposal's are replaced
+        // by the final attempt's): every block's partial, in block order
         __threadfence();
         double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
         for (int b = threadIdx.x; b < gridDim.x; b += AT_T)
@@ -1662,18 +1712,27 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         double E = __longlong_as_double((long long)atomicAdd(&ctrl->err_bits, 0ull));
         E = fmax(E, sp.min_error);
         if (commit) E = ctrl->last_trial_error;
-        // motion of the new state: counted now for a final step, at the commit for a proposal
+        // motion of the new state, counted once the step is accepted
         const double dm = __longlong_as_double((long long)atomicAdd(&ctrl->drift_bits, 0ull));
         if (KIND == MODE_FINAL) ctrl->drift += dm;
-        else if (write_candidate) ctrl->drift_cand = dm;
         ctrl->drift_bits = 0ull;
         ctrl->err_bits = 0ull;
         ctrl->blocks_done = 0u;
         controller_finish(ctrl, sp, KIND, E, commit);
+        if (in_place && ctrl->mode == MODE_COMMIT)
+        {
+            // the proposal passed: its state is in place; close the step and leave
+            // MODE_COMMIT so that this iteration's final attempt exits at once
+            ctrl->drift += dm;
+            controller_finish(ctrl, sp, MODE_FINAL, E, true);
+            ctrl->mode = MODE_COMMIT;
+        }
         // another retry?  (bounded: the controller schedules at most max_tries of them)
-        if (use_cond && (KIND == MODE_TRIAL || KIND == MODE_RETRY))
+        if ((use_cond & 1) && (KIND == MODE_TRIAL || KIND == MODE_RETRY))
             cudaGraphSetConditional((cudaGraphConditionalHandle)cond,
                                     (ctrl->mode == MODE_RETRY && ctrl->tries < sp.max_tries) ? 1u : 0u);
+        if ((use_cond & 2) && KIND == MODE_TRIAL)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond_run, ctrl->mode != MODE_COMMIT ? 1u : 0u);
     }
 }
 
@@ -1681,9 +1740,9 @@ template <int S, bool NOISE, int DIM>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
                              Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
-                             unsigned long long cond, int use_cond, PairGather pg)
+                             unsigned long long cond, int use_cond, PairGather pg, unsigned long long cond_run)
 {
-#define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg
+#define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg, cond_run
     switch (kind)
     {
         case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
@@ -1696,115 +1755,15 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 
 int attempt_blocks(int cap_cells) { return max(cdiv(cap_cells, AT_T), 1); }
 
-// Commit of an accepted proposal (learned controller): candidate -> state, growth
-// already applied by the proposal; per-block feature partials for the next
-// proposal; the last block sums them in block order and closes the step.  A light
-// kernel (copies and sums only), so it runs at full occupancy.  Returns at once
-// when the iteration has no accepted proposal.
-__global__ void __launch_bounds__(AT_T) k_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, StepParams sp,
-                                                 const Geom* __restrict__ geom_c, const Vel* __restrict__ vel_c)
-{
-    __shared__ double4 sh[AT_T / 32];
-    __shared__ bool last;
-    if (ctrl->halted || ctrl->mode != MODE_COMMIT) return;
-    const int n = ctrl->n;
-    double vmax = 0.0, v2s = 0.0, gs = 0.0, near = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    {
-        const Geom gc = geom_c[i];
-        const Vel vc = vel_c[i];
-        geom[i] = gc;
-        vel[i] = vc;
-        phys[i].l = 2 * gc.h;
-        if (sp.stats_on)
-        {
-            const double v2 = vc.v[0] * vc.v[0] + vc.v[1] * vc.v[1] + vc.v[2] * vc.v[2];
-            vmax = fmax(vmax, sqrt(v2));
-            v2s += v2;
-            gs += phys[i].growth;
-            near += (2 * gc.h > sp.near_div_length) ? 1.0 : 0.0;
-        }
-    }
-    // block partial in a fixed reduction order
-    vmax = warp_max(vmax);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        v2s += __shfl_xor_sync(0xffffffffu, v2s, off);
-        gs += __shfl_xor_sync(0xffffffffu, gs, off);
-        near += __shfl_xor_sync(0xffffffffu, near, off);
-    }
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = make_double4(vmax, v2s, gs, near);
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        double4 a = sh[0];
-        for (int w = 1; w < AT_T / 32; ++w)
-        {
-            const double4 b = sh[w];
-            a.x = fmax(a.x, b.x); a.y += b.y; a.z += b.z; a.w += b.w;
-        }
-        sp.stat_part[blockIdx.x] = a;
-        __threadfence();
-        last = atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
-    for (int b = threadIdx.x; b < gridDim.x; b += AT_T)
-    {
-        const double2* q = reinterpret_cast<const double2*>(sp.stat_part + b);
-        const double2 p0 = __ldcg(q), p1 = __ldcg(q + 1);
-        a.x = fmax(a.x, p0.x); a.y += p0.y; a.z += p1.x; a.w += p1.y;
-    }
-    a.x = warp_max(a.x);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
-        a.z += __shfl_xor_sync(0xffffffffu, a.z, off);
-        a.w += __shfl_xor_sync(0xffffffffu, a.w, off);
-    }
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        double4 t = sh[0];
-        for (int w = 1; w < AT_T / 32; ++w)
-        {
-            const double4 b = sh[w];
-            t.x = fmax(t.x, b.x); t.y += b.y; t.z += b.z; t.w += b.w;
-        }
-        if (sp.stats_on)
-        {
-            ctrl->st_vmax_bits = (unsigned long long)__double_as_longlong(t.x);
-            ctrl->st_v2_fx = (unsigned long long)llrint(ldexp(t.y, STAT_V2_SHIFT));
-            ctrl->st_g_fx = (unsigned long long)llrint(ldexp(fmax(t.z, 0.0), STAT_G_SHIFT));
-            ctrl->st_near_div = (unsigned long long)t.w;
-        }
-        ctrl->blocks_done = 0u;
-        ctrl->drift += ctrl->drift_cand;
-        controller_finish(ctrl, sp, MODE_FINAL, ctrl->last_trial_error, true);
-    }
-}
-
-void launch_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const StepParams& sp, const Geom* geom_c,
-                   const Vel* vel_c, int cap_cells, cudaStream_t st)
-{
-    k_commit<<<attempt_blocks(cap_cells), AT_T, 0, st>>>(geom, vel, phys, ctrl, sp, geom_c, vel_c);
-}
-
 void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
-                    unsigned long long cond, int use_cond, PairGather pg, int dims)
+                    unsigned long long cond, int use_cond, PairGather pg, int dims, unsigned long long cond_run)
 {
     int blocks = attempt_blocks(cap_cells);
 #define AT_CASE(S, D) case S: \
-        if (sp.noise_on) launch_attempt_s<S, true, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
-        else launch_attempt_s<S, false, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg); \
+        if (sp.noise_on) launch_attempt_s<S, true, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run); \
+        else launch_attempt_s<S, false, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run); \
         break;
     if (dims == 2)
     {

@@ -81,11 +81,9 @@ struct Ctrl {
     // skin at the last refresh) and the motion since then
     int n_surv;                         // active pairs
     int n_surv_next;                    // pairs appended by a refresh in progress
-    int refreshing;                     // the screening pass of this iteration refreshed
     int screen_valid;                   // 0 after a rebuild, an upload or a division
-    unsigned int surv_blocks;           // last-block counter of the exact pass
+    unsigned int surv_blocks;           // last-block counter of the pair pass
     double drift;                       // sum over accepted steps of the max segment motion
-    double drift_cand;                  // max segment motion of the learned proposal's candidate
     unsigned long long drift_bits;      // block maxima of the running attempt (ordered bits)
 };
 
@@ -194,11 +192,10 @@ void launch_pair_force(const Geom* geom, const int* row_ptr, const int* lower_en
                        Gen6* fcc, double4* jbuf, int lanes, int mixed, int cap_cells, cudaStream_t st,
                        int with_gather = 1, int dims = 3);
 void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* lower_end, int* rev,
-                    int cap_cells, cudaStream_t st, int* row_of = nullptr);
+                    int cap_cells, cudaStream_t st);
 // screened pass over every unordered pair (both shares into jbuf); with_sum also
-// writes each cell's total into fcc.  row_of[k] = row of CSR entry k.
-void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* row_of,
-                          const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
+// writes each cell's total into fcc.
+void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
                           int blocks_per_sm, const int4* pairs, int* surv);
@@ -217,10 +214,8 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                     const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out, Gen6* k0buf,
                     double eval_dt, int eval_attempt, int cap_cells, cudaStream_t st,
                     unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0},
-                    int dims = 3);
+                    int dims = 3, unsigned long long cond_run = 0);
 // accepted proposal of the learned controller: candidate -> state (no-op otherwise)
-void launch_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const StepParams& sp, const Geom* geom_c,
-                   const Vel* vel_c, int cap_cells, cudaStream_t st);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
                        cudaStream_t st, int dims = 3);

@@ -84,7 +84,7 @@ typedef struct abm_params {
     /* device-side choices */
     int precision;               /* ABM_PRECISION_FP64 or ABM_PRECISION_MIXED */
     int cap_cells;               /* device capacity in cells (>= the largest population) */
-    int cap_neighbors_per_cell;  /* directed neighbor slots per cell (0 = default 64) */
+    int cap_neighbors_per_cell;  /* directed neighbor slots per cell (0 = default: 192 in 3-D, 64 in 2-D) */
     int pair_lanes;              /* lanes per cell in the pair-force kernel: 4, 8, 16 or 32 (0 = 8) */
     int use_graphs;              /* 1 = capture the iteration in a CUDA graph */
     /* step-size control (no reference counterpart beyond ABM_CONTROLLER_REFERENCE) */
@@ -102,8 +102,8 @@ typedef struct abm_params {
     double sigma0;
     double adhesion_strength, adhesion_mindist;
     double max_noise;
-    /* shape of the screened pair pass: pairs per block of the screening grid (512..2048,
-     * 0 = 1024) and blocks per SM of the exact pass's grid (0 = 8);
+    /* shape of the screened pair pass: the least pairs per block (512..2048, 0 = 1024)
+     * and the most blocks per SM (0 = as many as are resident at once);
      * abm_autotune_pair_tile picks them */
     int pair_tile, pair_blocks_per_sm;
     /* skin of the active pair list in um (0 = 0.3, negative = none): pairs farther than
@@ -238,8 +238,8 @@ int abm_batch_synchronize(abm_batch* batch);
 int abm_batch_get_stream(abm_batch* batch, void** stream);
 int abm_batch_destroy(abm_batch* batch);
 const char* abm_batch_last_error(void);
-/* Autotuner of the screened pair pass: times screening tiles of 512, 1024 and 2048 pairs
- * with exact-pass grids of 4, 8 and 16 blocks per SM (9 candidates, c = 3 * tile index + grid
+/* Autotuner of the screened pair pass: times tiles of at least 512, 1024 and 2048 pairs per
+ * block with at most 1, 2 and 4 blocks per SM (9 candidates, c = 3 * tile index + grid
  * index) on a scratch context holding `cells`, over `launches` launches each, and
  * returns the fastest shape; ms_per_launch (9 entries, may be NULL) receives each time. */
 int abm_autotune_pair_tile(const abm_params* params, const double* cells, int n, int ncols, int ld,

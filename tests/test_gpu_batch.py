@@ -102,7 +102,7 @@ def test_batch_cell_limit_stops_each_replicate():
 def test_autotuner_picks_a_pair_tile():
     cells = replicates.start_state(5000, 9)
     best, times = abm_b200.autotune_pair_tile(cells, launches=5, **{k: v for k, v in replicates.CONFIG0.items()})
-    assert best[0] in (512, 1024, 2048) and best[1] in (4, 8, 16)
+    assert best[0] in (512, 1024, 2048) and best[1] in (1, 2, 4)
     assert len(times) == 9 and all(t > 0 for t in times.values())
     assert times[best] == min(times.values())
 
@@ -110,7 +110,7 @@ def test_autotuner_picks_a_pair_tile():
 def test_pair_tile_shapes_give_the_same_forces():
     cells = replicates.start_state(3000, 10)
     out = []
-    for tile, bpsm in ((512, 4), (1024, 8), (2048, 16)):
+    for tile, bpsm in ((512, 1), (1024, 2), (2048, 4)):
         s = abm_b200.Simulation(cap_cells=3100, pair_tile=tile, pair_blocks_per_sm=bpsm,
                                 **{k: v for k, v in replicates.CONFIG0.items()})
         s.upload_cells(cells)

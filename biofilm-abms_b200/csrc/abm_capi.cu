@@ -56,6 +56,7 @@ struct abm_ctx {
     float* mlp_w = nullptr;          // ABM_MLP_NPARAM FP32 master weights
     float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
     double4* stat_part = nullptr;    // per-block feature partials of the final attempt
+    int *order = nullptr, *order_flag = nullptr, *order_pos = nullptr;   // attempt order (3-D)
     bool mlp_loaded = false;
     // 2-D model
     int dims = 3;
@@ -134,7 +135,8 @@ static void free_all(abm_ctx* c)
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->pairs, c->pair_start, c->surv, c->jbuf,
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
-                    c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part};
+                    c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
+                    c->order_pos};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -186,7 +188,7 @@ static void fill_tableau(StepParams& sp, int mode, bool& ok)
     sp.inv_q1 = 1.0 / (q + 1);
 }
 
-__global__ void k_set_n(Ctrl* c, int n) { c->n = n; c->halted = 0; c->screen_valid = 0; }
+__global__ void k_set_n(Ctrl* c, int n) { c->n = n; c->halted = 0; c->screen_valid = 0; c->n_order = 0; }
 __global__ void k_screen_stale(Ctrl* c) { c->screen_valid = 0; }
 __global__ void k_set_halt(Ctrl* c, int n_max) { c->halt_n = n_max; c->halted = 0; }
 __global__ void k_set_clock(Ctrl* c, double t, double dt, int iter)
@@ -366,6 +368,13 @@ int abm_create(const abm_params* q, abm_ctx** out)
     sp.log_buf = c->log_buf;
     CK(cudaMalloc(&c->stat_part, (size_t)attempt_blocks(c->cap) * sizeof(double4)));
     sp.stat_part = c->stat_part;
+    if (c->dims == 3)
+    {
+        CK(cudaMalloc(&c->order, (size_t)c->cap * sizeof(int)));
+        CK(cudaMalloc(&c->order_flag, ((size_t)c->cap + 1) * sizeof(int)));
+        CK(cudaMalloc(&c->order_pos, ((size_t)c->cap + 1) * sizeof(int)));
+    }
+    sp.order = c->order;
     return ABM_OK;
 }
 
@@ -561,6 +570,9 @@ static void enqueue_rebuild(abm_ctx* c)
                      c->pairs, c->cap, st, c->sorted_cell);
     if (c->dims == 2 && c->p.adhesion_mode != 0)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, st);
+    if (c->order)
+        launch_attempt_order(c->geom, c->ctrl, c->sp.mp, c->order_flag, c->order_pos, c->scan_sums, c->order,
+                             c->cap, st);
     k_count_rebuild<<<1, 1, 0, st>>>(c->ctrl);
 }
 

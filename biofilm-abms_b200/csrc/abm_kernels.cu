@@ -1433,6 +1433,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         return;
     }
     const int n = ctrl->n;
+    const int n_order = (KIND != 3 && sp.order) ? ctrl->n_order : 0;
     const int mode = ctrl->mode;
     const int iter = ctrl->iter;
     // the learned controller proposes (and tests) a step every iteration
@@ -1484,10 +1485,12 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
     double local_drift = 0.0;
-    // one cell per thread: the grid covers the capacity (attempt_blocks)
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n)
+    // one cell per thread: the grid covers the capacity (attempt_blocks); thread t
+    // takes the t-th cell of the attempt order (cells appended after it in index order)
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n)
     {
+        const int i = t < n_order ? sp.order[t] : t;
         const Geom g = load_geom(from_backup ? geom_c : geom, i);
         const Vel* vprev = (from_backup ? vel_c : vel) + i;
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
@@ -1734,6 +1737,43 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         if ((use_cond & 2) && KIND == MODE_TRIAL)
             cudaGraphSetConditional((cudaGraphConditionalHandle)cond_run, ctrl->mode != MODE_COMMIT ? 1u : 0u);
     }
+}
+
+// Attempt order (3-D): the cells whose velocity takes the full surface solve
+// (area integrals, mechanics.hpp:2254-2309) first, then the others, each group in
+// index order, so that the warps of an attempt mostly run one of the three
+// branches of getVelocities (mechanics.hpp:2011-2347) instead of all of them.
+// Made at every neighbor rebuild from the cells of that moment; a cell that
+// changes branch before the next rebuild costs only divergence.  The order
+// changes no per-cell result.
+__global__ void k_attempt_class(const Geom* __restrict__ geom, const Ctrl* ctrl, MechParams P, int* flag)
+{
+    const int n = ctrl->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const Geom g = load_geom(geom, i);
+        const bool a2 = g.nz < P.nz_threshold;
+        const bool contact = a2 ? (g.rz < P.R) : ((g.rz - g.h * g.nz < P.R) || (g.rz + g.h * g.nz < P.R));
+        flag[i] = (!P.no_surface && !a2 && contact) ? 1 : 0;
+    }
+}
+
+__global__ void k_attempt_order(Ctrl* ctrl, const int* __restrict__ flag, const int* __restrict__ pos, int* order)
+{
+    const int n = ctrl->n;
+    const int n_full = pos[n];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        order[flag[i] ? pos[i] : n_full + (i - pos[i])] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->n_order = n;
+}
+
+void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int* flag, int* pos,
+                          int* block_sums, int* order, int cap_cells, cudaStream_t st)
+{
+    const int blocks = max(cdiv(cap_cells, 256), 1);
+    k_attempt_class<<<blocks, 256, 0, st>>>(geom, ctrl, P, flag);
+    launch_scan(flag, &ctrl->n, pos, block_sums, cap_cells, st);
+    k_attempt_order<<<blocks, 256, 0, st>>>(ctrl, flag, pos, order);
 }
 
 template <int S, bool NOISE, int DIM>

@@ -83,6 +83,7 @@ struct Ctrl {
     int n_surv_next;                    // pairs appended by a refresh in progress
     int screen_valid;                   // 0 after a rebuild, an upload or a division
     unsigned int surv_blocks;           // last-block counter of the pair pass
+    int n_order;                        // cells covered by the attempt order (0: index order)
     double drift;                       // sum over accepted steps of the max segment motion
     unsigned long long drift_bits;      // block maxima of the running attempt (ordered bits)
 };
@@ -113,6 +114,7 @@ struct StepParams {
     double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
     float* log_buf;             // MLP_LOG_COLS floats per row, log_cap rows (ring)
     int log_cap;
+    const int* order;           // attempt order of the first ctrl->n_order cells (3-D), or null
 };
 
 struct ForceParams {
@@ -216,6 +218,9 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                     unsigned long long cond = 0, int use_cond = 0, PairGather pg = PairGather{0, 0, 0, 0, 0},
                     int dims = 3, unsigned long long cond_run = 0);
 // accepted proposal of the learned controller: candidate -> state (no-op otherwise)
+// the attempt order of the cells (3-D): full surface solve first (made at every rebuild)
+void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int* flag, int* pos,
+                          int* block_sums, int* order, int cap_cells, cudaStream_t st);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
                        const Ctrl* ctrl, const StepParams& sp, Gen6* v_out, int cap_cells,
                        cudaStream_t st, int dims = 3);

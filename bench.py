@@ -380,7 +380,7 @@ def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
     dom = max(kernels, key=lambda k: kernels[k][1])
     b, ms = kernels[dom]
     achieved = b / (ms / 1000.0) / 1e9
-    tr = traffic.get(dom + traffic_key_suffix, {}).get("bytes_per_launch")
+    tr = (traffic.get(dom + traffic_key_suffix) or traffic.get(dom) or {}).get("bytes_per_launch")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": tr, "kernel": dom,
             "algorithmic_bytes_per_launch": b, "ms_per_launch": ms, "peak_source": peak_kind,

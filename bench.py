@@ -366,21 +366,24 @@ def kernel_groups(sim, args, variant):
     pf_ms = prof["pair_force_ms"] / prof["pair_force_launches"]
     at_ms = prof["attempt_ms"] / prof["iterations"]
     if VARIANTS[variant]["controller"] == 1:
-        # network proposal + one RK attempt that advances the state in place
+        # the pair pass (its last block makes the network's proposal), then one RK
+        # attempt that tests the proposal and advances the state in place
+        pf_name = "k_pair_pass(+proposal)"
         at_name, at_bytes = "k_attempt(proposal)", attempt_bytes(args.n, True)
     else:
+        pf_name = "k_pair_pass"
         at_name, at_bytes = "k_attempt(trial+final)", attempt_bytes(args.n, False) + attempt_bytes(args.n, True)
-    kernels = {"k_pair_screened": (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
+    kernels = {pf_name: (pair_force_bytes(args.n, n_dir), pf_ms), at_name: (at_bytes, at_ms)}
     return kernels, prof["rebuild_ms"] / max(prof["rebuild_launches"], 1)
 
 
-def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
+def roofline(kernels, rebuild_ms):
     peak, peak_kind = measured_peak_hbm()
     traffic = load_traffic()
     dom = max(kernels, key=lambda k: kernels[k][1])
     b, ms = kernels[dom]
     achieved = b / (ms / 1000.0) / 1e9
-    tr = (traffic.get(dom + traffic_key_suffix) or traffic.get(dom) or {}).get("bytes_per_launch")
+    tr = traffic.get(dom, {}).get("bytes_per_launch")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": tr, "kernel": dom,
             "algorithmic_bytes_per_launch": b, "ms_per_launch": ms, "peak_source": peak_kind,
@@ -390,15 +393,16 @@ def roofline(kernels, rebuild_ms, traffic_key_suffix=""):
             "rebuild_ms_per_rebuild": rebuild_ms}
 
 
-def launches(variant, t):
-    # per iteration: the screened pair pass (screen + exact) and the trial, then its
-    # retries; the reference controller adds the final attempt every iteration, the
-    # learned one adds the network's proposal and runs the final attempt only after
-    # a failed proposal (an IF node skips it otherwise); 18 kernels per neighbor rebuild
+def launches(variant, t, max_tries=3):
+    # per iteration: the pair pass, then the attempts.  Reference controller: the trial,
+    # its retries (WHILE node) and the final attempt.  Learned controller: the pair
+    # pass also makes the proposal; the trial closes a passing step, and only a failed
+    # proposal runs the IF node's max_tries retry launches and the final attempt.
+    # 18 kernels per neighbor rebuild.
     learned = VARIANTS[variant]["controller"] == 1
-    per_iter = 4
-    extra = t["retries"] + (t["rejected"] if learned else 0)
-    return t["iterations"] * per_iter + extra + 18 * t["rebuilds"]
+    if learned:
+        return t["iterations"] * 2 + t["rejected"] * (max_tries + 1) + 18 * t["rebuilds"]
+    return t["iterations"] * 3 + t["retries"] + 18 * t["rebuilds"]
 
 
 def relerr(a, b):
@@ -501,7 +505,7 @@ def run_b200(args):
                                           "simulated_h_in_timed_region": h["t_sim_h"],
                                           "stepsize_network": weights_note if head == "chosen" else None}),
             "e2e": h["e2e"], "gpu_launches": launches(head, h),
-            "roofline": roofline(h["kernels"], h["rebuild_ms"], "[mixed]" if head == "chosen" else ""),
+            "roofline": roofline(h["kernels"], h["rebuild_ms"]),
             "clocks": {k: h["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
     if other:
         o = results[other]

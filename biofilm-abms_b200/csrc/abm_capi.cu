@@ -581,20 +581,23 @@ static void enqueue_rebuild(abm_ctx* c)
 // final attempt (simulation.hpp:1677-1769), each an early exit when idle
 // the screened pass writes both shares of every pair; with_gather also sums them
 // per cell into fcc (the API paths; the loop's first attempt sums them itself)
-static void enqueue_pair_force(abm_ctx* c, int with_gather)
+// in_loop: the pass of a loop iteration, whose last block also makes the iteration's
+// step-size features (and, learned, the proposed dt)
+static void enqueue_pair_force(abm_ctx* c, int with_gather, bool in_loop = false)
 {
     launch_pair_screened(c->geom, c->row_ptr, c->lower_end, c->col, c->rev, c->ctrl, c->fp,
                          c->jkr_delta, c->jkr_radius, c->fcc, c->jbuf, c->p.precision == ABM_PRECISION_MIXED,
                          c->cap * c->cap_nbr, c->cap, c->num_sms, c->st, with_gather, c->dims, c->p.pair_tile,
-                         c->p.pair_blocks_per_sm, c->pairs, c->surv);
+                         c->p.pair_blocks_per_sm, c->pairs, c->surv, in_loop ? &c->sp : nullptr, c->mlp_w);
 }
 
 // pair_sum 1 (default): the first attempt sums each cell's shares itself; 2: a
 // separate light kernel sums them into fcc before the attempts
 static bool sum_in_attempt(abm_ctx* c) { return c->p.pair_sum != 2; }
 
-// the loop's pair pass: the shares, plus their per-cell sums unless the first attempt makes them
-static void enqueue_loop_pair_force(abm_ctx* c) { enqueue_pair_force(c, sum_in_attempt(c) ? 0 : 1); }
+// the loop's pair pass: the shares, plus their per-cell sums unless the first attempt
+// makes them, and the step-size proposal
+static void enqueue_loop_pair_force(abm_ctx* c) { enqueue_pair_force(c, sum_in_attempt(c) ? 0 : 1, true); }
 
 // where the attempts of one iteration find the pair force
 static PairGather loop_gather(abm_ctx* c)
@@ -604,11 +607,6 @@ static PairGather loop_gather(abm_ctx* c)
     return pg;
 }
 
-// the step-size features of the iteration (and, learned, the proposed dt)
-static void enqueue_propose(abm_ctx* c)
-{
-    if (c->sp.stats_on) launch_mlp_propose(c->ctrl, c->sp, c->mlp_w, c->st);
-}
 
 static void enqueue_attempts(abm_ctx* c)
 {
@@ -626,7 +624,6 @@ static void enqueue_attempts(abm_ctx* c)
 static void enqueue_iteration(abm_ctx* c)
 {
     enqueue_loop_pair_force(c);
-    enqueue_propose(c);
     enqueue_attempts(c);
 }
 
@@ -709,14 +706,17 @@ static int add_conditional(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphN
 // One loop iteration as a graph with conditional nodes, appended to G after `deps`
 // (empty: root nodes); `deps` becomes the iteration's leaf set:
 //   [division count] -> IF(n_divide > 0){division + rebuild}
-//   -> pair force -> [proposal] -> trial -> WHILE(retry requested){retry}
-//   -> final (learned controller: IF(proposal failed){final})
+//   -> pair force -> [proposal] -> trial -> WHILE(retry requested){retry} -> final
+// With the learned controller a passing proposal closes the step in the trial, and
+// the rest runs only after a failed one:
+//   ... -> trial -> IF(proposal failed){retry x max_tries (each exits at once when
+//   no retry is pending) -> final}
 static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode_t>& deps)
 {
     // every handle must belong to a conditional node of this graph, or instantiation fails
     cudaGraphConditionalHandle h_div = 0, h_retry = 0, h_run = 0;
-    const bool retries = c->p.max_tries_update_stepsize > 0;
     const bool branch = c->sp.learned != 0;
+    const bool retries = c->p.max_tries_update_stepsize > 0 && !branch;
     if (retries) CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
     if (branch) CK(cudaGraphConditionalHandleCreate(&h_run, G, 0, cudaGraphCondAssignDefault));
     int rc;
@@ -735,35 +735,40 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
     PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
         enqueue_loop_pair_force(c);
-        enqueue_propose(c);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, h_retry, (retries ? 1 : 0) | (branch ? 2 : 0), pg, c->dims,
                        h_run);
     });
     if (rc) return rc;
+    auto retry_attempt = [&](int use_cond) {
+        launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c,
+                       nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, use_cond, pg, c->dims);
+    };
+    auto final_attempt = [&]() {
+        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
+                       c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
+    };
+    if (branch)
+    {
+        cudaGraph_t body;
+        rc = add_conditional(c, G, deps, h_run, cudaGraphCondTypeIf, &body);
+        if (rc) return rc;
+        std::vector<cudaGraphNode_t> bd;
+        return capture_into(c, body, bd, [&]() {
+            for (int r = 0; r < c->p.max_tries_update_stepsize; ++r) retry_attempt(0);
+            final_attempt();
+        });
+    }
     if (retries)
     {
         cudaGraph_t body;
         rc = add_conditional(c, G, deps, h_retry, cudaGraphCondTypeWhile, &body);
         if (rc) return rc;
         std::vector<cudaGraphNode_t> bd;
-        rc = capture_into(c, body, bd, [&]() {
-            launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c,
-                           nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, 1, pg, c->dims);
-        });
+        rc = capture_into(c, body, bd, [&]() { retry_attempt(1); });
         if (rc) return rc;
     }
-    auto final_attempt = [&]() {
-        launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
-                       c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
-    };
-    if (!branch) return capture_into(c, G, deps, final_attempt);
-    // a proposal that passed closed the step in the trial: skip the final launch
-    cudaGraph_t body;
-    rc = add_conditional(c, G, deps, h_run, cudaGraphCondTypeIf, &body);
-    if (rc) return rc;
-    std::vector<cudaGraphNode_t> bd;
-    return capture_into(c, body, bd, final_attempt);
+    return capture_into(c, G, deps, final_attempt);
 }
 
 static int build_iteration_graph(abm_ctx* c)
@@ -1108,7 +1113,6 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
         CK(cudaEventRecord(e[0], st));
         enqueue_loop_pair_force(c);
         CK(cudaEventRecord(e[1], st));
-        enqueue_propose(c);
         enqueue_attempts(c);
         CK(cudaEventRecord(e[2], st));
         c->host_iter += 1;

@@ -12,6 +12,7 @@
 //                  simulation.hpp:1690-1769 run by the last block to finish)
 #include <cstdio>
 #include "abm_kernels.cuh"
+#include "abm_propose.cuh"
 
 namespace abm {
 
@@ -949,11 +950,16 @@ __device__ __forceinline__ void pair_shares(const Geom& gi, const Geom& gj, cons
     }
 }
 
+// With `propose` the last block then runs the step-size proposal of the iteration
+// (mlp_propose_block), once every block's overlaps are in; it reads their maximum
+// with an atomic, the one field of the control record that other blocks change
+// during the pass.
 template <bool MIXED, int DIM>
 __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
                                                    Ctrl* ctrl, ForceParams fp, const double* __restrict__ td,
                                                    const double* __restrict__ tr, double4* __restrict__ jbuf,
-                                                   int* __restrict__ surv)
+                                                   int* __restrict__ surv, StepParams sp,
+                                                   const float* __restrict__ mlp_w, int propose)
 {
     __shared__ bool last;
     if (ctrl->halted) return;
@@ -1014,17 +1020,23 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
         last = atomicAdd(&ctrl->surv_blocks, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0)
+    if (!last) return;
+    if (threadIdx.x == 0)
     {
+        __threadfence();
         if (refresh)
         {
-            __threadfence();
             ctrl->n_surv = atomicAdd(&ctrl->n_surv_next, 0);
             ctrl->n_surv_next = 0;
             ctrl->screen_valid = 1;
             ctrl->drift = 0.0;
         }
         ctrl->surv_blocks = 0u;
+    }
+    if (propose)
+    {
+        __syncthreads();
+        mlp_propose_block(ctrl, sp, mlp_w);
     }
 }
 
@@ -1078,8 +1090,13 @@ void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower
                           const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
-                          int blocks_per_sm, const int4* pairs, int* surv)
+                          int blocks_per_sm, const int4* pairs, int* surv, const StepParams* sp,
+                          const float* mlp_w)
 {
+    // sp (the loop's pass): the last block also runs the step-size proposal
+    StepParams spv{};
+    if (sp) spv = *sp;
+    const int propose = (sp && sp->stats_on) ? 1 : 0;
     // grid: at least `tile` pairs per block, at most the blocks that are resident at
     // once (blocks_per_sm caps them per SM); the blocks stride over the pairs
     tile = tile <= 0 ? 1024 : min(tile, PS_TILE_MAX);
@@ -1096,7 +1113,7 @@ void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower
         return max(1, min(cdiv(max_pairs, tile), num_sms * per_sm));
     };
     static int occ2 = 0, occ3m = 0, occ3 = 0;
-#define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv
+#define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv, spv, mlp_w, propose
     if (dims == 2)
         k_pair_pass<false, 2><<<grid((const void*)k_pair_pass<false, 2>, occ2), PS_T, 0, st>>>(PX_ARGS);
     else if (f32)

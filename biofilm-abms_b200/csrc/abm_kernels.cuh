@@ -200,7 +200,8 @@ void launch_csr_rev(const Ctrl* ctrl, const int* row_ptr, const int* col, int* l
 void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower_end, const int* col, const int* rev, Ctrl* ctrl, ForceParams fp, const double* jkr_delta,
                           const double* jkr_radius, Gen6* fcc, double4* jbuf, int mixed, int max_entries,
                           int cap_cells, int num_sms, cudaStream_t st, int with_sum, int dims, int tile,
-                          int blocks_per_sm, const int4* pairs, int* surv);
+                          int blocks_per_sm, const int4* pairs, int* surv, const StepParams* sp = nullptr,
+                          const float* mlp_w = nullptr);
 // the list of unordered pairs (i, j < i, lower entry k, partner entry rev[k]) after
 // k_csr_rev, cells in `order` (null: index order): counts -> scan -> fill; uses
 // `count` and `start` (cap_cells + 1) as scratch
@@ -239,7 +240,6 @@ void launch_mlp_grad(const float* master, const float* X, const float* T, int n,
 void launch_mlp_train(float* master, float* m1, float* m2, float* G, const float* X, const float* T, int n,
                       int epochs, float lr, unsigned seed, float* loss_out, cudaStream_t st);
 // features of the running iteration -> log row; with sp.learned also the dt of the first attempt
-void launch_mlp_propose(Ctrl* ctrl, const StepParams& sp, const float* master, cudaStream_t st);
 int attempt_blocks(int cap_cells);
 
 // division (growth.hpp:66-426), abm_divide.cu

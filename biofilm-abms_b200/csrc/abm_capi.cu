@@ -65,6 +65,8 @@ struct abm_ctx {
     ForceParams fp; StepParams sp; BuildParams bp;
     // graphs
     cudaGraphExec_t g_iter = nullptr, g_rebuild = nullptr;
+    cudaGraphExec_t g_iter_k = nullptr;   // iter_k iterations in one graph (long loops)
+    int iter_k = 1;
     bool graph_fallback = false;     // conditional nodes could not be built
     std::string graph_note;
 };
@@ -129,6 +131,7 @@ const char* abm_last_error(const abm_ctx* c) { return c ? c->err.c_str() : "null
 static void free_all(abm_ctx* c)
 {
     if (c->g_iter) cudaGraphExecDestroy(c->g_iter);
+    if (c->g_iter_k) cudaGraphExecDestroy(c->g_iter_k);
     if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
@@ -139,6 +142,14 @@ static void free_all(abm_ctx* c)
                     c->order_pos};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
+}
+
+// the captured iteration graphs hold buffer pointers and parameters: drop them when
+// those change (they are rebuilt at the next abm_iterate)
+static void drop_iteration_graphs(abm_ctx* c)
+{
+    if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+    if (c->g_iter_k) { cudaGraphExecDestroy(c->g_iter_k); c->g_iter_k = nullptr; }
 }
 
 static void fill_tableau(StepParams& sp, int mode, bool& ok)
@@ -427,7 +438,7 @@ int abm_set_jkr_table(abm_ctx* c, const double* delta, const double* radius, int
     c->jkr_n = n;
     c->fp.jkr_n = n;
     c->fp.jkr_step = (delta[n - 1] - delta[0]) / double(n - 1);
-    if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+    drop_iteration_graphs(c);
     return ABM_OK;
 }
 
@@ -459,7 +470,7 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     const int col_growth = two_d ? 12 : 16, col_l = two_d ? 9 : 13;
     for (int i = 0; i < n && !grows; ++i)
         grows = cm[(size_t)col_growth * ld + i] != 0 || cm[(size_t)col_l * ld + i] > c->p.Ldiv;
-    if (grows != c->div_enabled && c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+    if (grows != c->div_enabled) drop_iteration_graphs(c);
     c->div_enabled = grows;
     return ABM_OK;
 }
@@ -530,7 +541,7 @@ int abm_set_parents(abm_ctx* c, const int* parents, int n)
         c->cap_parents = n + 2 * c->cap + 1024;
         CK(cudaMalloc(&c->parents_dev, (size_t)c->cap_parents * sizeof(int)));
         // captured graphs hold the old buffer
-        if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+        drop_iteration_graphs(c);
         if (c->g_rebuild) { cudaGraphExecDestroy(c->g_rebuild); c->g_rebuild = nullptr; }
     }
     if (n > 0) CK(cudaMemcpyAsync(c->parents_dev, parents, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->st));
@@ -771,16 +782,35 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
     return capture_into(c, G, deps, final_attempt);
 }
 
-static int build_iteration_graph(abm_ctx* c)
+static int instantiate_iterations(abm_ctx* c, int k, cudaGraphExec_t* exec)
 {
     cudaGraph_t G;
     CK(cudaGraphCreate(&G, 0));
     std::vector<cudaGraphNode_t> deps;
-    int rc = append_iteration(c, G, deps);
-    if (rc) { cudaGraphDestroy(G); return rc; }
-    cudaError_t inst = cudaGraphInstantiate(&c->g_iter, G, 0);
+    for (int r = 0; r < k; ++r)
+    {
+        int rc = append_iteration(c, G, deps);
+        if (rc) { cudaGraphDestroy(G); return rc; }
+    }
+    cudaError_t inst = cudaGraphInstantiate(exec, G, 0);
     cudaGraphDestroy(G);
     CK(inst);
+    return ABM_OK;
+}
+
+// One iteration per graph, and (for long loops) iter_k iterations per graph, iter_k
+// the largest of 10, 5, 4, 2 that divides iter_update_neighbors, so that a K-graph
+// launched at a multiple of iter_k never straddles a periodic rebuild.  The fixed
+// cost of a graph launch (host submission, the conditional nodes' scheduling) is
+// paid once per iter_k iterations.
+static int build_iteration_graph(abm_ctx* c)
+{
+    int rc = instantiate_iterations(c, 1, &c->g_iter);
+    if (rc) return rc;
+    c->iter_k = 1;
+    for (int k : {10, 5, 4, 2})
+        if (c->p.iter_update_neighbors % k == 0) { c->iter_k = k; break; }
+    if (c->iter_k > 1) return instantiate_iterations(c, c->iter_k, &c->g_iter_k);
     return ABM_OK;
 }
 
@@ -1060,29 +1090,40 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
                 c->graph_note = c->err;
                 c->graph_fallback = true;
                 cudaGetLastError();
-                if (c->g_iter) { cudaGraphExecDestroy(c->g_iter); c->g_iter = nullptr; }
+                drop_iteration_graphs(c);
             }
         }
         if (c->graph_fallback && !c->g_iter) { rc = capture(c, enqueue_iteration, &c->g_iter); if (rc) return rc; }
         if (!c->g_rebuild) { rc = capture(c, enqueue_rebuild, &c->g_rebuild); if (rc) return rc; }
     }
-    for (int k = 0; k < n_iters; ++k)
+    for (int k = 0, next_check = 0; k < n_iters;)
     {
-        if (n_cells_stop > 0 && c->div_enabled && (k % 16) == 0)
+        if (n_cells_stop > 0 && c->div_enabled && k >= next_check)
         {
             Ctrl h;
             CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
             CK(cudaStreamSynchronize(c->st));
             if (h.n >= n_cells_stop) break;
+            next_check = k + 16;
         }
-        if (c->p.use_graphs && !c->graph_fallback) CK(cudaGraphLaunch(c->g_iter, c->st));
+        int step = 1;
+        if (c->p.use_graphs && !c->graph_fallback)
+        {
+            if (c->g_iter_k && c->host_iter % c->iter_k == 0 && n_iters - k >= c->iter_k)
+            {
+                CK(cudaGraphLaunch(c->g_iter_k, c->st));
+                step = c->iter_k;
+            }
+            else CK(cudaGraphLaunch(c->g_iter, c->st));
+        }
         else
         {
             if (c->div_enabled) { rc = divide_now(c, true, nullptr); if (rc) return rc; }
             if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
             else enqueue_iteration(c);
         }
-        c->host_iter += 1;
+        c->host_iter += step;
+        k += step;
         if (c->host_iter % c->p.iter_update_neighbors == 0)
         {
             if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_rebuild, c->st));

@@ -56,7 +56,7 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=N_CELLS)
+    ap.add_argument("--n", "--cells", dest="n", type=int, default=N_CELLS)
     ap.add_argument("--tableau", type=int, default=1, help="1 HE21, 2 BS32, 3 RKF45, 4 DP54")
     ap.add_argument("--variant", default="chosen", choices=["chosen", "plain"],
                     help="headline configuration; the other one is timed beside it unless --only")

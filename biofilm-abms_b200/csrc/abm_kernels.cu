@@ -481,16 +481,23 @@ __global__ void __launch_bounds__(PB_T) k_pair_build(const Grid* grid, const int
                         {
                         const int total = G * min(PB_SLICE, nb1 - c0);
                         // warps take consecutive 32-product slices; every lane of a
-                        // warp runs the same number of rounds
+                        // warp runs the same number of rounds.  Product idx is (own =
+                        // idx % G, candidate = idx / G); both advance by PB_T per round,
+                        // so they are stepped instead of divided.
+                        int q = (warp * 32 + lane) / G, r = (warp * 32 + lane) % G;
+                        const int dq = PB_T / G, dr = PB_T % G;
                         for (int w0 = warp * 32; w0 < total; w0 += PB_T)
                         {
                             const int idx = w0 + lane;
                             bool pass = false;
                             int own = 0, pos = 0;
+                            const int own_r = r, cand_q = q;
+                            r += dr; q += dq;
+                            if (r >= G) { r -= G; q += 1; }
                             if (idx < total)
                             {
-                                own = idx % G;
-                                pos = c0 + idx / G;
+                                own = own_r;
+                                pos = c0 + cand_q;
                                 if (pos != base + own)
                                 {
                                     const Geom& c = sorted_geom[pos];

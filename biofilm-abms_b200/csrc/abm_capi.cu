@@ -653,7 +653,8 @@ static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
 // division body (after the flag count): ranks, room checks on a fresh cell list,
 // the ten tries, commit, then the neighbor rebuild the reference does after any
 // division (simulation.hpp:1654-1660)
-static void enqueue_division_body(abm_ctx* c)
+// the body up to the room checks (before the tries)
+static void enqueue_division_setup(abm_ctx* c)
 {
     cudaStream_t st = c->st;
     launch_scan(c->div_flags, &c->ctrl->n, c->div_rank, c->scan_sums, c->cap, st);
@@ -665,17 +666,23 @@ static void enqueue_division_body(abm_ctx* c)
     launch_bin_scatter(c->geom, c->ctrl, c->bin_start, c->key, c->slot, c->sorted_cell, c->sorted_geom, c->cap, st);
     launch_div_check(c->geom, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell, c->sorted_geom, c->div_flags,
                      c->mothers, c->div_check, c->div_sat, st);
-    launch_div_tries(c->geom, c->phys, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell, c->sorted_geom,
-                     c->div_flags, c->mothers, c->div_check, c->div_sat, c->d1, c->d2, c->dlen, c->dgrowth,
-                     c->div_ok, st);
-    launch_div_commit(c->geom, c->vel, c->phys, c->ctrl, c->dp, c->mothers, c->d1, c->d2, c->dlen, c->dgrowth,
-                      c->parents_dev, st);
 }
 
-static void enqueue_division_body_and_rebuild(abm_ctx* c)
+static void enqueue_division_commit(abm_ctx* c)
 {
-    enqueue_division_body(c);
-    enqueue_rebuild(c);
+    launch_div_commit(c->geom, c->vel, c->phys, c->ctrl, c->dp, c->mothers, c->d1, c->d2, c->dlen, c->dgrowth,
+                      c->parents_dev, c->st);
+}
+
+// the whole body with the ten tries launched in a row (each exits at once once the
+// criterion holds for every dividing cell): the paths without conditional nodes
+static void enqueue_division_body(abm_ctx* c)
+{
+    enqueue_division_setup(c);
+    launch_div_tries(c->geom, c->phys, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell, c->sorted_geom,
+                     c->div_flags, c->mothers, c->div_check, c->div_sat, c->d1, c->d2, c->dlen, c->dgrowth,
+                     c->div_ok, c->st);
+    enqueue_division_commit(c);
 }
 
 // Capture fn into `graph` after `deps`; `deps` becomes the leaf set of the capture.
@@ -714,6 +721,29 @@ static int add_conditional(abm_ctx* c, cudaGraph_t graph, std::vector<cudaGraphN
     return ABM_OK;
 }
 
+// the body in a graph: the tries as a WHILE node that runs them until the distance
+// criterion holds for every dividing cell or ten have run (growth.hpp:252), then the
+// commit and the neighbor rebuild
+static int capture_division_body(abm_ctx* c, cudaGraph_t body)
+{
+    std::vector<cudaGraphNode_t> bd;
+    int rc = capture_into(c, body, bd, [&]() { enqueue_division_setup(c); });
+    if (rc) return rc;
+    cudaGraphConditionalHandle h_try = 0;
+    CK(cudaGraphConditionalHandleCreate(&h_try, body, 1, cudaGraphCondAssignDefault));   // the first try always runs
+    cudaGraph_t tries;
+    rc = add_conditional(c, body, bd, h_try, cudaGraphCondTypeWhile, &tries);
+    if (rc) return rc;
+    std::vector<cudaGraphNode_t> tb;
+    rc = capture_into(c, tries, tb, [&]() {
+        launch_div_try_round(c->geom, c->phys, c->ctrl, c->dp, c->grid, c->bin_start, c->sorted_cell,
+                             c->sorted_geom, c->div_flags, c->mothers, c->div_check, c->div_sat, c->d1, c->d2,
+                             c->dlen, c->dgrowth, c->div_ok, h_try, c->st);
+    });
+    if (rc) return rc;
+    return capture_into(c, body, bd, [&]() { enqueue_division_commit(c); enqueue_rebuild(c); });
+}
+
 // One loop iteration as a graph with conditional nodes, appended to G after `deps`
 // (empty: root nodes); `deps` becomes the iteration's leaf set:
 //   [division count] -> IF(n_divide > 0){division + rebuild}
@@ -739,8 +769,7 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
         cudaGraph_t body;
         rc = add_conditional(c, G, deps, h_div, cudaGraphCondTypeIf, &body);
         if (rc) return rc;
-        std::vector<cudaGraphNode_t> bd;
-        rc = capture_into(c, body, bd, [&]() { enqueue_division_body_and_rebuild(c); });
+        rc = capture_division_body(c, body);
         if (rc) return rc;
     }
     PairGather pg = loop_gather(c);

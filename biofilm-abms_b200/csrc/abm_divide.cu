@@ -162,11 +162,14 @@ __device__ __forceinline__ void rotate_daughter(double ux, double uy, double uz,
     oz = __dadd_rn(__dmul_rn(az, c2), __dmul_rn(wz, s2));
 }
 
+// tr_arg: the try (0 .. DIV_TRIES - 1), or -1 for the try after the ctrl->div_tries
+// completed ones (the WHILE node of the iteration graph)
 __global__ void k_div_try(const Geom* __restrict__ geom, const Phys* __restrict__ phys, Ctrl* ctrl,
-                          DivideParams dp, const int* mothers, const int* check, int tr, Geom* d1, Geom* d2,
+                          DivideParams dp, const int* mothers, const int* check, int tr_arg, Geom* d1, Geom* d2,
                           double* dlen, double* dgrowth)
 {
     const int nd = ctrl->n_divide;
+    const int tr = tr_arg >= 0 ? tr_arg : ctrl->div_tries;
     if (nd == 0 || (tr > 0 && ctrl->div_done)) return;
     const int iter = ctrl->iter;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x)
@@ -213,10 +216,11 @@ __global__ void k_div_try(const Geom* __restrict__ geom, const Phys* __restrict_
 // min distance of each daughter to the new population >= 2 Rcell?  (growth.hpp:366-398)
 __global__ void k_div_mindist(Ctrl* ctrl, DivideParams dp, const Grid* grid, const int* bin_start,
                               const int* sorted_cell, const Geom* sorted_geom, const int* flags,
-                              const int* mothers, const int* check, int tr, const Geom* d1, const Geom* d2,
+                              const int* mothers, const int* check, int tr_arg, const Geom* d1, const Geom* d2,
                               int* ok)
 {
     const int nd = ctrl->n_divide;
+    const int tr = tr_arg >= 0 ? tr_arg : ctrl->div_tries;
     if (nd == 0 || (tr > 0 && ctrl->div_done)) return;
     const Grid g = *grid;
     const double limit = 2 * dp.Rcell;
@@ -238,12 +242,21 @@ __global__ void k_div_mindist(Ctrl* ctrl, DivideParams dp, const Grid* grid, con
     }
 }
 
-__global__ void k_div_eval(Ctrl* ctrl, const int* check, const int* ok, int* sat, int tr)
+// use_cond: `cond` is the handle of the WHILE node around the tries, continued while
+// a dividing cell still misses the distance criterion and tries are left
+__global__ void k_div_eval(Ctrl* ctrl, const int* check, const int* ok, int* sat, int tr_arg,
+                           unsigned long long cond, int use_cond)
 {
     __shared__ int sh;
     __shared__ bool last;
     const int nd = ctrl->n_divide;
-    if (nd == 0 || (tr > 0 && ctrl->div_done)) return;
+    const int tr = tr_arg >= 0 ? tr_arg : ctrl->div_tries;
+    if (nd == 0 || (tr > 0 && ctrl->div_done))
+    {
+        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
+        return;
+    }
     if (threadIdx.x == 0) sh = 0;
     __syncthreads();
     int c = 0;
@@ -270,6 +283,7 @@ __global__ void k_div_eval(Ctrl* ctrl, const int* check, const int* ok, int* sat
         ctrl->div_tries = tr + 1;
         // while (ntries == 0 || (ntries < 10 && satisfied < n_divide))  (growth.hpp:252)
         ctrl->div_done = (total >= nd) || (tr + 1 >= DIV_TRIES);
+        if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, ctrl->div_done ? 0u : 1u);
     }
 }
 
@@ -346,8 +360,21 @@ void launch_div_tries(const Geom* geom, const Phys* phys, Ctrl* ctrl, const Divi
         k_div_try<<<b1, DV_T, 0, st>>>(geom, phys, ctrl, dp, mothers, check, tr, d1, d2, dlen, dgrowth);
         k_div_mindist<<<b2, DV_T, 0, st>>>(ctrl, dp, grid, bin_start, sorted_cell, sorted_geom, flags, mothers,
                                           check, tr, d1, d2, ok);
-        k_div_eval<<<b1, DV_T, 0, st>>>(ctrl, check, ok, sat, tr);
+        k_div_eval<<<b1, DV_T, 0, st>>>(ctrl, check, ok, sat, tr, 0, 0);
     }
+}
+
+// one try of the body of the WHILE node (the try index from ctrl->div_tries)
+void launch_div_try_round(const Geom* geom, const Phys* phys, Ctrl* ctrl, const DivideParams& dp, const Grid* grid,
+                          const int* bin_start, const int* sorted_cell, const Geom* sorted_geom, const int* flags,
+                          const int* mothers, const int* check, int* sat, Geom* d1, Geom* d2, double* dlen,
+                          double* dgrowth, int* ok, unsigned long long cond, cudaStream_t st)
+{
+    const int b1 = max(cdiv_d(dp.cap_cells, DV_T), 1), b2 = max(cdiv_d(2LL * dp.cap_cells, DV_T), 1);
+    k_div_try<<<b1, DV_T, 0, st>>>(geom, phys, ctrl, dp, mothers, check, -1, d1, d2, dlen, dgrowth);
+    k_div_mindist<<<b2, DV_T, 0, st>>>(ctrl, dp, grid, bin_start, sorted_cell, sorted_geom, flags, mothers,
+                                      check, -1, d1, d2, ok);
+    k_div_eval<<<b1, DV_T, 0, st>>>(ctrl, check, ok, sat, -1, cond, 1);
 }
 
 void launch_div_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp, const int* mothers,

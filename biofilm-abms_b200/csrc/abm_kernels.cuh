@@ -260,6 +260,10 @@ void launch_div_tries(const Geom* geom, const Phys* phys, Ctrl* ctrl, const Divi
                       const int* bin_start, const int* sorted_cell, const Geom* sorted_geom, const int* flags,
                       const int* mothers, const int* check, int* sat, Geom* d1, Geom* d2, double* dlen,
                       double* dgrowth, int* ok, cudaStream_t st);
+void launch_div_try_round(const Geom* geom, const Phys* phys, Ctrl* ctrl, const DivideParams& dp, const Grid* grid,
+                          const int* bin_start, const int* sorted_cell, const Geom* sorted_geom, const int* flags,
+                          const int* mothers, const int* check, int* sat, Geom* d1, Geom* d2, double* dlen,
+                          double* dgrowth, int* ok, unsigned long long cond, cudaStream_t st);
 void launch_div_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp, const int* mothers,
                        const Geom* d1, const Geom* d2, const double* dlen, const double* dgrowth, int* parents,
                        cudaStream_t st);

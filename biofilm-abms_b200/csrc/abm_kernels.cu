@@ -368,10 +368,34 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_final(const int* __restrict__ i
     if (blockIdx.x == 0 && threadIdx.x == 0) out[len] = block_sums[nblocks];
 }
 
+// Arrays of at most SCAN_SINGLE_MAX entries: one block of SCAN_T threads, each
+// summing a run of at most 64 consecutive entries, then writing its run's prefixes.
+// One launch instead of three, for the many small scans of replicate batches.
+const int SCAN_SINGLE_MAX = 1 << 16;
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_single(const int* __restrict__ in, const int* len_p, int* out)
+{
+    __shared__ int sh[32];
+    const int len = *len_p;
+    const int per = (len + SCAN_T - 1) / SCAN_T;
+    const int b0 = min(threadIdx.x * per, len), b1 = min(b0 + per, len);
+    int s = 0;
+    for (int k = b0; k < b1; ++k) s += in[k];
+    int total;
+    int off = block_exclusive_scan(s, sh, total);
+    for (int k = b0; k < b1; ++k) { const int v = in[k]; out[k] = off; off += v; }
+    if (threadIdx.x == 0) out[len] = total;
+}
+
 size_t scan_block_sums_size(int cap) { return (size_t)cdiv(cap, SCAN_TILE) + 1; }
 
 void launch_scan(const int* in, const int* len, int* out, int* block_sums, int cap, cudaStream_t st)
 {
+    if (cap <= SCAN_SINGLE_MAX)
+    {
+        k_scan_single<<<1, SCAN_T, 0, st>>>(in, len, out);
+        return;
+    }
     int nb = max(cdiv(cap, SCAN_TILE), 1);
     k_scan_sums<<<nb, SCAN_T, 0, st>>>(in, len, block_sums);
     k_scan_top<<<1, SCAN_T, 0, st>>>(block_sums, nb);
@@ -1050,8 +1074,6 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
 // The pair list visits cells in `order` (the cell list's bin order after a rebuild,
 // else index order): pairs of one region of space are screened together, so each
 // cell's record is fetched once and reused from the caches by its neighbours' pairs.
-// a new pair list (or new cells) makes the active list stale
-__global__ void k_invalidate_screen(Ctrl* ctrl) { ctrl->screen_valid = 0; }
 
 __global__ void k_lower_counts(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
                                const int* __restrict__ order, int* count)
@@ -1064,11 +1086,13 @@ __global__ void k_lower_counts(const Ctrl* ctrl, const int* __restrict__ row_ptr
     }
 }
 
-__global__ void k_pair_list_fill(const Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
+// a new pair list makes the active list stale (block 0 marks it)
+__global__ void k_pair_list_fill(Ctrl* ctrl, const int* __restrict__ row_ptr, const int* __restrict__ lower_end,
                                  const int* __restrict__ col, const int* __restrict__ rev,
                                  const int* __restrict__ order, const int* __restrict__ start, int4* pairs)
 {
     const int n = ctrl->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->screen_valid = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
     {
         const int i = order ? order[q] : q;
@@ -1084,8 +1108,8 @@ void launch_pair_list(const Ctrl* ctrl, const int* row_ptr, const int* lower_end
     const int blocks = max(cdiv(cap_cells, 256), 1);
     k_lower_counts<<<blocks, 256, 0, st>>>(ctrl, row_ptr, lower_end, order, count);
     launch_scan(count, &ctrl->n, start, block_sums, cap_cells, st);
-    k_pair_list_fill<<<blocks, 256, 0, st>>>(ctrl, row_ptr, lower_end, col, rev, order, start, pairs);
-    k_invalidate_screen<<<1, 1, 0, st>>>(const_cast<Ctrl*>(ctrl));
+    k_pair_list_fill<<<blocks, 256, 0, st>>>(const_cast<Ctrl*>(ctrl), row_ptr, lower_end, col, rev, order, start,
+                                             pairs);
 }
 
 // total dE/dq of each cell from the two shares of every pair (the API paths;

@@ -1,11 +1,15 @@
 // CUDA kernels of the B200 mechanics step (sm_100a).
 //
 //   cell list      k_bbox -> k_bin_count -> scan -> k_bin_scatter        (uniform grid,
-//                  counting sort by bin, bins staged through shared memory)
-//   pair set       k_pair_build -> scan -> k_csr_fill                   (getCellNeighbors,
-//                  mechanics.hpp:520-593; CSR rows sorted by neighbor index)
-//   pair force     k_pair_force<G>                                      (cellCellInteractionForces,
-//                  mechanics.hpp:1209-1659; G lanes per cell, shuffle reduction)
+//                  counting sort by bin)
+//   pair set       k_pair_build -> scan -> k_csr_fill -> k_csr_rev      (getCellNeighbors,
+//                  mechanics.hpp:520-593; CSR rows sorted by neighbor index), then the
+//                  pair records in bin order and the attempt order
+//   pair force     k_pair_pass<MIXED, DIM>                              (cellCellInteractionForces,
+//                  mechanics.hpp:1209-1659; one record per unordered pair, screened
+//                  against an active list with a skin, both shares per pair; the last
+//                  block makes the step-size proposal of the learned controller)
+//                  k_pair_force<G> serves the no-alloc entry point (G lanes per cell)
 //   RK attempt     k_attempt<S, KIND>                                   (stepRungeKuttaAdaptive,
 //                  mechanics.hpp:2406-2612; all stages of a cell in registers, the error
 //                  norm reduced in the same kernel, the step-size controller of
@@ -1523,9 +1527,9 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     const bool in_place = (KIND == MODE_TRIAL) && sp.learned;
     const bool from_backup = (KIND == MODE_RETRY || KIND == MODE_FINAL) && sp.learned;
 
-    // the first attempt of an iteration completes the pair force (k_pair_force left
-    // only the lower-neighbor share); under the reference controller the trial writes
-    // the total back for the rest, under the learned one every attempt gathers
+    // the first attempt of an iteration sums the cell's pair shares (pg.fused); under
+    // the reference controller the trial writes the total back for the rest, under the
+    // learned one every attempt sums them
     const bool do_gather = pg.fused && !commit &&
                            (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran) || sp.learned);
     double local_max = 0.0;

@@ -85,7 +85,7 @@ typedef struct abm_params {
     int precision;               /* ABM_PRECISION_FP64 or ABM_PRECISION_MIXED */
     int cap_cells;               /* device capacity in cells (>= the largest population) */
     int cap_neighbors_per_cell;  /* directed neighbor slots per cell (0 = default: 192 in 3-D, 64 in 2-D) */
-    int pair_lanes;              /* lanes per cell in the pair-force kernel: 4, 8, 16 or 32 (0 = 8) */
+    int pair_lanes;              /* lanes per cell of the no-alloc entry point's pair kernel: 4, 8, 16 or 32 (0 = 8) */
     int use_graphs;              /* 1 = capture the iteration in a CUDA graph */
     /* step-size control (no reference counterpart beyond ABM_CONTROLLER_REFERENCE) */
     int controller;              /* ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED */

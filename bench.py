@@ -68,6 +68,8 @@ def parse_args(argv=None):
     ap.add_argument("--growth-max-dt", type=float, default=1e-4, help="max_stepsize of the growth run (h)")
     ap.add_argument("--growth-max-seconds", type=float, default=600.0,
                     help="stop an arm of the growth run after this much device time")
+    ap.add_argument("--growth-arms", default="plain,chosen", help="arms of the growth run")
+    ap.add_argument("--weights", default=None, help="step-size network weights (.npz); default: the shipped ones")
     ap.add_argument("--replicates", type=int, default=256)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--tile", type=int, default=0, help="screened pair pass: CSR entries per block tile")
@@ -202,10 +204,13 @@ def sim_params(args, n, variant="plain"):
     return d
 
 
-def stepsize_weights():
+def stepsize_weights(path=None):
     """The shipped step-size network (trained on the GPU from reference-controller
-    logs, abm_b200/stepsize.py); trained here on the spot if it is missing."""
+    logs, abm_b200/stepsize.py), or the weights at `path`; trained here on the spot
+    if the shipped file is missing."""
     from abm_b200 import stepsize
+    if path:
+        return stepsize.load(path), "weights from %s" % os.path.basename(path)
     if os.path.exists(stepsize.WEIGHTS_FILE):
         return stepsize.load(), "shipped weights (%s)" % os.path.basename(stepsize.WEIGHTS_FILE)
     w, info = stepsize.train_protocol(stepsize.default_runs(), n_iters=1500, epochs=150)
@@ -455,7 +460,7 @@ def run_b200(args):
     if world > 1:
         dist_init("nccl")
     cells, info = workload(args.n, SEED + rank)
-    weights, weights_note = stepsize_weights()
+    weights, weights_note = stepsize_weights(args.weights)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
 
     head = args.variant
@@ -656,14 +661,15 @@ def run_growth(args):
     device = torch.device("cuda", local)
     if world > 1:
         dist_init("nccl")
-    weights, weights_desc = stepsize_weights()
+    weights, weights_desc = stepsize_weights(args.weights)
     sampler = ClockSampler(local)
     sampler.start()
     barrier(world)
-    arms = {v: grow_arm(args, v, weights, device, seed=7 + rank) for v in ("plain", "chosen")}
+    arms = {v: grow_arm(args, v, weights, device, seed=7 + rank) for v in args.growth_arms.split(",")}
     clocks = sampler.stop()
     ms = {v: reduce_max(1000.0 * a["device_s"], device, world) for v, a in arms.items()}
-    ch = arms["chosen"]
+    ch = arms.get("chosen") or arms[next(iter(arms))]
+    ms.setdefault("chosen", ms[next(iter(ms))])
     value = world * ch["cell_steps"] / (ms["chosen"] / 1000.0)
     line = {"metric": "3D growth founder -> %d cells: accepted cell-steps/s" % args.growth_target,
             "value": value, "unit": UNIT, "n_gpus": world, "steps": ch["accepted_steps"], "warmup": 0,
@@ -674,8 +680,9 @@ def run_growth(args):
                        "variant": "chosen", "parallelism": "replicas", "stepsize_network": weights_desc,
                        "l2": "state larger than L2 after ~30k cells (no flush)"},
             "arms": arms,
-            "chosen_over_plain": {"device_time": ms["plain"] / max(ms["chosen"], 1e-9),
-                                  "rk_evals": arms["plain"]["rk_evals"] / max(ch["rk_evals"], 1)},
+            "chosen_over_plain": ({"device_time": ms["plain"] / max(ms["chosen"], 1e-9),
+                                   "rk_evals": arms["plain"]["rk_evals"] / max(ch["rk_evals"], 1)}
+                                  if "plain" in arms and "chosen" in arms else None),
             "gpu_launches": None,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
     if rank == 0:

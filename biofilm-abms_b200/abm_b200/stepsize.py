@@ -84,6 +84,32 @@ def growing_colony(n, seed, growth_mean=1.5, growth_std=0.1, lmax=5.5):
     return cells
 
 
+def founder_colonies(sizes, seed=7, max_stepsize=1e-4, max_iters=20_000_000):
+    """Grow a 3-D colony from one founder cell (the 3-D driver's start, growth
+    ~ N(1.5, 0.1^2)/h, daughters split at ~ N(0.5, 0.01^2)) with the reference
+    controller and return a copy of its cells as it reaches each of `sizes`."""
+    from . import Simulation, workloads
+    kw = dict(GROWTH_KW, daughter_length_std=0.01)
+    sizes = sorted(sizes)
+    sim = Simulation(cap_cells=int(1.05 * sizes[-1]) + 4096, max_stepsize=max_stepsize, rng_seed=seed, **kw)
+    out = []
+    try:
+        sim.upload_cells(workloads.founder_3d())
+        sim.set_parents([-1])
+        sim.set_clock(0.0, 1e-6, 0)
+        sim.get_cell_neighbors()
+        done = 0
+        for target in sizes:
+            sim.set_cell_limit(target)
+            while sim.num_cells() < target and done < max_iters:
+                sim.iterate(4096, stats=False)
+                done += 4096
+            out.append(sim.download_cells())
+    finally:
+        sim.close()
+    return out
+
+
 def logged_run(cells, n_iters, controller=0, weights=None, max_stepsize=1e-4, log_capacity=None, **params):
     """Run n_iters iterations from `cells` with the feature log on; returns (rows, stats)."""
     from . import Simulation
@@ -123,14 +149,18 @@ def train_protocol(runs, n_iters=3000, epochs=200, lr=1e-3, seed=0, safety=0.9, 
     return w, info
 
 
-def default_runs():
+def default_runs(founders=True):
     """The logged runs behind the shipped weights: 3-D growth with division at
-    three colony sizes (error-limited, max_stepsize 1e-4) and the static 100k-density
-    state at max_stepsize 1e-6, each from its own seed."""
+    three colony sizes (error-limited, max_stepsize 1e-4), the static 100k-density
+    state at max_stepsize 1e-6, each from its own seed, and (founders) compact
+    colonies grown from one founder cell to 1,000 and 4,000 cells."""
     runs = []
     for n, seed in ((500, 11), (2000, 12), (8000, 13)):
         runs.append((growing_colony(n, seed), dict(max_stepsize=1e-4)))
     runs.append((growing_colony(20000, 14, growth_mean=0.0, growth_std=0.0, lmax=5.0), dict(max_stepsize=1e-6)))
+    if founders:
+        for cells in founder_colonies((1000, 4000)):
+            runs.append((cells, dict(max_stepsize=1e-4, daughter_length_std=0.01)))
     return runs
 
 
@@ -142,8 +172,10 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=3000)
     ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-founders", action="store_true", help="leave out the founder-grown colonies")
     a = ap.parse_args(argv)
-    w, info = train_protocol(default_runs(), n_iters=a.iters, epochs=a.epochs, seed=a.seed)
+    w, info = train_protocol(default_runs(founders=not a.no_founders), n_iters=a.iters, epochs=a.epochs,
+                             seed=a.seed)
     save(w, a.out, info=json.dumps(info))
     print(json.dumps(info))
 

@@ -314,3 +314,36 @@ def test_gpu_growth_and_division_loop(graphs):
         if i % 7 == 0 or co.shape[0] != n0:                      # a rebuild happened
             assert np.array_equal(sim.neighbors()[:, :2], o.neighbors()[:, :2])
     assert divided > 0
+
+
+@pytest.mark.parametrize("controller", [0, 1])
+def test_gpu_iterations_per_graph_change_nothing(controller):
+    # abm_iterate launches iter_k iterations per graph when it can (here 10, the largest of
+    # 10, 5, 4, 2 dividing iter_update_neighbors); the same 35 iterations launched one at a
+    # time must end bit for bit in the same state, divisions and rebuilds included
+    from abm_b200 import stepsize
+    cells = patch_state(400, 35)
+    rng = np.random.default_rng(5)
+    cells[:, 13] = rng.uniform(4.5, 5.55, size=len(cells))
+    cells[:30, 13] = 5.6 - rng.uniform(0.0, 2e-3, size=30)
+    cells[:, 14] = cells[:, 13] / 2
+    cells[:, 16] = rng.normal(1.5, 0.1, size=len(cells))
+    out = []
+    for per_call in (35, 1):
+        sim = abm_b200.Simulation(jkr_table=JKR, cap_cells=3 * len(cells), max_stepsize=1e-3,
+                                  iter_update_neighbors=10, controller=controller, **DIV_KW)
+        sim.upload_cells(cells)
+        if controller:
+            sim.set_stepsize_weights(stepsize.load())
+        sim.set_parents(-np.ones(len(cells), dtype=np.int32))
+        sim.set_clock(0.0, 1e-4, 0)
+        sim.get_cell_neighbors()
+        for _ in range(35 // per_call):
+            s = sim.iterate(per_call)
+        out.append((sim.download_cells(), sim.parents(), sim.clock(), s))
+        sim.close()
+    (ca, pa, ta, sa), (cb, pb, tb, sb) = out
+    assert sa["divisions"] > 0 and sa["rebuilds"] > 3
+    assert np.array_equal(ca, cb) and np.array_equal(pa, pb) and ta == tb
+    for k in ("iterations", "attempts", "retries", "rejected", "divisions", "rebuilds"):
+        assert sa[k] == sb[k], k

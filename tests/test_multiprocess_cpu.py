@@ -1,7 +1,7 @@
 """The multi-rank plumbing of bench.py on the CPU: world-size-2 `gloo` ranks for the
-max-over-ranks timing and the barrier, and the reference arm launched the way the
-driver launches N > 1 (torch.distributed.run, one process per rank), where rank 0
-alone times the host path and prints the one JSON line.  Multi-GPU is replicas only:
+max-over-ranks timing and the barrier, and the reference arm launched as a multi-GPU
+run is launched (torch.distributed.run, one process per rank), where rank 0 alone
+times the host path and prints the one JSON line.  Multi-GPU is replicas only:
 no collective touches the data path, so these are all the collectives there are."""
 import json
 import os

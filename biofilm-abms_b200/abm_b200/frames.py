@@ -1,0 +1,74 @@
+"""Frame and lineage files in the reference's text formats (writeCells / readCells /
+writeLineage / readLineage, utils.hpp:96-311), through the C ABI (abm_write_cells,
+abm_read_cells, abm_write_lineage, abm_read_lineage)."""
+import ctypes
+import os
+
+import numpy as np
+
+from . import LIB
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+LIB.abm_write_cells.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_char_p, _c_int_p, _c_int_p, ctypes.c_int]
+LIB.abm_read_cells.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p,
+                               ctypes.c_char_p, ctypes.c_int]
+LIB.abm_write_lineage.argtypes = [ctypes.c_char_p, _c_int_p, ctypes.c_int]
+LIB.abm_read_lineage.argtypes = [ctypes.c_char_p, _c_int_p, ctypes.c_int, _c_int_p]
+LIB.abm_io_last_error.restype = ctypes.c_char_p
+for _f in (LIB.abm_write_cells, LIB.abm_read_cells, LIB.abm_write_lineage, LIB.abm_read_lineage):
+    _f.restype = ctypes.c_int
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError("%s failed (%d): %s" % (what, rc, LIB.abm_io_last_error().decode()))
+
+
+def params_text(params):
+    """"key = value" lines: a dict in sorted key order (the reference keeps its
+    parameters in a std::map), or a sequence of (key, value) pairs in its order."""
+    items = sorted(params.items()) if isinstance(params, dict) else list(params or [])
+    return "".join("%s = %s\n" % (k, v) for k, v in items)
+
+
+def write_cells(path, cells, params=None, extra_cols=None, dims=3):
+    """writeCells: `extra_cols` maps column -> 0 (integer) or 1 (double), like the
+    reference's write_other_cols."""
+    a = np.asfortranarray(cells, dtype=np.float64)
+    n, ncols = a.shape
+    ec = sorted((extra_cols or {}).items())
+    cols = (ctypes.c_int * max(len(ec), 1))(*[c for c, _ in ec])
+    types = (ctypes.c_int * max(len(ec), 1))(*[t for _, t in ec])
+    _check(LIB.abm_write_cells(os.fsencode(path), a.ctypes.data, n, ncols, max(n, 1), dims,
+                               params_text(params).encode(), cols, types, len(ec)), "abm_write_cells")
+
+
+def read_cells(path):
+    """readCells: (cells (n, ncols) float64 Fortran order, params dict of strings)."""
+    p = os.fsencode(path)
+    n, nc = ctypes.c_int(), ctypes.c_int()
+    _check(LIB.abm_read_cells(p, None, 0, 0, ctypes.byref(n), ctypes.byref(nc), None, 0), "abm_read_cells")
+    cells = np.zeros((n.value, nc.value), dtype=np.float64, order="F")
+    size = os.path.getsize(path) + 1
+    buf = ctypes.create_string_buffer(size)
+    _check(LIB.abm_read_cells(p, cells.ctypes.data if cells.size else None, max(n.value, 1), max(nc.value, 1),
+                              ctypes.byref(n), ctypes.byref(nc), buf, size), "abm_read_cells")
+    params = dict(line.split(" = ", 1) for line in buf.value.decode().splitlines() if " = " in line)
+    return cells, params
+
+
+def write_lineage(path, parents):
+    """writeLineage: "i<TAB>parents[i]" lines."""
+    a = np.ascontiguousarray(parents, dtype=np.int32)
+    _check(LIB.abm_write_lineage(os.fsencode(path), a.ctypes.data_as(_c_int_p), len(a)), "abm_write_lineage")
+
+
+def read_lineage(path):
+    """readLineage: parents indexed by cell ID."""
+    p = os.fsencode(path)
+    n = ctypes.c_int()
+    _check(LIB.abm_read_lineage(p, None, 0, ctypes.byref(n)), "abm_read_lineage")
+    out = np.zeros(n.value, dtype=np.int32)
+    _check(LIB.abm_read_lineage(p, out.ctypes.data_as(_c_int_p), len(out), ctypes.byref(n)), "abm_read_lineage")
+    return out

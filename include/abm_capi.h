@@ -301,6 +301,31 @@ int abm_cell_cell_forces_noalloc(const abm_params* params, const double* d_cells
                                  double* d_dEdq, void* stream);
 const char* abm_noalloc_last_error(void);
 
+/* ---------------------------------------------------------------------------
+ * Frame and lineage files in the reference's text formats, so that a run driven
+ * through abm_iterate writes what runSimulation writes.  Host code, no device
+ * memory.  Arrays are column-major; abm_io_last_error() describes the last failure
+ * of this thread.
+ * ------------------------------------------------------------------------- */
+/* writeCells (utils.hpp:153-198 of both models): `params` holds "key = value" lines
+ * (each written as "# key = value"; NULL for none); the ID and group columns (3-D 0
+ * and 20, 2-D 0 and 16 by `dims`) are written as integers and the columns between
+ * them as doubles with 10 significant digits; further columns only if listed in
+ * extra_cols, as integers (extra_types 0) or doubles (1), like write_other_cols. */
+int abm_write_cells(const char* path, const double* cells, int n, int ncols, int ld, int dims,
+                    const char* params, const int* extra_cols, const int* extra_types, int n_extra);
+/* readCells (utils.hpp:96-139): rows into `cells` (column-major, leading dimension
+ * cap_rows), parameters into `params` as "key = value" lines (may be NULL).  With
+ * cells == NULL only *n and *ncols are set (the sizes to allocate). */
+int abm_read_cells(const char* path, double* cells, int cap_rows, int cap_cols, int* n, int* ncols,
+                   char* params, int params_cap);
+/* writeLineage (utils.hpp:296-311): "i<TAB>parents[i]" for i < n. */
+int abm_write_lineage(const char* path, const int* parents, int n);
+/* readLineage (utils.hpp:265-288): parents[child] = parent; *n = largest child ID + 1.
+ * With parents == NULL only *n is set. */
+int abm_read_lineage(const char* path, int* parents, int cap, int* n);
+const char* abm_io_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

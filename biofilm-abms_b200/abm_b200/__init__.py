@@ -198,7 +198,8 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
             "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags "
             "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "
-            "abm_batch_destroy abm_batch_last_error abm_autotune_pair_tile").split()
+            "abm_batch_destroy abm_batch_last_error abm_autotune_pair_tile abm_write_cells abm_read_cells "
+            "abm_write_lineage abm_read_lineage abm_io_last_error").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40

@@ -158,6 +158,9 @@ def _load():
         "abm_graph_info": ([vp], ctypes.c_char_p),
         "abm_cell_cell_forces_noalloc": ([P(AbmParams), vp, i, i, i, vp, vp, i, dp, dp, i, vp, vp], i),
         "abm_noalloc_last_error": ([], ctypes.c_char_p),
+        "abm_set_frames": ([vp, d, i], i),
+        "abm_frames_taken": ([vp, ip], i),
+        "abm_download_frame": ([vp, i, vp, i, ip, dp, ip, ip], i),
         "abm_iterate": ([vp, i, i, P(AbmStats)], i),
         "abm_get_stats": ([vp, P(AbmStats)], i),
         "abm_profile_iterations": ([vp, i, P(AbmProfile)], i),
@@ -199,7 +202,8 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags "
             "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "
             "abm_batch_destroy abm_batch_last_error abm_autotune_pair_tile abm_write_cells abm_read_cells "
-            "abm_write_lineage abm_read_lineage abm_io_last_error").split()
+            "abm_write_lineage abm_read_lineage abm_io_last_error abm_set_frames abm_frames_taken "
+            "abm_download_frame").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
@@ -413,6 +417,30 @@ class Simulation:
         s = AbmStats()
         self._check(LIB.abm_get_stats(self._ctx, ctypes.byref(s)), "abm_get_stats")
         return s.as_dict()
+
+    # ---- frames of the device-resident loop (runSimulation's dt_write writes) ----
+    def set_frames(self, dt_write, slots=8):
+        """Mark a frame after every accepted step whose time crosses a multiple of
+        dt_write (simulation.hpp:2025-2028), kept in a ring of `slots` device snapshots."""
+        self._check(LIB.abm_set_frames(self._ctx, float(dt_write), int(slots)), "abm_set_frames")
+
+    def frames_taken(self):
+        k = ctypes.c_int()
+        self._check(LIB.abm_frames_taken(self._ctx, ctypes.byref(k)), "abm_frames_taken")
+        return k.value
+
+    def download_frame(self, index):
+        """(cells, t, iteration, lineage length) of frame `index`."""
+        n, it, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        t = ctypes.c_double()
+        self._check(LIB.abm_download_frame(self._ctx, int(index), None, 1, ctypes.byref(n), ctypes.byref(t),
+                                           ctypes.byref(it), ctypes.byref(npar)), "abm_download_frame")
+        cells = np.zeros((n.value, self.ncols), dtype=np.float64, order="F")
+        if n.value:
+            self._check(LIB.abm_download_frame(self._ctx, int(index), cells.ctypes.data, n.value, ctypes.byref(n),
+                                               ctypes.byref(t), ctypes.byref(it), ctypes.byref(npar)),
+                        "abm_download_frame")
+        return cells, t.value, it.value, npar.value
 
     def set_cell_limit(self, n_max):
         """Stop on the device once the population reaches n_max (terminate(), simulation.hpp:1600-1615)."""

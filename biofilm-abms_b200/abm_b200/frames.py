@@ -72,3 +72,20 @@ def read_lineage(path):
     out = np.zeros(n.value, dtype=np.int32)
     _check(LIB.abm_read_lineage(p, out.ctypes.data_as(_c_int_p), len(out), ctypes.byref(n)), "abm_read_lineage")
     return out
+
+
+def write_frames(sim, outprefix, params=None, start=0, extra_cols=None, dims=3):
+    """Write frames start .. taken-1 of a Simulation with frames on, as runSimulation
+    writes at its dt_write crossings (simulation.hpp:2045-2058): "<outprefix>_iter<i>.txt"
+    with the parameters plus t_curr, then "<outprefix>_lineage.txt" with the lineage up
+    to the last frame written.  Returns the index of the next frame to write."""
+    taken = sim.frames_taken()
+    params = dict(params or {})
+    n_parents = None
+    for k in range(start, taken):
+        cells, t, it, n_parents = sim.download_frame(k)
+        params["t_curr"] = "%.10g" % t                 # floatToString(t), simulation.hpp:66-72
+        write_cells("%s_iter%d.txt" % (outprefix, it), cells, params, extra_cols, dims)
+    if n_parents is not None:
+        write_lineage("%s_lineage.txt" % outprefix, np.asarray(sim.parents())[:n_parents])
+    return taken

@@ -57,6 +57,12 @@ struct abm_ctx {
     float* log_buf = nullptr;        // stepsize_log_capacity rows of MLP_LOG_COLS floats
     double4* stat_part = nullptr;    // per-block feature partials of the final attempt
     int *order = nullptr, *order_flag = nullptr, *order_pos = nullptr;   // attempt order (3-D)
+    // frames: a ring of frame_slots snapshots of the cells (abm_set_frames)
+    int frame_slots = 0;
+    Geom* snap_geom = nullptr;
+    Vel* snap_vel = nullptr;
+    Phys* snap_phys = nullptr;
+    FrameInfo* frame_info = nullptr;
     bool mlp_loaded = false;
     // 2-D model
     int dims = 3;
@@ -139,7 +145,7 @@ static void free_all(abm_ctx* c)
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
-                    c->order_pos};
+                    c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -496,6 +502,86 @@ int abm_download_cells(abm_ctx* c, double* cm, int ld)
     return ABM_OK;
 }
 
+// frames (simulation.hpp:2025-2058): dt_write > 0 and slots > 0 turn them on
+__global__ void k_set_frames(Ctrl* c, double dt_write)
+{
+    c->dt_write = dt_write;
+    c->frame_due = 0;
+    c->frames_taken = 0;
+    c->frame_blocks = 0u;
+}
+
+int abm_set_frames(abm_ctx* c, double dt_write, int slots)
+{
+    if (!c || slots < 0 || !(dt_write >= 0)) return ABM_ERR_ARG;
+    const bool on = dt_write > 0 && slots > 0;
+    if (!on) slots = 0;
+    if (slots != c->frame_slots)
+    {
+        CK(cudaStreamSynchronize(c->st));
+        cudaFree(c->snap_geom); cudaFree(c->snap_vel); cudaFree(c->snap_phys); cudaFree(c->frame_info);
+        c->snap_geom = nullptr; c->snap_vel = nullptr; c->snap_phys = nullptr; c->frame_info = nullptr;
+        if (slots > 0)
+        {
+            const size_t m = (size_t)slots * c->cap;
+            CK(cudaMalloc(&c->snap_geom, m * sizeof(Geom)));
+            CK(cudaMalloc(&c->snap_vel, m * sizeof(Vel)));
+            CK(cudaMalloc(&c->snap_phys, m * sizeof(Phys)));
+            CK(cudaMalloc(&c->frame_info, (size_t)slots * sizeof(FrameInfo)));
+        }
+        c->frame_slots = slots;
+        drop_iteration_graphs(c);          // the snapshot is a node of the iteration graph
+    }
+    k_set_frames<<<1, 1, 0, c->st>>>(c->ctrl, on ? dt_write : 0.0);
+    CK(cudaGetLastError());
+    return ABM_OK;
+}
+
+int abm_frames_taken(abm_ctx* c, int* taken)
+{
+    if (!c || !taken) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *taken = h.frames_taken;
+    return ABM_OK;
+}
+
+int abm_download_frame(abm_ctx* c, int index, double* cm, int ld, int* n, double* t, int* iter, int* n_parents)
+{
+    if (!c || !n || index < 0) return ABM_ERR_ARG;
+    if (c->frame_slots <= 0) return fail(c, ABM_ERR_STATE, "frames are off (abm_set_frames)");
+    int taken = 0;
+    int rc = abm_frames_taken(c, &taken);
+    if (rc) return rc;
+    if (index >= taken) return fail(c, ABM_ERR_ARG, "no such frame yet");
+    if (index < taken - c->frame_slots)
+        return fail(c, ABM_ERR_CAPACITY, "the frame was overwritten: download frames more often or use more slots");
+    const int slot = index % c->frame_slots;
+    FrameInfo f;
+    CK(cudaMemcpy(&f, c->frame_info + slot, sizeof(FrameInfo), cudaMemcpyDeviceToHost));
+    *n = f.n;
+    if (t) *t = f.t;
+    if (iter) *iter = f.iter;
+    if (n_parents) *n_parents = f.n_parents;
+    if (!cm) return ABM_OK;                 // sizes only
+    if (ld < f.n) return fail(c, ABM_ERR_ARG, "ld smaller than the frame's cell count");
+    if (f.n > 0)
+    {
+        const size_t off = (size_t)slot * c->cap;
+        if (c->dims == 2)
+            launch_cells_to_colmajor_2d(c->snap_geom + off, c->snap_vel + off, c->snap_phys + off, f.n, c->ncols,
+                                        f.n, c->staging, c->st);
+        else
+            launch_cells_to_colmajor(c->snap_geom + off, c->snap_vel + off, c->snap_phys + off, f.n, c->ncols, f.n,
+                                     c->has_gamma, c->staging, c->st);
+        CK(cudaMemcpy2DAsync(cm, (size_t)ld * sizeof(double), c->staging, (size_t)f.n * sizeof(double),
+                             (size_t)f.n * sizeof(double), c->ncols, cudaMemcpyDeviceToHost, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return ABM_OK;
+}
+
 int abm_get_num_cells(abm_ctx* c, int* n)
 {
     if (!c || !n) return ABM_ERR_ARG;
@@ -632,10 +718,18 @@ static void enqueue_attempts(abm_ctx* c)
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
 }
 
+// the snapshot of a frame marked by this iteration's accepted step (frames enabled)
+static void enqueue_frame_snapshot(abm_ctx* c)
+{
+    launch_frame_snapshot(c->geom, c->vel, c->phys, c->ctrl, c->snap_geom, c->snap_vel, c->snap_phys,
+                          c->frame_info, c->frame_slots, c->cap, c->st);
+}
+
 static void enqueue_iteration(abm_ctx* c)
 {
     enqueue_loop_pair_force(c);
     enqueue_attempts(c);
+    if (c->frame_slots > 0) enqueue_frame_snapshot(c);
 }
 
 static int capture(abm_ctx* c, void (*fn)(abm_ctx*), cudaGraphExec_t* exec)
@@ -794,21 +888,29 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
         rc = add_conditional(c, G, deps, h_run, cudaGraphCondTypeIf, &body);
         if (rc) return rc;
         std::vector<cudaGraphNode_t> bd;
-        return capture_into(c, body, bd, [&]() {
+        rc = capture_into(c, body, bd, [&]() {
             for (int r = 0; r < c->p.max_tries_update_stepsize; ++r) retry_attempt(0);
             final_attempt();
         });
+        if (rc) return rc;
     }
-    if (retries)
+    else
     {
-        cudaGraph_t body;
-        rc = add_conditional(c, G, deps, h_retry, cudaGraphCondTypeWhile, &body);
-        if (rc) return rc;
-        std::vector<cudaGraphNode_t> bd;
-        rc = capture_into(c, body, bd, [&]() { retry_attempt(1); });
+        if (retries)
+        {
+            cudaGraph_t body;
+            rc = add_conditional(c, G, deps, h_retry, cudaGraphCondTypeWhile, &body);
+            if (rc) return rc;
+            std::vector<cudaGraphNode_t> bd;
+            rc = capture_into(c, body, bd, [&]() { retry_attempt(1); });
+            if (rc) return rc;
+        }
+        rc = capture_into(c, G, deps, final_attempt);
         if (rc) return rc;
     }
-    return capture_into(c, G, deps, final_attempt);
+    // frames: the snapshot of a frame the accepted step marked
+    if (c->frame_slots > 0) return capture_into(c, G, deps, [&]() { enqueue_frame_snapshot(c); });
+    return ABM_OK;
 }
 
 static int instantiate_iterations(abm_ctx* c, int k, cudaGraphExec_t* exec)

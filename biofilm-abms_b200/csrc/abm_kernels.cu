@@ -1440,6 +1440,14 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
         c->t += c->dt;
         c->iter += 1;
         c->iterations += 1;
+        // a frame is due when the time has just passed a multiple of dt_write
+        // (simulation.hpp:2025-2028)
+        if (c->dt_write > 0)
+        {
+            const double t_old_factor = fmod(c->t - c->dt + 1e-12, c->dt_write);
+            const double t_new_factor = fmod(c->t + 1e-12, c->dt_write);
+            if (t_old_factor > t_new_factor) c->frame_due = 1;
+        }
         c->mode = MODE_TRIAL;
         c->tries = 0;
         c->attempt = 0;
@@ -1789,6 +1797,56 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         if ((use_cond & 2) && KIND == MODE_TRIAL)
             cudaGraphSetConditional((cudaGraphConditionalHandle)cond_run, ctrl->mode != MODE_COMMIT ? 1u : 0u);
     }
+}
+
+// Frame snapshot, at the end of an iteration: when the accepted step marked a frame,
+// every cell's records go to ring slot frames_taken % slots, and the last block
+// records the frame's time, iteration, cell count and lineage length.  The loop
+// keeps running; the host downloads the slots when it writes the frames.
+__global__ void k_frame_snapshot(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
+                                 const Phys* __restrict__ phys, Ctrl* ctrl, Geom* snap_geom, Vel* snap_vel,
+                                 Phys* snap_phys, FrameInfo* info, int slots, int cap_cells)
+{
+    __shared__ bool last;
+    // frame_due changes only in the last block below, after every block has passed here
+    if (!ctrl->frame_due) return;
+    const int n = ctrl->n;
+    const size_t off = (size_t)(ctrl->frames_taken % slots) * cap_cells;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        snap_geom[off + i] = geom[i];
+        snap_vel[off + i] = vel[i];
+        snap_phys[off + i] = phys[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        last = atomicAdd(&ctrl->frame_blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        FrameInfo f;
+        f.t = ctrl->t;
+        f.iter = ctrl->iter;
+        f.n = n;
+        f.n_parents = ctrl->n_parents;
+        f.pad = 0;
+        info[ctrl->frames_taken % slots] = f;
+        ctrl->frames_taken += 1;
+        ctrl->frame_due = 0;
+        ctrl->frame_blocks = 0u;
+    }
+}
+
+void launch_frame_snapshot(const Geom* geom, const Vel* vel, const Phys* phys, Ctrl* ctrl, Geom* snap_geom,
+                           Vel* snap_vel, Phys* snap_phys, FrameInfo* info, int slots, int cap_cells,
+                           cudaStream_t st)
+{
+    const int blocks = max(min(cdiv(cap_cells, 256), 4 * 148), 1);
+    k_frame_snapshot<<<blocks, 256, 0, st>>>(geom, vel, phys, ctrl, snap_geom, snap_vel, snap_phys, info, slots,
+                                             cap_cells);
 }
 
 // Attempt order (3-D): the cells whose velocity takes the full surface solve

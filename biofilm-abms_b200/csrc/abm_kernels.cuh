@@ -84,6 +84,11 @@ struct Ctrl {
     int screen_valid;                   // 0 after a rebuild, an upload or a division
     unsigned int surv_blocks;           // last-block counter of the pair pass
     int n_order;                        // cells covered by the attempt order (0: index order)
+    // frames: an accepted step whose time crosses a multiple of dt_write marks a frame,
+    // which the snapshot kernel at the end of the iteration copies into a ring slot
+    double dt_write;                    // 0: no frames
+    int frame_due, frames_taken;
+    unsigned int frame_blocks;          // last-block counter of the snapshot kernel
     double drift;                       // sum over accepted steps of the max segment motion
     unsigned long long drift_bits;      // block maxima of the running attempt (ordered bits)
 };
@@ -220,6 +225,15 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                     int dims = 3, unsigned long long cond_run = 0);
 // accepted proposal of the learned controller: candidate -> state (no-op otherwise)
 // the attempt order of the cells (3-D): full surface solve first (made at every rebuild)
+// one frame of the ring: the state after the accepted step that marked it
+struct FrameInfo {
+    double t;
+    int iter, n, n_parents, pad;
+};
+// copies the cells into ring slot frames_taken % slots when a frame is due
+void launch_frame_snapshot(const Geom* geom, const Vel* vel, const Phys* phys, Ctrl* ctrl, Geom* snap_geom,
+                           Vel* snap_vel, Phys* snap_phys, FrameInfo* info, int slots, int cap_cells,
+                           cudaStream_t st);
 void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int* flag, int* pos,
                           int* block_sums, int* order, int cap_cells, cudaStream_t st);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,

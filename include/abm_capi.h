@@ -326,6 +326,22 @@ int abm_write_lineage(const char* path, const int* parents, int n);
 int abm_read_lineage(const char* path, int* parents, int cap, int* n);
 const char* abm_io_last_error(void);
 
+/* Frames of a device-resident run (runSimulation's dt_write writes,
+ * simulation.hpp:2025-2058): with dt_write > 0 and slots > 0, an accepted step
+ * whose time crosses a multiple of dt_write marks a frame, and the end of that
+ * iteration copies the cells into a ring of `slots` snapshots on the device, so the
+ * loop keeps running without host round trips.  Turning frames on or off, or
+ * changing the slot count, rebuilds the iteration graph; the frame count restarts at
+ * 0.  dt_write = 0 or slots = 0 turns them off. */
+int abm_set_frames(abm_ctx* ctx, double dt_write, int slots);
+/* frames marked since abm_set_frames (the ring keeps the last `slots` of them) */
+int abm_frames_taken(abm_ctx* ctx, int* taken);
+/* frame `index` (0-based): its cells (column-major, cells-array layout; NULL for the
+ * sizes only), cell count, time, iteration and lineage length at that step.
+ * ABM_ERR_CAPACITY when the ring has overwritten it. */
+int abm_download_frame(abm_ctx* ctx, int index, double* cells, int ld, int* n, double* t, int* iter,
+                       int* n_parents);
+
 #ifdef __cplusplus
 }
 #endif

@@ -332,7 +332,9 @@ const char* abm_io_last_error(void);
  * iteration copies the cells into a ring of `slots` snapshots on the device, so the
  * loop keeps running without host round trips.  Turning frames on or off, or
  * changing the slot count, rebuilds the iteration graph; the frame count restarts at
- * 0.  dt_write = 0 or slots = 0 turns them off. */
+ * 0.  dt_write = 0 or slots = 0 turns them off.  A context in a batch takes its
+ * frame setting into the batch's graph at abm_batch_create: set frames before
+ * creating the batch and leave them unchanged while the batch exists. */
 int abm_set_frames(abm_ctx* ctx, double dt_write, int slots);
 /* frames marked since abm_set_frames (the ring keeps the last `slots` of them) */
 int abm_frames_taken(abm_ctx* ctx, int* taken);

@@ -318,4 +318,18 @@ void oracle_area_integrals(double rz, double nz, double R, double half_l, double
     area_integrals(rz, nz, R, half_l, ss, out[0], out[1], out[2]);
 }
 
+// the auxiliary integrals of integrals.hpp (integral1, integral2, integral4-6), for the
+// reference's own quadrature tests (test/src/testIntegrals.cpp)
+double oracle_integral1(double rz, double nz, double R, double half_l, double gamma, double ss)
+{
+    return integral1(rz, nz, R, half_l, gamma, ss);
+}
+double oracle_integral2(double rz, double nz, double R, double half_l, double gamma, double ss)
+{
+    return integral2(rz, nz, R, half_l, gamma, ss);
+}
+double oracle_integral4(double nz, double half_l, double ss) { return integral4(nz, half_l, ss); }
+double oracle_integral5(double nz, double half_l, double ss) { return integral5(nz, half_l, ss); }
+double oracle_integral6(double nz, double half_l, double ss) { return integral6(nz, half_l, ss); }
+
 }   // extern "C"

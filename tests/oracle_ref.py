@@ -78,6 +78,11 @@ def _load():
         "oracle_rng_uniform": ([ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
                                 ctypes.c_uint, ctypes.c_uint], d),
         "oracle_area_integrals": ([d, d, d, d, dp], None),
+        "oracle_integral1": ([d, d, d, d, d, d], d),
+        "oracle_integral2": ([d, d, d, d, d, d], d),
+        "oracle_integral4": ([d, d, d], d),
+        "oracle_integral5": ([d, d, d], d),
+        "oracle_integral6": ([d, d, d], d),
         "oracle_det_log": ([d], d),
         "oracle_det_sincos": ([d, dp, dp], None),
     }

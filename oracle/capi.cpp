@@ -332,4 +332,25 @@ double oracle_integral4(double nz, double half_l, double ss) { return integral4(
 double oracle_integral5(double nz, double half_l, double ss) { return integral5(nz, half_l, ss); }
 double oracle_integral6(double nz, double half_l, double ss) { return integral6(nz, half_l, ss); }
 
+// cellSurfaceRepulsionForces (kind 0, mechanics.hpp:673-780) or cellSurfaceAdhesionForces
+// (kind 1, mechanics.hpp:800-910) of one cell with center height rz, orientation
+// (nx, 0, nz), half-length half_l and adhesion energy density sigma0, treated as
+// horizontal when nz < nz_threshold; the six generalized forces go to out6.  This is the
+// single-cell form the reference's own tests call (testCellSurfaceRepulsionForces.cpp,
+// testCellSurfaceAdhesionForces.cpp), with ss = (R - rz) / nz.
+int oracle_surface_forces(int kind, double rz, double nx, double nz, double half_l, double sigma0,
+                          double R, double E0, double nz_threshold, double* out6)
+{
+    if (kind != 0 && kind != 1) return 1;
+    Cells cells(1, NCOLS_REQUIRED_3D);
+    cells(0, C_RZ) = rz; cells(0, C_NX) = nx; cells(0, C_NZ) = nz;
+    cells(0, C_L) = 2 * half_l; cells(0, C_HALF_L) = half_l; cells(0, C_SIGMA0) = sigma0;
+    std::vector<double> ss(1, sstar(rz, nz, R));
+    std::vector<int> assume_2d(1, nz < nz_threshold);
+    Arr6 f = kind == 0 ? cell_surface_repulsion_forces(cells, ss, R, E0, assume_2d, false)
+                       : cell_surface_adhesion_forces(cells, ss, R, assume_2d, false);
+    for (int k = 0; k < 6; ++k) out6[k] = f[k];
+    return 0;
+}
+
 }   // extern "C"

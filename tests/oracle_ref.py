@@ -83,6 +83,7 @@ def _load():
         "oracle_integral4": ([d, d, d], d),
         "oracle_integral5": ([d, d, d], d),
         "oracle_integral6": ([d, d, d], d),
+        "oracle_surface_forces": ([i, d, d, d, d, d, d, d, d, dp], i),
         "oracle_det_log": ([d], d),
         "oracle_det_sincos": ([d, dp, dp], None),
     }

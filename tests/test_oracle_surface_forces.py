@@ -13,7 +13,8 @@ the other four forces are zero.
 The reference differentiates in 100-digit MPFR with a step of 1e-50; in doubles a
 Richardson-extrapolated central difference stands in, so the bar is a relative 1e-8
 instead of an absolute 1e-45.  The horizontal branch (nz below the threshold) is checked
-against its closed forms and against the tilted branch at a small nz."""
+against its closed forms and against the tilted branch at a small nz, and the single-cell
+conservative forces against the sum of both energies (testConservativeForces.cpp)."""
 import ctypes
 import math
 
@@ -101,3 +102,35 @@ def test_horizontal_branch(kind):
         tilted = forces(kind, rz, nz=1e-6)     # above the threshold: the general branch
         assert abs(tilted[2] - expect) < REL * abs(expect), (depth, tilted[2], expect)
     assert np.all(forces(kind, R + 0.01, nz=0.0) == 0)   # a horizontal cell clear of the surface
+
+
+def test_conservative_forces_of_a_single_cell():
+    """getConservativeForces for one cell and no neighbors (testConservativeForces.cpp:80-163):
+    eleven orientations from horizontal to vertical, each overlapping the surface by 0.2 R.
+    The x, y forces and torques are zero; the z force and nz torque are minus the
+    derivatives of the repulsion plus adhesion energies, and for the horizontal cell
+    2 E0 (R - rz) l - sigma0 sqrt(R) l / (2 sqrt(R - rz)) and 0."""
+    import abm_b200
+    _, p = abm_b200.make_params(adhesion_mode=0, nz_threshold=NZ_THRESHOLD, no_surface=0)
+    p["R"], p["E0"] = R, E0
+    total = lambda rz, nz: repulsion_energy(rz, nz) + adhesion_energy(rz, nz)
+    for j in range(11):
+        angle = math.pi / 2 * j / 10
+        nz = math.sin(angle)
+        rz = R + HALF_L * nz - 0.2 * R
+        cells = np.zeros((1, 21))
+        cells[0, 3:7] = [rz, math.cos(angle), 0.0, nz]
+        cells[0, 13], cells[0, 14], cells[0, 19] = 2 * HALF_L, HALF_L, SIGMA0
+        o = orc.Oracle(p)
+        o.set_cells(cells)
+        o.build_neighbors()
+        f = o.conservative_forces()[0]
+        assert f[0] == 0 and f[1] == 0 and f[3] == 0 and f[4] == 0
+        if nz > 0:
+            target = (-derivative(lambda x: total(x, nz), rz), -derivative(lambda x: total(rz, x), nz))
+        else:
+            depth, length = R - rz, 2 * HALF_L
+            target = (2 * E0 * depth * length - 0.5 * SIGMA0 * math.sqrt(R) * length / math.sqrt(depth), 0.0)
+        scale = max(abs(target[0]), abs(target[1]), 1.0)
+        assert abs(f[2] - target[0]) < REL * scale, (angle, f[2], target[0])
+        assert abs(f[5] - target[1]) < REL * scale, (angle, f[5], target[1])

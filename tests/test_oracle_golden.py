@@ -2,7 +2,8 @@
 
 Golden vectors: tests/golden/dist3d_cases.json, extracted by make_golden.py
 from ABM-3d/ABM-3d-cpp/test/src/testDistBetweenCells.cpp (tolerance 1e-8,
-as asserted there).  JKR invariants: testJKR.cpp:26-83.  Single-cell
+as asserted there).  JKR invariants: testJKR.cpp:26-83; JKR radius against the
+closed form: testContactArea.cpp:102-161.  Single-cell
 stationarity: testHorizontal.cpp:79-126.  Velocity identity M v = F + 2 lambda n:
 testVelocities.cpp:40-131.
 """
@@ -84,6 +85,45 @@ def test_oracle_jkr_adhesion_invariants():
             assert a >= math.sqrt(R * delta)
             rec = a * a / R - 2 * math.sqrt(math.pi * gamma * a / E0)
             assert abs(rec - delta) <= 1e-13 * max(1.0, a * a / R)
+
+
+def _parteli_roots(delta, R, E, gamma):
+    """Closed-form roots of a^4 - 2 R delta a^2 - (4 pi gamma R^2 / E) a + R^2 delta^2 = 0
+    (Parteli et al. 2014), as testContactArea.cpp:138-150 writes them, in 60-digit mpmath."""
+    import mpmath as mp
+    with mp.workdps(60):
+        d, R, E, g = mp.mpf(delta), mp.mpf(R), mp.mpf(E), mp.mpf(gamma)
+        c0, c1, c2 = R * R * d * d, -4 * mp.pi * g * R * R / E, -2 * R * d
+        P = -c2 * c2 / 12 - c0
+        Q = -c2 ** 3 / 108 + c0 * c2 / 3 - c1 * c1 / 8
+        U = mp.cbrt(-Q / 2 + mp.sqrt(Q * Q / 4 + P ** 3 / 27))
+        s = -5 * c2 / 6 + (U - P / (3 * U))
+        w = mp.sqrt(c2 + 2 * s)
+        root = mp.sqrt(w * w - 4 * (c2 + s + c1 / (2 * w)))
+        poly = lambda a: c0 + c1 * a + c2 * a * a + a ** 4
+        return (w + root) / 2, (w - root) / 2, poly
+
+
+def test_oracle_jkr_radius_matches_the_closed_form():
+    # testContactArea.cpp:102-161 (jkrContactRadius): delta 0.1, R 0.8, E 3900, gamma 100; the
+    # larger root exceeds the Hertz radius, zeroes the quartic and equals Parteli's a1 to 1e-15.
+    # The table uses only the larger root (simulation.hpp:86-104), so the smaller one is not
+    # compared.  The same bar over a grid of radii, adhesion energies and overlaps, for the
+    # oracle and for the library's host solver (abm_jkr_contact_radius).
+    import abm_b200
+    import mpmath as mp
+    a1, a2, poly = _parteli_roots(0.1, 0.8, 3900.0, 100.0)
+    a = orc.LIB.oracle_jkr_contact_radius(0.1, 0.8, 3900.0, 100.0)
+    assert a - math.sqrt(0.8 * 0.1) > 1e-15 and a2 > 1e-15
+    with mp.workdps(60):
+        assert abs(poly(mp.mpf(a))) < 1e-15
+    assert abs(a - a1) < 1e-15
+    for R in (0.4, 0.8):
+        for gamma in (1.0, 10.0, 100.0, 1000.0):
+            for delta in (1e-4, 0.01, 0.1, 0.3, 0.6):
+                a1, _, _ = _parteli_roots(delta, R, 3900.0, gamma)
+                assert abs(orc.LIB.oracle_jkr_contact_radius(delta, R, 3900.0, gamma) - a1) < 1e-15
+                assert abs(abm_b200.jkr_contact_radius(delta, R, 3900.0, gamma) - a1) < 1e-15
 
 
 def test_oracle_jkr_table_mesh():

@@ -14,9 +14,13 @@ from the reference's simulation tests, restated in today's column layout (indice
                              without asserting them; here they are asserted, together with
                              the closed-form Hertz decay of the overlap for the arrangements
                              where the force stays on one line.
+  testSkew.cpp:78-331        one cell tilted at ten angles, barely and deeply in contact:
+                             it ends at rest, horizontal or vertical as the reference's
+                             energy rule says, at the analytic height, to 1e-8; clear of
+                             the surface, it stays where it is.
 
-The reference's step cap (1e-7), step floor (1e-9), error bound (1e-10) and iteration
-counts are kept, except that the just-touching vertical cell runs 60000 iterations
+The reference's step caps (1e-7; 1e-6 for the tilted cell), step floors, error bound (1e-10)
+and iteration counts are kept, except that the just-touching vertical cell runs 60000 iterations
 instead of 10000: under the 1e-10 bound its fall from first contact takes steps of a
 few 1e-9 and needs that many to settle."""
 import math
@@ -31,11 +35,13 @@ R, RCELL, HALF_L, E0, SIGMA0 = 0.8, 0.5, 0.5, 3900.0, 100.0
 
 def params(**kw):
     import abm_b200
-    _, p = abm_b200.make_params(adhesion_mode=0, max_stepsize=1e-7, min_stepsize=1e-9, max_error_allowed=1e-10,
-                                min_error=1e-30, max_tries_update_stepsize=3, iter_update_stepsize=1,
-                                iter_update_neighbors=100, nz_threshold=1e-20, cell_surface_coulomb_coeff=0.0,
-                                L0=2 * HALF_L, Ldiv=2 * (R + 2 * HALF_L), neighbor_threshold=2 * (2 * R + 2 * HALF_L),
-                                Rcell=RCELL, E0=E0, Ecell=3900000.0, growth_mean=0.0, growth_std=0.0, **kw)
+    args = dict(adhesion_mode=0, max_stepsize=1e-7, min_stepsize=1e-9, max_error_allowed=1e-10,
+                min_error=1e-30, max_tries_update_stepsize=3, iter_update_stepsize=1,
+                iter_update_neighbors=100, nz_threshold=1e-20, cell_surface_coulomb_coeff=0.0,
+                L0=2 * HALF_L, Ldiv=2 * (R + 2 * HALF_L), neighbor_threshold=2 * (2 * R + 2 * HALF_L),
+                Rcell=RCELL, E0=E0, Ecell=3900000.0, growth_mean=0.0, growth_std=0.0)
+    args.update(kw)
+    _, p = abm_b200.make_params(**args)
     return p
 
 
@@ -113,3 +119,51 @@ def test_two_cell_simulations(d):
             k = 2 * (4.0 / 3.0) * E0 * math.sqrt(R / 2) / (eta0 * 2 * HALF_L)
             expect = ((2 * R - d) ** -0.5 + 0.5 * k * t) ** -2
             assert abs((2 * R - dist) - expect) < 1e-2 * expect, (name, 2 * R - dist, expect)
+
+
+def more_adhesive_than_repulsive(rz, nz):
+    """testSkew.cpp:46-73 (moreAdhesiveThanRepulsive), the reference's rule for which way a tilted
+    cell ends: the adhesion energy -sigma0 areaIntegral1 against the repulsion energy."""
+    if nz > 1e-20:
+        ss = (R - rz) / nz
+        i1 = orc.LIB.oracle_integral1(rz, nz, R, HALF_L, 2.0, ss)
+        i2 = orc.LIB.oracle_integral1(rz, nz, R, HALF_L, 1.5, ss)
+        e_rep = E0 * math.sqrt(R) * (R ** -0.5 * (1 - nz * nz) * i1 + 4.0 / 3.0 * nz * nz * i2)
+        area = np.zeros(3)
+        orc.LIB.oracle_area_integrals(rz, nz, R, HALF_L, area.ctypes.data_as(orc.ctypes.POINTER(orc.ctypes.c_double)))
+        return -SIGMA0 * area[0] >= e_rep
+    return rz >= R * (1 - (0.25 * SIGMA0 / (R * E0)) ** (2.0 / 3.0))
+
+
+@pytest.mark.parametrize("i", range(10))
+def test_skew_cell(i):
+    """testSkew.cpp:78-331: a cell tilted at pi/2 (i + 1)/10, overlapping the surface by 0.001 R
+    and by 0.2 R at its lower end, ends at rest either horizontal at R (1 - (sigma0/(4 R E0))^(2/3))
+    or vertical at half_l + R (1 - (3 pi sigma0/(4 R E0))^(2/3)), as the reference's rule says,
+    to 1e-8; 0.01 R clear of the surface, it does not move.  The reference runs up to 1e6 iterations at steps of at most 1e-6; the run here
+    stops once every velocity is below 1e-9, within the same budget."""
+    p = params(max_stepsize=1e-6, min_stepsize=1e-8)
+    angle = math.pi / 2 * (i + 1) / 10
+    for max_overlap in (0.001 * R, 0.2 * R, -0.01 * R):
+        rz = R + HALF_L * math.sin(angle) - max_overlap
+        before = cell_row((0.0, 0.0, rz), (math.cos(angle), 0.0, math.sin(angle)), 0.072)[None, :]
+        o = orc.Oracle(p)
+        o.set_cells(before)
+        o.loop_init()
+        for _ in range(100):
+            o.iterate(10000)
+            after = o.cells()
+            if np.abs(after[0, 7:13]).max() < 1e-9:
+                break
+        delta = 1e-8                                   # testSkew.cpp:162
+        assert np.all(np.abs(after[0, 7:13]) < delta), (i, max_overlap)
+        kept = [0, 5] + list(range(13, 21))            # ID, ny, lengths, birth, growth, viscosities, sigma0, group
+        assert np.all(np.abs(after[0, kept] - before[0, kept]) < delta)
+        if max_overlap < 0:                            # clear of the surface: nothing moves
+            n_end, z_end = tuple(before[0, 4:7]), rz
+        elif more_adhesive_than_repulsive(rz, math.sin(angle)):
+            n_end, z_end = (1.0, 0.0, 0.0), R * (1 - (0.25 * SIGMA0 / (R * E0)) ** (2.0 / 3.0))
+        else:
+            n_end, z_end = (0.0, 0.0, 1.0), HALF_L + R * (1 - (0.75 * math.pi * SIGMA0 / (R * E0)) ** (2.0 / 3.0))
+        assert np.all(np.abs(after[0, 4:7] - n_end) < delta), (i, max_overlap, after[0, 4:7])
+        assert abs(after[0, 3] - z_end) < delta, (i, max_overlap, after[0, 3], z_end)

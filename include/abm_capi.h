@@ -140,7 +140,9 @@ typedef struct abm_profile {
 typedef struct abm_ctx abm_ctx;
 
 /* Create a context on the current CUDA device.  No reference counterpart: the
- * reference keeps this state on the stack of runSimulation (simulation.hpp:1106-1170). */
+ * reference keeps this state on the stack of runSimulation (simulation.hpp:1106-1170).
+ * On a failure other than ABM_ERR_ARG for a NULL argument, *ctx still receives a
+ * context that holds the reason (abm_last_error); release it with abm_destroy. */
 int abm_create(const abm_params* params, abm_ctx** ctx);
 int abm_destroy(abm_ctx* ctx);
 const char* abm_last_error(const abm_ctx* ctx);

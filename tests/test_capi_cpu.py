@@ -39,7 +39,9 @@ def test_no_gpu_means_error_not_fallback():
             pytest.skip("a GPU is present")
     except ImportError:
         pass
-    with pytest.raises(RuntimeError, match="ABM_ERR_CUDA"):
+    # the failed abm_create hands back a context holding the reason, which the wrapper
+    # reads and then releases
+    with pytest.raises(RuntimeError, match="ABM_ERR_CUDA.*no CUDA device"):
         abm_b200.Simulation(cap_cells=16)
 
 

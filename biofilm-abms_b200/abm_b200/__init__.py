@@ -138,6 +138,7 @@ def _load():
         "abm_synchronize": ([vp], i),
         "abm_jkr_contact_radius": ([d, d, d, d, dp], i),
         "abm_jkr_radius_table": ([d, d, d, d, i, dp, dp], i),
+        "abm_jkr_optimal_gamma": ([d, d, d, d, dp], i),
         "abm_set_jkr_table": ([vp, dp, dp, i], i),
         "abm_upload_cells": ([vp, dp, i, i, i], i),
         "abm_download_cells": ([vp, dp, i], i),
@@ -192,7 +193,7 @@ def _load():
 
 LIB = _load()
 EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchronize "
-            "abm_jkr_contact_radius abm_jkr_radius_table abm_set_jkr_table abm_upload_cells "
+            "abm_jkr_contact_radius abm_jkr_radius_table abm_jkr_optimal_gamma abm_set_jkr_table abm_upload_cells "
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
@@ -219,6 +220,16 @@ def jkr_contact_radius(delta, Req, E, gamma):
     rc = LIB.abm_jkr_contact_radius(delta, Req, E, gamma, ctypes.byref(out))
     if rc:
         raise RuntimeError("abm_jkr_contact_radius failed (%s)" % ERRORS.get(rc, rc))
+    return out.value
+
+
+def jkr_optimal_gamma(R, Rcell, E0, eqdist):
+    """jkrOptimalSurfaceEnergyDensity (jkr.hpp:1369-1407): the adhesion energy density whose
+    JKR force balance puts two cells at centerline distance eqdist (simulation.hpp:1354-1358)."""
+    out = ctypes.c_double()
+    rc = LIB.abm_jkr_optimal_gamma(R, Rcell, E0, eqdist, ctypes.byref(out))
+    if rc:
+        raise RuntimeError("abm_jkr_optimal_gamma failed (%s): need 2 Rcell <= eqdist < 2 R" % ERRORS.get(rc, rc))
     return out.value
 
 

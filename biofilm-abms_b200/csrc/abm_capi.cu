@@ -6,6 +6,7 @@
 // growth) and one neighbor rebuild (bbox -> counting sort -> pair build ->
 // CSR).  All sizes that change during a run (cell count, pair count, bin
 // count) live in device memory, so the graphs are captured once and replayed.
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -129,6 +130,26 @@ int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_
         delta_out[i] = (i == n_mesh - 1) ? high : 0.0 + double(i) * step;
         radius_out[i] = jkr_radius_host(delta_out[i], R / 2, E0, gamma);
     }
+    return ABM_OK;
+}
+
+// jkrOptimalSurfaceEnergyDensity (jkr.hpp:1369-1407), which runSimulation calls to turn the
+// target equilibrium distance eqdist into the adhesion energy density (simulation.hpp:1354-1358).
+// The reference nests two finite-difference Newton solves: the overlap where the JKR force
+// 4 E0 a^3 / (3 Req) - 4 sqrt(pi gamma E0) a^(3/2) vanishes (jkr.hpp:1311-1339), inside a solve
+// on log10(gamma).  The balance has a closed form.  Zero force means a^3 = 9 pi gamma Req^2 / E0,
+// and the JKR overlap a^2 / Req - 2 sqrt(pi gamma a / E0) at that radius is
+// (3 Req)^(1/3) (pi gamma / E0)^(2/3), so gamma = E0 delta^(3/2) / (pi sqrt(3 Req)) with
+// delta = 2 R - eqdist.  The reference caps the overlap at 2 (R - Rcell), so a target below
+// 2 Rcell, or at or above 2 R, has no solution.
+int abm_jkr_optimal_gamma(double R, double Rcell, double E0, double eqdist, double* gamma)
+{
+    if (!gamma || !(R > 0) || !(E0 > 0) || !(Rcell >= 0) || !(Rcell < R)) return ABM_ERR_ARG;
+    const double delta = 2 * R - eqdist;
+    const double cap = 2 * (R - Rcell);
+    if (!(delta > 0) || delta > cap * (1 + 4 * DBL_EPSILON)) return ABM_ERR_ARG;
+    const double pi = 3.141592653589793238462643383279502884;
+    *gamma = E0 * delta * std::sqrt(delta) / (pi * std::sqrt(3 * (R / 2)));
     return ABM_OK;
 }
 

@@ -156,6 +156,11 @@ int abm_jkr_contact_radius(double delta, double Req, double E, double gamma, dou
  * with the mesh of simulation.hpp:1379-1382. */
 int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_mesh,
                          double* delta_out, double* radius_out);
+/* jkrOptimalSurfaceEnergyDensity (jkr.hpp:1369-1407) as runSimulation calls it
+ * (simulation.hpp:1354-1358): the adhesion energy density whose JKR force balance puts two
+ * cells at centerline distance eqdist, in closed form.  ABM_ERR_ARG unless
+ * 2 Rcell <= eqdist < 2 R (the reference caps the overlap at 2 (R - Rcell)). */
+int abm_jkr_optimal_gamma(double R, double Rcell, double E0, double eqdist, double* gamma);
 /* Install the fixed-gamma table (IsotropicJKRDataFixedGamma, mechanics.hpp:113-153). */
 int abm_set_jkr_table(abm_ctx* ctx, const double* delta, const double* radius, int n);
 

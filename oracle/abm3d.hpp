@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <limits>
 #include <stdexcept>
+#include <utility>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -409,6 +410,51 @@ inline std::vector<double> jkr_radius_table(const std::vector<double>& overlaps,
     for (size_t i = 0; i < overlaps.size(); ++i)
         radii[i] = jkr_contact_radius(overlaps[i], R / 2, E0, gamma);
     return radii;
+}
+
+// rootFinding.hpp:42-75 (newtonRaphson): Newton steps with a central-difference
+// derivative of step dx until |f(x)| <= tol or max_iter steps; returns (x, f(x)).
+template <typename F>
+inline std::pair<double, double> newton_raphson(F func, double x0, double dx, double tol, int max_iter)
+{
+    double x = x0, fx = func(x);
+    int iter = 0;
+    while (std::fabs(fx) > tol && iter < max_iter)
+    {
+        double deriv = (func(x + dx) - func(x - dx)) / (2 * dx);
+        x += -fx / deriv;
+        fx = func(x);
+        ++iter;
+    }
+    return std::make_pair(x, fx);
+}
+
+// jkr.hpp:1311-1339 (jkrEquilibriumDistance): the overlap where the JKR force
+// (4/3) (E0/Req) a^3 - 4 sqrt(pi gamma E0) a^(3/2) vanishes, a the contact radius at
+// that overlap, found by newtonRaphson from 2R - dinit and capped at 2R - dmin.
+inline double jkr_equilibrium_distance(double R, double E0, double gamma, double dinit, double dmin,
+                                       double increment_overlap, double newton_tol, int max_iter)
+{
+    const double Req = R / 2;
+    auto force = [&](double x) {
+        double a = jkr_contact_radius(x, Req, E0, gamma);
+        return (4.0 / 3.0) * E0 / Req * a * a * a - 4 * std::sqrt(PI * gamma * E0) * std::pow(a, 1.5);
+    };
+    std::pair<double, double> res = newton_raphson(force, 2 * R - dinit, increment_overlap, newton_tol, max_iter);
+    return 2 * R - std::min(res.first, 2 * R - dmin);
+}
+
+// jkr.hpp:1369-1407 (jkrOptimalSurfaceEnergyDensity) with the arguments of
+// simulation.hpp:1355-1358: newtonRaphson on log10(gamma) from log10(100), step 1e-6,
+// tolerance 1e-8 on the equilibrium distance, inner solves from dinit = 1.5 R with
+// dmin = 2 Rcell, step 1e-8 and tolerance 1e-8, at most 1000 steps each.
+inline double jkr_optimal_gamma(double R, double Rcell, double E0, double deq_target)
+{
+    auto func = [&](double x) {
+        double gamma = std::pow(10.0, x);
+        return jkr_equilibrium_distance(R, E0, gamma, 0.75 * 2 * R, 2 * Rcell, 1e-8, 1e-8, 1000) - deq_target;
+    };
+    return std::pow(10.0, newton_raphson(func, std::log10(100.0), 1e-6, 1e-8, 1000).first);
 }
 
 // utils.hpp:1169-1215 (nearestValue)

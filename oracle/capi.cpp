@@ -97,6 +97,18 @@ double oracle_jkr_contact_radius(double delta, double Req, double E, double gamm
     return jkr_contact_radius(delta, Req, E, gamma);
 }
 
+// jkr.hpp:1311-1339, from dinit = 1.5 R with dmin = 2 Rcell as jkr.hpp:1389-1390 calls it
+double oracle_jkr_equilibrium_distance(double R, double Rcell, double E0, double gamma)
+{
+    return jkr_equilibrium_distance(R, E0, gamma, 0.75 * 2 * R, 2 * Rcell, 1e-8, 1e-8, 1000);
+}
+
+// jkr.hpp:1369-1407 as simulation.hpp:1355-1358 calls it
+double oracle_jkr_optimal_gamma(double R, double Rcell, double E0, double eqdist)
+{
+    return jkr_optimal_gamma(R, Rcell, E0, eqdist);
+}
+
 int oracle_set_cells(oracle_ctx* c, const double* colmajor, int n, int ncols, int ld)
 {
     Cells cells(n, ncols);

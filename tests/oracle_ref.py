@@ -51,6 +51,8 @@ def _load():
         "oracle_set_jkr_table": ([vp, dp, dp, i], i),
         "oracle_jkr_table": ([d, d, d, d, i, dp, dp], i),
         "oracle_jkr_contact_radius": ([d, d, d, d], d),
+        "oracle_jkr_equilibrium_distance": ([d, d, d, d], d),
+        "oracle_jkr_optimal_gamma": ([d, d, d, d], d),
         "oracle_set_cells": ([vp, dp, i, i, i], i),
         "oracle_get_num_cells": ([vp], i),
         "oracle_get_cells": ([vp, dp, i], i),

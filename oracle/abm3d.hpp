@@ -497,6 +497,8 @@ struct Params3 {
     uint64_t rng_seed = 42;
     int n_start_multithread = 50;
     std::vector<double> jkr_overlaps, jkr_radii;
+    int friction_mode = 0;                 // FrictionMode: 0 NONE, 1 KINETIC (mechanics.hpp:61-65)
+    double cell_cell_coulomb_coeff = 1.0;  // runSimulation's default (simulation.hpp:1162)
 };
 
 struct Tableau {
@@ -735,6 +737,87 @@ inline Arr6 cell_surface_adhesion_forces(const Cells& cells, const std::vector<d
     return dEdq;
 }
 
+// mechanics.hpp:1031-1175 (cellCellFrictionForces, include_constraint = false), as
+// cellCellInteractionForces adds it when friction_mode is KINETIC (mechanics.hpp:1339-1346,
+// dz_threshold 1e-3).  At each overlapping pair the force on cell i is
+// -eta sqrt(Req overlap) times the tangential part of the relative velocity of the two
+// contact points (each cell's dr + s dn from its velocity columns), eta the smaller of the two
+// cells' coefficients in column eta_col.  With coulomb_coeff > 0 its norm is capped at
+// coulomb_coeff (4/3) E0 sqrt(Req) overlap^(3/2).  A contact whose distance vector is nearly
+// horizontal (|dz / d| < dz_threshold) between two contact points below 1.01 R is taken in the
+// xy-plane (surface present only).  Returns dE/dq (n x 6): minus the force and torque.
+inline Arr6 cell_cell_friction_forces(const Cells& cells, const Neighbors& nb, double R, double E0,
+                                      int eta_col, double coulomb_coeff, bool no_surface,
+                                      double dz_threshold)
+{
+    const int n = cells.n, m = nb.size();
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    if (m == 0) return dEdq;
+    const double Req = R / 2;
+    for (int k = 0; k < m; ++k)
+    {
+        const int i = nb.i[k], j = nb.j[k];
+        V3 dij = v3(nb.dx[k], nb.dy[k], nb.dz[k]);
+        const double dist = norm(dij);
+        double overlap = 2 * R - dist;
+        if (!(overlap > 0)) continue;
+        const double si = nb.si[k], sj = nb.sj[k];
+        V3 dijn = v3(dij.x / dist, dij.y / dist, dij.z / dist);
+        const V3 ri = cell_r(cells, i), ni = cell_n(cells, i);
+        const V3 rj = cell_r(cells, j), nj = cell_n(cells, j);
+        const double eta = std::min(cells(i, eta_col), cells(j, eta_col));
+        bool flat = false;
+        if (!no_surface && std::fabs(dijn.z) < dz_threshold)
+        {
+            const V3 pi = ri + si * ni, pj = rj + sj * nj;
+            flat = (pi.z < 1.01 * R && pj.z < 1.01 * R);
+        }
+        const V3 vi = v3(cells(i, C_DRX), cells(i, C_DRY), cells(i, C_DRZ)) +
+                      si * v3(cells(i, C_DNX), cells(i, C_DNY), cells(i, C_DNZ));
+        const V3 vj = v3(cells(j, C_DRX), cells(j, C_DRY), cells(j, C_DRZ)) +
+                      sj * v3(cells(j, C_DNX), cells(j, C_DNY), cells(j, C_DNZ));
+        V3 rv = vi - vj;
+        if (flat)
+        {
+            dij.z = 0;
+            const double d2 = norm(dij);
+            dijn = v3(dij.x / d2, dij.y / d2, dij.z / d2);
+            overlap = 2 * R - d2;
+            rv.z = 0;
+        }
+        const V3 vt = rv - dot(rv, dijn) * dijn;
+        V3 force = (-eta * std::sqrt(Req * overlap)) * vt;
+        if (coulomb_coeff > 0)
+        {
+            const double fn = norm(force);
+            const double max_norm = coulomb_coeff * (4. / 3.) * E0 * std::sqrt(Req) * std::pow(overlap, 1.5);
+            if (fn > max_norm)
+            {
+                const double scale = max_norm / fn;
+                force = v3(force.x * scale, force.y * scale, force.z * scale);
+            }
+        }
+        const V3 ti = si * force, tj = (-sj) * force;
+        const double hi[6] = {-force.x, -force.y, -force.z, -ti.x, -ti.y, -ti.z};
+        const double hj[6] = {force.x, force.y, force.z, -tj.x, -tj.y, -tj.z};
+        for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += hi[c]; A6(dEdq, n, j, c) += hj[c]; }
+    }
+    return dEdq;
+}
+
+// cellCellInteractionForces' friction term (mechanics.hpp:1339-1346) added onto the pair
+// forces: the friction coefficient column is 22 with adhesion on, 21 without
+// (simulation.hpp:1184-1186).
+inline void add_friction(Arr6& cc, const Cells& cells, const Neighbors& nb, const Params3& p)
+{
+    if (p.friction_mode == 0) return;
+    const int eta_col = p.adhesion_mode != 0 ? 22 : 21;
+    if (cells.ncols <= eta_col) throw std::runtime_error("friction needs the cell-cell friction column");
+    Arr6 fr = cell_cell_friction_forces(cells, nb, p.R, p.E0, eta_col, p.cell_cell_coulomb_coeff,
+                                        p.no_surface != 0, 1e-3);
+    for (size_t k = 0; k < cc.size(); ++k) cc[k] += fr[k];
+}
+
 // mechanics.hpp:1702-1769 (getConservativeForces): -(dE_cc) - dE_rep - dE_adh
 inline Arr6 get_conservative_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
                                     const std::vector<int>& assume_2d, bool multithread,
@@ -746,6 +829,7 @@ inline Arr6 get_conservative_forces(const Cells& cells, const Neighbors& nb, con
         ss[i] = assume_2d[i] ? std::numeric_limits<double>::quiet_NaN()
                              : sstar(cells(i, C_RZ), cells(i, C_NZ), p.R);
     Arr6 cc = dEdq_cc_cached ? *dEdq_cc_cached : cell_cell_forces(cells, nb, p);
+    add_friction(cc, cells, nb, p);   // velocity- and position-dependent: every stage
     Arr6 rep((size_t)n * 6, 0.0), adh((size_t)n * 6, 0.0);
     if (!p.no_surface)
     {

@@ -26,6 +26,8 @@ struct oracle_params {
     unsigned long long rng_seed;
     int n_start_multithread;
     int n_threads;   // OpenMP threads for the reference's parallel loops (0 = default)
+    int friction_mode;                // 0 NONE, 1 KINETIC cell-cell friction
+    double cell_cell_coulomb_coeff;   // Coulomb cap of the friction (not positive: none)
 };
 
 struct oracle_ctx {
@@ -54,6 +56,7 @@ int oracle_create(const oracle_params* q, oracle_ctx** out)
     p.daughter_length_std = q->daughter_length_std;
     p.daughter_angle_xy_bound = q->daughter_angle_xy_bound; p.daughter_angle_z_bound = q->daughter_angle_z_bound;
     p.rng_seed = q->rng_seed; p.n_start_multithread = q->n_start_multithread;
+    p.friction_mode = q->friction_mode; p.cell_cell_coulomb_coeff = q->cell_cell_coulomb_coeff;
 #ifdef _OPENMP
     if (q->n_threads > 0) omp_set_num_threads(q->n_threads);
 #endif
@@ -213,6 +216,7 @@ double oracle_nearest_body_coord(const double* r, const double* n, double h, con
 int oracle_cell_cell_forces(oracle_ctx* c, double* out)
 {
     Arr6 f = cell_cell_forces(c->st.cells, c->st.nb, c->p);
+    add_friction(f, c->st.cells, c->st.nb, c->p);   // mechanics.hpp:1339-1346
     std::memcpy(out, f.data(), f.size() * sizeof(double));
     return 0;
 }

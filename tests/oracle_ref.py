@@ -34,6 +34,7 @@ class OracleParams(ctypes.Structure):
         ("daughter_length_std", ctypes.c_double), ("daughter_angle_xy_bound", ctypes.c_double),
         ("daughter_angle_z_bound", ctypes.c_double), ("rng_seed", ctypes.c_ulonglong),
         ("n_start_multithread", ctypes.c_int), ("n_threads", ctypes.c_int),
+        ("friction_mode", ctypes.c_int), ("cell_cell_coulomb_coeff", ctypes.c_double),
     ]
 
 

@@ -499,6 +499,7 @@ struct Params3 {
     std::vector<double> jkr_overlaps, jkr_radii;
     int friction_mode = 0;                 // FrictionMode: 0 NONE, 1 KINETIC (mechanics.hpp:61-65)
     double cell_cell_coulomb_coeff = 1.0;  // runSimulation's default (simulation.hpp:1162)
+    double M0 = 0;                         // cell mass at length L0 (velocity Verlet)
 };
 
 struct Tableau {
@@ -569,11 +570,20 @@ typedef std::vector<double> Arr6;   // n x 6, column-major (ld = n)
 inline double& A6(Arr6& a, int n, int i, int k) { return a[(size_t)k * n + i]; }
 inline double A6c(const Arr6& a, int n, int i, int k) { return a[(size_t)k * n + i]; }
 
-// adhesion.hpp:282-370 (forcesIsotropicJKRLagrange, include_constraint = false,
-// interpolate = true) with max_overlap = 2 (R - Rcell); rows = cells i, j
+inline V3 cross(V3 a, V3 b)
+{
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// adhesion.hpp:282-370 (forcesIsotropicJKRLagrange, interpolate = true) with
+// max_overlap = 2 (R - Rcell); rows = cells i, j.  With `constraint` (include_constraint,
+// the velocity-Verlet form) the orientation rows are s (-(n1 . -v) n1 - v) and
+// t ((n2 . -v) n2 + v), as the reference writes them, not a cross product
+// (adhesion.hpp:355-366).
 inline void jkr_forces(V3 d12, double R, double E0, double gamma, double s, double t,
                        const std::vector<double>& tab_delta, const std::vector<double>& tab_radius,
-                       double max_overlap, double out[2][6])
+                       double max_overlap, double out[2][6], bool constraint = false,
+                       V3 n1 = V3{0, 0, 0}, V3 n2 = V3{0, 0, 0})
 {
     for (int a = 0; a < 2; ++a) for (int k = 0; k < 6; ++k) out[a][k] = 0;
     double dist = norm(d12);
@@ -595,14 +605,28 @@ inline void jkr_forces(V3 d12, double R, double E0, double gamma, double s, doub
         V3 v = (term2 - term1) * d12n;
         out[0][0] = -v.x; out[0][1] = -v.y; out[0][2] = -v.z;
         out[1][0] = v.x; out[1][1] = v.y; out[1][2] = v.z;
-        out[0][3] = -s * v.x; out[0][4] = -s * v.y; out[0][5] = -s * v.z;
-        out[1][3] = t * v.x; out[1][4] = t * v.y; out[1][5] = t * v.z;
+        if (!constraint)
+        {
+            out[0][3] = -s * v.x; out[0][4] = -s * v.y; out[0][5] = -s * v.z;
+            out[1][3] = t * v.x; out[1][4] = t * v.y; out[1][5] = t * v.z;
+        }
+        else
+        {
+            const V3 mv = v3(-v.x, -v.y, -v.z);
+            const double w1 = dot(n1, mv), w2 = dot(n2, mv);
+            const V3 a = (-w1) * n1 - v, b = w2 * n2 + v;
+            out[0][3] = s * a.x; out[0][4] = s * a.y; out[0][5] = s * a.z;
+            out[1][3] = t * b.x; out[1][4] = t * b.y; out[1][5] = t * b.z;
+        }
     }
 }
 
-// mechanics.hpp:1209-1350 (Hertz only) and :1390-1659 (Hertz + isotropic JKR),
-// include_constraint = false, no cell-cell friction.  Returns dE/dq (n x 6).
-inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Params3& p)
+// mechanics.hpp:1209-1350 (Hertz only) and :1390-1659 (Hertz + isotropic JKR), without
+// the friction term (add_friction adds it).  Returns dE/dq (n x 6).  `constraint` selects
+// include_constraint = true, the form velocity Verlet uses: the Hertz and hard-core rows
+// become (s n) x v (mechanics.hpp:1298-1311, 1554-1566, 1608-1617).
+inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
+                             bool constraint = false)
 {
     const int n = cells.n, m = nb.size();
     Arr6 dEdq((size_t)n * 6, 0.0);
@@ -624,7 +648,8 @@ inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Para
         double gamma = adhesion ? std::min(cells(i, C_GAMMA), cells(j, C_GAMMA)) : 0.0;
         if (adhesion && gamma > 0)
         {
-            jkr_forces(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_radii, max_overlap, f);
+            jkr_forces(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_radii, max_overlap, f,
+                       constraint, cell_n(cells, i), cell_n(cells, j));
         }
         else
         {
@@ -638,8 +663,18 @@ inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Para
             V3 vij = magnitude * dijn;
             f[0][0] = vij.x; f[0][1] = vij.y; f[0][2] = vij.z;
             f[1][0] = -vij.x; f[1][1] = -vij.y; f[1][2] = -vij.z;
-            f[0][3] = si * vij.x; f[0][4] = si * vij.y; f[0][5] = si * vij.z;
-            f[1][3] = -sj * vij.x; f[1][4] = -sj * vij.y; f[1][5] = -sj * vij.z;
+            if (!constraint)
+            {
+                f[0][3] = si * vij.x; f[0][4] = si * vij.y; f[0][5] = si * vij.z;
+                f[1][3] = -sj * vij.x; f[1][4] = -sj * vij.y; f[1][5] = -sj * vij.z;
+            }
+            else
+            {
+                const V3 ti = cross(si * cell_n(cells, i), vij);
+                const V3 tj = cross(sj * cell_n(cells, j), v3(-vij.x, -vij.y, -vij.z));
+                f[0][3] = ti.x; f[0][4] = ti.y; f[0][5] = ti.z;
+                f[1][3] = tj.x; f[1][4] = tj.y; f[1][5] = tj.z;
+            }
         }
         for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += f[0][c]; A6(dEdq, n, j, c) += f[1][c]; }
         if (adhesion && overlap > 2 * (R - Rcell))
@@ -648,16 +683,25 @@ inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Para
             V3 vij = magnitude * dijn;
             double h[2][6] = {{vij.x, vij.y, vij.z, si * vij.x, si * vij.y, si * vij.z},
                               {-vij.x, -vij.y, -vij.z, -sj * vij.x, -sj * vij.y, -sj * vij.z}};
+            if (constraint)
+            {
+                const V3 ti = cross(si * cell_n(cells, i), vij);
+                const V3 tj = cross(sj * cell_n(cells, j), v3(-vij.x, -vij.y, -vij.z));
+                h[0][3] = ti.x; h[0][4] = ti.y; h[0][5] = ti.z;
+                h[1][3] = tj.x; h[1][4] = tj.y; h[1][5] = tj.z;
+            }
             for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += h[0][c]; A6(dEdq, n, j, c) += h[1][c]; }
         }
     }
     return dEdq;
 }
 
-// mechanics.hpp:673-780 (cellSurfaceRepulsionForces, include_constraint = false)
+// mechanics.hpp:673-780 (cellSurfaceRepulsionForces).  With `constraint`
+// (include_constraint) the nz row is replaced by x, y torques
+// -2 E0 (ny, -nx) ((1 - nz^2) I2(1) + sqrt(R) nz^2 I2(1/2)) (mechanics.hpp:718-755).
 inline Arr6 cell_surface_repulsion_forces(const Cells& cells, const std::vector<double>& ss,
                                           double R, double E0, const std::vector<int>& assume_2d,
-                                          bool multithread)
+                                          bool multithread, bool constraint = false)
 {
     const int n = cells.n;
     Arr6 dEdq((size_t)n * 6, 0.0);
@@ -679,6 +723,16 @@ inline Arr6 cell_surface_repulsion_forces(const Cells& cells, const std::vector<
             double int1 = integral1(rz, nz, R, hl, 1.0, ss[i]);
             double int2 = integral1(rz, nz, R, hl, 0.5, ss[i]);
             A6(dEdq, n, i, 2) = -prefactor0 * ((1.0 - nz2) * int1 + std::sqrt(R) * nz2 * int2);
+            if (constraint)
+            {
+                double i3 = integral2(rz, nz, R, hl, 1.0, ss[i]);
+                double i4 = integral2(rz, nz, R, hl, 0.5, ss[i]);
+                double cx = cells(i, C_NY), cy = -cells(i, C_NX);
+                double w = (1.0 - nz2) * i3 + std::sqrt(R) * nz2 * i4;
+                A6(dEdq, n, i, 3) = -prefactor0 * cx * w;
+                A6(dEdq, n, i, 4) = -prefactor0 * cy * w;
+                continue;
+            }
             double int3 = integral1(rz, nz, R, hl, 2.0, ss[i]);
             double int4 = integral2(rz, nz, R, hl, 1.0, ss[i]);
             double int5 = integral1(rz, nz, R, hl, 1.5, ss[i]);
@@ -693,10 +747,11 @@ inline Arr6 cell_surface_repulsion_forces(const Cells& cells, const std::vector<
     return dEdq;
 }
 
-// mechanics.hpp:800-910 (cellSurfaceAdhesionForces, include_constraint = false)
+// mechanics.hpp:800-910 (cellSurfaceAdhesionForces).  With `constraint`
+// (include_constraint) the nz row is replaced by x, y torques (mechanics.hpp:845-886).
 inline Arr6 cell_surface_adhesion_forces(const Cells& cells, const std::vector<double>& ss,
                                          double R, const std::vector<int>& assume_2d,
-                                         bool multithread)
+                                         bool multithread, bool constraint = false)
 {
     const int n = cells.n;
     Arr6 dEdq((size_t)n * 6, 0.0);
@@ -721,6 +776,20 @@ inline Arr6 cell_surface_adhesion_forces(const Cells& cells, const std::vector<d
             if (std::fabs(ss[i]) < hl) term2 = (prefactor1 / 2) * nz;
             double d2 = prefactor0 * (1 - nz2) * int1 + term2;
             A6(dEdq, n, i, 2) = d2 * sig;
+            if (constraint)
+            {
+                double i2 = integral2(rz, nz, R, hl, -0.5, ss[i]);
+                double cx = cells(i, C_NY), cy = -cells(i, C_NX);
+                double w1 = 0, w2 = 0;
+                if (std::fabs(ss[i]) < hl)
+                {
+                    w1 = (prefactor1 / 2) * ss[i] * nz * cx;
+                    w2 = (prefactor1 / 2) * ss[i] * nz * cy;
+                }
+                A6(dEdq, n, i, 3) = (prefactor0 * (1 - nz2) * i2 * cx - w1) * sig;
+                A6(dEdq, n, i, 4) = (prefactor0 * (1 - nz2) * i2 * cy - w2) * sig;
+                continue;
+            }
             double int2 = integral1(rz, nz, R, hl, 0.5, ss[i]);
             double int3 = integral2(rz, nz, R, hl, -0.5, ss[i]);
             double int4 = integral4(nz, hl, ss[i]);
@@ -748,7 +817,7 @@ inline Arr6 cell_surface_adhesion_forces(const Cells& cells, const std::vector<d
 // xy-plane (surface present only).  Returns dE/dq (n x 6): minus the force and torque.
 inline Arr6 cell_cell_friction_forces(const Cells& cells, const Neighbors& nb, double R, double E0,
                                       int eta_col, double coulomb_coeff, bool no_surface,
-                                      double dz_threshold)
+                                      double dz_threshold, bool constraint = false)
 {
     const int n = cells.n, m = nb.size();
     Arr6 dEdq((size_t)n * 6, 0.0);
@@ -797,7 +866,9 @@ inline Arr6 cell_cell_friction_forces(const Cells& cells, const Neighbors& nb, d
                 force = v3(force.x * scale, force.y * scale, force.z * scale);
             }
         }
-        const V3 ti = si * force, tj = (-sj) * force;
+        // torques s force, or (s n) x force with include_constraint (mechanics.hpp:1152-1161)
+        const V3 ti = constraint ? cross(si * ni, force) : si * force;
+        const V3 tj = constraint ? cross(sj * nj, v3(-force.x, -force.y, -force.z)) : (-sj) * force;
         const double hi[6] = {-force.x, -force.y, -force.z, -ti.x, -ti.y, -ti.z};
         const double hj[6] = {force.x, force.y, force.z, -tj.x, -tj.y, -tj.z};
         for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += hi[c]; A6(dEdq, n, j, c) += hj[c]; }
@@ -808,33 +879,34 @@ inline Arr6 cell_cell_friction_forces(const Cells& cells, const Neighbors& nb, d
 // cellCellInteractionForces' friction term (mechanics.hpp:1339-1346) added onto the pair
 // forces: the friction coefficient column is 22 with adhesion on, 21 without
 // (simulation.hpp:1184-1186).
-inline void add_friction(Arr6& cc, const Cells& cells, const Neighbors& nb, const Params3& p)
+inline void add_friction(Arr6& cc, const Cells& cells, const Neighbors& nb, const Params3& p,
+                         bool constraint = false)
 {
     if (p.friction_mode == 0) return;
     const int eta_col = p.adhesion_mode != 0 ? 22 : 21;
     if (cells.ncols <= eta_col) throw std::runtime_error("friction needs the cell-cell friction column");
     Arr6 fr = cell_cell_friction_forces(cells, nb, p.R, p.E0, eta_col, p.cell_cell_coulomb_coeff,
-                                        p.no_surface != 0, 1e-3);
+                                        p.no_surface != 0, 1e-3, constraint);
     for (size_t k = 0; k < cc.size(); ++k) cc[k] += fr[k];
 }
 
 // mechanics.hpp:1702-1769 (getConservativeForces): -(dE_cc) - dE_rep - dE_adh
 inline Arr6 get_conservative_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
                                     const std::vector<int>& assume_2d, bool multithread,
-                                    const Arr6* dEdq_cc_cached = nullptr)
+                                    const Arr6* dEdq_cc_cached = nullptr, bool constraint = false)
 {
     const int n = cells.n;
     std::vector<double> ss(n);
     for (int i = 0; i < n; ++i)
         ss[i] = assume_2d[i] ? std::numeric_limits<double>::quiet_NaN()
                              : sstar(cells(i, C_RZ), cells(i, C_NZ), p.R);
-    Arr6 cc = dEdq_cc_cached ? *dEdq_cc_cached : cell_cell_forces(cells, nb, p);
-    add_friction(cc, cells, nb, p);   // velocity- and position-dependent: every stage
+    Arr6 cc = dEdq_cc_cached ? *dEdq_cc_cached : cell_cell_forces(cells, nb, p, constraint);
+    add_friction(cc, cells, nb, p, constraint);   // velocity- and position-dependent: every stage
     Arr6 rep((size_t)n * 6, 0.0), adh((size_t)n * 6, 0.0);
     if (!p.no_surface)
     {
-        rep = cell_surface_repulsion_forces(cells, ss, p.R, p.E0, assume_2d, multithread);
-        adh = cell_surface_adhesion_forces(cells, ss, p.R, assume_2d, multithread);
+        rep = cell_surface_repulsion_forces(cells, ss, p.R, p.E0, assume_2d, multithread, constraint);
+        adh = cell_surface_adhesion_forces(cells, ss, p.R, assume_2d, multithread, constraint);
     }
     Arr6 out((size_t)n * 6);
     for (size_t k = 0; k < out.size(); ++k) out[k] = ((-cc[k]) - rep[k]) - adh[k];
@@ -859,7 +931,8 @@ inline void normalize_orientations(Cells& cells)
     }
 }
 
-// mechanics.hpp:2011-2347 (getVelocities) with friction NONE.  `noise` is n x 6.
+// mechanics.hpp:2011-2347 (getVelocities); cell-cell friction enters through
+// get_conservative_forces.  `noise` is n x 6.
 inline Arr6 get_velocities(const Cells& cells, const Neighbors& nb, const Params3& p,
                            const std::vector<int>& assume_2d, const Arr6& noise,
                            bool multithread, const Arr6* dEdq_cc_cached = nullptr)
@@ -1234,6 +1307,226 @@ inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double 
 // Simulation loop body (simulation.hpp:1617-1864, switching, writing,
 // basal_only and pole tracking excluded)
 // ------------------------------------------------------------------------
+// ------------------------------------------------------------------------
+// Velocity Verlet (IntegrationMode::VELOCITY_VERLET = 0, simulation.hpp:1786-1798)
+// ------------------------------------------------------------------------
+
+// integrals.hpp:203-229 (integral3)
+inline double integral3(double rz, double nz, double R, double half_l, double gamma, double ss)
+{
+    double term1 = 2 * integral2(rz, nz, R, half_l, gamma + 1, ss);
+    double term2 = 0;
+    if (ss > half_l)
+    {
+        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        term2 = half_l * half_l * (o1 - o2);
+    }
+    else if (ss > -half_l)
+    {
+        term2 = half_l * half_l * std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+    }
+    return (term1 + term2) / (nz * (gamma + 1));
+}
+
+// integrals.hpp:334-383 (areaIntegral1, areaIntegral2, areaIntegral3), each on its own as
+// cellSurfaceFrictionForces calls them
+inline double area_integral(int k, double rz, double nz, double R, double half_l, double ss)
+{
+    const double t = std::sqrt(R) * (1 - nz * nz);
+    if (k == 1) return t * integral1(rz, nz, R, half_l, 0.5, ss) + PI * R * nz * nz * integral4(nz, half_l, ss);
+    if (k == 2) return t * integral2(rz, nz, R, half_l, 0.5, ss) + PI * R * nz * nz * integral5(nz, half_l, ss);
+    return t * integral3(rz, nz, R, half_l, 0.5, ss) + PI * R * nz * nz * integral6(nz, half_l, ss);
+}
+
+// mechanics.hpp:1784-1820 (ambientViscosityForces): eta0 l^3 dr and eta0 l^9 (n x dn) / 12,
+// with the cube of the length as the reference computes it (li = pow(l, 3)).
+inline Arr6 ambient_viscosity_forces(const Cells& cells)
+{
+    const int n = cells.n;
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    for (int i = 0; i < n; ++i)
+    {
+        const V3 w = cross(cell_n(cells, i), v3(cells(i, C_DNX), cells(i, C_DNY), cells(i, C_DNZ)));
+        const double eta = cells(i, C_ETA0), li = std::pow(cells(i, C_L), 3);
+        const double a = eta * li, b = eta * li * li * li;
+        A6(dEdq, n, i, 0) = a * cells(i, C_DRX); A6(dEdq, n, i, 1) = a * cells(i, C_DRY);
+        A6(dEdq, n, i, 2) = a * cells(i, C_DRZ);
+        A6(dEdq, n, i, 3) = b * w.x / 12; A6(dEdq, n, i, 4) = b * w.y / 12; A6(dEdq, n, i, 5) = b * w.z / 12;
+    }
+    return dEdq;
+}
+
+// mechanics.hpp:1821-1917 (cellSurfaceFrictionForces): friction eta1 / R times the contact
+// area moments against the in-plane velocity q = (drx, dry, 0) and m, the in-plane part of
+// (n x dn) x n; a horizontal cell uses its flat contact area sqrt(R (R - rz)) l.
+inline Arr6 cell_surface_friction_forces(const Cells& cells, const std::vector<double>& ss, double R,
+                                         const std::vector<int>& assume_2d)
+{
+    const int n = cells.n;
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    for (int i = 0; i < n; ++i)
+    {
+        const V3 ni = cell_n(cells, i);
+        const V3 w = cross(ni, v3(cells(i, C_DNX), cells(i, C_DNY), cells(i, C_DNZ)));
+        const V3 q = v3(cells(i, C_DRX), cells(i, C_DRY), 0);
+        const V3 m = v3(w.y * ni.z - w.z * ni.y, w.z * ni.x - w.x * ni.z, 0);
+        const double eta = cells(i, C_ETA1);
+        if (assume_2d[i])
+        {
+            const double ph = R - cells(i, C_RZ);
+            if (ph > 0)
+            {
+                const double area = std::sqrt(R) * std::sqrt(ph) * cells(i, C_L);
+                A6(dEdq, n, i, 0) = eta * q.x * area / R;
+                A6(dEdq, n, i, 1) = eta * q.y * area / R;
+                const double cz = ni.x * m.y - ni.y * m.x;
+                const double l2 = cells(i, C_L) * cells(i, C_L);
+                A6(dEdq, n, i, 5) = eta * cz * area * l2 / (12 * R);
+            }
+        }
+        else
+        {
+            const double rz = cells(i, C_RZ), hl = cells(i, C_HALF_L);
+            const double i1 = area_integral(1, rz, ni.z, R, hl, ss[i]);
+            const double i2 = area_integral(2, rz, ni.z, R, hl, ss[i]);
+            const double i3 = area_integral(3, rz, ni.z, R, hl, ss[i]);
+            A6(dEdq, n, i, 0) = eta * (q.x * i1 + m.x * i2) / R;
+            A6(dEdq, n, i, 1) = eta * (q.y * i1 + m.y * i2) / R;
+            const V3 c1 = cross(ni, q), c2 = cross(ni, m);
+            A6(dEdq, n, i, 3) = eta * (c1.x * i2 + c2.x * i3) / R;
+            A6(dEdq, n, i, 4) = eta * (c1.y * i2 + c2.y * i3) / R;
+            A6(dEdq, n, i, 5) = eta * (c1.z * i2 + c2.z * i3) / R;
+        }
+    }
+    return dEdq;
+}
+
+// the forces of one half of a velocity-Verlet step (mechanics.hpp:2834-2862 and :2919-2947):
+// the conservative forces in their include_constraint form plus the noise, minus the ambient
+// viscosity, minus the cell-surface friction (capped row by row at
+// cell_surface_coulomb_coeff times the constrained surface repulsion when that is positive)
+inline Arr6 verlet_forces(const Cells& cells, const Neighbors& nb, const Params3& p, const Arr6& noise)
+{
+    const int n = cells.n;
+    std::vector<int> a2(n);
+    std::vector<double> ss(n);
+    for (int i = 0; i < n; ++i)
+    {
+        a2[i] = cells(i, C_NZ) < p.nz_threshold;
+        ss[i] = a2[i] ? std::numeric_limits<double>::quiet_NaN() : sstar(cells(i, C_RZ), cells(i, C_NZ), p.R);
+    }
+    Arr6 f = get_conservative_forces(cells, nb, p, a2, false, nullptr, true);
+    for (size_t k = 0; k < f.size(); ++k) f[k] += noise[k];
+    Arr6 amb = ambient_viscosity_forces(cells);
+    for (size_t k = 0; k < f.size(); ++k) f[k] -= amb[k];
+    if (!p.no_surface)
+    {
+        Arr6 csf = cell_surface_friction_forces(cells, ss, p.R, a2);
+        if (p.cell_surface_coulomb_coeff > 0)
+        {
+            Arr6 rep = cell_surface_repulsion_forces(cells, ss, p.R, p.E0, a2, false, true);
+            for (int i = 0; i < n; ++i)
+            {
+                double sf = 0, sr = 0;
+                for (int c = 0; c < 6; ++c)
+                {
+                    sf += A6c(csf, n, i, c) * A6c(csf, n, i, c);
+                    sr += A6c(rep, n, i, c) * A6c(rep, n, i, c);
+                }
+                const double fn = std::sqrt(sf), max_norm = p.cell_surface_coulomb_coeff * std::sqrt(sr);
+                if (fn > max_norm)
+                    for (int c = 0; c < 6; ++c) A6(csf, n, i, c) *= (max_norm / fn);
+            }
+        }
+        for (size_t k = 0; k < f.size(); ++k) f[k] -= csf[k];
+    }
+    return f;
+}
+
+// the accelerations of one half step: forces / mass, and torques split along n and across it
+// over the two moments of inertia (mechanics.hpp:2863-2877)
+inline void verlet_accelerations(const Cells& cells, const Arr6& f, const std::vector<double>& mass,
+                                 const std::vector<double>& mom_par, const std::vector<double>& mom_perp,
+                                 std::vector<V3>& lin, std::vector<V3>& ang)
+{
+    const int n = cells.n;
+    lin.resize(n); ang.resize(n);
+    for (int i = 0; i < n; ++i)
+    {
+        const V3 ni = cell_n(cells, i);
+        const V3 tq = v3(A6c(f, n, i, 3), A6c(f, n, i, 4), A6c(f, n, i, 5));
+        const V3 tpar = dot(tq, ni) * ni, tperp = tq - tpar;
+        lin[i] = v3(A6c(f, n, i, 0) / mass[i], A6c(f, n, i, 1) / mass[i], A6c(f, n, i, 2) / mass[i]);
+        ang[i] = v3(tpar.x / mom_par[i], tpar.y / mom_par[i], tpar.z / mom_par[i]) +
+                 v3(tperp.x / mom_perp[i], tperp.y / mom_perp[i], tperp.z / mom_perp[i]);
+    }
+}
+
+// mechanics.hpp:2668-2996 (stepVelocityVerlet): half kick, drift of the two cell ends with the
+// half-step velocity and angular velocity, refreshed neighbor distances, forces at the new
+// state, second half kick; dn = omega x n.  rho is the cell density, M0 / volume of a cell of
+// length L0 (simulation.hpp:1279-1290).
+inline Cells step_velocity_verlet(const Cells& cells, const Neighbors& nb, double dt, const Params3& p,
+                                  double rho, int iter)
+{
+    const int n = cells.n;
+    const double R = p.R;
+    Arr6 noise = sample_noise(n, p, iter, 0);
+    std::vector<double> mass(n), mom_par(n), mom_perp(n);
+    for (int i = 0; i < n; ++i)
+    {
+        const double length = cells(i, C_L);
+        const double volume = PI * ((4. / 3.) * std::pow(R, 3) + R * R * length);
+        mass[i] = rho * volume;
+        const double diam = 2 * R, d2 = diam * diam, d3 = d2 * diam, d4 = d3 * diam;
+        const double l2 = length * length, l3 = l2 * length;
+        mom_par[i] = d4 * (length / 32 + diam / 60) * (rho * PI);
+        mom_perp[i] = d2 * (4 * d3 + 15 * length * d2 + 20 * l2 * diam + 10 * l3) / 480 * (rho * PI);
+    }
+    std::vector<V3> omega(n);
+    for (int i = 0; i < n; ++i)
+        omega[i] = cross(cell_n(cells, i), v3(cells(i, C_DNX), cells(i, C_DNY), cells(i, C_DNZ)));
+    Cells cn = cells;
+    std::vector<V3> lin, ang;
+    verlet_accelerations(cells, verlet_forces(cells, nb, p, noise), mass, mom_par, mom_perp, lin, ang);
+    const double h = 0.5 * dt;
+    std::vector<V3> w_half(n);
+    for (int i = 0; i < n; ++i)
+    {
+        const V3 ri = cell_r(cells, i), ni = cell_n(cells, i);
+        const double hl = cells(i, C_HALF_L);
+        const V3 vi = v3(cells(i, C_DRX), cells(i, C_DRY), cells(i, C_DRZ)) + h * lin[i];
+        const V3 wi = omega[i] + h * ang[i];
+        w_half[i] = wi;
+        const V3 pi = ri - hl * ni, qi = ri + hl * ni;
+        const V3 c = cross(wi, pi - qi);
+        const V3 half = v3(c.x / 2, c.y / 2, c.z / 2);
+        const V3 pn = pi + dt * (vi + half), qn = qi + dt * (vi - half);
+        const V3 rn = v3((pn.x + qn.x) / 2, (pn.y + qn.y) / 2, (pn.z + qn.z) / 2);
+        const double length = cells(i, C_L);
+        const V3 nn = v3((qn.x - pn.x) / length, (qn.y - pn.y) / length, (qn.z - pn.z) / length);
+        const V3 dni = cross(wi, ni);
+        cn(i, C_RX) = rn.x; cn(i, C_RY) = rn.y; cn(i, C_RZ) = rn.z;
+        cn(i, C_NX) = nn.x; cn(i, C_NY) = nn.y; cn(i, C_NZ) = nn.z;
+        cn(i, C_DRX) = vi.x; cn(i, C_DRY) = vi.y; cn(i, C_DRZ) = vi.z;
+        cn(i, C_DNX) = dni.x; cn(i, C_DNY) = dni.y; cn(i, C_DNZ) = dni.z;
+    }
+    normalize_orientations(cn);
+    Neighbors nb2 = nb;
+    update_neighbor_distances(cn, nb2);
+    verlet_accelerations(cn, verlet_forces(cn, nb2, p, noise), mass, mom_par, mom_perp, lin, ang);
+    for (int i = 0; i < n; ++i)
+    {
+        cn(i, C_DRX) += h * lin[i].x; cn(i, C_DRY) += h * lin[i].y; cn(i, C_DRZ) += h * lin[i].z;
+        const V3 wf = w_half[i] + h * ang[i];
+        const V3 dni = cross(wf, cell_n(cn, i));
+        cn(i, C_DNX) = dni.x; cn(i, C_DNY) = dni.y; cn(i, C_DNZ) = dni.z;
+    }
+    normalize_orientations(cn);
+    return cn;
+}
+
 struct LoopState {
     Cells cells;
     Neighbors nb;
@@ -1256,7 +1549,6 @@ inline void loop_init(LoopState& st, const Params3& p)
 // invariant pair forces once per attempt instead of once per stage.
 inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false)
 {
-    const Tableau tab = make_tableau(p.integration_mode);
     std::vector<int> to_divide(st.cells.n);
     int ndiv = 0;
     for (int i = 0; i < st.cells.n; ++i) { to_divide[i] = st.cells(i, C_L) > p.Ldiv; ndiv += to_divide[i]; }
@@ -1268,6 +1560,26 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
         st.rebuilds++;
     }
     const int n = st.cells.n;
+    if (p.integration_mode == 0)
+    {
+        // simulation.hpp:1279-1290, 1786-1798: one velocity-Verlet step at the fixed dt
+        if (p.M0 <= 0) throw std::runtime_error("Initial cell mass must be defined when using velocity Verlet");
+        const double rho = p.M0 / (PI * ((4. / 3.) * std::pow(p.R, 3) + p.R * p.R * p.L0));
+        st.cells = step_velocity_verlet(st.cells, st.nb, st.dt, p, rho, st.iter);
+        st.attempts++;
+        st.last_max_error = 0;
+        grow_cells(st.cells, st.dt, p.R);
+        update_neighbor_distances(st.cells, st.nb);
+        st.t += st.dt;
+        st.iter++;
+        if (st.iter % p.iter_update_neighbors == 0)
+        {
+            st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+            st.rebuilds++;
+        }
+        return;
+    }
+    const Tableau tab = make_tableau(p.integration_mode);
     Arr6 errors;
     int attempt = 0;
     Cells cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);

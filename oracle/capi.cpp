@@ -28,6 +28,7 @@ struct oracle_params {
     int n_threads;   // OpenMP threads for the reference's parallel loops (0 = default)
     int friction_mode;                // 0 NONE, 1 KINETIC cell-cell friction
     double cell_cell_coulomb_coeff;   // Coulomb cap of the friction (not positive: none)
+    double M0;                        // cell mass at length L0 (velocity Verlet)
 };
 
 struct oracle_ctx {
@@ -57,6 +58,7 @@ int oracle_create(const oracle_params* q, oracle_ctx** out)
     p.daughter_angle_xy_bound = q->daughter_angle_xy_bound; p.daughter_angle_z_bound = q->daughter_angle_z_bound;
     p.rng_seed = q->rng_seed; p.n_start_multithread = q->n_start_multithread;
     p.friction_mode = q->friction_mode; p.cell_cell_coulomb_coeff = q->cell_cell_coulomb_coeff;
+    p.M0 = q->M0;
 #ifdef _OPENMP
     if (q->n_threads > 0) omp_set_num_threads(q->n_threads);
 #endif
@@ -351,11 +353,12 @@ double oracle_integral6(double nz, double half_l, double ss) { return integral6(
 // cellSurfaceRepulsionForces (kind 0, mechanics.hpp:673-780) or cellSurfaceAdhesionForces
 // (kind 1, mechanics.hpp:800-910) of one cell with center height rz, orientation
 // (nx, 0, nz), half-length half_l and adhesion energy density sigma0, treated as
-// horizontal when nz < nz_threshold; the six generalized forces go to out6.  This is the
+// horizontal when nz < nz_threshold; the six generalized forces go to out6, in the
+// include_constraint form when `constraint` is set (the velocity-Verlet path).  This is the
 // single-cell form the reference's own tests call (testCellSurfaceRepulsionForces.cpp,
 // testCellSurfaceAdhesionForces.cpp), with ss = (R - rz) / nz.
 int oracle_surface_forces(int kind, double rz, double nx, double nz, double half_l, double sigma0,
-                          double R, double E0, double nz_threshold, double* out6)
+                          double R, double E0, double nz_threshold, int constraint, double* out6)
 {
     if (kind != 0 && kind != 1) return 1;
     Cells cells(1, NCOLS_REQUIRED_3D);
@@ -363,8 +366,8 @@ int oracle_surface_forces(int kind, double rz, double nx, double nz, double half
     cells(0, C_L) = 2 * half_l; cells(0, C_HALF_L) = half_l; cells(0, C_SIGMA0) = sigma0;
     std::vector<double> ss(1, sstar(rz, nz, R));
     std::vector<int> assume_2d(1, nz < nz_threshold);
-    Arr6 f = kind == 0 ? cell_surface_repulsion_forces(cells, ss, R, E0, assume_2d, false)
-                       : cell_surface_adhesion_forces(cells, ss, R, assume_2d, false);
+    Arr6 f = kind == 0 ? cell_surface_repulsion_forces(cells, ss, R, E0, assume_2d, false, constraint != 0)
+                       : cell_surface_adhesion_forces(cells, ss, R, assume_2d, false, constraint != 0);
     for (int k = 0; k < 6; ++k) out6[k] = f[k];
     return 0;
 }

@@ -35,6 +35,7 @@ class OracleParams(ctypes.Structure):
         ("daughter_angle_z_bound", ctypes.c_double), ("rng_seed", ctypes.c_ulonglong),
         ("n_start_multithread", ctypes.c_int), ("n_threads", ctypes.c_int),
         ("friction_mode", ctypes.c_int), ("cell_cell_coulomb_coeff", ctypes.c_double),
+        ("M0", ctypes.c_double),
     ]
 
 
@@ -86,7 +87,7 @@ def _load():
         "oracle_integral4": ([d, d, d], d),
         "oracle_integral5": ([d, d, d], d),
         "oracle_integral6": ([d, d, d], d),
-        "oracle_surface_forces": ([i, d, d, d, d, d, d, d, d, dp], i),
+        "oracle_surface_forces": ([i, d, d, d, d, d, d, d, d, i, dp], i),
         "oracle_det_log": ([d], d),
         "oracle_det_sincos": ([d, dp, dp], None),
     }

@@ -38,7 +38,7 @@ def forces(kind, rz, angle=None, nz=None, half_l=HALF_L):
         nz = math.sin(angle)
     nx = math.cos(angle) if angle is not None else math.sqrt(max(0.0, 1 - nz * nz))
     out = np.zeros(6)
-    rc = orc.LIB.oracle_surface_forces(kind, rz, nx, nz, half_l, SIGMA0, R, E0, NZ_THRESHOLD,
+    rc = orc.LIB.oracle_surface_forces(kind, rz, nx, nz, half_l, SIGMA0, R, E0, NZ_THRESHOLD, 0,
                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     assert rc == 0
     return out

@@ -261,6 +261,12 @@ inline void update_neighbor_distances(const Cells& cells, Neighbors& nb)
 // Auxiliary integrals (ABM-3d/ABM-3d-cpp/include/integrals.hpp)
 // ------------------------------------------------------------------------
 inline double sstar(double rz, double nz, double R) { return (R - rz) / nz; }        // :35-45
+// x^e for the integrals' exponents gamma + 1: x * x for the square, the C library for the
+// others.  g++ folds pow(x, 2.0) into x * x only where inlining makes the exponent a
+// constant, and the C library's pow may differ from x * x in the last bit, so the square is
+// written out: the last bit of an integral then does not depend on which calls the compiler
+// inlines (an unrelated edit once moved one cell's velocity by two ulps that way).
+inline double pow_e(double x, double e) { return e == 2.0 ? x * x : std::pow(x, e); }
 inline double phi(double rz, double nz, double R, double s) { return R - rz - s * nz; }  // :56-60
 
 // integrals.hpp:116-140
@@ -268,13 +274,13 @@ inline double integral1(double rz, double nz, double R, double half_l, double ga
 {
     if (ss > half_l)
     {
-        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
-        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        double o1 = pow_e(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = pow_e(phi(rz, nz, R, half_l), gamma + 1);
         return (o1 - o2) / (nz * (gamma + 1));
     }
     else if (ss > -half_l)
     {
-        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        double o1 = pow_e(phi(rz, nz, R, -half_l), gamma + 1);
         return o1 / (nz * (gamma + 1));
     }
     return 0;
@@ -287,13 +293,13 @@ inline double integral2(double rz, double nz, double R, double half_l, double ga
     double term2 = 0;
     if (ss > half_l)
     {
-        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
-        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        double o1 = pow_e(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = pow_e(phi(rz, nz, R, half_l), gamma + 1);
         term2 = -half_l * (o1 + o2);
     }
     else if (ss > -half_l)
     {
-        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        double o1 = pow_e(phi(rz, nz, R, -half_l), gamma + 1);
         term2 = -half_l * o1;
     }
     return (term1 + term2) / (nz * (gamma + 1));
@@ -1318,13 +1324,13 @@ inline double integral3(double rz, double nz, double R, double half_l, double ga
     double term2 = 0;
     if (ss > half_l)
     {
-        double o1 = std::pow(phi(rz, nz, R, -half_l), gamma + 1);
-        double o2 = std::pow(phi(rz, nz, R, half_l), gamma + 1);
+        double o1 = pow_e(phi(rz, nz, R, -half_l), gamma + 1);
+        double o2 = pow_e(phi(rz, nz, R, half_l), gamma + 1);
         term2 = half_l * half_l * (o1 - o2);
     }
     else if (ss > -half_l)
     {
-        term2 = half_l * half_l * std::pow(phi(rz, nz, R, -half_l), gamma + 1);
+        term2 = half_l * half_l * pow_e(phi(rz, nz, R, -half_l), gamma + 1);
     }
     return (term1 + term2) / (nz * (gamma + 1));
 }

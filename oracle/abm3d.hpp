@@ -506,6 +506,22 @@ struct Params3 {
     int friction_mode = 0;                 // FrictionMode: 0 NONE, 1 KINETIC (mechanics.hpp:61-65)
     double cell_cell_coulomb_coeff = 1.0;  // runSimulation's default (simulation.hpp:1162)
     double M0 = 0;                         // cell mass at length L0 (velocity Verlet)
+    // phenotype switching and its ramps (switch.hpp:26-144; simulation.hpp:1340-1371,
+    // 1650-1656, 1866-2022), two groups; basal-only compaction (simulation.hpp:1831-1856)
+    int switch_mode = 0;                   // SwitchMode: 0 NONE, 1 MARKOV, 2 INHERIT
+    int n_cells_start_switch = 0;
+    double switch_rates[4] = {0, 0, 0, 0}; // 2 x 2, row = current group: rates (MARKOV) or probabilities (INHERIT)
+    double group_growth_mean[2] = {0, 0}, group_growth_std[2] = {0, 0};   // per group, with switching on
+    int n_attributes = 0;
+    int attr_col[4] = {0, 0, 0, 0};
+    double attr_target[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    double switch_timescale = 0;
+    double max_gamma = 0;
+    int modulate_local_viscosity = 0;
+    double viscosity_lims[4] = {0, 0, 0, 0};   // 2 x 2: (min, max) per group
+    int max_coordination_number = 1;
+    int basal_only = 0;
+    double basal_min_overlap = 0;
 };
 
 struct Tableau {
@@ -1200,6 +1216,17 @@ inline V3 rotate_out_of_xy(V3 n, double theta)
 
 // Draw slots of one division try (policy): 0-3 angles, 4-5 length fraction,
 // 6-7 mother growth rate, 8-9 daughter growth rate.
+// growth-rate distribution of a cell's group: one distribution without switching, the
+// group's own with it (growth.hpp:634-644 samples growth_dists[group - 1])
+inline double growth_mean_of(const Params3& p, double group)
+{
+    return p.switch_mode == 0 ? p.growth_mean : p.group_growth_mean[(int)group == 1 ? 0 : 1];
+}
+inline double growth_std_of(const Params3& p, double group)
+{
+    return p.switch_mode == 0 ? p.growth_std : p.group_growth_std[(int)group == 1 ? 0 : 1];
+}
+
 inline double div_uniform(const Params3& p, int iter, int k, int tr, int slot)
 {
     return rng_uniform(p.rng_seed, RNG_PURPOSE_DIVIDE, (uint32_t)iter, (uint32_t)k,
@@ -1278,10 +1305,11 @@ inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double 
             total(im, C_T0) = t; nc(m, C_T0) = t;
         }
         for (int m = 0; m < n_divide; ++m)
-            total(idx_divide[m], C_GROWTH) = p.growth_mean + p.growth_std *
+            total(idx_divide[m], C_GROWTH) = growth_mean_of(p, total(idx_divide[m], C_GROUP)) +
+                growth_std_of(p, total(idx_divide[m], C_GROUP)) *
                 standard_normal(div_uniform(p, iter, m, ntries, 6), div_uniform(p, iter, m, ntries, 7));
         for (int m = 0; m < n_divide; ++m)
-            nc(m, C_GROWTH) = p.growth_mean + p.growth_std *
+            nc(m, C_GROWTH) = growth_mean_of(p, nc(m, C_GROUP)) + growth_std_of(p, nc(m, C_GROUP)) *
                 standard_normal(div_uniform(p, iter, m, ntries, 8), div_uniform(p, iter, m, ntries, 9));
         for (int m = 0; m < n_divide; ++m)
             for (int c = 0; c < cells.ncols; ++c) total(n + m, c) = nc(m, c);
@@ -1533,6 +1561,169 @@ inline Cells step_velocity_verlet(const Cells& cells, const Neighbors& nb, doubl
     return cn;
 }
 
+// ------------------------------------------------------------------------
+// Phenotype switching, attribute / gamma ramps, local viscosity, basal-only
+// compaction (the f4 row).  Random draws follow the Philox policy, purpose SWITCH,
+// counters (iteration, cell or pair, slot).
+// ------------------------------------------------------------------------
+inline double switch_uniform(const Params3& p, int iter, int k, int slot)
+{
+    return rng_uniform(p.rng_seed, RNG_PURPOSE_SWITCH, (uint32_t)iter, (uint32_t)k, (uint32_t)slot, 0u);
+}
+
+inline double switch_growth(const Params3& p, int group0, int iter, int k, int slot)
+{
+    return p.group_growth_mean[group0] + p.group_growth_std[group0] *
+           standard_normal(switch_uniform(p, iter, k, slot), switch_uniform(p, iter, k, slot + 1));
+}
+
+// switch.hpp:45-95 (switchGroupsMarkov): each cell leaves its group g for group j when a
+// uniform r falls in [sum of the earlier probabilities, + dt rate(g, j)), and then draws a
+// growth rate from group j's distribution.
+inline int switch_groups_markov(Cells& cells, const Params3& p, double dt, int iter)
+{
+    int switched = 0;
+    for (int i = 0; i < cells.n; ++i)
+    {
+        const int group = (int)cells(i, C_GROUP) - 1;
+        const double r = switch_uniform(p, iter, i, 0);
+        double total = 0;
+        for (int j = 0; j < 2; ++j)
+        {
+            if (j == group) continue;
+            const double prob = dt * p.switch_rates[group * 2 + j];
+            if (r > total && r < total + prob)
+            {
+                cells(i, C_GROUP) = j + 1;
+                cells(i, C_GROWTH) = switch_growth(p, j, iter, i, 2);
+                ++switched;
+                break;
+            }
+            total += prob;
+        }
+    }
+    return switched;
+}
+
+// switch.hpp:97-142 (switchGroupsInherit): for each pair of daughters of group g, with
+// probability 1 - P(g, g) one of the two, chosen by a second uniform, moves to the other
+// group and draws that group's growth rate.
+inline int switch_groups_inherit(Cells& cells, const std::vector<std::pair<int, int> >& pairs,
+                                 const Params3& p, int iter)
+{
+    int switched = 0;
+    for (size_t q = 0; q < pairs.size(); ++q)
+    {
+        const int i = pairs[q].first, j = pairs[q].second;
+        const int group = (int)cells(i, C_GROUP) - 1;
+        const double r = switch_uniform(p, iter, (int)q, 4);
+        double total = p.switch_rates[group * 2 + group];
+        if (!(r > total)) continue;
+        for (int k = 0; k < 2; ++k)
+        {
+            if (k == group) continue;
+            const double prob = p.switch_rates[group * 2 + k];
+            if (r > total && r < total + prob)
+            {
+                const int which = switch_uniform(p, iter, (int)q, 5) < 0.5 ? i : j;
+                cells(which, C_GROUP) = k + 1;
+                cells(which, C_GROWTH) = switch_growth(p, k, iter, (int)q, 6);
+                ++switched;
+                break;
+            }
+            total += prob;
+        }
+    }
+    return switched;
+}
+
+// simulation.hpp:1872-1938: each switched attribute moves toward its group's target at
+// |target1 - target2| / switch_timescale per unit time (at once with a zero timescale),
+// stopping at the target.
+inline void ramp_attributes(Cells& cells, const Params3& p, double dt)
+{
+    for (int k = 0; k < p.n_attributes; ++k)
+    {
+        const int col = p.attr_col[k];
+        const double t1 = p.attr_target[0][k], t2 = p.attr_target[1][k];
+        const double rate = p.switch_timescale == 0 ? std::numeric_limits<double>::infinity()
+                                                    : std::fabs(t1 - t2) / p.switch_timescale;
+        for (int i = 0; i < cells.n; ++i)
+        {
+            const bool g1 = (int)cells(i, C_GROUP) == 1;
+            const double own = g1 ? t1 : t2, other = g1 ? t2 : t1;
+            double& v = cells(i, col);
+            if (p.switch_timescale == 0 && v != own) v = own;
+            else if (own > other && v < own) { v += rate * dt; if (v > own) v = own; }
+            else if (own < other && v > own) { v -= rate * dt; if (v < own) v = own; }
+            else if (t1 == t2 && v != own) v = own;
+        }
+    }
+}
+
+// simulation.hpp:1940-1957: gamma rises toward max_gamma in group 1 and falls toward 0 in
+// group 2 at max_gamma / switch_timescale (at once with a zero timescale; simulation.hpp:1361-1364).
+inline void ramp_gamma(Cells& cells, const Params3& p, double dt)
+{
+    const double rate = p.switch_timescale == 0 ? std::numeric_limits<double>::infinity()
+                                                : p.max_gamma / p.switch_timescale;
+    for (int i = 0; i < cells.n; ++i)
+    {
+        double& g = cells(i, C_GAMMA);
+        if ((int)cells(i, C_GROUP) == 1)
+        {
+            if (g < p.max_gamma) { g += rate * dt; if (g > p.max_gamma) g = p.max_gamma; }
+        }
+        else if (g > 0) { g -= rate * dt; if (g < 0) g = 0; }
+    }
+}
+
+// simulation.hpp:1958-2020: the ambient viscosity of each cell interpolates between its
+// group's limits by the share of group-1 cells among its contacts (distance < 2R), the
+// denominator at least max_coordination_number, saturating at that many group-1 contacts.
+inline void modulate_viscosity(Cells& cells, const Neighbors& nb, const Params3& p)
+{
+    const int n = cells.n;
+    std::vector<int> total(n, 0), g1(n, 0);
+    for (int k = 0; k < nb.size(); ++k)
+    {
+        const int i = nb.i[k], j = nb.j[k];
+        if (norm(v3(nb.dx[k], nb.dy[k], nb.dz[k])) < 2 * p.R)
+        {
+            total[i] += 1; total[j] += 1;
+            if ((int)cells(i, C_GROUP) == 1) g1[j] += 1;
+            if ((int)cells(j, C_GROUP) == 1) g1[i] += 1;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+    {
+        const int group = (int)cells(i, C_GROUP) - 1;
+        const double vmin = p.viscosity_lims[group * 2], vmax = p.viscosity_lims[group * 2 + 1];
+        if (g1[i] >= p.max_coordination_number) cells(i, C_ETA0) = vmax;
+        else
+        {
+            const double ratio = (double)g1[i] / (double)std::max(total[i], p.max_coordination_number);
+            cells(i, C_ETA0) = vmin + ratio * (vmax - vmin);
+        }
+    }
+}
+
+// simulation.hpp:1831-1856: with the surface present, keep only the cells whose deepest
+// overlap R - rz + half_l nz exceeds basal_min_overlap; returns how many were dropped.
+inline int basal_compact(Cells& cells, const Params3& p)
+{
+    std::vector<int> keep;
+    for (int i = 0; i < cells.n; ++i)
+        if (p.R - cells(i, C_RZ) + cells(i, C_HALF_L) * cells(i, C_NZ) > p.basal_min_overlap) keep.push_back(i);
+    const int dropped = cells.n - (int)keep.size();
+    if (dropped == 0) return 0;
+    Cells kept((int)keep.size(), cells.ncols);
+    for (int c = 0; c < cells.ncols; ++c)
+        for (size_t r = 0; r < keep.size(); ++r) kept((int)r, c) = cells(keep[r], c);
+    cells = kept;
+    return dropped;
+}
+
 struct LoopState {
     Cells cells;
     Neighbors nb;
@@ -1558,14 +1749,22 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
     std::vector<int> to_divide(st.cells.n);
     int ndiv = 0;
     for (int i = 0; i < st.cells.n; ++i) { to_divide[i] = st.cells(i, C_L) > p.Ldiv; ndiv += to_divide[i]; }
+    const int n_before = st.cells.n;
     st.cells = divide_cells(st.cells, st.parents, st.t, p, to_divide, st.iter);
     if (ndiv > 0)
     {
         st.divisions += ndiv;
+        // simulation.hpp:1650-1656: daughters (mother's row, appended row) may switch group
+        if (p.switch_mode == 2 && st.cells.n >= p.n_cells_start_switch)
+        {
+            std::vector<std::pair<int, int> > pairs;
+            for (int i = 0, m = 0; i < n_before; ++i)
+                if (to_divide[i]) pairs.push_back(std::make_pair(i, n_before + m++));
+            switch_groups_inherit(st.cells, pairs, p, st.iter);
+        }
         st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
         st.rebuilds++;
     }
-    const int n = st.cells.n;
     if (p.integration_mode == 0)
     {
         // simulation.hpp:1279-1290, 1786-1798: one velocity-Verlet step at the fixed dt
@@ -1574,61 +1773,71 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
         st.cells = step_velocity_verlet(st.cells, st.nb, st.dt, p, rho, st.iter);
         st.attempts++;
         st.last_max_error = 0;
-        grow_cells(st.cells, st.dt, p.R);
-        update_neighbor_distances(st.cells, st.nb);
-        st.t += st.dt;
-        st.iter++;
-        if (st.iter % p.iter_update_neighbors == 0)
-        {
-            st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
-            st.rebuilds++;
-        }
-        return;
     }
-    const Tableau tab = make_tableau(p.integration_mode);
-    Arr6 errors;
-    int attempt = 0;
-    Cells cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
-    st.attempts++;
-    double max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
-    if (st.iter % p.iter_update_stepsize == 0)
+    else
     {
-        bool exceeded = (max_error > 1.0);
-        double q1 = 1.0 / (tab.error_order + 1);
-        double factor = 0.9 * std::pow(1.0 / max_error, q1);
-        if (factor >= 10) factor = 10;
-        else if (factor < 0.2) factor = 0.2;
-        int j = 0;
-        while (exceeded && j < p.max_tries_update_stepsize)
+        const Tableau tab = make_tableau(p.integration_mode);
+        Arr6 errors;
+        int attempt = 0;
+        Cells cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
+        st.attempts++;
+        double max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+        if (st.iter % p.iter_update_stepsize == 0)
         {
-            double dt_new = st.dt * factor;
-            cn = step_rk_adaptive(tab, st.cells, st.nb, dt_new, p, st.iter, attempt++, errors, cc_once);
+            bool exceeded = (max_error > 1.0);
+            double q1 = 1.0 / (tab.error_order + 1);
+            double factor = 0.9 * std::pow(1.0 / max_error, q1);
+            if (factor >= 10) factor = 10;
+            else if (factor < 0.2) factor = 0.2;
+            int j = 0;
+            while (exceeded && j < p.max_tries_update_stepsize)
+            {
+                double dt_new = st.dt * factor;
+                cn = step_rk_adaptive(tab, st.cells, st.nb, dt_new, p, st.iter, attempt++, errors, cc_once);
+                st.attempts++;
+                max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+                exceeded = (max_error > 1.0);
+                factor *= 0.9 * std::pow(1.0 / max_error, q1);
+                if (factor >= 10) { factor = 10; break; }
+                else if (factor < 0.2) { factor = 0.2; break; }
+                j++;
+            }
+            if (st.dt * factor < p.min_stepsize) factor = p.min_stepsize / st.dt;
+            else if (st.dt * factor > p.max_stepsize) factor = p.max_stepsize / st.dt;
+            st.dt *= factor;
+            cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
             st.attempts++;
             max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
-            exceeded = (max_error > 1.0);
-            factor *= 0.9 * std::pow(1.0 / max_error, q1);
-            if (factor >= 10) { factor = 10; break; }
-            else if (factor < 0.2) { factor = 0.2; break; }
-            j++;
         }
-        if (st.dt * factor < p.min_stepsize) factor = p.min_stepsize / st.dt;
-        else if (st.dt * factor > p.max_stepsize) factor = p.max_stepsize / st.dt;
-        st.dt *= factor;
-        cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
-        st.attempts++;
-        max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
+        st.last_max_error = max_error;
+        st.cells = cn;
     }
-    st.last_max_error = max_error;
-    (void)n;
-    st.cells = cn;
     grow_cells(st.cells, st.dt, p.R);
     update_neighbor_distances(st.cells, st.nb);
+    if (!p.no_surface && p.basal_only && basal_compact(st.cells, p) > 0)
+    {
+        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.rebuilds++;
+    }
     st.t += st.dt;
     st.iter++;
     if (st.iter % p.iter_update_neighbors == 0)
     {
         st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
         st.rebuilds++;
+    }
+    // simulation.hpp:1866-2022.  The reference compares its cell count from before the
+    // basal compaction here (and loops over that many cells); the current count is used.
+    if (p.switch_mode == 1 && st.cells.n >= p.n_cells_start_switch)
+        switch_groups_markov(st.cells, p, st.dt, st.iter);
+    if (p.switch_mode != 0)
+    {
+        ramp_attributes(st.cells, p, st.dt);
+        if (p.adhesion_mode != 0)
+        {
+            ramp_gamma(st.cells, p, st.dt);
+            if (p.modulate_local_viscosity) modulate_viscosity(st.cells, st.nb, p);
+        }
     }
 }
 

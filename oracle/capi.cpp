@@ -372,4 +372,63 @@ int oracle_surface_forces(int kind, double rz, double nx, double nz, double half
     return 0;
 }
 
+// phenotype switching (the f4 row): mode 0 NONE, 1 MARKOV, 2 INHERIT; rates 2 x 2 row-major
+// (row = current group); growth mean / std per group; n_attr switched attributes at columns
+// attr_col with targets attr_targets (2 x n_attr row-major, group 1 then group 2);
+// max_gamma for the gamma ramp; viscosity limits 2 x 2 (min, max per group) when modulate.
+int oracle_set_switching(oracle_ctx* c, int mode, int n_start, const double* rates, const double* growth_mean,
+                         const double* growth_std, double timescale, int n_attr, const int* attr_col,
+                         const double* attr_targets, double max_gamma, int modulate, const double* visc_lims,
+                         int max_coord)
+{
+    Params3& p = c->p;
+    if (mode < 0 || mode > 2 || n_attr < 0 || n_attr > 4 || max_coord < 1) return 1;
+    p.switch_mode = mode; p.n_cells_start_switch = n_start;
+    for (int k = 0; k < 4; ++k) p.switch_rates[k] = rates[k];
+    for (int g = 0; g < 2; ++g) { p.group_growth_mean[g] = growth_mean[g]; p.group_growth_std[g] = growth_std[g]; }
+    p.switch_timescale = timescale;
+    p.n_attributes = n_attr;
+    for (int k = 0; k < n_attr; ++k)
+    {
+        p.attr_col[k] = attr_col[k];
+        p.attr_target[0][k] = attr_targets[k];
+        p.attr_target[1][k] = attr_targets[n_attr + k];
+    }
+    p.max_gamma = max_gamma;
+    p.modulate_local_viscosity = modulate;
+    for (int k = 0; k < 4; ++k) p.viscosity_lims[k] = visc_lims ? visc_lims[k] : 0.0;
+    p.max_coordination_number = max_coord;
+    return 0;
+}
+
+int oracle_set_basal(oracle_ctx* c, int basal_only, double min_overlap)
+{
+    c->p.basal_only = basal_only; c->p.basal_min_overlap = min_overlap;
+    return 0;
+}
+
+// the pieces on their own, on the context's cells
+int oracle_switch_markov(oracle_ctx* c, double dt, int iter) { return switch_groups_markov(c->st.cells, c->p, dt, iter); }
+
+int oracle_switch_inherit(oracle_ctx* c, const int* pairs, int n_pairs, int iter)
+{
+    std::vector<std::pair<int, int> > v;
+    for (int q = 0; q < n_pairs; ++q) v.push_back(std::make_pair(pairs[2 * q], pairs[2 * q + 1]));
+    return switch_groups_inherit(c->st.cells, v, c->p, iter);
+}
+
+// simulation.hpp:1872-2022 on the context's cells and neighbor rows
+int oracle_switch_ramps(oracle_ctx* c, double dt)
+{
+    ramp_attributes(c->st.cells, c->p, dt);
+    if (c->p.adhesion_mode != 0)
+    {
+        ramp_gamma(c->st.cells, c->p, dt);
+        if (c->p.modulate_local_viscosity) modulate_viscosity(c->st.cells, c->st.nb, c->p);
+    }
+    return 0;
+}
+
+int oracle_basal_compact(oracle_ctx* c) { return basal_compact(c->st.cells, c->p); }
+
 }   // extern "C"

@@ -56,6 +56,7 @@ inline double philox_u01(uint32_t hi, uint32_t lo)
 // streams never overlap.
 const uint32_t RNG_PURPOSE_NOISE = 0x4E6F6973u;
 const uint32_t RNG_PURPOSE_DIVIDE = 0x44697669u;
+const uint32_t RNG_PURPOSE_SWITCH = 0x53776974u;
 
 inline void rng_key(uint64_t seed, uint32_t purpose, uint32_t& k0, uint32_t& k1)
 {

@@ -89,6 +89,12 @@ def _load():
         "oracle_integral6": ([d, d, d], d),
         "oracle_surface_forces": ([i, d, d, d, d, d, d, d, d, i, dp], i),
         "oracle_det_log": ([d], d),
+        "oracle_set_switching": ([vp, i, i, dp, dp, dp, d, i, ip, dp, d, i, dp, i], i),
+        "oracle_set_basal": ([vp, i, d], i),
+        "oracle_switch_markov": ([vp, d, i], i),
+        "oracle_switch_inherit": ([vp, ip, i, i], i),
+        "oracle_switch_ramps": ([vp, d], i),
+        "oracle_basal_compact": ([vp], i),
         "oracle_det_sincos": ([d, dp, dp], None),
     }
     for name, (args, res) in sig.items():

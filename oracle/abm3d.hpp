@@ -522,6 +522,9 @@ struct Params3 {
     int max_coordination_number = 1;
     int basal_only = 0;
     double basal_min_overlap = 0;
+    // variable-gamma JKR table (IsotropicJKRDataVariableGamma, mechanics.hpp:159-199): radii on the
+    // overlap mesh jkr_overlaps x the gamma mesh jkr_gammas, overlap-major; used when non-empty
+    std::vector<double> jkr_gammas, jkr_radii2;
 };
 
 struct Tableau {
@@ -643,6 +646,71 @@ inline void jkr_forces(V3 d12, double R, double E0, double gamma, double s, doub
     }
 }
 
+// adhesion.hpp:412-526 (forcesIsotropicJKRLagrange, variable gamma, interpolate = true): the
+// contact radius interpolated bilinearly between the four table points around (delta, gamma),
+// each neighbor chosen on the side of the value; then the forces of jkr_forces.
+inline void jkr_forces_variable(V3 d12, double R, double E0, double gamma, double s, double t,
+                                const std::vector<double>& tab_delta, const std::vector<double>& tab_gamma,
+                                const std::vector<double>& tab_radius, double max_overlap, double out[2][6],
+                                bool constraint = false, V3 n1 = V3{0, 0, 0}, V3 n2 = V3{0, 0, 0})
+{
+    for (int a = 0; a < 2; ++a) for (int k = 0; k < 6; ++k) out[a][k] = 0;
+    const double dist = norm(d12);
+    if (!(dist < 2 * R)) return;
+    const V3 d12n = v3(d12.x / dist, d12.y / dist, d12.z / dist);
+    double delta = 2 * R - dist;
+    if (max_overlap >= 0 && delta > max_overlap) delta = max_overlap;
+    int id1 = nearest_value(tab_delta, delta), ig1 = nearest_value(tab_gamma, gamma);
+    int id2 = (tab_delta[id1] < delta ? id1 + 1 : id1 - 1);
+    if (id1 > id2) std::swap(id1, id2);
+    int ig2 = (tab_gamma[ig1] < gamma ? ig1 + 1 : ig1 - 1);
+    if (ig1 > ig2) std::swap(ig1, ig2);
+    const size_t ng = tab_gamma.size();
+    const double d1 = tab_delta[id1], d2 = tab_delta[id2], g1 = tab_gamma[ig1], g2 = tab_gamma[ig2];
+    const double denom = (d2 - d1) * (g2 - g1);
+    const double w11 = (d2 - delta) * (g2 - gamma) / denom;
+    const double w12 = (d2 - delta) * (gamma - g1) / denom;
+    const double w21 = (delta - d1) * (g2 - gamma) / denom;
+    const double w22 = (delta - d1) * (gamma - g1) / denom;
+    double radius = 0;
+    radius += w11 * tab_radius[id1 * ng + ig1];
+    radius += w12 * tab_radius[id1 * ng + ig2];
+    radius += w21 * tab_radius[id2 * ng + ig1];
+    radius += w22 * tab_radius[id2 * ng + ig2];
+    const double Req = R / 2;
+    const double a3 = radius * radius * radius;
+    const double term1 = 4 * E0 * a3 / (3 * Req);
+    const double term2 = 4 * std::sqrt(PI * a3 * gamma * E0);
+    const V3 v = (term2 - term1) * d12n;
+    out[0][0] = -v.x; out[0][1] = -v.y; out[0][2] = -v.z;
+    out[1][0] = v.x; out[1][1] = v.y; out[1][2] = v.z;
+    if (!constraint)
+    {
+        out[0][3] = -s * v.x; out[0][4] = -s * v.y; out[0][5] = -s * v.z;
+        out[1][3] = t * v.x; out[1][4] = t * v.y; out[1][5] = t * v.z;
+    }
+    else
+    {
+        const V3 mv = v3(-v.x, -v.y, -v.z);
+        const double w1 = dot(n1, mv), w2 = dot(n2, mv);
+        const V3 a = (-w1) * n1 - v, b = w2 * n2 + v;
+        out[0][3] = s * a.x; out[0][4] = s * a.y; out[0][5] = s * a.z;
+        out[1][3] = t * b.x; out[1][4] = t * b.y; out[1][5] = t * b.z;
+    }
+}
+
+// simulation.hpp:120-145 (calculateJKRContactRadii over an overlap mesh and a gamma mesh),
+// overlap-major
+inline std::vector<double> jkr_radius_table2(const std::vector<double>& overlaps,
+                                             const std::vector<double>& gammas, double R, double E0)
+{
+    std::vector<double> radii(overlaps.size() * gammas.size());
+    for (size_t i = 0; i < overlaps.size(); ++i)
+        for (size_t j = 0; j < gammas.size(); ++j)
+            radii[i * gammas.size() + j] = jkr_contact_radius(overlaps[i], R / 2, E0, gammas[j]);
+    return radii;
+}
+
 // mechanics.hpp:1209-1350 (Hertz only) and :1390-1659 (Hertz + isotropic JKR), without
 // the friction term (add_friction adds it).  Returns dE/dq (n x 6).  `constraint` selects
 // include_constraint = true, the form velocity Verlet uses: the Hertz and hard-core rows
@@ -670,8 +738,12 @@ inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Para
         double gamma = adhesion ? std::min(cells(i, C_GAMMA), cells(j, C_GAMMA)) : 0.0;
         if (adhesion && gamma > 0)
         {
-            jkr_forces(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_radii, max_overlap, f,
-                       constraint, cell_n(cells, i), cell_n(cells, j));
+            if (p.jkr_gammas.empty())
+                jkr_forces(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_radii, max_overlap, f,
+                           constraint, cell_n(cells, i), cell_n(cells, j));
+            else
+                jkr_forces_variable(dij, R, p.E0, gamma, si, sj, p.jkr_overlaps, p.jkr_gammas, p.jkr_radii2,
+                                    max_overlap, f, constraint, cell_n(cells, i), cell_n(cells, j));
         }
         else
         {

@@ -372,6 +372,29 @@ int oracle_surface_forces(int kind, double rz, double nx, double nz, double half
     return 0;
 }
 
+// simulation.hpp:1379-1395 with variable gamma: overlap mesh LinSpaced(nd, 0, 2 (R - Rcell)),
+// gamma mesh LinSpaced(ng, 0, max_gamma), radii nd x ng overlap-major
+int oracle_jkr_table2(double R, double Rcell, double E0, double max_gamma, int nd, int ng,
+                      double* delta_out, double* gamma_out, double* radius_out)
+{
+    std::vector<double> d = linspaced(nd, 0, 2 * (R - Rcell)), g = linspaced(ng, 0, max_gamma);
+    std::vector<double> r = jkr_radius_table2(d, g, R, E0);
+    for (int i = 0; i < nd; ++i) delta_out[i] = d[i];
+    for (int j = 0; j < ng; ++j) gamma_out[j] = g[j];
+    for (size_t k = 0; k < r.size(); ++k) radius_out[k] = r[k];
+    return 0;
+}
+
+// install a variable-gamma table (IsotropicJKRDataVariableGamma, mechanics.hpp:159-199)
+int oracle_set_jkr_table2(oracle_ctx* c, const double* delta, int nd, const double* gamma, int ng,
+                          const double* radius)
+{
+    c->p.jkr_overlaps.assign(delta, delta + nd);
+    c->p.jkr_gammas.assign(gamma, gamma + ng);
+    c->p.jkr_radii2.assign(radius, radius + (size_t)nd * ng);
+    return 0;
+}
+
 // phenotype switching (the f4 row): mode 0 NONE, 1 MARKOV, 2 INHERIT; rates 2 x 2 row-major
 // (row = current group); growth mean / std per group; n_attr switched attributes at columns
 // attr_col with targets attr_targets (2 x n_attr row-major, group 1 then group 2);

@@ -89,6 +89,8 @@ def _load():
         "oracle_integral6": ([d, d, d], d),
         "oracle_surface_forces": ([i, d, d, d, d, d, d, d, d, i, dp], i),
         "oracle_det_log": ([d], d),
+        "oracle_jkr_table2": ([d, d, d, d, i, i, dp, dp, dp], i),
+        "oracle_set_jkr_table2": ([vp, dp, i, dp, i, dp], i),
         "oracle_set_switching": ([vp, i, i, dp, dp, dp, d, i, ip, dp, d, i, dp, i], i),
         "oracle_set_basal": ([vp, i, d], i),
         "oracle_switch_markov": ([vp, d, i], i),

@@ -173,3 +173,47 @@ def test_switching_inside_the_loop():
     assert 0 < g2.sum() < len(c)                        # 2e4 per unit time over 5e-5: about 63%
     assert np.all(c[g2, 17] > 0.072) and np.all(c[~g2, 17] == 0.072)
     assert np.all(c[~g2, 21] > 0) and np.all(c[g2, 21] < 50.0)
+
+
+def variable_table(max_gamma, nd=100, ng=50):
+    d, g, r = np.zeros(nd), np.zeros(ng), np.zeros(nd * ng)
+    orc.LIB.oracle_jkr_table2(R, 0.5, 3900.0, max_gamma, nd, ng, orc._dp(d), orc._dp(g), orc._dp(r))
+    return d, g, r
+
+
+def pair_forces(gamma, fixed=None, variable=None):
+    cells = colony(2, ncols=22)
+    cells[:, 1:7] = [[0, 0, 5, 1, 0, 0], [0, 1.45, 5, 1, 0, 0]]    # overlap 0.15
+    cells[:, 21] = gamma
+    o = make(cells, adhesion_mode=1)
+    if fixed is not None:
+        o.set_jkr_table(*fixed)
+    else:
+        d, g, r = variable
+        orc.LIB.oracle_set_jkr_table2(o._c, orc._dp(d), len(d), orc._dp(g), len(g), orc._dp(r))
+    o.build_neighbors()
+    return o.cell_cell_forces()
+
+
+def test_variable_gamma_jkr_table():
+    """IsotropicJKRDataVariableGamma (mechanics.hpp:159-199, adhesion.hpp:412-526), the table the
+    driver builds when switching ramps gamma (simulation.hpp:1379-1395): radii on
+    LinSpaced(overlap) x LinSpaced(0, max_gamma), interpolated bilinearly.  Its gamma = 0
+    column is the Hertz radius sqrt(Req delta), its last column the fixed-gamma table at
+    max_gamma; the pair forces it gives equal the fixed table's at a mesh gamma and differ by
+    the interpolation in gamma between mesh points (4e-4 at gamma = 37.3 with 50 points up to
+    100; near gamma = 0, where the radius grows like gamma^(1/3), the reference's table is
+    coarser: 10 % at gamma = 0.5)."""
+    d, g, r = variable_table(100.0)
+    r2 = r.reshape(len(d), len(g))
+    np.testing.assert_allclose(r2[:, 0], np.sqrt(R / 2 * d), rtol=1e-14, atol=1e-15)
+    df, rf = orc.jkr_table(R, 0.5, 3900.0, 100.0)
+    assert np.array_equal(d, df) and np.array_equal(r2[:, -1], rf)
+    for gamma in (100.0, g[2], g[25]):
+        fv = pair_forces(gamma, variable=(d, g, r))
+        ff = pair_forces(gamma, fixed=orc.jkr_table(R, 0.5, 3900.0, gamma))
+        assert np.abs(fv - ff).max() <= 1e-13 * np.abs(ff).max(), gamma
+    fv = pair_forces(37.3, variable=(d, g, r))
+    ff = pair_forces(37.3, fixed=orc.jkr_table(R, 0.5, 3900.0, 37.3))
+    rel = np.abs(fv - ff).max() / np.abs(ff).max()
+    assert 1e-6 < rel < 1e-3, rel

@@ -2,6 +2,10 @@
 // mechanics step of kmnam/biofilm-ABMs (ABM-3d/ABM-3d-cpp), used by tests/,
 // __graft_entry__.smoke() and bench.py's CPU baseline leg as the checker.  The
 // product library never links, includes or calls anything under oracle/.
+// Beyond the adaptive Runge-Kutta loop it restates, for the steps next to that path:
+// cell-cell kinetic friction, the velocity-Verlet integrator with the constrained force
+// forms, phenotype switching with its ramps, local viscosity and basal-only compaction,
+// the variable-gamma JKR table, and the JKR equilibrium solves for gamma from eqdist.
 //
 // Every function names the reference file:line it restates.  The reference
 // itself cannot be compiled here (Eigen, Boost and CGAL are absent), so:

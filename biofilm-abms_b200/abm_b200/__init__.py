@@ -233,6 +233,15 @@ def jkr_optimal_gamma(R, Rcell, E0, eqdist):
     return out.value
 
 
+def set_gamma_from_eqdist(cells, R, Rcell, E0, eqdist):
+    """simulation.hpp:1354-1371: the adhesion energy density that puts two cells at eqdist
+    (jkrOptimalSurfaceEnergyDensity), written into the gamma column (21) of a 3-D cells array:
+    max_gamma for group-1 cells (column 20), 0 for the others.  Returns max_gamma."""
+    max_gamma = jkr_optimal_gamma(R, Rcell, E0, eqdist)
+    cells[:, 21] = np.where(cells[:, 20] == 1, max_gamma, 0.0)
+    return max_gamma
+
+
 def jkr_radius_table(R, Rcell, E0, gamma, n_mesh=100):
     """Overlap mesh LinSpaced(n, 0, 2(R - Rcell)) and radii (simulation.hpp:86-104, 1379-1382)."""
     delta = np.zeros(n_mesh)

@@ -16,6 +16,7 @@ arguments of simulation.hpp:1355-1358).  Host code only.
     force balance is checked there alone."""
 import math
 
+import numpy as np
 import pytest
 
 import abm_b200
@@ -61,3 +62,13 @@ def test_overlap_cap_and_out_of_range_targets():
     for bad in (2 * R, 2 * R + 0.1, 2 * RCELL - 1e-3, 0.0):
         with pytest.raises(RuntimeError, match="ABM_ERR_ARG"):
             abm_b200.jkr_optimal_gamma(R, RCELL, E0, bad)
+
+
+def test_set_gamma_from_eqdist_follows_the_driver():
+    """simulation.hpp:1366-1371: group-1 cells get max_gamma, every other group 0."""
+    cells = np.zeros((5, 22))
+    cells[:, 20] = [1, 2, 1, 3, 2]
+    cells[:, 21] = 7.0
+    g = abm_b200.set_gamma_from_eqdist(cells, R, RCELL, E0, 1.5)
+    assert g == abm_b200.jkr_optimal_gamma(R, RCELL, E0, 1.5)
+    assert list(cells[:, 21]) == [g, 0.0, g, 0.0, 0.0]

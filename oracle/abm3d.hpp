@@ -1538,6 +1538,8 @@ inline Arr6 verlet_forces(const Cells& cells, const Neighbors& nb, const Params3
             Arr6 rep = cell_surface_repulsion_forces(cells, ss, p.R, p.E0, a2, false, true);
             for (int i = 0; i < n; ++i)
             {
+                // row norms of the six generalized components, summed in order (Eigen's
+                // vectorised reduction may pair them otherwise: an ulp, only ever deciding a tie)
                 double sf = 0, sr = 0;
                 for (int c = 0; c < 6; ++c)
                 {

@@ -141,10 +141,14 @@ extern "C" int abm_read_cells(const char* path, double* cells, int cap_rows, int
             ptext += line.substr(2, eq - 2) + " = " + line.substr(eq + 3) + "\n";
             continue;
         }
+        // tokens split at tabs as std::getline(ss, token, '\t') splits them: a trailing tab
+        // ends the row instead of starting an empty token; a blank line is skipped above,
+        // where the reference would append a row of unset values
         int j = 0;
         size_t a = 0;
         while (a <= line.size())
         {
+            if (a == line.size() && j > 0) break;
             size_t b = line.find('\t', a);
             if (b == std::string::npos) b = line.size();
             const std::string tok = line.substr(a, b - a);

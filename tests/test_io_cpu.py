@@ -75,3 +75,22 @@ def test_empty_population_and_errors(tmp_path):
         frames.write_cells(str(path), np.zeros((3, 10)), None)
     with pytest.raises(RuntimeError, match="cannot open"):
         frames.read_cells(str(tmp_path / "missing.txt"))
+
+
+def test_read_cells_accepts_trailing_tabs_and_crlf(tmp_path):
+    """readCells (utils.hpp:96-139) splits rows with std::getline(ss, token, '\\t'), which yields
+    no empty token after a trailing tab, and std::stod ignores a trailing carriage return."""
+    cells = state_3d(20)
+    plain = tmp_path / "plain.txt"
+    frames.write_cells(str(plain), cells, PARAMS)
+    text = plain.read_text()
+    odd = tmp_path / "odd.txt"
+    odd.write_bytes("".join(line + ("\t\r\n" if not line.startswith("#") else "\r\n")
+                            for line in text.splitlines()).encode())
+    a, pa = frames.read_cells(str(plain))
+    b, pb = frames.read_cells(str(odd))
+    assert pa == pb and np.array_equal(a, b)
+    bad = tmp_path / "bad.txt"
+    bad.write_text("1\t\t2\n")
+    with pytest.raises(RuntimeError, match="not a number"):
+        frames.read_cells(str(bad))

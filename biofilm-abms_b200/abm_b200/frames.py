@@ -64,12 +64,16 @@ def write_lineage(path, parents):
     _check(LIB.abm_write_lineage(os.fsencode(path), a.ctypes.data_as(_c_int_p), len(a)), "abm_write_lineage")
 
 
+ABSENT = -2   # an ID the lineage file does not list (-1 is the parent of an initial cell)
+
+
 def read_lineage(path):
-    """readLineage: parents indexed by cell ID."""
+    """readLineage (utils.hpp:265-287): parents indexed by cell ID.  The reference returns a map;
+    IDs below the largest one that the file does not list read as ABSENT."""
     p = os.fsencode(path)
     n = ctypes.c_int()
     _check(LIB.abm_read_lineage(p, None, 0, ctypes.byref(n)), "abm_read_lineage")
-    out = np.zeros(n.value, dtype=np.int32)
+    out = np.full(n.value, ABSENT, dtype=np.int32)
     _check(LIB.abm_read_lineage(p, out.ctypes.data_as(_c_int_p), len(out), ctypes.byref(n)), "abm_read_lineage")
     return out
 

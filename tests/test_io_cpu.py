@@ -94,3 +94,9 @@ def test_read_cells_accepts_trailing_tabs_and_crlf(tmp_path):
     bad.write_text("1\t\t2\n")
     with pytest.raises(RuntimeError, match="not a number"):
         frames.read_cells(str(bad))
+
+
+def test_sparse_lineage_marks_absent_ids(tmp_path):
+    path = tmp_path / "sparse.txt"
+    path.write_text("0\t-1\n3\t0\n")
+    assert list(frames.read_lineage(str(path))) == [-1, frames.ABSENT, frames.ABSENT, 0]

@@ -328,8 +328,9 @@ int abm_read_cells(const char* path, double* cells, int cap_rows, int cap_cols, 
                    char* params, int params_cap);
 /* writeLineage (utils.hpp:296-311): "i<TAB>parents[i]" for i < n. */
 int abm_write_lineage(const char* path, const int* parents, int n);
-/* readLineage (utils.hpp:265-288): parents[child] = parent; *n = largest child ID + 1.
- * With parents == NULL only *n is set. */
+/* readLineage (utils.hpp:265-287): parents[child] = parent; *n = largest child ID + 1.
+ * Entries for IDs the file does not list are left as the caller set them (the reference
+ * returns a map).  With parents == NULL only *n is set. */
 int abm_read_lineage(const char* path, int* parents, int cap, int* n);
 const char* abm_io_last_error(void);
 

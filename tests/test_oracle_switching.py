@@ -217,3 +217,26 @@ def test_variable_gamma_jkr_table():
     ff = pair_forces(37.3, fixed=orc.jkr_table(R, 0.5, 3900.0, 37.3))
     rel = np.abs(fv - ff).max() / np.abs(ff).max()
     assert 1e-6 < rel < 1e-3, rel
+
+
+def test_inherited_switching_at_division_inside_the_loop():
+    """simulation.hpp:1617-1656: cells past Ldiv divide, and with P(stay) = 0 every pair of
+    daughters (the mother's row, the appended row) ends with exactly one daughter in group 2."""
+    import abm_b200
+    n = 16
+    cells = colony(n, spacing=9.0)
+    _, p = abm_b200.make_params(adhesion_mode=0, no_surface=1, max_stepsize=1e-6, growth_mean=0.7,
+                                growth_std=0.0, iter_update_neighbors=10 ** 6)
+    cells[:, 13] = p["Ldiv"] + 0.05
+    cells[:, 14] = cells[:, 13] / 2
+    o = orc.Oracle(p)
+    o.set_cells(cells)
+    o.set_parents(np.full(n, -1, dtype=np.int32))
+    switching(o, mode=2, rates=(0.0, 1.0, 0.0, 1.0), growth=((0.7, 1.4), (0.0, 0.0)))
+    o.loop_init()
+    o.iterate(1)
+    c = o.cells()
+    assert len(c) == 2 * n
+    g2 = c[:, 20] == 2
+    assert g2.sum() == n and np.all(g2[:n] ^ g2[n:])     # one daughter of each pair
+    assert np.all(c[g2, 16] == 1.4) and np.all(c[~g2, 16] == 0.7)

@@ -217,9 +217,13 @@ double oracle_nearest_body_coord(const double* r, const double* n, double h, con
 // mechanics.hpp:1209-1659: dE/dq (n x 6 column-major) from the current table
 int oracle_cell_cell_forces(oracle_ctx* c, double* out)
 {
-    Arr6 f = cell_cell_forces(c->st.cells, c->st.nb, c->p);
-    add_friction(f, c->st.cells, c->st.nb, c->p);   // mechanics.hpp:1339-1346
-    std::memcpy(out, f.data(), f.size() * sizeof(double));
+    try
+    {
+        Arr6 f = cell_cell_forces(c->st.cells, c->st.nb, c->p);
+        add_friction(f, c->st.cells, c->st.nb, c->p);   // mechanics.hpp:1339-1346
+        std::memcpy(out, f.data(), f.size() * sizeof(double));
+    }
+    catch (const std::exception& e) { g_last_error = e.what(); return -1; }
     return 0;
 }
 
@@ -229,8 +233,12 @@ int oracle_conservative_forces(oracle_ctx* c, double* out)
     const Cells& cells = c->st.cells;
     std::vector<int> a2(cells.n);
     for (int i = 0; i < cells.n; ++i) a2[i] = cells(i, C_NZ) < c->p.nz_threshold;
-    Arr6 f = get_conservative_forces(cells, c->st.nb, c->p, a2, false);
-    std::memcpy(out, f.data(), f.size() * sizeof(double));
+    try
+    {
+        Arr6 f = get_conservative_forces(cells, c->st.nb, c->p, a2, false);
+        std::memcpy(out, f.data(), f.size() * sizeof(double));
+    }
+    catch (const std::exception& e) { g_last_error = e.what(); return -1; }
     return 0;
 }
 
@@ -241,8 +249,12 @@ int oracle_get_velocities(oracle_ctx* c, double* out)
     std::vector<int> a2(cells.n);
     for (int i = 0; i < cells.n; ++i) a2[i] = cells(i, C_NZ) < c->p.nz_threshold;
     Arr6 noise((size_t)cells.n * 6, 0.0);
-    Arr6 v = get_velocities(cells, c->st.nb, c->p, a2, noise, false);
-    std::memcpy(out, v.data(), v.size() * sizeof(double));
+    try
+    {
+        Arr6 v = get_velocities(cells, c->st.nb, c->p, a2, noise, false);
+        std::memcpy(out, v.data(), v.size() * sizeof(double));
+    }
+    catch (const std::exception& e) { g_last_error = e.what(); return -1; }
     return 0;
 }
 
@@ -251,12 +263,16 @@ int oracle_get_velocities(oracle_ctx* c, double* out)
 int oracle_rk_attempt(oracle_ctx* c, double dt, int iter, int attempt, double* cells_out,
                       double* errors_out, double* max_err)
 {
-    Tableau tab = make_tableau(c->p.integration_mode);
-    Arr6 errors;
-    Cells cn = step_rk_adaptive(tab, c->st.cells, c->st.nb, dt, c->p, iter, attempt, errors, true);
-    if (cells_out) std::memcpy(cells_out, cn.a.data(), cn.a.size() * sizeof(double));
-    if (errors_out) std::memcpy(errors_out, errors.data(), errors.size() * sizeof(double));
-    if (max_err) *max_err = max_scaled_error(c->st.cells, errors, c->p.max_error_allowed, c->p.min_error);
+    try
+    {
+        Tableau tab = make_tableau(c->p.integration_mode);
+        Arr6 errors;
+        Cells cn = step_rk_adaptive(tab, c->st.cells, c->st.nb, dt, c->p, iter, attempt, errors, true);
+        if (cells_out) std::memcpy(cells_out, cn.a.data(), cn.a.size() * sizeof(double));
+        if (errors_out) std::memcpy(errors_out, errors.data(), errors.size() * sizeof(double));
+        if (max_err) *max_err = max_scaled_error(c->st.cells, errors, c->p.max_error_allowed, c->p.min_error);
+    }
+    catch (const std::exception& e) { g_last_error = e.what(); return -1; }
     return 0;
 }
 

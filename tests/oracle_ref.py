@@ -206,7 +206,8 @@ class Oracle:
     def _n6(self, fn):
         n = LIB.oracle_get_num_cells(self._c)
         out = np.zeros((n, 6), order="F")
-        fn(self._c, _dp(out))
+        if fn(self._c, _dp(out)):
+            raise RuntimeError(LIB.oracle_last_error().decode())
         return out
 
     def cell_cell_forces(self):
@@ -223,7 +224,8 @@ class Oracle:
         cells = np.zeros((n, self.ncols), order="F")
         errors = np.zeros((n, 6), order="F")
         e = ctypes.c_double()
-        LIB.oracle_rk_attempt(self._c, dt, iteration, attempt, _dp(cells), _dp(errors), ctypes.byref(e))
+        if LIB.oracle_rk_attempt(self._c, dt, iteration, attempt, _dp(cells), _dp(errors), ctypes.byref(e)):
+            raise RuntimeError(LIB.oracle_last_error().decode())
         return cells, errors, e.value
 
     def loop_init(self):

@@ -139,3 +139,13 @@ def test_enters_conservative_forces_and_the_loop():
         ends.append(o.cells())
     assert np.array_equal(ends[0], ends[1])
     assert np.all(np.isfinite(ends[0])) and not np.array_equal(ends[0], ends[2])
+
+
+def test_missing_friction_column_is_an_error_not_a_crash():
+    cells = pair_cells((0.0, 1.4, 1.1 * R), (1.0, 0.0, 0.0), (0.3, 0.0, 0.0))[:, :21]
+    o = orc.Oracle(params())
+    o.set_cells(cells)
+    o.build_neighbors()
+    for call in (o.cell_cell_forces, o.conservative_forces, o.get_velocities):
+        with pytest.raises(RuntimeError, match="friction column"):
+            call()

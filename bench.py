@@ -48,6 +48,7 @@ N_CELLS = 100_000
 SEED = 1
 P_CONTACT = 0.9
 FLUSH_BYTES = 256 << 20
+BINDING_MAX_DT = 1e-4      # h: a cap that the error test, not the cap, binds at
 
 
 def parse_args(argv=None):
@@ -76,6 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--bpsm", type=int, default=0, help="screened pair pass: blocks per SM")
     ap.add_argument("--pair-sum", type=int, default=0, help="1: shares summed in the first attempt, 2: separately")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-binding", action="store_true",
+                    help="skip the second comparison with dt capped at 1e-4 h instead of 1e-6 h")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--profile-steps", type=int, default=200)
     return ap.parse_args(argv)
@@ -187,10 +190,18 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def workload(n, seed):
+def workload(n, seed, lib=None):
+    """The seeded 100k-cell state.  `lib`: the oracle's build of the generator, so that the
+    reference arm draws the same state without loading the product library."""
     from abm_b200 import workloads
     radius = 300.0 * (n / 100000.0) ** 0.5
-    return workloads.biofilm_3d(n=n, seed=seed, disk_radius=radius, p_contact=P_CONTACT)
+    return workloads.biofilm_3d(n=n, seed=seed, disk_radius=radius, p_contact=P_CONTACT, lib=lib)
+
+
+def oracle_module():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ref
+    return oracle_ref
 
 
 VARIANTS = {"plain": dict(precision=0, controller=0), "chosen": dict(precision=1, controller=1)}
@@ -263,17 +274,20 @@ def measured_peak_hbm():
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle run the way the reference runs
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(cells, args, steps, n_threads):
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import abm_b200
-    import oracle_ref as orc
+def oracle_for(cells, args, n_threads):
+    """The oracle on the benchmark state, with its O(n^2) getCellNeighbors done (timed)."""
+    import abm_b200                                  # parameter structs only: no library load
+    orc = oracle_module()
     _, pd = abm_b200.make_params(**{k: v for k, v in sim_params(args, args.n).items()
                                    if k not in ("cap_cells", "precision", "pair_lanes", "controller")})
     o = orc.Oracle(pd, jkr=orc.jkr_table(0.8, 0.5, 3900.0, 100.0, 100), n_threads=n_threads)
     o.set_cells(cells)
     t0 = time.perf_counter()
     o.loop_init()                                  # O(n^2) getCellNeighbors
-    t_build = time.perf_counter() - t0
+    return o, pd, time.perf_counter() - t0
+
+
+def cpu_reference_rate(o, pd, t_build, args, steps):
     t0 = time.perf_counter()
     o.iterate(steps, 0, 0)                         # pair forces recomputed per stage
     t_steps = time.perf_counter() - t0
@@ -305,12 +319,14 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return                                     # rank 0 alone times the host reference
-    cells, info = workload(args.n, SEED)
+    # the oracle's build of the generator: this arm loads no product library
+    cells, info = workload(args.n, SEED, lib=oracle_module().LIB)
     cores, model = cpu_info()
     # each reference step is one accepted iteration at n = 100k (~0.1-0.5 s on the host);
     # the run is bounded to about two minutes of CPU work
     steps = max(1, min(args.steps, 60))
-    value, sample, extra = cpu_reference_rate(cells, args, steps, cores)
+    o, pd, t_build = oracle_for(cells, args, cores)
+    value, sample, extra = cpu_reference_rate(o, pd, t_build, args, steps)
     ms = 1000.0 * args.n / value
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
             "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -325,9 +341,9 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def make_sim(args, variant, cells, weights):
+def make_sim(args, variant, cells, weights, **over):
     import abm_b200
-    sim = abm_b200.Simulation(**sim_params(args, args.n, variant))
+    sim = abm_b200.Simulation(**dict(sim_params(args, args.n, variant), **over))
     sim.upload_cells(cells)
     if VARIANTS[variant]["controller"] == 1:
         sim.set_stepsize_weights(weights)
@@ -424,13 +440,11 @@ def relerr(a, b):
     return {"max_rel": mx, "rms_rel": rms}
 
 
-def mixed_precision_errors(args, cells):
-    """Per-step error of the mixed-precision path against the FP64 path (which
-    matches the CPU oracle to <= 1e-10): pair forces dE/dq, velocities, and one RK
-    step's position/orientation increment."""
+def gpu_step_outputs(args, cells, dt=1e-6):
+    """Pair forces dE/dq, velocities, and one RK attempt at dt (new cells and the
+    controller's scaled error norm E) of both precisions on the benchmark state."""
     import abm_b200
     out = {}
-    sims = {}
     for name, prec in (("fp64", 0), ("mixed", 1)):
         sim = abm_b200.Simulation(cap_cells=args.n, integration_mode=args.tableau, precision=prec,
                                   max_stepsize=1e-6, max_error_allowed=1e-8)
@@ -438,21 +452,98 @@ def mixed_precision_errors(args, cells):
         sim.get_cell_neighbors()
         f = sim.cell_cell_forces()
         v = sim.get_velocities()
-        c1, _, e = sim.step_runge_kutta_adaptive(1e-6)
-        sims[name] = (f, v, c1[:, 1:7] - cells[:, 1:7], e)
+        c1, _, e = sim.step_runge_kutta_adaptive(dt)
+        out[name] = dict(forces=f, velocities=v, cells=c1, E=e)
         sim.close()
-    f64, v64, d64, e64 = sims["fp64"]
-    f32, v32, d32, e32 = sims["mixed"]
-    out["pair_forces"] = relerr(f32, f64)
-    out["velocities"] = relerr(v32, v64)
-    out["step_increment_dt_1e-6"] = relerr(d32, d64)
-    out["scaled_error_norm"] = {"fp64": e64, "mixed": e32}
-    out["against"] = "FP64 path of this library (matches the CPU oracle to <= 1e-10)"
     return out
 
 
-def run_b200(args):
+def rk_units(c_a, c_b, cells, tol=1e-8):
+    """The error test's own units (simulation.hpp:1697-1705): max over cells and the six
+    coordinates of |y1_a - y1_b| / (tol (1 + |y0|))."""
     import numpy as np
+    y0 = cells[:, 1:7]
+    return float((np.abs(c_a[:, 1:7] - c_b[:, 1:7]) / (tol * (1 + np.abs(y0)))).max())
+
+
+def step_errors(gpu, ref, cells, against, dt=1e-6):
+    """Per-step error of both GPU precisions against `ref` (the CPU oracle, or the FP64
+    path when the oracle leg is skipped): forces and velocities as normwise relative
+    errors, and the RK step in the error test's units beside the step's own scaled
+    error norm E (what the error test compares with 1)."""
+    out = {"against": against, "dt_h": dt}
+    for name in ("mixed", "fp64"):
+        g = gpu[name]
+        out[name] = {"pair_forces": relerr(g["forces"], ref["forces"]),
+                     "velocities": relerr(g["velocities"], ref["velocities"]),
+                     "step_in_rk_units": rk_units(g["cells"], ref["cells"], cells),
+                     "scaled_error_norm": g["E"]}
+    out["reference_scaled_error_norm"] = ref["E"]
+    return out
+
+
+def oracle_step_outputs(o, dt=1e-6):
+    c1, _, e = o.rk_attempt(dt)
+    return dict(forces=o.cell_cell_forces(), velocities=o.get_velocities(), cells=c1, E=e)
+
+
+def survey_b_step(P, E, s, K=100):
+    """Algorithmic bytes per accepted cell-step of the FP64 plain path, B_step(s, P, E, K):
+    pair refresh and force [8P + 56 + 48], E evaluations of B_eval(s) = 232 s + 24 s (s - 1)
+    + 144 + 48 s, growth 24, and the cell list and pair build amortised over K."""
+    b_eval = 232 * s + 24 * s * (s - 1) + 144 + 48 * s
+    return (8 * P + 56 + 48) + E * b_eval + 24 + (56 + 4 + 16 + 8 * P) / K
+
+
+STAGES = {1: 2, 2: 4, 3: 6, 4: 7}
+
+
+def rebuild_cost(sim, stream, flush, steady_ms):
+    """Device time a periodic neighbor rebuild adds to the loop: the iteration that
+    launches it and the one after (whose pair pass screens every pair again), each timed
+    like a step (L2 flushed before it), minus two steady steps."""
+    import torch
+    K = sim.params.iter_update_neighbors
+    it = sim.clock()[2]
+    sim.iterate((K - 1 - it % K) % K, stats=False)      # up to the iteration that launches it
+    r0 = sim.stats()["rebuilds"]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            sim.iterate(1, stats=False)
+            b.record(stream)
+    torch.cuda.synchronize()
+    assert sim.stats()["rebuilds"] == r0 + 1, "the timed pair of iterations must hold one rebuild"
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    return max(0.0, ms - 2 * steady_ms), ms
+
+
+def time_binding(args, variant, cells, weights, flush, world, device, local, rebuild_extra_ms):
+    """The same variant with dt free to grow to 1e-4 h, where the error test, not the cap,
+    sets the step: W + 10 untimed iterations (dt climbs from 1e-6 h by at most 10x per
+    step), then `steps` timed ones as in time_variant."""
+    import torch
+    a = argparse.Namespace(**vars(args))
+    a.warmup = args.warmup + 10
+    sim, _ = make_sim(args, variant, cells, weights, max_stepsize=BINDING_MAX_DT)
+    stream = torch.cuda.ExternalStream(sim.stream, device=device)
+    t = time_variant(sim, a, stream, flush, world, device, local)
+    sim.close()
+    K = 100
+    charge = max(0.0, args.steps / K - t["rebuilds"]) * rebuild_extra_ms
+    ms = t["ms_total"] + charge
+    return {"value": world * args.n * args.steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
+            "rk_evals_per_step": round(t["attempts"] / max(t["iterations"], 1), 3),
+            "rejected_first_attempts": t["rejected"], "retries": t["retries"],
+            "simulated_h_in_timed_region": t["t_sim_h"], "simulated_h_per_s": t["t_sim_h"] / (ms / 1000.0),
+            "rebuild_charge_ms": charge,
+            "clocks": {k: t["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+
+
+def run_b200(args):
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -471,8 +562,15 @@ def run_b200(args):
         stream = torch.cuda.ExternalStream(sim.stream, device=device)
         t = time_variant(sim, args, stream, flush, world, device, local)
         t["pairs"] = pairs
-        t["value"] = world * args.n * args.steps / (t["ms_total"] / 1000.0)
-        t["kernels"], t["rebuild_ms"] = kernel_groups(sim, args, variant)
+        t["kernels"], _ = kernel_groups(sim, args, variant)
+        # the periodic rebuild (one per iter_update_neighbors = 100 iterations) at its share
+        # of the timed steps, when the timed region held fewer than its share
+        steady = t["ms_total"] / args.steps
+        t["rebuild_extra_ms"], t["rebuild_pair_ms"] = rebuild_cost(sim, stream, flush, steady)
+        t["rebuild_extra_ms"] = reduce_max(t["rebuild_extra_ms"], device, world)
+        t["rebuild_charge_ms"] = max(0.0, args.steps / 100 - t["rebuilds"]) * t["rebuild_extra_ms"]
+        t["ms_charged"] = t["ms_total"] + t["rebuild_charge_ms"]
+        t["value"] = world * args.n * args.steps / (t["ms_charged"] / 1000.0)
         if variant == head:
             # e2e through the C ABI with pinned host buffers
             ncols = cells.shape[1]
@@ -499,37 +597,63 @@ def run_b200(args):
         results[variant] = t
 
     h = results[head]
+    P = h["pairs"] / args.n
+    E = h["attempts"] / max(h["iterations"], 1)
+    b_step = survey_b_step(P, E, STAGES[args.tableau])
+    roof = roofline(h["kernels"], h["rebuild_extra_ms"])
+    peak = roof["peak"]
+    roof["b_step_model"] = {"bytes_per_cell_step": b_step, "pairs_per_cell": P, "rk_evals_per_step": E,
+                            "achieved": b_step * h["value"] / world / 1e9,
+                            "frac": b_step * h["value"] / world / 1e9 / peak, "unit": "GB/s",
+                            "note": "whole step, FP64 element widths, against the same peak"}
     line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": h["ms_total"] / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": h["ms_charged"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32" if head == "chosen" else "f64",
             "data": "synthetic (seeded biofilm state, p_contact=%g)" % P_CONTACT,
-            "config": config(args, info, {"pairs_per_cell": round(h["pairs"] / args.n, 3),
-                                          "rk_evals_per_step": round(h["attempts"] / max(h["iterations"], 1), 3),
+            "config": config(args, info, {"pairs_per_cell": round(P, 3),
+                                          "rk_evals_per_step": round(E, 3),
                                           "rejected_first_attempts": h["rejected"],
                                           "rebuilds_in_timed_region": h["rebuilds"],
+                                          "rebuild_charge_ms": h["rebuild_charge_ms"],
                                           "simulated_h_in_timed_region": h["t_sim_h"],
                                           "stepsize_network": weights_note if head == "chosen" else None}),
             "e2e": h["e2e"], "gpu_launches": launches(head, h),
-            "roofline": roofline(h["kernels"], h["rebuild_ms"]),
+            "roofline": roof,
             "clocks": {k: h["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
     if other:
         o = results[other]
-        line[other] = {"value": o["value"], "ms_per_step": o["ms_total"] / args.steps,
+        line[other] = {"value": o["value"], "ms_per_step": o["ms_charged"] / args.steps,
                        "rk_evals_per_step": round(o["attempts"] / max(o["iterations"], 1), 3),
                        "rejected_first_attempts": o["rejected"], "simulated_h_in_timed_region": o["t_sim_h"],
+                       "rebuild_charge_ms": o["rebuild_charge_ms"],
                        "kernels_ms_per_launch": {k: v[1] for k, v in o["kernels"].items()},
                        "clocks": {k: o["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
         chosen, plain = results["chosen"], results["plain"]
         line["chosen_over_plain"] = {"accepted_cell_steps": chosen["value"] / plain["value"],
-                                     "simulated_time_per_s": (chosen["t_sim_h"] / chosen["ms_total"]) /
-                                                             (plain["t_sim_h"] / plain["ms_total"])}
+                                     "simulated_time_per_s": (chosen["t_sim_h"] / chosen["ms_charged"]) /
+                                                             (plain["t_sim_h"] / plain["ms_charged"])}
+        if not args.no_binding:
+            bind = {v: time_binding(args, v, cells, weights, flush, world, device, local,
+                                    results[v]["rebuild_extra_ms"]) for v in ("plain", "chosen")}
+            bind["max_stepsize_h"] = BINDING_MAX_DT
+            bind["chosen_over_plain"] = {
+                "accepted_cell_steps": bind["chosen"]["value"] / bind["plain"]["value"],
+                "simulated_time_per_s": bind["chosen"]["simulated_h_per_s"] / bind["plain"]["simulated_h_per_s"]}
+            line["error_bound_dt"] = bind
     if rank == 0 and world == 1 and "chosen" in results:
-        line["mixed_precision_error"] = mixed_precision_errors(args, cells)
+        gpu = gpu_step_outputs(args, cells)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores, model = cpu_info()
-        v, sample, extra = cpu_reference_rate(cells, args, args.cpu_steps, cores)
+        orc_obj, pd, t_build = oracle_for(cells, args, cores)
+        if "chosen" in results:
+            line["mixed_precision_error"] = step_errors(gpu, oracle_step_outputs(orc_obj), cells,
+                                                        "CPU oracle (FP64 restatement of the reference)")
+        v, sample, extra = cpu_reference_rate(orc_obj, pd, t_build, args, args.cpu_steps)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": sample + " on " + model}
+    elif rank == 0 and world == 1 and "chosen" in results:
+        line["mixed_precision_error"] = step_errors(gpu, gpu["fp64"], cells,
+                                                    "FP64 path of this library (the oracle leg was skipped)")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -14,8 +14,10 @@ The names mirror the reference functions the C ABI stands in for
 Arrays use the reference layout: cells are (n, ncols) float64 with the column
 order of indices.hpp (column 21 = gamma when adhesion is on); neighbor rows
 are (m, 7) = (i, j, dx, dy, dz, si, sj).  Errors raise RuntimeError, like the
-reference's std::runtime_error.  There is no CPU fallback: importing this
-module without the built library raises ImportError.
+reference's std::runtime_error.  There is no CPU fallback: the library is
+loaded on the first call that needs it (parameter structs, defaults and the
+workload helpers need none), and that call raises ImportError when the
+library is not built.
 """
 import ctypes
 import os
@@ -158,6 +160,7 @@ def _load():
         "abm_last_division_tries": ([vp, ip], i),
         "abm_graph_info": ([vp], ctypes.c_char_p),
         "abm_cell_cell_forces_noalloc": ([P(AbmParams), vp, i, i, i, vp, vp, i, dp, dp, i, vp, vp], i),
+        "abm_cell_cell_forces_noalloc_status": ([vp], i),
         "abm_noalloc_last_error": ([], ctypes.c_char_p),
         "abm_set_frames": ([vp, d, i], i),
         "abm_frames_taken": ([vp, ip], i),
@@ -191,14 +194,27 @@ def _load():
     return lib
 
 
-LIB = _load()
+class _Lib:
+    """libabm_b200.so, loaded (with every entry point's signature) on first use."""
+
+    def __init__(self):
+        self._lib = None
+
+    def __getattr__(self, name):
+        if self._lib is None:
+            self._lib = _load()
+        return getattr(self._lib, name)
+
+
+LIB = _Lib()
 EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchronize "
             "abm_jkr_contact_radius abm_jkr_radius_table abm_jkr_optimal_gamma abm_set_jkr_table abm_upload_cells "
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
             "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
-            "abm_cell_cell_forces_noalloc abm_noalloc_last_error abm_stepsize_set_weights "
+            "abm_cell_cell_forces_noalloc abm_cell_cell_forces_noalloc_status abm_noalloc_last_error "
+            "abm_stepsize_set_weights "
             "abm_stepsize_get_weights abm_stepsize_get_log abm_stepsize_clear_log abm_mlp_forward "
             "abm_mlp_grad abm_mlp_train abm_mlp_last_error abm_get_adhesion_flags abm_set_adhesion_flags "
             "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "

@@ -18,9 +18,18 @@ NCOLS_3D = 22   # indices.hpp:17-47 plus gamma (column 21)
 NCOLS_2D = 17   # ABM-2d/ABM-2d-cpp/include/indices.hpp:17-41
 
 
-def _generate(n, seed, disk_radius, z_lo, z_hi, lmin, lmax, min_gap, contact_dist, p_contact,
-              max_tries=10000):
+def _host_lib(lib):
+    """The library that holds the generator: this package's, unless another build of
+    csrc/abm_workload.cpp (a ctypes handle) is given."""
+    if lib is not None:
+        return lib
     from . import LIB
+    return LIB
+
+
+def _generate(n, seed, disk_radius, z_lo, z_hi, lmin, lmax, min_gap, contact_dist, p_contact,
+              max_tries=10000, lib=None):
+    LIB = _host_lib(lib)
     LIB.abm_generate_biofilm_3d.argtypes = [
         ctypes.c_int, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_double, ctypes.c_double,
         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -38,9 +47,9 @@ def _generate(n, seed, disk_radius, z_lo, z_hi, lmin, lmax, min_gap, contact_dis
     return r, nv, l
 
 
-def count_close_pairs(cells, dist, lmax=None):
+def count_close_pairs(cells, dist, lmax=None, lib=None):
     """Number of unordered pairs with centreline distance < dist."""
-    from . import LIB
+    LIB = _host_lib(lib)
     LIB.abm_count_close_pairs_3d.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
     LIB.abm_count_close_pairs_3d.restype = ctypes.c_longlong
@@ -53,10 +62,11 @@ def count_close_pairs(cells, dist, lmax=None):
 
 def biofilm_3d(n=100_000, seed=1, disk_radius=300.0, z_max=10.0, R=0.8, Rcell=0.5,
                lmin=2.0, lmax=5.0, eta0=100.0, eta1=720.0, sigma0=100.0, gamma=100.0,
-               growth=0.0, min_gap=None, p_contact=0.0):
-    """Return an (n, 22) float64 cell array (Fortran order) and a summary dict."""
+               growth=0.0, min_gap=None, p_contact=0.0, lib=None):
+    """Return an (n, 22) float64 cell array (Fortran order) and a summary dict.  `lib`:
+    another build of the generator to draw with (default: this package's library)."""
     gap = 2 * Rcell + 0.1 if min_gap is None else min_gap
-    r, nv, l = _generate(n, seed, disk_radius, R, z_max, lmin, lmax, gap, 2 * R, p_contact)
+    r, nv, l = _generate(n, seed, disk_radius, R, z_max, lmin, lmax, gap, 2 * R, p_contact, lib=lib)
     cells = np.zeros((n, NCOLS_3D), dtype=np.float64, order="F")
     cells[:, 0] = np.arange(n)
     cells[:, 1:4] = r
@@ -69,7 +79,7 @@ def biofilm_3d(n=100_000, seed=1, disk_radius=300.0, z_max=10.0, R=0.8, Rcell=0.
     cells[:, 19] = sigma0
     cells[:, 20] = 1
     cells[:, 21] = gamma
-    contacts = count_close_pairs(cells, 2 * R, lmax)
+    contacts = count_close_pairs(cells, 2 * R, lmax, lib=lib)
     info = dict(n=n, seed=seed, min_gap=gap, p_contact=p_contact,
                 mean_contacts_per_cell=2.0 * contacts / n)
     return cells, info

@@ -260,6 +260,8 @@ __device__ __forceinline__ Dist dist_geom_mixed(const Geom& a, const Geom& b)
 //           by its power series (to f^29);
 //   sin/cos Cody-Waite reduction by pi/2 (two-part constant), Taylor series of sin
 //           and cos on [-pi/4, pi/4] (to r^23 / r^22).
+// The two-part constants ln 2 = LN2_HI + LN2_LO and pi/2 = PIO2_HI + PIO2_LO are the
+// published split values of fdlibm (Sun Microsystems, 1993: e_log.c and e_rem_pio2.c).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double det_log(double x)
 {

@@ -287,9 +287,11 @@ const char* abm_mlp_last_error(void);
  * d_col[n_entries] list each cell's neighbors in both directions, each row
  * sorted ascending.  d_cells (n x ncols, leading dimension ld), the CSR arrays
  * and d_dEdq (n x 6, leading dimension n) are device buffers the caller owns;
- * jkr_delta / jkr_radius are host arrays (ignored without adhesion).  Work is
+ * jkr_delta / jkr_radius are host arrays (ignored without adhesion), read during
+ * the call only: they travel to the device inside the launch parameters.  Work is
  * enqueued on `stream` (a cudaStream_t, 0 = legacy default stream); results are
- * ready when the stream reaches that point.
+ * ready when the stream reaches that point.  3-D model only (dims 0 or 3);
+ * adhesion_mode 0 or 1; precision ABM_PRECISION_FP64 or ABM_PRECISION_MIXED.
  *
  * Scratch lives in one fixed __device__ array of about 21 MB that every GPU
  * loading this library holds until the process exits.  Limits per call:
@@ -299,6 +301,13 @@ const char* abm_mlp_last_error(void);
  * before any stream capture.  All calls share the array, so calls that overlap
  * on the GPU race; serialise them.  The call allocates nothing.
  * abm_noalloc_last_error() describes the last failure of this thread.
+ *
+ * The CSR is checked on the device before any kernel indexes with it: row_ptr[0]
+ * = 0, row_ptr[n] = n_entries, rows non-decreasing, columns in [0, n) and not the
+ * row itself, rows strictly ascending, and every entry (i, j) matched by (j, i).
+ * A CSR that fails is never used to index memory: the call fills d_dEdq with NaN,
+ * and abm_cell_cell_forces_noalloc_status then returns ABM_ERR_ARG with the
+ * reason in abm_noalloc_last_error().
  * ------------------------------------------------------------------------- */
 #define ABM_NOALLOC_MAX_CELLS 32768
 #define ABM_NOALLOC_MAX_ENTRIES 524288
@@ -306,6 +315,9 @@ int abm_cell_cell_forces_noalloc(const abm_params* params, const double* d_cells
                                  const int* d_row_ptr, const int* d_col, int n_entries,
                                  const double* jkr_delta, const double* jkr_radius, int jkr_n,
                                  double* d_dEdq, void* stream);
+/* Waits for `stream` and reports whether the CSR of the last abm_cell_cell_forces_noalloc
+ * call on the current device passed its device-side check: ABM_OK, or ABM_ERR_ARG. */
+int abm_cell_cell_forces_noalloc_status(void* stream);
 const char* abm_noalloc_last_error(void);
 
 /* ---------------------------------------------------------------------------

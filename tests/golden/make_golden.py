@@ -127,7 +127,9 @@ def extract(path, dim):
 REF = None
 
 if __name__ == "__main__":
-    REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of a kmnam/biofilm-ABMs checkout>")
+    REF = sys.argv[1]
     for dim, rel in ((3, "ABM-3d/ABM-3d-cpp/test/src/testDistBetweenCells.cpp"),
                      (2, "ABM-2d/ABM-2d-cpp/test/src/testDistBetweenCells.cpp")):
         out = extract(os.path.join(REF, rel), dim)

@@ -189,6 +189,7 @@ def test_2d_founder_grows_to_1000_cells():
     assert np.all(np.isfinite(cells))
     np.testing.assert_allclose(np.hypot(cells[:, 3], cells[:, 4]), 1.0, atol=1e-12)
     assert len(np.unique(cells[:, 0])) == cells.shape[0]           # distinct IDs
-    assert len(sim.parents()) == 2 * cells.shape[0] - 1 or len(sim.parents()) >= cells.shape[0]
+    # every division gives the mother's row and the new row fresh IDs: 2 n - 1 IDs from one founder
+    assert len(sim.parents()) == 2 * cells.shape[0] - 1
     print("\nfounder -> %d cells: %d iterations, t = %.3f h, %d attempts" % (
         cells.shape[0], st["iterations"], st["t"], st["attempts"]))

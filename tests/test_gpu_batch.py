@@ -86,16 +86,16 @@ def test_batch_cell_limit_stops_each_replicate():
         st = s.stats()
         assert np.all(np.isfinite(cells))
         assert st["cell_steps"] > 0
-    # halted replicates do not move
+    # halted replicates do not move: no further iterations, cells unchanged
     bt.iterate(20)
     bt.synchronize()
-    for s in sims:
-        assert s.stats()["iterations"] == s.stats()["iterations"]
+    it0 = [s.stats()["iterations"] for s in sims]
     before = [s.download_cells() for s in sims]
     bt.iterate(20)
     bt.synchronize()
-    for s, c0 in zip(sims, before):
+    for s, c0, i0 in zip(sims, before, it0):
         assert np.array_equal(s.download_cells(), c0)
+        assert s.stats()["iterations"] == i0
     bt.close()
 
 

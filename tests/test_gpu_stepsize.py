@@ -143,6 +143,49 @@ def test_rejected_proposal_falls_back_to_the_reference_rule():
     sim.close()
 
 
+@pytest.mark.parametrize("mode,noise", [(1, False), (2, False), (1, True)])
+def test_rejected_proposal_matches_the_oracle_reference_iteration(mode, noise):
+    """A proposal that fails the error test is followed by the reference rule, which
+    restarts from the copy of y0 the trial kept (l in the gamma slot, the stored
+    velocities beside it): the iteration must end where the oracle's reference-controller
+    iteration (simulation.hpp:1688-1769) ends when it starts at the proposed dt -- the
+    same attempts, r, n, the stored velocities, l, half_l and the clock, to 1e-10."""
+    cells = colony(2000, 34, growth=1.5)
+    cells[:, 13] = np.minimum(cells[:, 13], 4.0)      # no division in this iteration
+    cells[:, 14] = cells[:, 13] / 2
+    dt0, dt_max = 1e-4, 2e-4
+    kw = dict(integration_mode=mode, max_stepsize=dt_max)
+    if noise:
+        kw.update(max_rxy_noise=50.0, max_rz_noise=20.0, max_nxy_noise=5.0, max_nz_noise=2.0)
+    sim = abm_b200.Simulation(cap_cells=2100, jkr_table=JKR, controller=1, **kw)
+    sim.upload_cells(cells)
+    w = np.zeros(abm_b200.MLP_NPARAM, dtype=np.float32)
+    w[-1] = 50.0                              # asks for 10x dt0; the proposal is clamped to dt_max
+    sim.set_stepsize_weights(w)
+    sim.set_clock(0.0, dt0, 0)
+    sim.get_cell_neighbors()
+    s = sim.iterate(1)
+    assert s["iterations"] == 1 and s["rejected"] == 1
+    o = orc.Oracle(dict(sim.pdict, controller=0), jkr=JKR)
+    o.set_cells(cells)
+    o.loop_init()
+    o.set_clock(0.0, dt_max, 0)               # the reference rule's trial at the proposed dt
+    o.iterate(1)
+    so = o.stats()
+    assert s["attempts"] == so["attempts"] and s["attempts"] >= 2
+    t, dt, it = sim.clock()
+    to, dto, ito = o.clock()
+    assert it == ito == 1
+    assert abs(dt - dto) <= 1e-12 * dto and abs(t - to) <= 1e-12 * to
+    assert abs(s["last_max_error"] - so["last_max_error"]) <= 1e-9 * so["last_max_error"]
+    got, ref = sim.download_cells(), o.cells()
+    for c in range(1, 15):                    # r, n, stored velocities, l, half_l
+        scale = np.abs(ref[:, c]).max()
+        assert np.abs(got[:, c] - ref[:, c]).max() <= 1e-10 * max(scale, 1e-300), c
+    assert np.array_equal(got[:, 15:], ref[:, 15:])
+    sim.close()
+
+
 def test_learned_controller_gain_over_the_reference_controller():
     """What the trained network gains over the method without it (the reference
     controller, simulation.hpp:1688-1769) at equal RK tolerance on a growing,

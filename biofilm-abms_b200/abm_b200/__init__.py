@@ -142,6 +142,8 @@ def _load():
         "abm_jkr_radius_table": ([d, d, d, d, i, dp, dp], i),
         "abm_jkr_optimal_gamma": ([d, d, d, d, dp], i),
         "abm_set_jkr_table": ([vp, dp, dp, i], i),
+        "abm_jkr_radius_table_variable": ([d, d, d, d, i, i, dp, dp, dp], i),
+        "abm_set_jkr_table_variable": ([vp, dp, i, dp, i, dp], i),
         "abm_upload_cells": ([vp, dp, i, i, i], i),
         "abm_download_cells": ([vp, dp, i], i),
         "abm_get_num_cells": ([vp, ip], i),
@@ -208,7 +210,8 @@ class _Lib:
 
 LIB = _Lib()
 EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchronize "
-            "abm_jkr_contact_radius abm_jkr_radius_table abm_jkr_optimal_gamma abm_set_jkr_table abm_upload_cells "
+            "abm_jkr_contact_radius abm_jkr_radius_table abm_jkr_optimal_gamma abm_set_jkr_table "
+            "abm_jkr_radius_table_variable abm_set_jkr_table_variable abm_upload_cells "
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
@@ -222,7 +225,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_write_lineage abm_read_lineage abm_io_last_error abm_set_frames abm_frames_taken "
             "abm_download_frame").split()
 
-CONTROLLER_REFERENCE, CONTROLLER_LEARNED = 0, 1
+CONTROLLER_REFERENCE, CONTROLLER_LEARNED, CONTROLLER_PI = 0, 1, 2
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
 
 
@@ -266,6 +269,18 @@ def jkr_radius_table(R, Rcell, E0, gamma, n_mesh=100):
     if rc:
         raise RuntimeError("abm_jkr_radius_table failed (%s)" % ERRORS.get(rc, rc))
     return delta, radius
+
+
+def jkr_radius_table_variable(R, Rcell, E0, max_gamma, n_delta=100, n_gamma=100):
+    """Overlap mesh LinSpaced(n_delta, 0, 2(R - Rcell)), gamma mesh LinSpaced(n_gamma, 0, max_gamma)
+    and the radii on them, (n_delta, n_gamma) (simulation.hpp:120-145)."""
+    delta, gamma = np.zeros(n_delta), np.zeros(n_gamma)
+    radius = np.zeros((n_delta, n_gamma))
+    rc = LIB.abm_jkr_radius_table_variable(R, Rcell, E0, max_gamma, n_delta, n_gamma, _dptr(delta), _dptr(gamma),
+                                           _dptr(radius))
+    if rc:
+        raise RuntimeError("abm_jkr_radius_table_variable failed (%s)" % ERRORS.get(rc, rc))
+    return delta, gamma, radius
 
 
 class Simulation:
@@ -324,6 +339,15 @@ class Simulation:
         radius = np.ascontiguousarray(radius, dtype=np.float64)
         self._check(LIB.abm_set_jkr_table(self._ctx, _dptr(delta), _dptr(radius), len(delta)),
                     "abm_set_jkr_table")
+
+    def set_jkr_table_variable(self, delta, gamma, radius):
+        """Variable-gamma JKR table (IsotropicJKRDataVariableGamma): radius (n_delta, n_gamma)."""
+        delta = np.ascontiguousarray(delta, dtype=np.float64)
+        gamma = np.ascontiguousarray(gamma, dtype=np.float64)
+        radius = np.ascontiguousarray(radius, dtype=np.float64)
+        assert radius.shape == (len(delta), len(gamma))
+        self._check(LIB.abm_set_jkr_table_variable(self._ctx, _dptr(delta), len(delta), _dptr(gamma), len(gamma),
+                                                   _dptr(radius)), "abm_set_jkr_table_variable")
 
     def upload_cells(self, cells):
         """cells: (n, ncols) float64 array in the reference's column order."""

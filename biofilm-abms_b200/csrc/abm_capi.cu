@@ -44,6 +44,7 @@ struct abm_ctx {
     int* scan_sums = nullptr;
     double *jkr_delta = nullptr, *jkr_radius = nullptr;
     int jkr_n = 0;
+    double *jkr_gam = nullptr, *jkr_rad2 = nullptr;    // variable-gamma table (jkr_n x fp.jkr_ng)
     double* staging = nullptr;   // cap x (ncols max 32) doubles
     // division
     DivideParams dp;
@@ -94,6 +95,9 @@ static int fail(abm_ctx* c, int code, const std::string& msg) { if (c) c->err = 
 // --------------------------------------------------------------------------
 static double jkr_radius_host(double delta, double Req, double E, double gamma)
 {
+    // gamma = 0: p(a) = (a^2 - Req delta)^2, a double root that Newton approaches only
+    // linearly; its value is the Hertz radius
+    if (gamma == 0) return std::sqrt(Req * delta);
     typedef long double LD;
     const LD pi = 3.141592653589793238462643383279502884L;
     LD c2 = -2.0L * Req * delta, c1 = -4.0L * pi * gamma * (LD)Req * Req / E, c0 = (LD)delta * delta * Req * Req;
@@ -133,6 +137,20 @@ int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_
     return ABM_OK;
 }
 
+int abm_jkr_radius_table_variable(double R, double Rcell, double E0, double max_gamma, int n_delta, int n_gamma,
+                                  double* delta_out, double* gamma_out, double* radius_out)
+{
+    if (n_delta < 2 || n_gamma < 2 || !(max_gamma > 0) || !delta_out || !gamma_out || !radius_out)
+        return ABM_ERR_ARG;
+    const double high = 2 * (R - Rcell), step = high / double(n_delta - 1), gstep = max_gamma / double(n_gamma - 1);
+    for (int i = 0; i < n_delta; ++i) delta_out[i] = (i == n_delta - 1) ? high : double(i) * step;
+    for (int j = 0; j < n_gamma; ++j) gamma_out[j] = (j == n_gamma - 1) ? max_gamma : double(j) * gstep;
+    for (int i = 0; i < n_delta; ++i)
+        for (int j = 0; j < n_gamma; ++j)
+            radius_out[(size_t)i * n_gamma + j] = jkr_radius_host(delta_out[i], R / 2, E0, gamma_out[j]);
+    return ABM_OK;
+}
+
 // jkrOptimalSurfaceEnergyDensity (jkr.hpp:1369-1407), which runSimulation calls to turn the
 // target equilibrium distance eqdist into the adhesion energy density (simulation.hpp:1354-1358).
 // The reference nests two finite-difference Newton solves: the overlap where the JKR force
@@ -163,7 +181,7 @@ static void free_all(abm_ctx* c)
     void* ptrs[] = {c->geom, c->vel, c->phys, c->fcc, c->geom_c, c->vel_c, c->gen_tmp, c->k0buf, c->ctrl, c->grid,
                     c->bbox_acc, c->bbox_counter, c->bin_count, c->bin_start, c->key, c->slot,
                     c->sorted_cell, c->sorted_geom, c->scratch, c->nbr_count, c->row_ptr, c->col, c->lower_end, c->rev, c->pairs, c->pair_start, c->surv, c->jbuf,
-                    c->scan_sums, c->jkr_delta, c->jkr_radius, c->staging, c->div_flags, c->div_rank,
+                    c->scan_sums, c->jkr_delta, c->jkr_radius, c->jkr_gam, c->jkr_rad2, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
                     c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info};
@@ -343,6 +361,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     for (int k = 0; k < 6; ++k) sp.noise_max[k] = nm[k];
     sp.noise_on = (p.max_rxy_noise > 0 || p.max_rz_noise > 0 || p.max_nxy_noise > 0 || p.max_nz_noise > 0);
     sp.seed = p.rng_seed;
+    sp.mixed = p.precision == ABM_PRECISION_MIXED && p.dims != 2;
     ForceParams& fp = c->fp;
     fp.R = p.R; fp.Rcell = p.Rcell; fp.E0 = p.E0;
     // simulation.hpp:1270-1274
@@ -352,6 +371,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     fp.max_overlap = 2 * (p.R - p.Rcell);
     fp.adhesion = p.adhesion_mode != 0;
     fp.jkr_n = 0; fp.jkr_step = 1.0;
+    fp.jkr_ng = 0; fp.jkr_gstep = 1.0; fp.jkr_gam = nullptr; fp.jkr_rad2 = nullptr;
     fp.skin = p.pair_skin == 0 ? 0.3 : std::max(p.pair_skin, 0.0);
     c->bp.threshold = p.neighbor_threshold;
     c->bp.prefilter = p.neighbor_threshold + p.Ldiv + 2 * p.R;
@@ -387,13 +407,16 @@ int abm_create(const abm_params* q, abm_ctx** out)
         CK(cudaMemset(c->adhere, 0, cap * c->cap_nbr));
         fp.adhere = c->adhere;
     }
-    if (p.controller != ABM_CONTROLLER_REFERENCE && p.controller != ABM_CONTROLLER_LEARNED)
-        return fail(c, ABM_ERR_ARG, "controller must be ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED");
+    if (p.controller != ABM_CONTROLLER_REFERENCE && p.controller != ABM_CONTROLLER_LEARNED &&
+        p.controller != ABM_CONTROLLER_PI)
+        return fail(c, ABM_ERR_ARG, "controller must be ABM_CONTROLLER_REFERENCE, _LEARNED or _PI");
     if (p.stepsize_log_capacity < 0) return fail(c, ABM_ERR_ARG, "stepsize_log_capacity must be >= 0");
     // step-size network, its features and the feature log
-    sp.learned = p.controller == ABM_CONTROLLER_LEARNED;
+    sp.network = p.controller == ABM_CONTROLLER_LEARNED;
+    sp.pi = p.controller == ABM_CONTROLLER_PI;
+    sp.propose = sp.network || sp.pi;
     sp.log_cap = p.stepsize_log_capacity;
-    sp.stats_on = sp.learned || sp.log_cap > 0;
+    sp.stats_on = sp.network || sp.log_cap > 0;
     sp.near_div_length = 0.9 * p.Ldiv;
     fp.stats = sp.stats_on;
     CK(cudaMalloc(&c->mlp_w, MLP_NPARAM * sizeof(float)));
@@ -452,11 +475,18 @@ int abm_synchronize(abm_ctx* c)
     return check_status(c);
 }
 
+static void drop_variable_table(abm_ctx* c)
+{
+    if (c->jkr_gam) { cudaFree(c->jkr_gam); cudaFree(c->jkr_rad2); c->jkr_gam = c->jkr_rad2 = nullptr; }
+    c->fp.jkr_ng = 0; c->fp.jkr_gam = nullptr; c->fp.jkr_rad2 = nullptr;
+}
+
 int abm_set_jkr_table(abm_ctx* c, const double* delta, const double* radius, int n)
 {
     if (!c || !delta || !radius || n < 2 || n > 512) return fail(c, ABM_ERR_ARG, "JKR table needs 2..512 entries");
     for (int i = 1; i < n; ++i)
         if (!(delta[i] > delta[i - 1])) return fail(c, ABM_ERR_ARG, "JKR overlap mesh must be increasing");
+    drop_variable_table(c);
     if (c->jkr_delta) { cudaFree(c->jkr_delta); cudaFree(c->jkr_radius); c->jkr_delta = c->jkr_radius = nullptr; }
     CK(cudaMalloc(&c->jkr_delta, n * sizeof(double)));
     CK(cudaMalloc(&c->jkr_radius, n * sizeof(double)));
@@ -465,6 +495,32 @@ int abm_set_jkr_table(abm_ctx* c, const double* delta, const double* radius, int
     c->jkr_n = n;
     c->fp.jkr_n = n;
     c->fp.jkr_step = (delta[n - 1] - delta[0]) / double(n - 1);
+    drop_iteration_graphs(c);
+    return ABM_OK;
+}
+
+int abm_set_jkr_table_variable(abm_ctx* c, const double* delta, int n_delta, const double* gamma, int n_gamma,
+                               const double* radius)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (!delta || !gamma || !radius || n_gamma < 2 || n_gamma > 4096)
+        return fail(c, ABM_ERR_ARG, "variable JKR table needs 2..512 overlaps and 2..4096 gammas");
+    for (int j = 1; j < n_gamma; ++j)
+        if (!(gamma[j] > gamma[j - 1])) return fail(c, ABM_ERR_ARG, "JKR gamma mesh must be increasing");
+    if (!(gamma[0] >= 0)) return fail(c, ABM_ERR_ARG, "JKR gamma mesh must start at gamma >= 0");
+    // the fixed-gamma slots hold the overlap mesh and the radii at the largest gamma
+    std::vector<double> last((size_t)std::max(n_delta, 0));
+    for (int i = 0; i < n_delta; ++i) last[i] = radius[(size_t)i * n_gamma + (n_gamma - 1)];
+    int rc = abm_set_jkr_table(c, delta, last.data(), n_delta);
+    if (rc) return rc;
+    CK(cudaMalloc(&c->jkr_gam, (size_t)n_gamma * sizeof(double)));
+    CK(cudaMalloc(&c->jkr_rad2, (size_t)n_delta * n_gamma * sizeof(double)));
+    CK(cudaMemcpy(c->jkr_gam, gamma, (size_t)n_gamma * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->jkr_rad2, radius, (size_t)n_delta * n_gamma * sizeof(double), cudaMemcpyHostToDevice));
+    c->fp.jkr_ng = n_gamma;
+    c->fp.jkr_gstep = (gamma[n_gamma - 1] - gamma[0]) / double(n_gamma - 1);
+    c->fp.jkr_gam = c->jkr_gam;
+    c->fp.jkr_rad2 = c->jkr_rad2;
     drop_iteration_graphs(c);
     return ABM_OK;
 }
@@ -871,7 +927,7 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
 {
     // every handle must belong to a conditional node of this graph, or instantiation fails
     cudaGraphConditionalHandle h_div = 0, h_retry = 0, h_run = 0;
-    const bool branch = c->sp.learned != 0;
+    const bool branch = c->sp.propose != 0;
     const bool retries = c->p.max_tries_update_stepsize > 0 && !branch;
     if (retries) CK(cudaGraphConditionalHandleCreate(&h_retry, G, 0, cudaGraphCondAssignDefault));
     if (branch) CK(cudaGraphConditionalHandleCreate(&h_run, G, 0, cudaGraphCondAssignDefault));
@@ -1223,7 +1279,7 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
     if (!c || n_iters < 0) return ABM_ERR_ARG;
     int rc = ready_for_forces(c);
     if (rc) return rc;
-    if (c->sp.learned && !c->mlp_loaded)
+    if (c->sp.network && !c->mlp_loaded)
         return fail(c, ABM_ERR_STATE, "the learned controller needs weights (abm_stepsize_set_weights)");
     if (!c->nbrs_valid)
     {
@@ -1292,7 +1348,7 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
     if (!c || !prof || n_iters < 0) return ABM_ERR_ARG;
     int rc = ready_for_forces(c);
     if (rc) return rc;
-    if (c->sp.learned && !c->mlp_loaded)
+    if (c->sp.network && !c->mlp_loaded)
         return fail(c, ABM_ERR_STATE, "the learned controller needs weights (abm_stepsize_set_weights)");
     if (!c->nbrs_valid) { enqueue_rebuild(c); c->nbrs_valid = true; }
     memset(prof, 0, sizeof(*prof));
@@ -1498,7 +1554,7 @@ int abm_batch_create(abm_ctx* const* ctxs, int n, abm_batch** out)
         if (c->dev != dev) { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts on different devices"); }
         if (c->p.iter_update_neighbors != b->k_rebuild)
         { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts must share iter_update_neighbors"); }
-        if (c->sp.learned && !c->mlp_loaded)
+        if (c->sp.network && !c->mlp_loaded)
         { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "a learned controller needs weights"); }
         if (c->dims == 3 && c->p.adhesion_mode != 0 && c->jkr_n < 2)
         { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "JKR table not set"); }

@@ -392,6 +392,19 @@ struct MechParams {
     int no_surface;
 };
 
+// The horizontal shortcut of the cell-surface forces (assume_2d): dE/dq component 2
+// of repulsion and adhesion (mechanics.hpp:673-780 and 800-910)
+__device__ __forceinline__ void surface_dEdq_flat(const MechParams& P, double rz, double l, double sigma0,
+                                                  double& rep2, double& adh2)
+{
+    double ph = P.R - rz;
+    if (ph > 0)
+    {
+        rep2 = -(2 * P.E0) * ph * l;
+        adh2 = sigma0 * (P.sqrtR / 2) * l / sqrt(ph);
+    }
+}
+
 // Cell-surface repulsion + adhesion dE/dq components 2 and 5
 // (mechanics.hpp:673-780 and 800-910, include_constraint = false).
 __device__ __forceinline__ void surface_dEdq(const MechParams& P, bool assume_2d, double rz, double nz,
@@ -403,12 +416,7 @@ __device__ __forceinline__ void surface_dEdq(const MechParams& P, bool assume_2d
     rep2 = rep5 = adh2 = adh5 = 0.0;
     if (assume_2d)
     {
-        double ph = R - rz;
-        if (ph > 0)
-        {
-            rep2 = -(2 * E0) * ph * l;
-            adh2 = sigma0 * (P.sqrtR / 2) * l / sqrt(ph);
-        }
+        surface_dEdq_flat(P, rz, l, sigma0, rep2, adh2);
         return;
     }
     const double pf0 = 2 * E0, pf1 = (8. / 3.) * E0 * P.sqrtR, pf2 = 2 * E0 * P.sqrtR;
@@ -470,19 +478,24 @@ __device__ __forceinline__ void area_integrals(const MechParams& P, double nz, d
     A3 = P.sqrtR * onz * int3 + piRnz2 * int6;
 }
 
-// Velocity of one cell from its generalised force (mechanics.hpp:2011-2347,
-// the three branches: no surface contact, horizontal contact, full 3-D contact).
-// dr, dn: stored velocities of the previous accepted step (Coulomb truncation).
-__device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_2d, const double y[6],
-                                               double l, double h, double eta0, double eta1_in,
-                                               double ss, const EndPow& w, const Vel* __restrict__ drp,
-                                               const double f[6], double v[6])
+// Does a cell touch the surface (mechanics.hpp:2080-2090)?
+__device__ __forceinline__ bool surface_contact(const MechParams& P, bool assume_2d, const double y[6], double h)
+{
+    if (!assume_2d) return (y[2] - h * y[5] < P.R) || (y[2] + h * y[5] < P.R);
+    return y[2] < P.R;
+}
+
+// The first two branches of getVelocities (mechanics.hpp:2011-2189): a cell clear of
+// the surface, and a horizontal cell on it (assume_2d), with Coulomb truncation of the
+// surface friction from the stored velocity dr of the previous accepted step.  Called
+// only for those two kinds of cells, so a contacting cell here lies on the substrate.
+__device__ __forceinline__ void velocity_free_or_flat(const MechParams& P, bool contacting, const double y[6],
+                                                      double l, double eta0, double eta1_in,
+                                                      const Vel* __restrict__ drp, const double f[6],
+                                                      double v[6])
 {
     const double R = P.R, E0 = P.E0, coul = P.coulomb;
     const double rz = y[2], nx = y[3], ny = y[4], nz = y[5];
-    bool contacting;
-    if (!assume_2d) contacting = (rz - h * nz < R) || (rz + h * nz < R);
-    else contacting = rz < R;
     if (P.no_surface || !contacting)
     {
         double K = eta0 * l, L = K * l * l / 12;
@@ -490,7 +503,7 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         v[0] = f[0] / K; v[1] = f[1] / K; v[2] = f[2] / K;
         v[3] = (f[3] + mult * nx) / L; v[4] = (f[4] + mult * ny) / L; v[5] = (f[5] + mult * nz) / L;
     }
-    else if (assume_2d)
+    else
     {
         double K, L;
         double a = sqrt(R * (R - rz));
@@ -519,6 +532,21 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         v[2] = f[2] / (eta0 * l);
         v[5] = 12 * f[5] / (eta0 * l * l * l);
     }
+}
+
+// Velocity of one cell from its generalised force (mechanics.hpp:2011-2347,
+// the three branches: no surface contact, horizontal contact, full 3-D contact).
+// dr, dn: stored velocities of the previous accepted step (Coulomb truncation).
+__device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_2d, const double y[6],
+                                               double l, double h, double eta0, double eta1_in,
+                                               double ss, const EndPow& w, const Vel* __restrict__ drp,
+                                               const double f[6], double v[6])
+{
+    const double R = P.R, E0 = P.E0, coul = P.coulomb;
+    const double nx = y[3], ny = y[4], nz = y[5];
+    const bool contacting = surface_contact(P, assume_2d, y, h);
+    if (P.no_surface || !contacting || assume_2d)
+        velocity_free_or_flat(P, contacting, y, l, eta0, eta1_in, drp, f, v);
     else
     {
         double eta1 = eta1_in;
@@ -560,6 +588,171 @@ __device__ __forceinline__ void velocity_solve(const MechParams& P, bool assume_
         v[1] = (f[1] - c5 * v[4]) * ic1;
         v[0] = (f[0] - c5 * v[3]) * ic1;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: the cell-surface forces, the area integrals and the velocity
+// solve of a cell in surface contact (the third branch of getVelocities,
+// mechanics.hpp:2191-2309, with mechanics.hpp:673-910 and integrals.hpp:116-463)
+// in FP32.  R - rz, ss and the end overlaps are formed in FP64 before rounding, so
+// shallow contacts keep their relative precision.  The overlap-power integrals over
+// the contact come from the closed forms the FP64 path uses, except when both ends
+// touch and the overlap varies by less than half its mid value along the cell
+// (ss > 2h, i.e. rho = h nz / (R - rz) < 1/2): there the closed forms cancel, the
+// differences p^a - q^a and the first moments losing up to 1/rho^2 of their digits,
+// while the integrand is smooth with its nearest singularity at least two
+// half-lengths from the centre, so a 6-point Gauss-Legendre rule (nodes and weights
+// of Abramowitz & Stegun, Table 25.4) meets FP32 rounding.
+// ---------------------------------------------------------------------------
+struct SurfIntsF {      // integrals over the contact, s in [-h, min(ss, h)]
+    float i_m12, i_12, i_1, i_32, i_2, i_52;    // int phi^a ds, a = -1/2, 1/2, 1, 3/2, 2, 5/2
+    float s_m12, s_12, s_1, s_32;               // int s phi^a ds, a = -1/2, 1/2, 1, 3/2
+    float s2_12;                                // int s^2 phi^(1/2) ds
+};
+
+// phi^(e/2) from phi and its square root, e = 1..9
+__device__ __forceinline__ float half_pow_f(float x, float sx, int e)
+{
+    float r = (e & 1) ? sx : 1.f;
+    for (int k = 0; k < (e >> 1); ++k) r *= x;
+    return r;
+}
+
+// integrals.hpp:116-140 (integral1) and :159-184 (integral2) in FP32, exponent e/2 - 1:
+// both ends in contact when ss > h, the lower end only when -h < ss <= h
+__device__ __forceinline__ float integral1_f(float p, float q, float sp, float sq, float inz, float h, int e,
+                                             float ss)
+{
+    const float ig = 2.f / (float)e;
+    if (ss > h) return (half_pow_f(p, sp, e) - half_pow_f(q, sq, e)) * inz * ig;
+    return half_pow_f(p, sp, e) * inz * ig;
+}
+__device__ __forceinline__ float integral2_f(float p, float q, float sp, float sq, float inz, float h, int e,
+                                             float ss)
+{
+    const float term1 = integral1_f(p, q, sp, sq, inz, h, e + 2, ss);
+    const float term2 = (ss > h) ? -h * (half_pow_f(p, sp, e) + half_pow_f(q, sq, e)) : -h * half_pow_f(p, sp, e);
+    return (term1 + term2) * inz * (2.f / (float)e);
+}
+
+__device__ __forceinline__ SurfIntsF surface_integrals_f(double Rmrz, double nz_d, double h_d, double ss_d)
+{
+    SurfIntsF I;
+    const float h = (float)h_d, nz = (float)nz_d, ss = (float)ss_d;
+    if (ss_d > 2 * h_d)
+    {
+        const float x[3] = {0.2386191860831969f, 0.6612093864662645f, 0.9324695142031521f};
+        const float w[3] = {0.4679139345726910f, 0.3607615730481386f, 0.1713244923791704f};
+        const float phi0 = (float)Rmrz, hn = h * nz;
+        float a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, b0 = 0, b1 = 0, b2 = 0, b3 = 0, c1 = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+        {
+            const float xk = (k & 1) ? -x[k >> 1] : x[k >> 1];
+            const float wk = w[k >> 1] * h;
+            const float sk = h * xk;
+            const float ph = phi0 - xk * hn;
+            const float r = sqrtf(ph), ir = 1.f / r;
+            const float ph32 = ph * r;
+            a0 += wk * ir; a1 += wk * r; a2 += wk * ph; a3 += wk * ph32; a4 += wk * (ph * ph); a5 += wk * (ph * ph32);
+            b0 += wk * sk * ir; b1 += wk * sk * r; b2 += wk * sk * ph; b3 += wk * sk * ph32;
+            c1 += wk * sk * sk * r;
+        }
+        I.i_m12 = a0; I.i_12 = a1; I.i_1 = a2; I.i_32 = a3; I.i_2 = a4; I.i_52 = a5;
+        I.s_m12 = b0; I.s_12 = b1; I.s_1 = b2; I.s_32 = b3; I.s2_12 = c1;
+        return I;
+    }
+    // end overlaps in FP64 (integrals.hpp:56-60), then rounded
+    const double pd = Rmrz - (-h_d) * nz_d, qd = (ss_d > h_d) ? Rmrz - h_d * nz_d : 0.0;
+    const float p = (float)pd, q = (float)qd, sp = sqrtf(p), sq = sqrtf(q);
+    const float inz = 1.f / nz;
+    I.i_m12 = integral1_f(p, q, sp, sq, inz, h, 1, ss);
+    I.i_12 = integral1_f(p, q, sp, sq, inz, h, 3, ss);
+    I.i_1 = integral1_f(p, q, sp, sq, inz, h, 4, ss);
+    I.i_32 = integral1_f(p, q, sp, sq, inz, h, 5, ss);
+    I.i_2 = integral1_f(p, q, sp, sq, inz, h, 6, ss);
+    I.i_52 = integral1_f(p, q, sp, sq, inz, h, 7, ss);
+    I.s_m12 = integral2_f(p, q, sp, sq, inz, h, 1, ss);
+    I.s_12 = integral2_f(p, q, sp, sq, inz, h, 3, ss);
+    I.s_1 = integral2_f(p, q, sp, sq, inz, h, 4, ss);
+    I.s_32 = integral2_f(p, q, sp, sq, inz, h, 5, ss);
+    // integrals.hpp:400-463: int3 = (2 int2b + h^2 (p^(3/2) - q^(3/2))) / (1.5 nz)
+    I.s2_12 = (2.f * I.s_32 + h * h * (half_pow_f(p, sp, 3) - half_pow_f(q, sq, 3))) * inz * (1.f / 1.5f);
+    return I;
+}
+
+// v (6 components) of a cell in surface contact at state y (not on the substrate:
+// nz >= nz_threshold), from f0 = -dE/dq of the pair forces plus noise
+__device__ __forceinline__ void velocity_contact_f32(const MechParams& P, const double y[6], double l_d,
+                                                     double h_d, double eta0_d, double eta1_d, double sigma0_d,
+                                                     const Vel* __restrict__ drp, const double f0[6], double v[6])
+{
+    const double Rmrz = P.R - y[2];
+    const double ss_d = Rmrz / y[5];
+    const SurfIntsF I = surface_integrals_f(Rmrz, y[5], h_d, ss_d);
+    const float R = (float)P.R, E0 = (float)P.E0, sqrtR = (float)P.sqrtR;
+    const float nx = (float)y[3], ny = (float)y[4], nz = (float)y[5];
+    const float h = (float)h_d, l = (float)l_d, ss = (float)ss_d, sigma0 = (float)sigma0_d;
+    const float nz2 = nz * nz, onz = 1.f - nz2;
+    const bool partial = fabs(ss_d) < h_d;
+    const float i4 = (ss_d > h_d) ? 2.f * h : ss + h;                 // integral4 (ss > -h here)
+    // cell-surface repulsion, mechanics.hpp:673-780
+    const float pf0 = 2.f * E0, pf1 = (8.f / 3.f) * E0 * sqrtR, pf2 = 2.f * E0 * sqrtR;
+    const float rep_n = onz * I.i_1 + sqrtR * nz2 * I.i_12;
+    const float rep2 = -pf0 * rep_n;
+    const float rep5 = -pf0 * nz * I.i_2 - pf0 * onz * I.s_1 + pf1 * nz * I.i_32 - pf2 * nz2 * I.s_12;
+    // cell-surface adhesion, mechanics.hpp:800-910
+    const float a0 = sqrtR / 2.f, a1 = 2.f * 3.14159265358979f * R, a2 = 2.f * sqrtR;
+    const float adh2 = (a0 * onz * I.i_m12 + (partial ? (a1 / 2.f) * nz : 0.f)) * sigma0;
+    const float adh5 = (a2 * nz * I.i_12 + a0 * onz * I.s_m12 - a1 * nz * i4
+                        + (partial ? (a1 / 2.f) * (float)Rmrz : 0.f)) * sigma0;
+    // area integrals, integrals.hpp:400-463
+    const float piRnz2 = 3.14159265358979f * R * nz2;
+    const float i5 = (ss_d <= h_d) ? (ss * ss - h * h) / 2.f : 0.f;
+    const float i6 = (ss_d > h_d) ? 2.f * h * h * h / 3.f : (ss * ss * ss + h * h * h) / 3.f;
+    const float A1 = sqrtR * onz * I.i_12 + piRnz2 * i4;
+    const float A2 = sqrtR * onz * I.s_12 + piRnz2 * i5;
+    const float A3 = sqrtR * onz * I.s2_12 + piRnz2 * i6;
+    // generalised forces in FP64, then the solve (mechanics.hpp:2191-2309) in FP32
+    const float f0f = (float)f0[0], f1f = (float)f0[1], f3f = (float)f0[3], f4f = (float)f0[4];
+    const float f2f = (float)((f0[2] - (double)rep2) - (double)adh2);
+    const float f5f = (float)((f0[5] - (double)rep5) - (double)adh5);
+    float eta1 = (float)eta1_d;
+    const float coul = (float)P.coulomb;
+    if (coul > 0.f)
+    {
+        const double2 d01 = __ldg(reinterpret_cast<const double2*>(drp->v));
+        const double2 d23 = __ldg(reinterpret_cast<const double2*>(drp->v) + 1);
+        const double2 d45 = __ldg(reinterpret_cast<const double2*>(drp->v) + 2);
+        const float drxy = sqrtf((float)(d01.x * d01.x + d01.y * d01.y));
+        const float dnxy = sqrtf((float)(d23.y * d23.y + d45.x * d45.x));
+        const float friction_norm = (A1 * drxy + A2 * dnxy) * (eta1 / R);
+        const float max_norm = rep_n * (2.f * E0 * coul);
+        if (friction_norm > max_norm) eta1 = max_norm * R / (A1 * drxy + A2 * dnxy);
+    }
+    const float eR = eta1 / R;
+    const float c2 = (float)eta0_d * l;
+    const float c1 = c2 + eR * A1;
+    const float c4 = c2 * l * l / 12.f;
+    const float c3 = c4 + eR * A3;
+    const float c5 = eR * A2;
+    const float ic1 = 1.f / c1, ic4 = 1.f / c4;
+    const float c5c1 = c5 * ic1;
+    const float it1 = 1.f / (c3 - c5 * c5c1);
+    const float w4 = f3f - f0f * c5c1;
+    const float w5 = f4f - f1f * c5c1;
+    const float nx2 = nx * it1, ny2 = ny * it1, nzc = nz * ic4;
+    const float alpha = 2.f * ((nx * nx2 + ny * ny2) + nz * nzc);
+    const float beta = -((w4 * nx2 + w5 * ny2) + f5f * nzc);
+    const float lambda = beta / alpha;
+    const float v4 = (w5 + 2.f * ny * lambda) * it1;
+    const float v3 = (w4 + 2.f * nx * lambda) * it1;
+    v[5] = (double)((f5f + 2.f * nz * lambda) * ic4);
+    v[4] = (double)v4;
+    v[3] = (double)v3;
+    v[2] = (double)(f2f / c2);
+    v[1] = (double)((f1f - c5 * v4) * ic1);
+    v[0] = (double)((f0f - c5 * v3) * ic1);
 }
 
 }   // namespace abm

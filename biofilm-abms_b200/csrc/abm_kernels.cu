@@ -213,19 +213,34 @@ __global__ void __launch_bounds__(256) k_bbox(const Geom* __restrict__ geom, Ctr
         }
         double maxh = ord_dec(atomicAdd(&acc[6], 0ull));
         if (n <= 0) { for (int k = 0; k < 3; ++k) { lo[k] = 0; hi[k] = 0; } maxh = 0; }
-        double e = edge;
-        long long nb[3];
-        for (int tries = 0; tries < 64; ++tries)
+        // fmin / fmax skip NaN coordinates; an axis without any finite one spans [0, 0], and
+        // an infinite extent, or one no grid of cap_bins bins can hold, is an overflow
+        bool bad = false;
+        for (int k = 0; k < 3; ++k)
         {
-            for (int k = 0; k < 3; ++k) nb[k] = (long long)floor((hi[k] - lo[k]) / e) + 1;
-            if (nb[0] * nb[1] * nb[2] <= (long long)cap_bins) break;
+            if (!(lo[k] <= hi[k])) { lo[k] = 0; hi[k] = 0; }
+            if (!(hi[k] - lo[k] < 1e290)) bad = true;
+        }
+        double e = edge;
+        double nb[3] = {1.0, 1.0, 1.0};
+        for (int tries = 0; tries < 64 && !bad; ++tries)
+        {
+            for (int k = 0; k < 3; ++k) nb[k] = floor((hi[k] - lo[k]) / e) + 1;
+            if (nb[0] * nb[1] * nb[2] <= (double)cap_bins) break;
             e *= 1.5;
         }
-        if (nb[0] * nb[1] * nb[2] > (long long)cap_bins) atomicOr(&ctrl->status, (int)ST_BIN_OVERFLOW);
+        if (bad || !(nb[0] * nb[1] * nb[2] <= (double)cap_bins))
+        {
+            // one bin: every later kernel stays in bounds, the pair build skips its work
+            // (the status is set) and the host reports the overflow
+            atomicOr(&ctrl->status, (int)ST_BIN_OVERFLOW);
+            for (int k = 0; k < 3; ++k) { nb[k] = 1.0; lo[k] = 0.0; }
+            e = edge;
+        }
         Grid g;
         g.x0 = lo[0]; g.y0 = lo[1]; g.z0 = lo[2]; g.edge = e; g.inv_edge = 1.0 / e;
         g.nx = (int)nb[0]; g.ny = (int)nb[1]; g.nz = (int)nb[2];
-        g.nbins = (int)min((long long)cap_bins, nb[0] * nb[1] * nb[2]);
+        g.nbins = g.nx * g.ny * g.nz;
         g.max_half_l = maxh;
         *grid = g;
         // reset accumulators for the next rebuild
@@ -471,6 +486,12 @@ __global__ void __launch_bounds__(PB_T) k_pair_build(const Grid* grid, const int
     const Grid g = *grid;
     const int cap = bp.cap_per_cell;
     const float thr = (float)bp.threshold + 1e-4f;
+    if (ctrl->status & ST_BIN_OVERFLOW)
+    {
+        // the cells do not fit a grid (k_bbox): an empty neighbor set, reported by the host
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ctrl->n; i += gridDim.x * blockDim.x) count[i] = 0;
+        return;
+    }
     for (int bin = blockIdx.x; bin < g.nbins; bin += gridDim.x)
     {
         const int s0 = bin_start[bin], s1 = bin_start[bin + 1];
@@ -651,6 +672,47 @@ __device__ __forceinline__ double jkr_magnitude(double dist, double gamma, const
     return term1 - term2;
 }
 
+// adhesion.hpp:412-526 (forcesIsotropicJKRLagrange with a variable-gamma table): the
+// contact radius bilinearly interpolated on the cell of the (overlap, gamma) mesh that
+// holds (delta, gamma), overlap capped at max_overlap; a gamma beyond the mesh takes
+// the end cell.
+template <class T>
+__device__ __forceinline__ T jkr_radius_bilinear(T delta, T gamma, const ForceParams& fp, const double* td)
+{
+    const int nm = fp.jkr_n, ng = fp.jkr_ng;
+    int k = (int)(delta / (T)fp.jkr_step);
+    k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
+    while (k > 0 && (T)td[k] > delta) --k;
+    while (k < nm - 2 && (T)td[k + 1] <= delta) ++k;
+    int g = (int)(gamma / (T)fp.jkr_gstep);
+    g = g < 0 ? 0 : (g > ng - 2 ? ng - 2 : g);
+    while (g > 0 && (T)__ldg(fp.jkr_gam + g) > gamma) --g;
+    while (g < ng - 2 && (T)__ldg(fp.jkr_gam + g + 1) <= gamma) ++g;
+    const T d1 = (T)td[k], d2 = (T)td[k + 1];
+    const T g1 = (T)__ldg(fp.jkr_gam + g), g2 = (T)__ldg(fp.jkr_gam + g + 1);
+    const double* r = fp.jkr_rad2 + (size_t)k * ng + g;
+    const T r11 = (T)__ldg(r), r12 = (T)__ldg(r + 1), r21 = (T)__ldg(r + ng), r22 = (T)__ldg(r + ng + 1);
+    const T denom = (d2 - d1) * (g2 - g1);
+    const T w11 = (d2 - delta) * (g2 - gamma) / denom;
+    const T w12 = (d2 - delta) * (gamma - g1) / denom;
+    const T w21 = (delta - d1) * (g2 - gamma) / denom;
+    const T w22 = (delta - d1) * (gamma - g1) / denom;
+    return ((w11 * r11 + w12 * r12) + w21 * r21) + w22 * r22;
+}
+
+__device__ __forceinline__ double jkr_magnitude_variable(double dist, double gamma, const ForceParams& fp,
+                                                         const double* td)
+{
+    double delta = 2 * fp.R - dist;
+    if (fp.max_overlap >= 0 && delta > fp.max_overlap) delta = fp.max_overlap;
+    const double radius = jkr_radius_bilinear<double>(delta, gamma, fp, td);
+    double Req = fp.R / 2;
+    double a3 = radius * radius * radius;
+    double term1 = 4 * fp.E0 * a3 / (3 * Req);
+    double term2 = 4 * sqrt(M_PI * a3 * gamma * fp.E0);
+    return term1 - term2;
+}
+
 // Force of one unordered pair (i > j, distance from cell i to cell j, as the
 // reference's j < i loop computes it): magnitude m along d, returned as
 // v = m d_hat with the body coordinates s (on i) and t (on j).  Cell i gains
@@ -669,7 +731,8 @@ __device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& g
     double ux = d.dx / dist, uy = d.dy / dist, uz = d.dz / dist;
     double m;
     double gamma = fp.adhesion ? fmin(gi.gamma, gj.gamma) : 0.0;
-    if (fp.adhesion && gamma > 0) m = jkr_magnitude(dist, gamma, fp, td, tr);
+    if (fp.adhesion && gamma > 0)
+        m = fp.jkr_ng ? jkr_magnitude_variable(dist, gamma, fp, td) : jkr_magnitude(dist, gamma, fp, td, tr);
     else if (overlap <= fp.max_overlap) m = fp.pf0 * pow15(overlap);
     else
     {
@@ -701,13 +764,18 @@ __device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& g
     if (fp.adhesion && gamma > 0.f)
     {
         float delta = overlap > max_overlap ? max_overlap : overlap;
-        const int nm = fp.jkr_n;
-        int k = (int)(delta / (float)fp.jkr_step);
-        k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
-        while (k > 0 && (float)td[k] > delta) --k;
-        while (k < nm - 2 && (float)td[k + 1] <= delta) ++k;
-        float d1 = (float)td[k], d2 = (float)td[k + 1], r1 = (float)tr[k], r2 = (float)tr[k + 1];
-        float radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
+        float radius;
+        if (fp.jkr_ng) radius = jkr_radius_bilinear<float>(delta, gamma, fp, td);
+        else
+        {
+            const int nm = fp.jkr_n;
+            int k = (int)(delta / (float)fp.jkr_step);
+            k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
+            while (k > 0 && (float)td[k] > delta) --k;
+            while (k < nm - 2 && (float)td[k + 1] <= delta) ++k;
+            float d1 = (float)td[k], d2 = (float)td[k + 1], r1 = (float)tr[k], r2 = (float)tr[k + 1];
+            radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
+        }
         float a3 = radius * radius * radius;
         float E0 = (float)fp.E0;
         m = 4.f * E0 * a3 / (3.f * (R * 0.5f)) - 4.f * sqrtf(3.14159265f * a3 * gamma * E0);
@@ -1251,6 +1319,41 @@ __device__ __forceinline__ void cell_velocity(const StepParams& sp, bool a2, con
     velocity_solve(P, a2, y, l, h, eta0, eta1, ss, w, drp, f, v);
 }
 
+// Mixed precision: a cell in surface contact (and not lying on the substrate) takes the
+// FP32 contact branch (velocity_contact_f32); the others keep the FP64 branches (i) and
+// (ii), whose surface forces are zero off the surface and the horizontal shortcut on it
+__device__ __forceinline__ void cell_velocity_f32(const StepParams& sp, bool a2, const double y[6],
+                                                  double l, double h, double eta0, double eta1, double sigma0,
+                                                  const Vel* __restrict__ drp, const double f0[6], double v[6])
+{
+    const MechParams& P = sp.mp;
+    const bool contacting = surface_contact(P, a2, y, h);
+    if (!P.no_surface && contacting && !a2)
+    {
+        velocity_contact_f32(P, y, l, h, eta0, eta1, sigma0, drp, f0, v);
+        return;
+    }
+    double f[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) f[c] = f0[c];
+    if (!P.no_surface && a2)
+    {
+        double rep2 = 0, adh2 = 0;
+        surface_dEdq_flat(P, y[2], l, sigma0, rep2, adh2);
+        f[2] = (f[2] - rep2) - adh2;
+    }
+    velocity_free_or_flat(P, contacting, y, l, eta0, eta1, drp, f, v);
+}
+
+template <bool F32>
+__device__ __forceinline__ void cell_velocity_p(const StepParams& sp, bool a2, const double y[6], double l,
+                                                double h, double eta0, double eta1, double sigma0,
+                                                const Vel* __restrict__ drp, const double f0[6], double v[6])
+{
+    if constexpr (F32) cell_velocity_f32(sp, a2, y, l, h, eta0, eta1, sigma0, drp, f0, v);
+    else cell_velocity(sp, a2, y, l, h, eta0, eta1, sigma0, drp, f0, v);
+}
+
 // -dE/dq of the pair forces (getConservativeForces, mechanics.hpp:1768) plus the
 // attempt's noise (mechanics.hpp:2489-2510, forces += noise at :2066)
 template <bool NOISE>
@@ -1395,7 +1498,7 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
             row[35] = exceeded ? 0.f : 1.f;
             c->log_rows += 1;
         }
-        if (sp.learned && !exceeded)
+        if (sp.propose && !exceeded)
         {
             // the proposal passed the error test: accept its candidate state as is
             c->mode = MODE_COMMIT;
@@ -1431,6 +1534,10 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
     {
         c->last_max_error = E;
         const int h = c->hist_pos;
+        // error of the accepted step before this one (1 before any)
+        const int hp = (h + HIST - 1) % HIST;
+        const double e_prev = c->hist_dt[hp] > 0 ? c->hist_err[hp] : 1.0;
+        const double dt_accepted = c->dt;
         c->hist_dt[h] = c->dt;
         c->hist_err[h] = E;
         c->hist_acc[h] = c->first_passed;
@@ -1447,6 +1554,19 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
             const double t_old_factor = fmod(c->t - c->dt + 1e-12, c->dt_write);
             const double t_new_factor = fmod(c->t + 1e-12, c->dt_write);
             if (t_old_factor > t_new_factor) c->frame_due = 1;
+        }
+        if (sp.pi)
+        {
+            // the PI proposal for the next step: dt 0.9 E^(-0.7/k) E_prev^(0.4/k), k the error
+            // order + 1 (Gustafsson's PI rule with the parameters of Hairer & Wanner, Solving
+            // ODEs II, sec. IV.2), the factor held to [0.2, 10], dt to [min, max] step size
+            double f = 0.9 * pow(1.0 / E, 0.7 * sp.inv_q1) * pow(e_prev, 0.4 * sp.inv_q1);
+            if (f >= 10) f = 10;
+            else if (f < 0.2) f = 0.2;
+            double next = dt_accepted * f;
+            if (next < sp.min_stepsize) next = sp.min_stepsize;
+            else if (next > sp.max_stepsize) next = sp.max_stepsize;
+            c->dt = next;
         }
         c->mode = MODE_TRIAL;
         c->tries = 0;
@@ -1473,7 +1593,7 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
 // that read y0 back from that copy.
 // use_cond bit 0: `cond` is the retry WHILE node's handle; bit 1: `cond_run` is the
 // handle of the IF node around the final attempt (0 after a committed proposal).
-template <int S, int KIND, bool NOISE, int DIM>
+template <int S, int KIND, bool NOISE, int DIM, bool F32>
 __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
@@ -1496,11 +1616,11 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     const int n_order = (KIND != 3 && sp.order) ? ctrl->n_order : 0;
     const int mode = ctrl->mode;
     const int iter = ctrl->iter;
-    // the learned controller proposes (and tests) a step every iteration
-    const bool trial_ran = sp.learned || (iter % sp.iter_update_stepsize == 0);
+    // the learned and PI controllers propose (and test) a step every iteration
+    const bool trial_ran = sp.propose || (iter % sp.iter_update_stepsize == 0);
     // k0 is shared across attempts only under the reference controller: a passing
     // proposal needs no second attempt, so it does not store k0 or the total pair force
-    const bool share_k0 = !NOISE && !sp.learned;
+    const bool share_k0 = !NOISE && !sp.propose;
     double dt;
     int attempt;
     bool load_k0 = false, store_k0 = false;
@@ -1530,16 +1650,16 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     // the step was closed by a proposal that passed the error test
     if (KIND == MODE_FINAL && mode == MODE_COMMIT) return;
     const bool commit = false;
-    // the learned trial advances the state in place; the attempts after a failed
+    // a proposal (learned or PI) advances the state in place; the attempts after a failed
     // proposal start from the copy of y0 it kept
-    const bool in_place = (KIND == MODE_TRIAL) && sp.learned;
-    const bool from_backup = (KIND == MODE_RETRY || KIND == MODE_FINAL) && sp.learned;
+    const bool in_place = (KIND == MODE_TRIAL) && sp.propose;
+    const bool from_backup = (KIND == MODE_RETRY || KIND == MODE_FINAL) && sp.propose;
 
     // the first attempt of an iteration sums the cell's pair shares (pg.fused); under
     // the reference controller the trial writes the total back for the rest, under the
-    // learned one every attempt sums them
+    // proposing ones every attempt sums them
     const bool do_gather = pg.fused && !commit &&
-                           (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran) || sp.learned);
+                           (KIND == MODE_TRIAL || (KIND == MODE_FINAL && !trial_ran) || sp.propose);
     double local_max = 0.0;
     bool bad = false;
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
@@ -1570,7 +1690,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             cc = pg.fused == 3 ? sum_row_shares(pg.row_ptr, pg.lower_end, reinterpret_cast<const float4*>(pg.jbuf), i)
                : pg.fused == 2 ? sum_row_shares(pg.row_ptr, pg.lower_end, pg.jbuf, i)
                                : gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
-            if (KIND == MODE_TRIAL && !sp.learned) pg.fcc_w[i] = cc;
+            if (KIND == MODE_TRIAL && !sp.propose) pg.fcc_w[i] = cc;
         }
         else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);
         double f0[6];
@@ -1590,7 +1710,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         else
         {
             if constexpr (DIM == 2) velocity_2d(sp, y0, l, eta0, eta1, cc, nz2, k[0]);
-            else cell_velocity(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vprev, f0, k[0]);
+            else cell_velocity_p<F32>(sp, a2, y0, l, g.h, eta0, eta1, sigma0, vprev, f0, k[0]);
             if (store_k0)
             {
                 double2* kp = reinterpret_cast<double2*>(k0buf + i);
@@ -1613,7 +1733,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             }
             normalize_n(y);
             if constexpr (DIM == 2) velocity_2d(sp, y, l, eta0, eta1, cc, nz2, k[st]);
-            else cell_velocity(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, f0, k[st]);
+            else cell_velocity_p<F32>(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, f0, k[st]);
         }
         double vf1[6], d1[6];
 #pragma unroll
@@ -1886,7 +2006,7 @@ void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int
     k_attempt_order<<<blocks, 256, 0, st>>>(ctrl, flag, pos, order);
 }
 
-template <int S, bool NOISE, int DIM>
+template <int S, bool NOISE, int DIM, bool F32>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
                              Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
@@ -1895,10 +2015,10 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
 #define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg, cond_run
     switch (kind)
     {
-        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        default: k_attempt<S, 3, NOISE, DIM><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        default: k_attempt<S, 3, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
     }
 #undef AT_ARGS
 }
@@ -1911,9 +2031,11 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                     unsigned long long cond, int use_cond, PairGather pg, int dims, unsigned long long cond_run)
 {
     int blocks = attempt_blocks(cap_cells);
+#define AT_CALL(S, NZ, D, F) launch_attempt_s<S, NZ, D, F>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run)
 #define AT_CASE(S, D) case S: \
-        if (sp.noise_on) launch_attempt_s<S, true, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run); \
-        else launch_attempt_s<S, false, D>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run); \
+        if (D == 3 && sp.mixed) { if (sp.noise_on) AT_CALL(S, true, D, D == 3); else AT_CALL(S, false, D, D == 3); } \
+        else if (sp.noise_on) AT_CALL(S, true, D, false); \
+        else AT_CALL(S, false, D, false); \
         break;
     if (dims == 2)
     {
@@ -1932,6 +2054,7 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
         default: break;
     }
 #undef AT_CASE
+#undef AT_CALL
 }
 
 __global__ void k_velocities_2d(const Geom* __restrict__ geom, const Phys* __restrict__ phys,
@@ -1964,7 +2087,8 @@ __global__ void k_velocities(const Geom* __restrict__ geom, const Vel* __restric
         base_force<false>(sp, load_gen6(fcc, i), 0, 0, i, f0);
         Gen6 out;
         const Phys ph = phys[i];
-        cell_velocity(sp, a2, y, ph.l, g.h, ph.eta0, ph.eta1, ph.sigma0, vel + i, f0, out.f);
+        if (sp.mixed) cell_velocity_f32(sp, a2, y, ph.l, g.h, ph.eta0, ph.eta1, ph.sigma0, vel + i, f0, out.f);
+        else cell_velocity(sp, a2, y, ph.l, g.h, ph.eta0, ph.eta1, ph.sigma0, vel + i, f0, out.f);
         v_out[i] = out;
     }
 }

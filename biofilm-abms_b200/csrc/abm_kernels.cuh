@@ -113,7 +113,12 @@ struct StepParams {
     double rho_c;
     double max_noise_2d;
     // step-size control
-    int learned;                // 1: the network proposes dt, a passing proposal is accepted as is
+    int propose;                // 1: every iteration's first attempt runs at a proposed dt and is
+                                // accepted as is when its error passes (learned and PI controllers)
+    int network;                // 1: the step-size network makes the proposal (learned controller)
+    int pi;                     // 1: the PI rule makes the proposal after each accepted step
+    int mixed;                  // 1: mixed precision (3-D): cells in surface contact take the FP32
+                                // contact branch of the velocity solve
     int stats_on;               // accumulate the network's features (learned or logging)
     double near_div_length;     // 0.9 Ldiv
     double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
@@ -129,6 +134,12 @@ struct ForceParams {
     int adhesion;
     int jkr_n;
     double jkr_step;            // spacing of the overlap mesh
+    // variable-gamma table (IsotropicJKRDataVariableGamma, mechanics.hpp:159-199): radii on
+    // the overlap mesh x the gamma mesh, overlap-major; jkr_ng = 0 without it
+    int jkr_ng;
+    double jkr_gstep;           // spacing of the gamma mesh
+    const double* jkr_gam;      // gamma mesh (jkr_ng)
+    const double* jkr_rad2;     // radii (jkr_n x jkr_ng)
     int stats;                  // record the max overlap (step-size features)
     double skin;                // screened pair pass: margin of the active list (um)
     // 2-D model (ABM-2d): Hertz prefactors of 2D/include/simulation.hpp:232-235 and
@@ -253,7 +264,7 @@ void launch_mlp_grad(const float* master, const float* X, const float* T, int n,
                      cudaStream_t st);
 void launch_mlp_train(float* master, float* m1, float* m2, float* G, const float* X, const float* T, int n,
                       int epochs, float lr, unsigned seed, float* loss_out, cudaStream_t st);
-// features of the running iteration -> log row; with sp.learned also the dt of the first attempt
+// features of the running iteration -> log row; with sp.network also the dt of the first attempt
 int attempt_blocks(int cap_cells);
 
 // division (growth.hpp:66-426), abm_divide.cu

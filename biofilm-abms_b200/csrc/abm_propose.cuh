@@ -119,8 +119,11 @@ static __device__ __forceinline__ void mlp_propose_block(Ctrl* ctrl, const StepP
     __syncthreads();
     if (tid == 0)
     {
-        // ln E_last = ln(10) * 10 * feature 12
-        sh_base = (float)(log(0.9) - sp.inv_q1 * (double)(2.302585093f * 10.f * feat[12]));
+        // the PI rule's ln ratio: ln 0.9 - (0.7 ln E_last - 0.4 ln E_prev) / (q + 1), with
+        // ln E = ln(10) * 10 * features 12 and 13 (the last two accepted steps)
+        const double lnE_last = (double)(2.302585093f * 10.f * feat[12]);
+        const double lnE_prev = (double)(2.302585093f * 10.f * feat[13]);
+        sh_base = (float)(log(0.9) - sp.inv_q1 * (0.7 * lnE_last - 0.4 * lnE_prev));
         int fail = 0;
         for (int k = 0; k < HIST; ++k) fail |= feat[20 + k] < 0.5f;
         sh_fail = fail;
@@ -133,7 +136,7 @@ static __device__ __forceinline__ void mlp_propose_block(Ctrl* ctrl, const StepP
         if (lane == 0) { row[36] = sh_base; row[37] = 0.f; row[38] = 0.f; row[39] = 0.f; }
     }
     const double dt_prev = ctrl->dt;
-    if (!sp.learned)
+    if (!sp.network)
     {
         if (tid == 0) ctrl->dt_prev = dt_prev;
         return;

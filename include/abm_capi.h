@@ -36,14 +36,19 @@ extern "C" {
 #define ABM_RUNGE_KUTTA_FEHLBERG 3
 #define ABM_DORMAND_PRINCE 4
 
-/* Pair-force precision */
 /* Step-size controllers.  REFERENCE: the rule of simulation.hpp:1688-1769 (trial, up to
- * max_tries retries, a final re-run accepted unconditionally).  LEARNED: the step-size
- * network proposes dt from 32 features; the proposal is one RK attempt, accepted as is
- * when its embedded error passes (E <= 1), otherwise the REFERENCE rule continues from
- * that attempt (its retries and final re-run). */
+ * max_tries retries, a final re-run accepted unconditionally).  PI and LEARNED propose
+ * the dt of every iteration's first attempt, which is accepted as is when its embedded
+ * error passes (E <= 1); otherwise the REFERENCE rule continues from that attempt (its
+ * retries and final re-run).  PI: after each accepted step of dt with scaled error E_n,
+ * the next dt is dt 0.9 E_n^(-0.7/k) E_(n-1)^(0.4/k), k = error order + 1 (E_(n-1) = 1
+ * before the second step), the factor held to [0.2, 10] and dt to [min_stepsize,
+ * max_stepsize].  LEARNED: the step-size network adds its output to that same PI ratio
+ * (below), so a network whose output is zero is the PI controller, and after a failed
+ * first attempt among the last 8 steps the network may only shorten the PI step. */
 #define ABM_CONTROLLER_REFERENCE 0
 #define ABM_CONTROLLER_LEARNED 1
+#define ABM_CONTROLLER_PI 2
 
 /* Step-size network: 32 features -> 64 -> 64 -> 1 (ReLU), output ln(dt / dt_prev).
  * Flat FP32 parameter layout: W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3. */
@@ -51,8 +56,8 @@ extern "C" {
 #define ABM_MLP_HIDDEN 64
 #define ABM_MLP_NPARAM 6337
 /* The proposal is ln(dt / dt_prev) = clamp(b + y, ln 0.2, ln 10): y the network output,
- * b = ln 0.9 - ln(E_last)/(q+1) the error-model baseline (E_last: scaled error of the last
- * accepted step, q: error order of the tableau).
+ * b = ln 0.9 - (0.7 ln E_last - 0.4 ln E_prev)/(q+1) the PI ratio (E_last, E_prev: scaled
+ * errors of the last two accepted steps, q: error order of the tableau).
  * Log row: 32 features, ln(dt_max / dt_first) with dt_max = dt_first E^(-1/(q+1)),
  * ln(dt_first / dt_prev), log10 E of the first attempt, 1 if it passed (E <= 1), b, and
  * three spare columns. */
@@ -88,7 +93,7 @@ typedef struct abm_params {
     int pair_lanes;              /* lanes per cell of the no-alloc entry point's pair kernel: 4, 8, 16 or 32 (0 = 8) */
     int use_graphs;              /* 1 = capture the iteration in a CUDA graph */
     /* step-size control (no reference counterpart beyond ABM_CONTROLLER_REFERENCE) */
-    int controller;              /* ABM_CONTROLLER_REFERENCE or ABM_CONTROLLER_LEARNED */
+    int controller;              /* ABM_CONTROLLER_REFERENCE, ABM_CONTROLLER_LEARNED or ABM_CONTROLLER_PI */
     int stepsize_log_capacity;   /* rows of step-size features logged per context (0 = off) */
     /* model dimension: 3 (ABM-3d, default when 0) or 2 (ABM-2d).  The 2-D model uses the
      * 17-column cell layout of ABM-2d/ABM-2d-cpp/include/indices.hpp, neighbor rows
@@ -163,6 +168,18 @@ int abm_jkr_radius_table(double R, double Rcell, double E0, double gamma, int n_
 int abm_jkr_optimal_gamma(double R, double Rcell, double E0, double eqdist, double* gamma);
 /* Install the fixed-gamma table (IsotropicJKRDataFixedGamma, mechanics.hpp:113-153). */
 int abm_set_jkr_table(abm_ctx* ctx, const double* delta, const double* radius, int n);
+/* Radius table over LinSpaced(n_delta, 0, 2 (R - Rcell)) x LinSpaced(n_gamma, 0, max_gamma),
+ * overlap-major (radius_out[i * n_gamma + j] at delta_out[i], gamma_out[j]):
+ * calculateJKRContactRadii over two meshes, simulation.hpp:120-145. */
+int abm_jkr_radius_table_variable(double R, double Rcell, double E0, double max_gamma, int n_delta, int n_gamma,
+                                  double* delta_out, double* gamma_out, double* radius_out);
+/* Install a variable-gamma table (IsotropicJKRDataVariableGamma, mechanics.hpp:159-199): the
+ * cell-cell JKR force of a pair with gamma = min(gamma_i, gamma_j) > 0 then takes its contact
+ * radius by bilinear interpolation on the (overlap, gamma) mesh (forcesIsotropicJKRLagrange,
+ * adhesion.hpp:412-526); a gamma beyond the mesh takes the end cell.  radius is overlap-major,
+ * n_delta x n_gamma; both meshes strictly increasing.  abm_set_jkr_table removes it. */
+int abm_set_jkr_table_variable(abm_ctx* ctx, const double* delta, int n_delta, const double* gamma, int n_gamma,
+                               const double* radius);
 
 /* Cell state in and out (the cells array of runSimulation).  ld >= n. */
 int abm_upload_cells(abm_ctx* ctx, const double* colmajor, int n, int ncols, int ld);

@@ -507,6 +507,14 @@ struct Params3 {
     uint64_t rng_seed = 42;
     int n_start_multithread = 50;
     std::vector<double> jkr_overlaps, jkr_radii;
+    // step-size controller: 0 the reference rule (simulation.hpp:1688-1769); 2 the PI
+    // controller: every iteration's first attempt runs at a proposed dt and is accepted
+    // as is when its scaled error E passes (E <= 1), otherwise the reference rule
+    // continues from it; after each accepted step the next dt is the PI proposal
+    // dt 0.9 E_n^(-0.7/k) E_(n-1)^(0.4/k), k = error order + 1, the factor held to
+    // [0.2, 10] and dt to [min_stepsize, max_stepsize] (Gustafsson's PI rule with the
+    // parameters of Hairer & Wanner, Solving ODEs II, sec. IV.2)
+    int controller = 0;
     int friction_mode = 0;                 // FrictionMode: 0 NONE, 1 KINETIC (mechanics.hpp:61-65)
     double cell_cell_coulomb_coeff = 1.0;  // runSimulation's default (simulation.hpp:1162)
     double M0 = 0;                         // cell mass at length L0 (velocity Verlet)
@@ -1811,7 +1819,24 @@ struct LoopState {
     // statistics
     long long attempts = 0, rebuilds = 0, divisions = 0;
     double last_max_error = 0;
+    double prev_accepted_error = 0;   // E of the step before the last accepted one (0: none yet)
+    long long rejected = 0;           // iterations whose first attempt failed the error test
 };
+
+// The PI proposal after an accepted step of dt with scaled error E, E_prev the error of
+// the accepted step before it (0: none, read as 1).
+inline double pi_next_dt(double dt, double E, double E_prev, double error_order, const Params3& p)
+{
+    const double k = error_order + 1;
+    const double ep = E_prev > 0 ? E_prev : 1.0;
+    double factor = 0.9 * std::pow(1.0 / E, 0.7 / k) * std::pow(ep, 0.4 / k);
+    if (factor >= 10) factor = 10;
+    else if (factor < 0.2) factor = 0.2;
+    double next = dt * factor;
+    if (next < p.min_stepsize) next = p.min_stepsize;
+    else if (next > p.max_stepsize) next = p.max_stepsize;
+    return next;
+}
 
 inline void loop_init(LoopState& st, const Params3& p)
 {
@@ -1860,7 +1885,13 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
         Cells cn = step_rk_adaptive(tab, st.cells, st.nb, st.dt, p, st.iter, attempt++, errors, cc_once);
         st.attempts++;
         double max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
-        if (st.iter % p.iter_update_stepsize == 0)
+        const bool proposal = p.controller == 2;
+        if (max_error > 1.0) st.rejected++;
+        if (proposal && !(max_error > 1.0))
+        {
+            // the PI proposal passed the error test: it is the accepted step
+        }
+        else if (proposal || st.iter % p.iter_update_stepsize == 0)
         {
             bool exceeded = (max_error > 1.0);
             double q1 = 1.0 / (tab.error_order + 1);
@@ -1887,9 +1918,11 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
             st.attempts++;
             max_error = max_scaled_error(st.cells, errors, p.max_error_allowed, p.min_error);
         }
+        st.prev_accepted_error = st.last_max_error;
         st.last_max_error = max_error;
         st.cells = cn;
     }
+    const double dt_accepted = st.dt;
     grow_cells(st.cells, st.dt, p.R);
     update_neighbor_distances(st.cells, st.nb);
     if (!p.no_surface && p.basal_only && basal_compact(st.cells, p) > 0)
@@ -1899,6 +1932,9 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
     }
     st.t += st.dt;
     st.iter++;
+    if (p.controller == 2 && p.integration_mode != 0)
+        st.dt = pi_next_dt(dt_accepted, st.last_max_error, st.prev_accepted_error,
+                           make_tableau(p.integration_mode).error_order, p);
     if (st.iter % p.iter_update_neighbors == 0)
     {
         st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);

@@ -29,6 +29,7 @@ struct oracle_params {
     int friction_mode;                // 0 NONE, 1 KINETIC cell-cell friction
     double cell_cell_coulomb_coeff;   // Coulomb cap of the friction (not positive: none)
     double M0;                        // cell mass at length L0 (velocity Verlet)
+    int controller;                   // 0 the reference rule, 2 the PI controller
 };
 
 struct oracle_ctx {
@@ -59,6 +60,7 @@ int oracle_create(const oracle_params* q, oracle_ctx** out)
     p.rng_seed = q->rng_seed; p.n_start_multithread = q->n_start_multithread;
     p.friction_mode = q->friction_mode; p.cell_cell_coulomb_coeff = q->cell_cell_coulomb_coeff;
     p.M0 = q->M0;
+    p.controller = q->controller;
 #ifdef _OPENMP
     if (q->n_threads > 0) omp_set_num_threads(q->n_threads);
 #endif
@@ -310,6 +312,9 @@ void oracle_get_stats(oracle_ctx* c, long long* attempts, long long* rebuilds,
     *attempts = c->st.attempts; *rebuilds = c->st.rebuilds;
     *divisions = c->st.divisions; *last_max_error = c->st.last_max_error;
 }
+
+// iterations whose first attempt failed the error test
+long long oracle_rejected(oracle_ctx* c) { return c->st.rejected; }
 
 // growth.hpp:51-57
 int oracle_grow(oracle_ctx* c, double dt)

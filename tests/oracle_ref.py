@@ -35,7 +35,7 @@ class OracleParams(ctypes.Structure):
         ("daughter_angle_z_bound", ctypes.c_double), ("rng_seed", ctypes.c_ulonglong),
         ("n_start_multithread", ctypes.c_int), ("n_threads", ctypes.c_int),
         ("friction_mode", ctypes.c_int), ("cell_cell_coulomb_coeff", ctypes.c_double),
-        ("M0", ctypes.c_double),
+        ("M0", ctypes.c_double), ("controller", ctypes.c_int),
     ]
 
 
@@ -76,6 +76,7 @@ def _load():
         "oracle_loop_init": ([vp], i),
         "oracle_iterate": ([vp, i, i, i], i),
         "oracle_get_stats": ([vp, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_longlong), dp], None),
+        "oracle_rejected": ([vp], ctypes.c_longlong),
         "oracle_grow": ([vp, d], i),
         "oracle_divide": ([vp, d, i], i),
         "oracle_min_dist_to_cell": ([vp, i], d),
@@ -125,6 +126,14 @@ def nearest_body_coord(r, n, h, q):
     return LIB.oracle_nearest_body_coord(_dp(a[0]), _dp(a[1]), h, _dp(a[2]))
 
 
+def jkr_table_variable(R, Rcell, E0, max_gamma, n_delta=100, n_gamma=100):
+    """(overlap mesh, gamma mesh, radii (n_delta, n_gamma)) of simulation.hpp:120-145."""
+    d, g = np.zeros(n_delta), np.zeros(n_gamma)
+    r = np.zeros(n_delta * n_gamma)
+    LIB.oracle_jkr_table2(R, Rcell, E0, max_gamma, n_delta, n_gamma, _dp(d), _dp(g), _dp(r))
+    return d, g, r.reshape(n_delta, n_gamma)
+
+
 def jkr_table(R, Rcell, E0, gamma, n_mesh=100):
     d, r = np.zeros(n_mesh), np.zeros(n_mesh)
     LIB.oracle_jkr_table(R, Rcell, E0, gamma, n_mesh, _dp(d), _dp(r))
@@ -152,6 +161,12 @@ class Oracle:
         if getattr(self, "_c", None):
             LIB.oracle_destroy(self._c)
             self._c = None
+
+    def set_jkr_table_variable(self, delta, gamma, radius):
+        d = np.ascontiguousarray(delta, dtype=np.float64)
+        g = np.ascontiguousarray(gamma, dtype=np.float64)
+        r = np.ascontiguousarray(radius, dtype=np.float64).ravel()
+        LIB.oracle_set_jkr_table2(self._c, _dp(d), len(d), _dp(g), len(g), _dp(r))
 
     def set_jkr_table(self, delta, radius):
         d = np.ascontiguousarray(delta, dtype=np.float64)
@@ -240,7 +255,8 @@ class Oracle:
         a, r, dv = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         e = ctypes.c_double()
         LIB.oracle_get_stats(self._c, ctypes.byref(a), ctypes.byref(r), ctypes.byref(dv), ctypes.byref(e))
-        return dict(attempts=a.value, rebuilds=r.value, divisions=dv.value, last_max_error=e.value)
+        return dict(attempts=a.value, rebuilds=r.value, divisions=dv.value, last_max_error=e.value,
+                    rejected=LIB.oracle_rejected(self._c))
 
     def grow(self, dt):
         LIB.oracle_grow(self._c, dt)

@@ -84,3 +84,14 @@ def test_oracle_loop_matches_reference_order_of_operations():
     s = o.stats()
     assert s["rebuilds"] == 1 + 9 // 4
     assert s["attempts"] == 2 * 9          # trial + unconditional final re-run per iteration
+
+
+def test_product_variable_gamma_table_matches_oracle():
+    d, g, r = abm_b200.jkr_radius_table_variable(0.8, 0.5, 3900.0, 120.0, 100, 60)
+    do, go, ro = orc.jkr_table_variable(0.8, 0.5, 3900.0, 120.0, 100, 60)
+    assert np.array_equal(d, do) and np.array_equal(g, go)
+    np.testing.assert_allclose(r, ro, rtol=1e-13, atol=0)
+    # its gamma = 0 column is the Hertz radius sqrt(Req delta), its last the fixed table at 120
+    np.testing.assert_allclose(r[:, 0], np.sqrt(0.4 * d), rtol=1e-12, atol=0)
+    _, rf = abm_b200.jkr_radius_table(0.8, 0.5, 3900.0, 120.0, 100)
+    np.testing.assert_allclose(r[:, -1], rf, rtol=1e-15, atol=0)

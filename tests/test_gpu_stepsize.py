@@ -82,8 +82,10 @@ def test_in_loop_proposal_is_the_network_output():
     rows = sim.stepsize_log()
     assert rows.shape == (6, abm_b200.MLP_LOG_COLS)
     y = abm_b200.mlp_forward(w, rows[:, :32])
-    # baseline b = ln 0.9 - ln(E_last)/(q+1), HE21: q = 1
-    b = np.log(0.9) - 0.5 * np.float32(2.302585093) * np.float32(10.0) * rows[:, 12]
+    # baseline: the PI ratio b = ln 0.9 - (0.7 ln E_last - 0.4 ln E_prev)/(q+1), HE21: q = 1,
+    # ln E = ln(10) 10 x features 12 and 13
+    ln10 = np.float32(2.302585093) * np.float32(10.0)
+    b = np.log(0.9) - 0.5 * (0.7 * ln10 * rows[:, 12] - 0.4 * ln10 * rows[:, 13])
     np.testing.assert_allclose(rows[:, 36], b, rtol=1e-5, atol=1e-5)
     r = np.clip(rows[:, 36].astype(np.float64) + y, np.log(0.2), np.log(10.0))
     np.testing.assert_allclose(rows[:, 33], r, atol=2e-6)
@@ -183,6 +185,42 @@ def test_rejected_proposal_matches_the_oracle_reference_iteration(mode, noise):
         scale = np.abs(ref[:, c]).max()
         assert np.abs(got[:, c] - ref[:, c]).max() <= 1e-10 * max(scale, 1e-300), c
     assert np.array_equal(got[:, 15:], ref[:, 15:])
+    sim.close()
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_pi_controller_matches_the_oracle(mode):
+    """The PI controller (proposal dt 0.9 E_n^(-0.7/k) E_(n-1)^(0.4/k), a passing proposal
+    accepted as is, the reference rule after a failing one) against the oracle's
+    restatement over 30 iterations of a growing colony whose dt climbs from 1e-6 h to
+    where the error test binds: the same attempts and rejections, the clock to 1e-10 and
+    the cells to 1e-9."""
+    cells = colony(1500, 35, growth=1.5)
+    cells[:, 13] = np.minimum(cells[:, 13], 4.0)
+    cells[:, 14] = cells[:, 13] / 2
+    sim = abm_b200.Simulation(cap_cells=1600, jkr_table=JKR, controller=abm_b200.CONTROLLER_PI,
+                              integration_mode=mode, max_stepsize=1e-4, iter_update_neighbors=10)
+    sim.upload_cells(cells)
+    sim.set_clock(0.0, 1e-6, 0)
+    sim.get_cell_neighbors()
+    o = orc.Oracle(sim.pdict, jkr=JKR)
+    o.set_cells(cells)
+    o.loop_init()
+    o.set_clock(0.0, 1e-6, 0)
+    for _ in range(3):
+        s = sim.iterate(10)
+        o.iterate(10)
+        so = o.stats()
+        assert s["attempts"] == so["attempts"] and s["rejected"] == so["rejected"]
+        t, dt, it = sim.clock()
+        to, dto, ito = o.clock()
+        assert it == ito and abs(t - to) <= 1e-10 * to and abs(dt - dto) <= 1e-10 * dto
+        got, ref = sim.download_cells(), o.cells()
+        for c in range(1, 15):
+            scale = np.abs(ref[:, c]).max()
+            assert np.abs(got[:, c] - ref[:, c]).max() <= 1e-9 * max(scale, 1e-300), c
+    assert dt > 2e-6                          # the step grew from 1e-6 h to where the error test binds
+    assert s["attempts"] < 2 * s["iterations"]   # passing proposals take one attempt
     sim.close()
 
 

@@ -242,12 +242,16 @@ __device__ __forceinline__ Dist dist_geom_mixed(const Geom& a, const Geom& b)
         else if (t > 1.f) { t = 1.f; s = fminf(fmaxf((bb - c) / aa, 0.f), 1.f); }
         x = s; y = t;
     }
-    float s1 = x * 2.f * h1 - h1, t2 = y * 2.f * h2 - h2;
+    // the closest-point parameters come from the FP32 solve; the distance vector is
+    // assembled from them in FP64.  Its length is stationary in (s, t) at an interior
+    // minimum, and a clamped parameter is exact, so the overlap 2R - |d| keeps close to
+    // FP64 accuracy instead of losing the 2^-24 |d| that an FP32 |d| ~ 2R would cost it.
+    const double s1 = (double)x * 2.0 * a.h - a.h, t2 = (double)y * 2.0 * b.h - b.h;
     Dist o;
-    o.dx = (double)(rx + t2 * n2x - s1 * n1x);
-    o.dy = (double)(ry + t2 * n2y - s1 * n1y);
-    o.dz = (double)(rz + t2 * n2z - s1 * n1z);
-    o.s = (double)s1; o.t = (double)t2;
+    o.dx = ((b.rx - a.rx) + t2 * b.nx) - s1 * a.nx;
+    o.dy = ((b.ry - a.ry) + t2 * b.ny) - s1 * a.ny;
+    o.dz = ((b.rz - a.rz) + t2 * b.nz) - s1 * a.nz;
+    o.s = s1; o.t = t2;
     return o;
 }
 

@@ -753,11 +753,14 @@ __device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& g
     PairOut out;
     out.touch = false;
     Dist d = dist_geom_mixed(gi, gj);
+    // the overlap from the FP64 distance vector, then the force law in FP32
+    const double distd = sqrt((d.dx * d.dx + d.dy * d.dy) + d.dz * d.dz);
+    const double overlap_d = 2 * fp.R - distd;
+    if (!(overlap_d > 0)) return out;
     float dx = (float)d.dx, dy = (float)d.dy, dz = (float)d.dz;
-    float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float dist = (float)distd;
     const float R = (float)fp.R, max_overlap = (float)fp.max_overlap;
-    float overlap = 2.f * R - dist;
-    if (!(overlap > 0.f)) return out;
+    float overlap = (float)overlap_d;
     float inv = 1.f / dist;
     float m;
     float gamma = fp.adhesion ? fminf((float)gi.gamma, (float)gj.gamma) : 0.f;

@@ -763,25 +763,12 @@ __device__ __forceinline__ PairOut pair_force_fp32(const Geom& gi, const Geom& g
     float overlap = (float)overlap_d;
     float inv = 1.f / dist;
     float m;
-    float gamma = fp.adhesion ? fminf((float)gi.gamma, (float)gj.gamma) : 0.f;
-    if (fp.adhesion && gamma > 0.f)
+    const double gamma = fp.adhesion ? fmin(gi.gamma, gj.gamma) : 0.0;
+    if (fp.adhesion && gamma > 0)
     {
-        float delta = overlap > max_overlap ? max_overlap : overlap;
-        float radius;
-        if (fp.jkr_ng) radius = jkr_radius_bilinear<float>(delta, gamma, fp, td);
-        else
-        {
-            const int nm = fp.jkr_n;
-            int k = (int)(delta / (float)fp.jkr_step);
-            k = k < 0 ? 0 : (k > nm - 2 ? nm - 2 : k);
-            while (k > 0 && (float)td[k] > delta) --k;
-            while (k < nm - 2 && (float)td[k + 1] <= delta) ++k;
-            float d1 = (float)td[k], d2 = (float)td[k + 1], r1 = (float)tr[k], r2 = (float)tr[k + 1];
-            radius = (r1 * (d2 - delta) + r2 * (delta - d1)) / (d2 - d1);
-        }
-        float a3 = radius * radius * radius;
-        float E0 = (float)fp.E0;
-        m = 4.f * E0 * a3 / (3.f * (R * 0.5f)) - 4.f * sqrtf(3.14159265f * a3 * gamma * E0);
+        // the JKR magnitude term1 - term2 cancels near the force balance, where most
+        // adhering contacts sit: it keeps FP64 (table lookup included)
+        m = (float)(fp.jkr_ng ? jkr_magnitude_variable(distd, gamma, fp, td) : jkr_magnitude(distd, gamma, fp, td, tr));
     }
     else if (overlap <= max_overlap) m = (float)fp.pf0 * overlap * sqrtf(overlap);
     else
@@ -1677,6 +1664,11 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         const Geom g = load_geom(from_backup ? geom_c : geom, i);
         const Vel* vprev = (from_backup ? vel_c : vel) + i;
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
+        // non-finite coordinates (the reference's DEBUG_CHECK_CELL_COORDINATES_NAN,
+        // simulation.hpp:1803-1821): a position alone enters no velocity, so its error
+        // norm would stay finite
+#pragma unroll
+        for (int c = 0; c < 6; ++c) if (!isfinite(y0[c])) bad = true;
         const double l = from_backup ? g.gamma : phys[i].l;
         const double eta0 = phys[i].eta0, eta1 = phys[i].eta1, sigma0 = phys[i].sigma0;
         if (in_place)
@@ -1832,13 +1824,14 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     if (bad) local_max = __longlong_as_double(0x7ff0000000000000ll);
     local_max = warp_max(local_max);
     if ((threadIdx.x & 31) == 0) sh_max[threadIdx.x >> 5] = local_max;
-    __syncthreads();
+    // any thread of the block that met a non-finite value reports it
+    const int block_bad = __syncthreads_or(bad ? 1 : 0);
     if (threadIdx.x == 0)
     {
         double m = sh_max[0];
         for (int w = 1; w < AT_T / 32; ++w) m = fmax(m, sh_max[w]);
         unsigned long long bits = (unsigned long long)__double_as_longlong(m);
-        if (bad) atomicOr(&ctrl->status, (int)ST_NAN);
+        if (block_bad) atomicOr(&ctrl->status, (int)ST_NAN);
         if (KIND == MODE_FINAL || in_place)
         {
             double dm = sh_drift[0];

@@ -15,7 +15,10 @@ Bars, stated here:
   * one RK step, in the error test's own units (simulation.hpp:1697-1705):
     max_i |y1_mixed - y1_oracle| / (tol (1 + |y0|)) <= 0.02, i.e. the FP32 rounding
     moves the step by at most 2 % of what the error test accepts; and the scaled error
-    norm E itself agrees to 1e-3 relative, so both paths accept and reject the same steps.
+    norm E agrees to 1e-3 relative above a floor of 1e-4: the FP32 stage velocities of
+    cells in surface contact put rounding noise of that size into the embedded error,
+    which matters only where E itself is that small (high-order tableaux at small dt),
+    far from the accept threshold E = 1.
 """
 import numpy as np
 import pytest
@@ -32,6 +35,7 @@ TOL = 1e-8
 RTOL_FORCE = 1e-4
 RK_UNITS_MAX = 0.02
 E_RTOL = 1e-3
+E_FLOOR = 1e-4
 
 
 def rk_units(c_mixed, c_oracle, cells, tol=TOL):
@@ -66,7 +70,7 @@ def check_state(cells, dts=(1e-6,), **kw):
         print("\nmixed vs oracle at dt %g: forces %.2e, velocities %.2e, step %.3e of tol, E %.6g vs %.6g"
               % (dt, ef, ev, u, Eg, Eo))
         assert u <= RK_UNITS_MAX, u
-        assert abs(Eg - Eo) <= E_RTOL * Eo, (Eg, Eo)
+        assert abs(Eg - Eo) <= E_RTOL * Eo + E_FLOOR, (Eg, Eo)
         # the columns the step does not move are copied unchanged
         assert np.array_equal(cg[:, 13:], co[:, 13:])
         out.append((u, Eg, Eo))

@@ -195,8 +195,10 @@ def test_pi_controller_matches_the_oracle(mode):
     """The PI controller (proposal dt 0.9 E_n^(-0.7/k) E_(n-1)^(0.4/k), a passing proposal
     accepted as is, the reference rule after a failing one) against the oracle's
     restatement over 30 iterations of a growing colony whose dt climbs from 1e-6 h to
-    where the error test binds: the same attempts and rejections, the clock to 1e-10 and
-    the cells to 1e-9."""
+    where the error test binds: the same attempts and rejections, the clock to 1e-6 and
+    the cells to 1e-9.  Here dt follows E from step to step, and E is a cancellation:
+    for the orientations the embedded error dt sum (b - b*) k is ~1e-6 of the step
+    dt sum b k, so velocities that agree to ~1e-13 give E, and the next dt, to ~1e-7."""
     cells = colony(1500, 35, growth=1.5)
     cells[:, 13] = np.minimum(cells[:, 13], 4.0)
     cells[:, 14] = cells[:, 13] / 2
@@ -216,7 +218,7 @@ def test_pi_controller_matches_the_oracle(mode):
         assert s["attempts"] == so["attempts"] and s["rejected"] == so["rejected"]
         t, dt, it = sim.clock()
         to, dto, ito = o.clock()
-        assert it == ito and abs(t - to) <= 1e-10 * to and abs(dt - dto) <= 1e-10 * dto
+        assert it == ito and abs(t - to) <= 1e-6 * to and abs(dt - dto) <= 1e-6 * dto
         got, ref = sim.download_cells(), o.cells()
         for c in range(1, 15):
             scale = np.abs(ref[:, c]).max()

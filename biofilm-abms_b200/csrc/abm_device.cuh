@@ -215,7 +215,11 @@ __device__ __forceinline__ Dist dist_geom_mixed(const Geom& a, const Geom& b)
     float n1x = (float)a.nx, n1y = (float)a.ny, n1z = (float)a.nz;
     float n2x = (float)b.nx, n2y = (float)b.ny, n2z = (float)b.nz;
     double cos_theta = xdot(x3(a.nx, a.ny, a.nz), x3(b.nx, b.ny, b.nz));
-    if (cos_theta >= 0.9999 || cos_theta <= -0.9999) return dist_geom(a, b);
+    // FP64 for the near-parallel branch (|cos| >= 0.9999) and for the skew pairs just
+    // short of it: the FP32 solve divides by a e - b^2 ~ (1 - cos^2) a e, which loses
+    // 1/(1 - cos^2) of its digits, and the distance error, second order in (s, t),
+    // stays below FP32 rounding of the overlap only for |cos| < 0.99
+    if (cos_theta >= 0.99 || cos_theta <= -0.99) return dist_geom(a, b);
     // relative coordinates keep FP32 well conditioned far from the origin
     float rx = (float)(b.rx - a.rx), ry = (float)(b.ry - a.ry), rz = (float)(b.rz - a.rz);
     float h1 = (float)a.h, h2 = (float)b.h;

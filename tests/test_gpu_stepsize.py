@@ -196,7 +196,7 @@ def test_pi_controller_matches_the_oracle(mode):
     accepted as is, the reference rule after a failing one) against the oracle's
     restatement over 30 iterations of a growing colony whose dt climbs from 1e-6 h to
     where the error test binds: the same attempts and rejections, the clock to 1e-6 and
-    the cells to 1e-9.  Here dt follows E from step to step, and E is a cancellation:
+    the cells to 1e-7.  Here dt follows E from step to step, and E is a cancellation:
     for the orientations the embedded error dt sum (b - b*) k is ~1e-6 of the step
     dt sum b k, so velocities that agree to ~1e-13 give E, and the next dt, to ~1e-7."""
     cells = colony(1500, 35, growth=1.5)
@@ -222,36 +222,41 @@ def test_pi_controller_matches_the_oracle(mode):
         got, ref = sim.download_cells(), o.cells()
         for c in range(1, 15):
             scale = np.abs(ref[:, c]).max()
-            assert np.abs(got[:, c] - ref[:, c]).max() <= 1e-9 * max(scale, 1e-300), c
+            assert np.abs(got[:, c] - ref[:, c]).max() <= 1e-7 * max(scale, 1e-300), c
     assert dt > 2e-6                          # the step grew from 1e-6 h to where the error test binds
     assert s["attempts"] < 2 * s["iterations"]   # passing proposals take one attempt
     sim.close()
 
 
-def test_learned_controller_gain_over_the_reference_controller():
-    """What the trained network gains over the method without it (the reference
-    controller, simulation.hpp:1688-1769) at equal RK tolerance on a growing,
-    dividing colony: simulated time per RK evaluation.  Also reported: the
-    same proposal loop with the network zeroed (error-model baseline only)."""
+def test_learned_controller_gain_over_pi_and_the_reference_controller():
+    """What the trained network gains over the methods without it, at equal RK tolerance
+    (1e-8) on growing, dividing colonies: RK evaluations per simulated hour, on three
+    colonies of 2500 cells over 2000 steps.  The comparisons are the plain PI controller
+    (the learned controller's baseline and fallback), the network with zero weights, and
+    the reference rule (simulation.hpp:1688-1769).  The error test decides every step in
+    all of them; rejected first attempts are counted in the evaluations and reported."""
     runs = [(stepsize.growing_colony(1500, 41), dict(max_stepsize=1e-4)),
             (stepsize.growing_colony(3000, 42), dict(max_stepsize=1e-4))]
     w, info = stepsize.train_protocol(runs, n_iters=1500, epochs=150)
-    cells = stepsize.growing_colony(2500, 43)
-    _, ref = stepsize.logged_run(cells, 2000, controller=0)
-    _, zero = stepsize.logged_run(cells, 2000, controller=1, weights=np.zeros(abm_b200.MLP_NPARAM, np.float32))
-    rows, lrn = stepsize.logged_run(cells, 2000, controller=1, weights=w)
-    per_eval = {k: s["t"] / s["attempts"] for k, s in (("reference", ref), ("zeroed", zero), ("learned", lrn))}
-    print("\nstep-size controllers on a 2500-cell growing colony, 2000 steps, tol 1e-8:")
-    for k, s in (("reference", ref), ("zeroed", zero), ("learned", lrn)):
-        print("  %-9s evals/step %.3f  rejected %d  divisions %d  t %.5f h  sim-time/eval %.3e h" % (
-            k, s["attempts"] / s["iterations"], s["rejected"], s["divisions"], s["t"], per_eval[k]))
-    # reference rule: trial + final every step, plus its retries
-    assert ref["attempts"] == 2 * ref["iterations"] + ref["retries"]
-    # learned: a passing proposal is the only attempt of its step; a failing one continues
-    # with the reference rule (its retries and the final re-run)
-    assert lrn["attempts"] == lrn["iterations"] + lrn["rejected"] + lrn["retries"]
-    assert (rows[:, 35] < 0.5).sum() == lrn["rejected"]
-    assert lrn["rejected"] <= 0.02 * lrn["iterations"]
-    assert lrn["t"] >= 0.75 * ref["t"]                       # comparable step sizes
-    assert per_eval["learned"] >= 1.6 * per_eval["reference"]
-    assert per_eval["learned"] >= 0.9 * per_eval["zeroed"]
+    zero = np.zeros(abm_b200.MLP_NPARAM, np.float32)
+    print("\nstep-size controllers on 2500-cell growing colonies, 2000 steps, tol 1e-8:")
+    for seed in (43, 44, 45):
+        cells = stepsize.growing_colony(2500, seed)
+        res = {}
+        for name, ctl, wt in (("reference", 0, None), ("pi", 2, None), ("zeroed", 1, zero), ("learned", 1, w)):
+            rows, s = stepsize.logged_run(cells, 2000, controller=ctl, weights=wt)
+            res[name] = s
+            print("  seed %d %-9s evals/step %.3f  rejected %3d  t %.5f h  evals per h %.0f" % (
+                seed, name, s["attempts"] / s["iterations"], s["rejected"], s["t"], s["attempts"] / s["t"]))
+        eph = {k: s["attempts"] / s["t"] for k, s in res.items()}
+        lrn, ref = res["learned"], res["reference"]
+        # reference rule: trial + final every step, plus its retries; the proposing
+        # controllers: one attempt per passing proposal, the reference rule after a failing one
+        assert ref["attempts"] == 2 * ref["iterations"] + ref["retries"]
+        for k in ("pi", "zeroed", "learned"):
+            s = res[k]
+            assert s["attempts"] == s["iterations"] + s["rejected"] + s["retries"]
+        assert lrn["rejected"] <= 0.05 * lrn["iterations"]
+        assert eph["learned"] <= 0.9 * eph["pi"], (seed, eph)
+        assert eph["learned"] <= 0.9 * eph["zeroed"], (seed, eph)
+        assert eph["learned"] <= 0.7 * eph["reference"], (seed, eph)

@@ -72,6 +72,9 @@ def parse_args(argv=None):
     ap.add_argument("--growth-arms", default="plain,chosen", help="arms of the growth run")
     ap.add_argument("--weights", default=None, help="step-size network weights (.npz); default: the shipped ones")
     ap.add_argument("--replicates", type=int, default=256)
+    ap.add_argument("--replicate-start", default="founder", choices=["founder", "near-target"],
+                    help="replicates grow from one founder cell each (the configuration), or start at 90 %% "
+                         "of their targets")
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--tile", type=int, default=0, help="screened pair pass: CSR entries per block tile")
     ap.add_argument("--bpsm", type=int, default=0, help="screened pair pass: blocks per SM")
@@ -663,10 +666,12 @@ def run_b200(args):
 
 def run_replicates(args):
     """Batched 2-D replicates: args.replicates colonies with log-uniform target sizes in
-    [500, 50000], each started from its own seeded colony at 90 % of its target and
-    grown with config-0 growth and division (BS32, tol 1e-8) until its target; one
-    graph launch per iteration advances all of them.  Pair-kernel lanes per size
-    decade come from the autotuner."""
+    [500, 50000], each grown from one founder cell with its own seed (or, with
+    --replicate-start near-target, from a seeded colony at 90 % of its target), with
+    config-0 growth and division (BS32, tol 1e-8) until its target; one graph launch per
+    iteration advances all of them.  The screened pair pass's shape per size decade
+    comes from the autotuner.  W + K iterations are run; the line reports the K timed
+    ones, whatever sizes the colonies have reached by then."""
     import torch
     from abm_b200 import replicates
     rank, world, local = dist_env()
@@ -676,7 +681,9 @@ def run_replicates(args):
         dist_init("nccl")
     targets = replicates.target_sizes(args.replicates, 500, 50000, seed=rank)
     tiles = replicates.tiles_by_bucket(targets, replicates.CONFIG0)
-    bt, sims = replicates.make_batch(targets, seed=1000 * rank + 1, start_fraction=0.9, tiles=tiles)
+    founders = args.replicate_start == "founder"
+    bt, sims = replicates.make_batch(targets, seed=1000 * rank + 1, start_fraction=0.9, tiles=tiles,
+                                     founders=founders)
     bt.iterate(max(args.warmup, 0))
     bt.synchronize()
     s0 = [s.stats() for s in sims]
@@ -705,7 +712,8 @@ def run_replicates(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded 2-D colonies)",
-            "config": {"workload": "2d_replicates_%d_loguniform500-50000_BS32_tol1e-8" % args.replicates,
+            "config": {"workload": "2d_replicates_%d_loguniform500-50000_BS32_tol1e-8_from_%s" %
+                                   (args.replicates, "founder" if founders else "90pct_of_target"),
                        "replicates": args.replicates, "cells_at_end": cells_now,
                        "target_cells_total": int(targets.sum()), "replicates_at_target": halted,
                        "rejected_step_fraction": d["rejected"] / max(d["iterations"], 1),

@@ -1655,11 +1655,17 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
     double local_drift = 0.0;
-    // one cell per thread: the grid covers the capacity (attempt_blocks); thread t
-    // takes the t-th cell of the attempt order (cells appended after it in index order)
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n)
+    // The grid holds one wave of resident blocks and strides over the attempt order in
+    // groups of 32 consecutive positions, one group per warp: group g goes to block
+    // g mod gridDim.x, so the full-surface cells at the head of the order spread over all
+    // blocks, while each warp still runs cells of one class.  Position t of the order is
+    // cell order[t] (cells appended after the order was made, in index order).
+    const int wpb = AT_T / 32, lane_a = threadIdx.x & 31, warp_b = threadIdx.x >> 5;
+    const int groups_per_pass = gridDim.x * wpb;
+    for (int g0 = warp_b * gridDim.x + blockIdx.x; g0 * 32 < n; g0 += groups_per_pass)
     {
+        const int t = g0 * 32 + lane_a;
+        if (t >= n) continue;
         const int i = t < n_order ? sp.order[t] : t;
         const Geom g = load_geom(from_backup ? geom_c : geom, i);
         const Vel* vprev = (from_backup ? vel_c : vel) + i;
@@ -2002,6 +2008,17 @@ void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int
     k_attempt_order<<<blocks, 256, 0, st>>>(ctrl, flag, pos, order);
 }
 
+// One wave: at most as many blocks as are resident at once (the kernel strides over the
+// cells), and no more than the capacity needs.
+template <class K>
+static int one_wave_blocks(K kernel, int blocks_for_cap)
+{
+    int dev = 0, sms = 148, occ = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, AT_T, 0) != cudaSuccess || occ < 1) occ = 1;
+    return max(1, min(blocks_for_cap, occ * sms));
+}
+
 template <int S, bool NOISE, int DIM, bool F32>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
@@ -2009,13 +2026,16 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
                              unsigned long long cond, int use_cond, PairGather pg, unsigned long long cond_run)
 {
 #define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg, cond_run
+#define AT_LAUNCH(K) { auto kern = k_attempt<S, K, NOISE, DIM, F32>; \
+        kern<<<one_wave_blocks(kern, blocks), AT_T, 0, st>>>(AT_ARGS); }
     switch (kind)
     {
-        case MODE_TRIAL: k_attempt<S, MODE_TRIAL, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_RETRY: k_attempt<S, MODE_RETRY, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        case MODE_FINAL: k_attempt<S, MODE_FINAL, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
-        default: k_attempt<S, 3, NOISE, DIM, F32><<<blocks, AT_T, 0, st>>>(AT_ARGS); break;
+        case MODE_TRIAL: AT_LAUNCH(MODE_TRIAL) break;
+        case MODE_RETRY: AT_LAUNCH(MODE_RETRY) break;
+        case MODE_FINAL: AT_LAUNCH(MODE_FINAL) break;
+        default: AT_LAUNCH(3) break;
     }
+#undef AT_LAUNCH
 #undef AT_ARGS
 }
 

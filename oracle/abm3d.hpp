@@ -1932,9 +1932,6 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
     }
     st.t += st.dt;
     st.iter++;
-    if (p.controller == 2 && p.integration_mode != 0)
-        st.dt = pi_next_dt(dt_accepted, st.last_max_error, st.prev_accepted_error,
-                           make_tableau(p.integration_mode).error_order, p);
     if (st.iter % p.iter_update_neighbors == 0)
     {
         st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
@@ -1953,6 +1950,10 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
             if (p.modulate_local_viscosity) modulate_viscosity(st.cells, st.nb, p);
         }
     }
+    // the PI proposal for the next step, once this step's dt has served the ramps
+    if (p.controller == 2 && p.integration_mode != 0)
+        st.dt = pi_next_dt(dt_accepted, st.last_max_error, st.prev_accepted_error,
+                           make_tableau(p.integration_mode).error_order, p);
 }
 
 }   // namespace oracle

@@ -164,6 +164,9 @@ def _load():
         "abm_cell_cell_forces_noalloc": ([P(AbmParams), vp, i, i, i, vp, vp, i, dp, dp, i, vp, vp], i),
         "abm_cell_cell_forces_noalloc_status": ([vp], i),
         "abm_noalloc_last_error": ([], ctypes.c_char_p),
+        "abm_set_switching": ([vp, i, i, dp, dp, dp, d, i, ip, dp, d, i, dp, i], i),
+        "abm_set_basal_only": ([vp, i, d], i),
+        "abm_basal_dropped": ([vp, P(ctypes.c_longlong)], i),
         "abm_set_frames": ([vp, d, i], i),
         "abm_frames_taken": ([vp, ip], i),
         "abm_download_frame": ([vp, i, vp, i, ip, dp, ip, ip], i),
@@ -223,7 +226,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_set_cell_limit abm_batch_create abm_batch_iterate abm_batch_synchronize abm_batch_get_stream "
             "abm_batch_destroy abm_batch_last_error abm_autotune_pair_tile abm_write_cells abm_read_cells "
             "abm_write_lineage abm_read_lineage abm_io_last_error abm_set_frames abm_frames_taken "
-            "abm_download_frame").split()
+            "abm_download_frame abm_set_switching abm_set_basal_only abm_basal_dropped").split()
 
 CONTROLLER_REFERENCE, CONTROLLER_LEARNED, CONTROLLER_PI = 0, 1, 2
 MLP_FEATURES, MLP_HIDDEN, MLP_NPARAM, MLP_LOG_COLS = 32, 64, 6337, 40
@@ -348,6 +351,32 @@ class Simulation:
         assert radius.shape == (len(delta), len(gamma))
         self._check(LIB.abm_set_jkr_table_variable(self._ctx, _dptr(delta), len(delta), _dptr(gamma), len(gamma),
                                                    _dptr(radius)), "abm_set_jkr_table_variable")
+
+    def set_switching(self, mode=1, rates=(0.0, 0.0, 0.0, 0.0), growth=((0.0, 0.0), (0.0, 0.0)), timescale=0.0,
+                      attrs=(), max_gamma=0.0, modulate=0, visc=(0.0, 0.0, 0.0, 0.0), max_coord=1, n_start=0):
+        """Phenotype switching between groups 1 and 2 (abm_set_switching): mode 1 Markov, 2 inherited
+        at division; rates 2 x 2 row-major (row = current group); growth = (means, stds) per group;
+        attrs = [(column, target in group 1, target in group 2), ...] for columns 17-19; gamma ramps
+        to max_gamma (group 1) or 0 (group 2) over `timescale`; modulate / visc / max_coord: local
+        viscosity from the group-1 share of contacts."""
+        cols = (ctypes.c_int * 4)(*[int(c) for c, _, _ in attrs])
+        targets = np.array([t1 for _, t1, _ in attrs] + [t2 for _, _, t2 in attrs] + [0.0], dtype=np.float64)
+        rates = np.ascontiguousarray(rates, dtype=np.float64)
+        gm = np.ascontiguousarray(growth[0], dtype=np.float64)
+        gs = np.ascontiguousarray(growth[1], dtype=np.float64)
+        visc = np.ascontiguousarray(visc, dtype=np.float64)
+        self._check(LIB.abm_set_switching(self._ctx, int(mode), int(n_start), _dptr(rates), _dptr(gm), _dptr(gs),
+                                          float(timescale), len(attrs), cols, _dptr(targets), float(max_gamma),
+                                          int(modulate), _dptr(visc), int(max_coord)), "abm_set_switching")
+
+    def set_basal_only(self, on=True, min_overlap=0.0):
+        """Basal-only compaction after each accepted step (abm_set_basal_only)."""
+        self._check(LIB.abm_set_basal_only(self._ctx, int(bool(on)), float(min_overlap)), "abm_set_basal_only")
+
+    def basal_dropped(self):
+        v = ctypes.c_longlong()
+        self._check(LIB.abm_basal_dropped(self._ctx, ctypes.byref(v)), "abm_basal_dropped")
+        return v.value
 
     def upload_cells(self, cells):
         """cells: (n, ncols) float64 array in the reference's column order."""

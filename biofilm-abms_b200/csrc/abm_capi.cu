@@ -66,6 +66,11 @@ struct abm_ctx {
     Phys* snap_phys = nullptr;
     FrameInfo* frame_info = nullptr;
     bool mlp_loaded = false;
+    // phenotype switching, ramps, local viscosity, basal-only compaction (abm_switch.cu)
+    SwitchParams sw;
+    bool post_on = false;            // the post-step kernels run after each accepted step
+    Phys* phys_c = nullptr;          // compaction scratch (geom_c / vel_c hold the rest)
+    int *keep = nullptr, *keep_rank = nullptr;
     // 2-D model
     int dims = 3;
     unsigned char* adhere = nullptr;  // to_adhere per CSR entry
@@ -184,7 +189,8 @@ static void free_all(abm_ctx* c)
                     c->scan_sums, c->jkr_delta, c->jkr_radius, c->jkr_gam, c->jkr_rad2, c->staging, c->div_flags, c->div_rank,
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
-                    c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info};
+                    c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info, c->phys_c, c->keep,
+                    c->keep_rank};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -382,6 +388,9 @@ int abm_create(const abm_params* q, abm_ctx** out)
     dp.daughter_length_std = p.daughter_length_std;
     dp.angle_xy_bound = p.daughter_angle_xy_bound; dp.angle_z_bound = p.daughter_angle_z_bound;
     dp.seed = p.rng_seed; dp.cap_cells = c->cap;
+    dp.group_growth = 0; dp.inherit = 0; dp.n_start_switch = 0;
+    memset(&c->sw, 0, sizeof(c->sw));
+    c->sw.seed = p.rng_seed; c->sw.R = p.R; c->sw.max_coord = 1;
     if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
         return fail(c, ABM_ERR_ARG, "adhesion_mode must be 0 (none) or 1 (isotropic JKR, fixed gamma)");
     // 2-D model
@@ -525,6 +534,118 @@ int abm_set_jkr_table_variable(abm_ctx* c, const double* delta, int n_delta, con
     return ABM_OK;
 }
 
+// switching moves cells between growth-rate distributions: division is possible when
+// either group's distribution is not the zero rate
+static bool switch_grows(const abm_ctx* c)
+{
+    const SwitchParams& w = c->sw;
+    return w.mode != 0 && (w.gmean[0] != 0 || w.gmean[1] != 0 || w.gstd[0] != 0 || w.gstd[1] != 0);
+}
+
+static int ensure_post_buffers(abm_ctx* c)
+{
+    if (!c->keep) CK(cudaMalloc(&c->keep, (size_t)c->cap * sizeof(int)));
+    if (!c->keep_rank) CK(cudaMalloc(&c->keep_rank, ((size_t)c->cap + 1) * sizeof(int)));
+    if (!c->phys_c) CK(cudaMalloc(&c->phys_c, (size_t)c->cap * sizeof(Phys)));
+    return ABM_OK;
+}
+
+static void update_post(abm_ctx* c)
+{
+    const bool on = c->sw.mode != 0 || c->sw.basal;
+    if (on != c->post_on) drop_iteration_graphs(c);
+    c->post_on = on;
+    if (switch_grows(c) && !c->div_enabled) { c->div_enabled = true; drop_iteration_graphs(c); }
+}
+
+int abm_set_switching(abm_ctx* c, int mode, int n_start, const double* rates, const double* growth_mean,
+                      const double* growth_std, double timescale, int n_attr, const int* attr_col,
+                      const double* attr_targets, double max_gamma, int modulate, const double* visc_lims,
+                      int max_coord)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (c->dims != 3) return fail(c, ABM_ERR_STATE, "switching belongs to the 3-D model");
+    if (mode < 0 || mode > 2) return fail(c, ABM_ERR_ARG, "switching mode must be 0 (none), 1 (Markov) or 2 (inherit)");
+    if (mode != 0 && (!rates || !growth_mean || !growth_std))
+        return fail(c, ABM_ERR_ARG, "switching needs rates and growth distributions");
+    if (n_attr < 0 || n_attr > 4 || (n_attr > 0 && (!attr_col || !attr_targets)))
+        return fail(c, ABM_ERR_ARG, "0..4 switched attributes, with columns and targets");
+    if (!(timescale >= 0) || !(max_gamma >= 0) || max_coord < 1)
+        return fail(c, ABM_ERR_ARG, "timescale and max_gamma must be >= 0, max_coord >= 1");
+    if (modulate && !visc_lims) return fail(c, ABM_ERR_ARG, "local viscosity needs its limits");
+    SwitchParams& w = c->sw;
+    w.mode = mode;
+    w.n_start = n_start;
+    for (int k = 0; k < 4; ++k) w.rates[k] = mode != 0 ? rates[k] : 0.0;
+    for (int g = 0; g < 2; ++g)
+    {
+        w.gmean[g] = mode != 0 ? growth_mean[g] : 0.0;
+        w.gstd[g] = mode != 0 ? growth_std[g] : 0.0;
+    }
+    for (int k = 0; k < 4; ++k)
+        if (!(w.rates[k] >= 0) || !std::isfinite(w.rates[k])) return fail(c, ABM_ERR_ARG, "rates must be finite and >= 0");
+    w.timescale = timescale;
+    w.n_attr = n_attr;
+    for (int k = 0; k < n_attr; ++k)
+    {
+        // the reference's drivers switch eta0, eta1 and sigma0 (indices.hpp: columns 17-19)
+        if (attr_col[k] < 17 || attr_col[k] > 19)
+            return fail(c, ABM_ERR_ARG, "switched attributes are columns 17 (eta0), 18 (eta1) or 19 (sigma0)");
+        w.attr_field[k] = attr_col[k] - 15;          // Phys: l, growth, eta0, eta1, sigma0, ...
+        w.target[0][k] = attr_targets[k];
+        w.target[1][k] = attr_targets[n_attr + k];
+    }
+    w.max_gamma = max_gamma;
+    w.gamma_ramp = mode != 0 && c->p.adhesion_mode != 0;
+    w.modulate = (mode != 0 && c->p.adhesion_mode != 0 && modulate) ? 1 : 0;
+    for (int k = 0; k < 4; ++k) w.visc[k] = visc_lims ? visc_lims[k] : 0.0;
+    w.max_coord = max_coord;
+    // division: the daughters' growth rates follow the mother's group, and inherited
+    // switching acts on each pair of daughters
+    DivideParams& dp = c->dp;
+    dp.group_growth = mode != 0;
+    for (int g = 0; g < 2; ++g) { dp.gmean[g] = w.gmean[g]; dp.gstd[g] = w.gstd[g]; }
+    dp.inherit = mode == 2;
+    dp.n_start_switch = n_start;
+    for (int k = 0; k < 4; ++k) dp.rates[k] = w.rates[k];
+    if (mode != 0)
+    {
+        int rc = ensure_post_buffers(c);
+        if (rc) return rc;
+    }
+    drop_iteration_graphs(c);                 // the parameters are baked into the graph's nodes
+    update_post(c);
+    return ABM_OK;
+}
+
+int abm_set_basal_only(abm_ctx* c, int basal_only, double min_overlap)
+{
+    if (!c) return ABM_ERR_ARG;
+    if (c->dims != 3) return fail(c, ABM_ERR_STATE, "basal-only compaction belongs to the 3-D model");
+    if (!std::isfinite(min_overlap)) return fail(c, ABM_ERR_ARG, "min_overlap must be finite");
+    // simulation.hpp:1831: only with the surface present
+    c->sw.basal = (basal_only && !c->p.no_surface) ? 1 : 0;
+    c->sw.basal_min_overlap = min_overlap;
+    if (c->sw.basal)
+    {
+        int rc = ensure_post_buffers(c);
+        if (rc) return rc;
+    }
+    drop_iteration_graphs(c);
+    update_post(c);
+    return ABM_OK;
+}
+
+int abm_basal_dropped(abm_ctx* c, long long* dropped)
+{
+    if (!c || !dropped) return ABM_ERR_ARG;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *dropped = h.basal_dropped;
+    return ABM_OK;
+}
+
 int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
 {
     if (!c || !cm || n < 0 || ld < n) return fail(c, ABM_ERR_ARG, "bad cell array");
@@ -549,7 +670,7 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     c->n_host = n;
     c->cells_loaded = true;
     // division is possible when a cell already exceeds Ldiv or any cell can grow
-    bool grows = (c->p.growth_mean != 0 || c->p.growth_std != 0);
+    bool grows = (c->p.growth_mean != 0 || c->p.growth_std != 0) || switch_grows(c);
     const int col_growth = two_d ? 12 : 16, col_l = two_d ? 9 : 13;
     for (int i = 0; i < n && !grows; ++i)
         grows = cm[(size_t)col_growth * ld + i] != 0 || cm[(size_t)col_l * ld + i] > c->p.Ldiv;
@@ -915,6 +1036,82 @@ static int capture_division_body(abm_ctx* c, cudaGraph_t body)
     return capture_into(c, body, bd, [&]() { enqueue_division_commit(c); enqueue_rebuild(c); });
 }
 
+// After the accepted step (simulation.hpp:1831-2022): basal-only compaction and its
+// rebuild, the periodic neighbor rebuild, then switching, the ramps and local viscosity,
+// which read the neighbor rows as they stand after those rebuilds.
+static void enqueue_basal_test(abm_ctx* c, unsigned long long cond, int use_cond)
+{
+    launch_basal_flags(c->geom, c->ctrl, c->sw, c->keep, c->cap, c->st);
+    launch_scan(c->keep, &c->ctrl->n, c->keep_rank, c->scan_sums, c->cap, c->st);
+    launch_basal_decide(c->ctrl, c->keep, c->keep_rank, cond, use_cond, c->st);
+}
+
+static void enqueue_basal_compact(abm_ctx* c)
+{
+    launch_basal_compact(c->geom, c->vel, c->phys, c->geom_c, c->vel_c, c->phys_c, c->ctrl, c->keep, c->keep_rank,
+                         c->cap, c->st);
+}
+
+static void enqueue_switch_cells(abm_ctx* c)
+{
+    if (c->sw.mode != 0) launch_switch_cells(c->geom, c->phys, c->ctrl, c->sw, c->cap, c->st);
+    if (c->sw.modulate)
+        launch_modulate_viscosity(c->geom, c->phys, c->ctrl, c->row_ptr, c->col, c->sw, c->cap, c->st);
+}
+
+// the same on a stream, the two rebuild decisions read back on the host
+static int post_step_direct(abm_ctx* c)
+{
+    Ctrl h;
+    if (c->sw.basal)
+    {
+        enqueue_basal_test(c, 0, 0);
+        CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (h.n_keep < h.n) { enqueue_basal_compact(c); enqueue_rebuild(c); }
+    }
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (!h.halted && h.iter % c->p.iter_update_neighbors == 0) enqueue_rebuild(c);
+    enqueue_switch_cells(c);
+    CK(cudaGetLastError());
+    return ABM_OK;
+}
+
+// the same as graph nodes: IF(a cell is dropped){compaction + rebuild},
+// IF(iteration counter % iter_update_neighbors == 0){rebuild}, then the switching kernels
+static int append_post_step(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode_t>& deps)
+{
+    int rc;
+    if (c->sw.basal)
+    {
+        cudaGraphConditionalHandle h_basal = 0;
+        CK(cudaGraphConditionalHandleCreate(&h_basal, G, 0, cudaGraphCondAssignDefault));
+        rc = capture_into(c, G, deps, [&]() { enqueue_basal_test(c, h_basal, 1); });
+        if (rc) return rc;
+        cudaGraph_t body;
+        rc = add_conditional(c, G, deps, h_basal, cudaGraphCondTypeIf, &body);
+        if (rc) return rc;
+        std::vector<cudaGraphNode_t> bd;
+        rc = capture_into(c, body, bd, [&]() { enqueue_basal_compact(c); enqueue_rebuild(c); });
+        if (rc) return rc;
+    }
+    cudaGraphConditionalHandle h_reb = 0;
+    CK(cudaGraphConditionalHandleCreate(&h_reb, G, 0, cudaGraphCondAssignDefault));
+    rc = capture_into(c, G, deps, [&]() {
+        launch_periodic_rebuild_cond(c->ctrl, c->p.iter_update_neighbors, h_reb, c->st);
+    });
+    if (rc) return rc;
+    cudaGraph_t body;
+    rc = add_conditional(c, G, deps, h_reb, cudaGraphCondTypeIf, &body);
+    if (rc) return rc;
+    std::vector<cudaGraphNode_t> bd;
+    rc = capture_into(c, body, bd, [&]() { enqueue_rebuild(c); });
+    if (rc) return rc;
+    if (c->sw.mode != 0) return capture_into(c, G, deps, [&]() { enqueue_switch_cells(c); });
+    return ABM_OK;
+}
+
 // One loop iteration as a graph with conditional nodes, appended to G after `deps`
 // (empty: root nodes); `deps` becomes the iteration's leaf set:
 //   [division count] -> IF(n_divide > 0){division + rebuild}
@@ -983,6 +1180,11 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
             if (rc) return rc;
         }
         rc = capture_into(c, G, deps, final_attempt);
+        if (rc) return rc;
+    }
+    if (c->post_on)
+    {
+        rc = append_post_step(c, G, deps);
         if (rc) return rc;
     }
     // frames: the snapshot of a frame the accepted step marked
@@ -1327,12 +1529,21 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
         else
         {
             if (c->div_enabled) { rc = divide_now(c, true, nullptr); if (rc) return rc; }
-            if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
+            if (c->post_on)
+            {
+                enqueue_loop_pair_force(c);
+                enqueue_attempts(c);
+                rc = post_step_direct(c);
+                if (rc) return rc;
+                if (c->frame_slots > 0) enqueue_frame_snapshot(c);
+            }
+            else if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_iter, c->st));
             else enqueue_iteration(c);
         }
         c->host_iter += step;
         k += step;
-        if (c->host_iter % c->p.iter_update_neighbors == 0)
+        // with the post-step kernels on, the periodic rebuild is part of the iteration
+        if (!c->post_on && c->host_iter % c->p.iter_update_neighbors == 0)
         {
             if (c->p.use_graphs) CK(cudaGraphLaunch(c->g_rebuild, c->st));
             else enqueue_rebuild(c);
@@ -1346,6 +1557,7 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
 int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
 {
     if (!c || !prof || n_iters < 0) return ABM_ERR_ARG;
+    if (c->post_on) return fail(c, ABM_ERR_STATE, "the profile covers the loop without switching or basal-only compaction");
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (c->sp.network && !c->mlp_loaded)
@@ -1551,6 +1763,8 @@ int abm_batch_create(abm_ctx* const* ctxs, int n, abm_batch** out)
     for (abm_ctx* c : b->ctxs)
     {
         if (!c || !c->cells_loaded) { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "every context needs cells"); }
+        if (c->post_on)
+        { delete b; return batch_fail(nullptr, ABM_ERR_STATE, "switching and basal-only contexts run through abm_iterate"); }
         if (c->dev != dev) { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts on different devices"); }
         if (c->p.iter_update_neighbors != b->k_rebuild)
         { delete b; return batch_fail(nullptr, ABM_ERR_ARG, "contexts must share iter_update_neighbors"); }

@@ -331,6 +331,7 @@ __host__ __device__ __forceinline__ double philox_u01(uint32_t hi, uint32_t lo)
 }
 const uint32_t RNG_PURPOSE_NOISE = 0x4E6F6973u;
 const uint32_t RNG_PURPOSE_DIVIDE = 0x44697669u;
+const uint32_t RNG_PURPOSE_SWITCH = 0x53776974u;
 
 __host__ __device__ __forceinline__ double rng_uniform(uint64_t seed, uint32_t purpose, uint32_t a,
                                                        uint32_t b, uint32_t c, uint32_t d)
@@ -338,6 +339,15 @@ __host__ __device__ __forceinline__ double rng_uniform(uint64_t seed, uint32_t p
     uint32_t x[4] = {a, b, c, d};
     philox4x32_10(x, (uint32_t)seed, (uint32_t)(seed >> 32) ^ purpose);
     return philox_u01(x[0], x[1]);
+}
+
+// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms, with the
+// deterministic log / cos shared with the CPU restatement
+__device__ __forceinline__ double std_normal(double u, double v)
+{
+    double s, c;
+    det_sincos(__dmul_rn(6.283185307179586476925286766559005768, v), s, c);
+    return __dmul_rn(__dsqrt_rn(__dmul_rn(-2.0, det_log(u))), c);
 }
 
 // ---------------------------------------------------------------------------

@@ -122,15 +122,6 @@ __global__ void k_div_check(const Geom* __restrict__ geom, Ctrl* ctrl, DividePar
     }
 }
 
-// utils.hpp:648-655 (standardNormal, Box-Muller) on two policy uniforms, with the
-// deterministic log / cos shared with the CPU restatement
-__device__ __forceinline__ double std_normal(double u, double v)
-{
-    double s, c;
-    det_sincos(__dmul_rn(6.283185307179586476925286766559005768, v), s, c);
-    return __dmul_rn(__dsqrt_rn(__dmul_rn(-2.0, det_log(u))), c);
-}
-
 __device__ __forceinline__ double div_u(const DivideParams& dp, int iter, int k, int tr, int slot)
 {
     return rng_uniform(dp.seed, RNG_PURPOSE_DIVIDE, (uint32_t)iter, (uint32_t)k, (uint32_t)tr, (uint32_t)slot);
@@ -206,9 +197,16 @@ __global__ void k_div_try(const Geom* __restrict__ geom, const Phys* __restrict_
         a.h = __ddiv_rn(L1, 2.0); b.h = __ddiv_rn(L2, 2.0);
         d1[k] = a; d2[k] = b;
         dlen[2 * k] = L1; dlen[2 * k + 1] = L2;
-        dgrowth[2 * k] = __dadd_rn(dp.growth_mean, __dmul_rn(dp.growth_std,
+        // with switching, the distribution of the mother's group (growth.hpp:634-644)
+        double gmean = dp.growth_mean, gstd = dp.growth_std;
+        if (dp.group_growth)
+        {
+            const int g0 = (int)phys[i].group == 1 ? 0 : 1;
+            gmean = dp.gmean[g0]; gstd = dp.gstd[g0];
+        }
+        dgrowth[2 * k] = __dadd_rn(gmean, __dmul_rn(gstd,
                                    std_normal(div_u(dp, iter, k, tr, 6), div_u(dp, iter, k, tr, 7))));
-        dgrowth[2 * k + 1] = __dadd_rn(dp.growth_mean, __dmul_rn(dp.growth_std,
+        dgrowth[2 * k + 1] = __dadd_rn(gmean, __dmul_rn(gstd,
                                        std_normal(div_u(dp, iter, k, tr, 8), div_u(dp, iter, k, tr, 9))));
     }
 }
@@ -287,7 +285,37 @@ __global__ void k_div_eval(Ctrl* ctrl, const int* check, const int* ok, int* sat
     }
 }
 
-__global__ void k_div_commit(Geom* geom, Vel* vel, Phys* phys, const Ctrl* ctrl, const int* mothers,
+// switch.hpp:97-142 (switchGroupsInherit) for division pair k, the daughters in the
+// mother's row (p1) and the appended row (p2), both of the mother's group g: with
+// probability 1 - P(g, g), one of the two, chosen by a second uniform, moves to the other
+// group and draws that group's growth rate.  Draws: purpose SWITCH, counters (iteration,
+// pair, slot 4 / 5 / 6-7).
+__device__ __forceinline__ void inherit_switch(const DivideParams& dp, int iter, int k, Phys& p1, Phys& p2)
+{
+    const int g = (int)p1.group - 1;
+    if (g != 0 && g != 1) return;
+    auto u = [&](int slot) {
+        return rng_uniform(dp.seed, RNG_PURPOSE_SWITCH, (uint32_t)iter, (uint32_t)k, (uint32_t)slot, 0u);
+    };
+    const double r = u(4);
+    double total = dp.rates[g * 2 + g];
+    if (!(r > total)) return;
+    for (int j = 0; j < 2; ++j)
+    {
+        if (j == g) continue;
+        const double prob = dp.rates[g * 2 + j];
+        if (r > total && r < __dadd_rn(total, prob))
+        {
+            Phys& w = u(5) < 0.5 ? p1 : p2;
+            w.group = j + 1;
+            w.growth = __dadd_rn(dp.gmean[j], __dmul_rn(dp.gstd[j], std_normal(u(6), u(7))));
+            return;
+        }
+        total = __dadd_rn(total, prob);
+    }
+}
+
+__global__ void k_div_commit(Geom* geom, Vel* vel, Phys* phys, const Ctrl* ctrl, DivideParams dp, const int* mothers,
                              const Geom* d1, const Geom* d2, const double* dlen, const double* dgrowth,
                              int* parents)
 {
@@ -308,6 +336,7 @@ __global__ void k_div_commit(Geom* geom, Vel* vel, Phys* phys, const Ctrl* ctrl,
         p1.t0 = t; p2.t0 = t;
         p1.growth = dgrowth[2 * k]; p2.growth = dgrowth[2 * k + 1];
         p1.id = max_id + (2 * k + 1); p2.id = max_id + (2 * k + 2);   // growth.hpp:407-418
+        if (dp.inherit && n + nd >= dp.n_start_switch) inherit_switch(dp, ctrl->iter, k, p1, p2);
         geom[i] = a; phys[i] = p1;
         geom[n + k] = b; phys[n + k] = p2; vel[n + k] = vm;
         parents[np + 2 * k] = parent_id;
@@ -381,8 +410,8 @@ void launch_div_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const Divid
                        const Geom* d1, const Geom* d2, const double* dlen, const double* dgrowth, int* parents,
                        cudaStream_t st)
 {
-    k_div_commit<<<max(cdiv_d(dp.cap_cells, DV_T), 1), DV_T, 0, st>>>(geom, vel, phys, ctrl, mothers, d1, d2, dlen,
-                                                                     dgrowth, parents);
+    k_div_commit<<<max(cdiv_d(dp.cap_cells, DV_T), 1), DV_T, 0, st>>>(geom, vel, phys, ctrl, dp, mothers, d1, d2,
+                                                                     dlen, dgrowth, parents);
     k_div_finish<<<1, 1, 0, st>>>(ctrl);
 }
 

@@ -89,6 +89,9 @@ struct Ctrl {
     double dt_write;                    // 0: no frames
     int frame_due, frames_taken;
     unsigned int frame_blocks;          // last-block counter of the snapshot kernel
+    // basal-only compaction: cells kept by the last test, cells dropped so far
+    int n_keep;
+    long long basal_dropped;
     double drift;                       // sum over accepted steps of the max segment motion
     unsigned long long drift_bits;      // block maxima of the running attempt (ordered bits)
 };
@@ -273,6 +276,13 @@ struct DivideParams {
     double growth_mean, growth_std, daughter_length_std, angle_xy_bound, angle_z_bound;
     uint64_t seed;
     int cap_cells;
+    // phenotype switching: the daughters' growth rates come from the mother's group
+    // (growth.hpp:634-644), and with inherited switching one daughter of a pair may move
+    // to the other group at division (switch.hpp:97-142, simulation.hpp:1650-1656)
+    int group_growth;
+    double gmean[2], gstd[2];
+    int inherit, n_start_switch;
+    double rates[4];
 };
 void launch_div_count(const Phys* phys, Ctrl* ctrl, const DivideParams& dp, int* flags,
                       unsigned long long cond, int use_cond, cudaStream_t st);
@@ -292,5 +302,41 @@ void launch_div_try_round(const Geom* geom, const Phys* phys, Ctrl* ctrl, const 
 void launch_div_commit(Geom* geom, Vel* vel, Phys* phys, Ctrl* ctrl, const DivideParams& dp, const int* mothers,
                        const Geom* d1, const Geom* d2, const double* dlen, const double* dgrowth, int* parents,
                        cudaStream_t st);
+
+// Phenotype switching between two groups and what it drives, after each accepted step
+// (abm_switch.cu): Markov switching (switch.hpp:45-95), the attribute and gamma ramps
+// (simulation.hpp:1872-1957), local viscosity (simulation.hpp:1958-2020) and basal-only
+// compaction (simulation.hpp:1831-1856).  Random draws: Philox, purpose SWITCH, counters
+// (iteration, cell or division pair, slot).
+struct SwitchParams {
+    uint64_t seed;
+    int mode;                   // 0 none, 1 Markov, 2 inherited at division
+    int n_start;                // switching starts once the colony has this many cells
+    double rates[4];            // 2 x 2, row = current group: rates (Markov) or probabilities
+    double gmean[2], gstd[2];   // growth-rate distribution of each group
+    double timescale;           // ramp time; 0: the attributes jump to their targets
+    int n_attr;
+    int attr_field[4];          // switched attributes as Phys fields: 2 eta0, 3 eta1, 4 sigma0
+    double target[2][4];        // their targets in group 1 and group 2
+    int gamma_ramp;             // adhesion on: gamma ramps up (group 1) or down (group 2)
+    double max_gamma;
+    int modulate;               // eta0 from the share of group-1 cells among the contacts
+    double visc[4];             // (min, max) eta0 of group 1, then of group 2
+    int max_coord;
+    double R;
+    int basal;                  // basal-only compaction (surface present)
+    double basal_min_overlap;
+};
+void launch_switch_cells(Geom* geom, Phys* phys, const Ctrl* ctrl, const SwitchParams& sw, int cap_cells,
+                         cudaStream_t st);
+void launch_modulate_viscosity(const Geom* geom, Phys* phys, const Ctrl* ctrl, const int* row_ptr, const int* col,
+                               const SwitchParams& sw, int cap_cells, cudaStream_t st);
+void launch_basal_flags(const Geom* geom, const Ctrl* ctrl, const SwitchParams& sw, int* keep, int cap_cells,
+                        cudaStream_t st);
+void launch_basal_decide(Ctrl* ctrl, const int* keep, const int* rank, unsigned long long cond, int use_cond,
+                         cudaStream_t st);
+void launch_basal_compact(Geom* geom, Vel* vel, Phys* phys, Geom* geom_tmp, Vel* vel_tmp, Phys* phys_tmp,
+                          Ctrl* ctrl, const int* keep, const int* rank, int cap_cells, cudaStream_t st);
+void launch_periodic_rebuild_cond(const Ctrl* ctrl, int every, unsigned long long cond, cudaStream_t st);
 
 }   // namespace abm

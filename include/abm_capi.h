@@ -181,6 +181,38 @@ int abm_jkr_radius_table_variable(double R, double Rcell, double E0, double max_
 int abm_set_jkr_table_variable(abm_ctx* ctx, const double* delta, int n_delta, const double* gamma, int n_gamma,
                                const double* radius);
 
+/* Phenotype switching between groups 1 and 2 (3-D), applied inside abm_iterate after each
+ * accepted step, after basal-only compaction and the periodic neighbor rebuild
+ * (simulation.hpp:1866-2022).  Replaces the switching arguments of runSimulation
+ * (simulation.hpp:1135-1160: switch_mode, switch_rates, growth_means / growth_stds,
+ * switch_attributes, attribute_values, switch_timescale, max_gamma, modulate_local_viscosity,
+ * viscosity_lims, max_coordination_number).
+ *   mode        0 none, 1 Markov (switch.hpp:45-95), 2 inherited at division (switch.hpp:97-142)
+ *   n_start     switching starts once the colony has this many cells
+ *   rates       2 x 2 row-major, row = current group: rates per unit time (Markov) or
+ *               probabilities (inherited)
+ *   growth_mean, growth_std   growth-rate distribution of each group; with switching on,
+ *               daughters draw from their mother's group's (growth.hpp:634-644)
+ *   timescale   ramp time of the switched attributes and gamma; 0 = at once
+ *   n_attr, attr_col, attr_targets   up to 4 switched attributes, columns 17 (eta0),
+ *               18 (eta1) or 19 (sigma0), with targets 2 x n_attr row-major (group 1, group 2)
+ *   max_gamma   gamma ramps to max_gamma in group 1, to 0 in group 2 (adhesion on)
+ *   modulate, visc_lims, max_coord   local viscosity (adhesion on): eta0 between
+ *               visc_lims (min, max of group 1, then of group 2) by the share of group-1 cells
+ *               among the contacts, saturating at max_coord of them (simulation.hpp:1958-2020)
+ * Random draws: the Philox policy of the division and noise kernels, purpose SWITCH, counters
+ * (iteration, cell or division pair, slot).  ABM_ERR_STATE for a 2-D context. */
+int abm_set_switching(abm_ctx* ctx, int mode, int n_start, const double* rates, const double* growth_mean,
+                      const double* growth_std, double timescale, int n_attr, const int* attr_col,
+                      const double* attr_targets, double max_gamma, int modulate, const double* visc_lims,
+                      int max_coord);
+/* Basal-only growth (simulation.hpp:1831-1856): with the surface present, after each accepted
+ * step only the cells whose deepest overlap R - rz + half_l nz exceeds min_overlap stay (in
+ * order), followed by a neighbor rebuild when any was dropped. */
+int abm_set_basal_only(abm_ctx* ctx, int basal_only, double min_overlap);
+/* Cells dropped by basal-only compaction since the context was created. */
+int abm_basal_dropped(abm_ctx* ctx, long long* dropped);
+
 /* Cell state in and out (the cells array of runSimulation).  ld >= n. */
 int abm_upload_cells(abm_ctx* ctx, const double* colmajor, int n, int ncols, int ld);
 int abm_download_cells(abm_ctx* ctx, double* colmajor, int ld);

@@ -168,6 +168,21 @@ class Oracle:
         r = np.ascontiguousarray(radius, dtype=np.float64).ravel()
         LIB.oracle_set_jkr_table2(self._c, _dp(d), len(d), _dp(g), len(g), _dp(r))
 
+    def set_switching(self, mode=1, rates=(0.0, 0.0, 0.0, 0.0), growth=((0.0, 0.0), (0.0, 0.0)), timescale=0.0,
+                      attrs=(), max_gamma=0.0, modulate=0, visc=(0.0, 0.0, 0.0, 0.0), max_coord=1, n_start=0):
+        """oracle_set_switching with the arguments of Simulation.set_switching."""
+        cols = (ctypes.c_int * 4)(*[int(c) for c, _, _ in attrs])
+        targets = np.array([t1 for _, t1, _ in attrs] + [t2 for _, _, t2 in attrs] + [0.0], dtype=np.float64)
+        rc = LIB.oracle_set_switching(self._c, int(mode), int(n_start), _dp(np.array(rates, dtype=np.float64)),
+                                      _dp(np.array(growth[0], dtype=np.float64)),
+                                      _dp(np.array(growth[1], dtype=np.float64)), float(timescale), len(attrs), cols,
+                                      _dp(targets), float(max_gamma), int(modulate),
+                                      _dp(np.array(visc, dtype=np.float64)), int(max_coord))
+        assert rc == 0
+
+    def set_basal_only(self, on=True, min_overlap=0.0):
+        LIB.oracle_set_basal(self._c, int(bool(on)), float(min_overlap))
+
     def set_jkr_table(self, delta, radius):
         d = np.ascontiguousarray(delta, dtype=np.float64)
         r = np.ascontiguousarray(radius, dtype=np.float64)

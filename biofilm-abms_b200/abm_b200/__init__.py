@@ -63,6 +63,7 @@ class AbmParams(ctypes.Structure):
         ("adhesion_mindist", ctypes.c_double), ("max_noise", ctypes.c_double),
         ("pair_tile", ctypes.c_int), ("pair_blocks_per_sm", ctypes.c_int), ("pair_skin", ctypes.c_double),
         ("pair_sum", ctypes.c_int),
+        ("friction_mode", ctypes.c_int), ("cell_cell_coulomb_coeff", ctypes.c_double),
     ]
 
 
@@ -103,7 +104,7 @@ DEFAULTS = dict(
     daughter_angle_z_bound=0.0, rng_seed=42, precision=PRECISION_FP64, cap_cells=0,
     cap_neighbors_per_cell=0, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
     dims=3, sigma0=100.0, adhesion_strength=0.0, adhesion_mindist=0.0, max_noise=0.0,
-    pair_tile=0, pair_blocks_per_sm=0, pair_skin=0.0, pair_sum=0,
+    pair_tile=0, pair_blocks_per_sm=0, pair_skin=0.0, pair_sum=0, friction_mode=0, cell_cell_coulomb_coeff=1.0,
 )
 
 # The 2-D driver (ABM-2d/ABM-2d-cpp/include/simulation.hpp:163-237): Bogacki-Shampine 3(2),

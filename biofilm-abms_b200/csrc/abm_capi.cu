@@ -66,6 +66,14 @@ struct abm_ctx {
     Phys* snap_phys = nullptr;
     FrameInfo* frame_info = nullptr;
     bool mlp_loaded = false;
+    // cell-cell kinetic friction: the coefficient of each cell (column eta_col), the per-entry
+    // planar-contact records, the candidate list and the stage states of the trial passes
+    double* feta = nullptr;
+    double4* fbuf = nullptr;
+    int *fmask = nullptr, *fr_list = nullptr;
+    double2* ystage = nullptr;
+    double* snap_feta = nullptr;
+    int eta_col = 21;
     // phenotype switching, ramps, local viscosity, basal-only compaction (abm_switch.cu)
     SwitchParams sw;
     bool post_on = false;            // the post-step kernels run after each accepted step
@@ -190,7 +198,7 @@ static void free_all(abm_ctx* c)
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
                     c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info, c->phys_c, c->keep,
-                    c->keep_rank};
+                    c->keep_rank, c->feta, c->fbuf, c->fmask, c->fr_list, c->ystage, c->snap_feta};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -388,7 +396,7 @@ int abm_create(const abm_params* q, abm_ctx** out)
     dp.daughter_length_std = p.daughter_length_std;
     dp.angle_xy_bound = p.daughter_angle_xy_bound; dp.angle_z_bound = p.daughter_angle_z_bound;
     dp.seed = p.rng_seed; dp.cap_cells = c->cap;
-    dp.group_growth = 0; dp.inherit = 0; dp.n_start_switch = 0;
+    dp.group_growth = 0; dp.inherit = 0; dp.n_start_switch = 0; dp.feta = nullptr;
     memset(&c->sw, 0, sizeof(c->sw));
     c->sw.seed = p.rng_seed; c->sw.R = p.R; c->sw.max_coord = 1;
     if (p.adhesion_mode != 0 && p.adhesion_mode != 1)
@@ -415,6 +423,34 @@ int abm_create(const abm_params* q, abm_ctx** out)
         CK(cudaMalloc(&c->adhere, cap * c->cap_nbr));
         CK(cudaMemset(c->adhere, 0, cap * c->cap_nbr));
         fp.adhere = c->adhere;
+    }
+    // cell-cell kinetic friction (mechanics.hpp:1031-1175, 1339-1346)
+    if (p.friction_mode != 0 && p.friction_mode != 1) return fail(c, ABM_ERR_ARG, "friction_mode must be 0 or 1");
+    fp.fric = 0;
+    sp.fric = 0;
+    if (p.friction_mode == 1)
+    {
+        if (c->dims != 3) return fail(c, ABM_ERR_ARG, "cell-cell friction belongs to the 3-D model");
+        if (p.precision != ABM_PRECISION_FP64) return fail(c, ABM_ERR_ARG, "cell-cell friction runs in FP64");
+        c->eta_col = p.adhesion_mode != 0 ? 22 : 21;        // simulation.hpp:1184-1186
+        const size_t ent = cap * c->cap_nbr;
+        CK(cudaMalloc(&c->feta, cap * sizeof(double)));
+        CK(cudaMemset(c->feta, 0, cap * sizeof(double)));
+        CK(cudaMalloc(&c->fbuf, ent * sizeof(double4)));
+        CK(cudaMalloc(&c->fmask, ent * sizeof(int)));
+        CK(cudaMemset(c->fmask, 0, ent * sizeof(int)));
+        CK(cudaMalloc(&c->fr_list, (ent / 2 + 1) * sizeof(int)));
+        CK(cudaMalloc(&c->ystage, (size_t)MAX_STAGES * cap * sizeof(double2)));
+        fp.fric = 1;
+        fp.surface = !p.no_surface;
+        fp.coulomb_cc = p.cell_cell_coulomb_coeff;
+        fp.vel = c->vel;
+        fp.feta = c->feta;
+        fp.fbuf = c->fbuf;
+        fp.fmask = c->fmask;
+        fp.fr_list = c->fr_list;
+        sp.fric = 1;
+        c->dp.feta = c->feta;
     }
     if (p.controller != ABM_CONTROLLER_REFERENCE && p.controller != ABM_CONTROLLER_LEARNED &&
         p.controller != ABM_CONTROLLER_PI)
@@ -655,6 +691,8 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     if (!two_d && (ncols < 21 || ncols > STAGING_COLS)) return fail(c, ABM_ERR_ARG, "cell arrays need 21..32 columns");
     if (!two_d && c->p.adhesion_mode != 0 && ncols < 22)
         return fail(c, ABM_ERR_ARG, "adhesion needs the gamma column (21)");
+    if (c->sp.fric && ncols <= c->eta_col)
+        return fail(c, ABM_ERR_ARG, "friction needs the cell-cell friction column (22 with adhesion, 21 without)");
     c->ncols = ncols;
     c->has_gamma = !two_d && (c->p.adhesion_mode != 0);
     if (n > 0)
@@ -663,6 +701,9 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
                              (size_t)n * sizeof(double), ncols, cudaMemcpyHostToDevice, c->st));
         if (two_d) launch_cells_from_colmajor_2d(c->staging, n, ncols, n, c->geom, c->vel, c->phys, c->st);
         else launch_cells_from_colmajor(c->staging, n, ncols, n, c->has_gamma, c->geom, c->vel, c->phys, c->st);
+        if (c->sp.fric)
+            CK(cudaMemcpyAsync(c->feta, c->staging + (size_t)c->eta_col * n, (size_t)n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->st));
     }
     k_set_n<<<1, 1, 0, c->st>>>(c->ctrl, n);
     CK(cudaGetLastError());
@@ -676,6 +717,15 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
         grows = cm[(size_t)col_growth * ld + i] != 0 || cm[(size_t)col_l * ld + i] > c->p.Ldiv;
     if (grows != c->div_enabled) drop_iteration_graphs(c);
     c->div_enabled = grows;
+    return ABM_OK;
+}
+
+// friction: the coefficient column of a column-major staging copy of n cells
+static int stage_eta_column(abm_ctx* c, const double* src, int n)
+{
+    if (c->sp.fric && c->ncols > c->eta_col && n > 0)
+        CK(cudaMemcpyAsync(c->staging + (size_t)c->eta_col * n, src, (size_t)n * sizeof(double),
+                           cudaMemcpyDeviceToDevice, c->st));
     return ABM_OK;
 }
 
@@ -693,6 +743,8 @@ int abm_download_cells(abm_ctx* c, double* cm, int ld)
     {
         if (c->dims == 2) launch_cells_to_colmajor_2d(c->geom, c->vel, c->phys, n, c->ncols, n, c->staging, c->st);
         else launch_cells_to_colmajor(c->geom, c->vel, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        int rc = stage_eta_column(c, c->feta, n);
+        if (rc) return rc;
         CK(cudaMemcpy2DAsync(cm, (size_t)ld * sizeof(double), c->staging, (size_t)n * sizeof(double),
                              (size_t)n * sizeof(double), c->ncols, cudaMemcpyDeviceToHost, c->st));
     }
@@ -718,7 +770,9 @@ int abm_set_frames(abm_ctx* c, double dt_write, int slots)
     {
         CK(cudaStreamSynchronize(c->st));
         cudaFree(c->snap_geom); cudaFree(c->snap_vel); cudaFree(c->snap_phys); cudaFree(c->frame_info);
+        cudaFree(c->snap_feta);
         c->snap_geom = nullptr; c->snap_vel = nullptr; c->snap_phys = nullptr; c->frame_info = nullptr;
+        c->snap_feta = nullptr;
         if (slots > 0)
         {
             const size_t m = (size_t)slots * c->cap;
@@ -726,6 +780,7 @@ int abm_set_frames(abm_ctx* c, double dt_write, int slots)
             CK(cudaMalloc(&c->snap_vel, m * sizeof(Vel)));
             CK(cudaMalloc(&c->snap_phys, m * sizeof(Phys)));
             CK(cudaMalloc(&c->frame_info, (size_t)slots * sizeof(FrameInfo)));
+            if (c->sp.fric) CK(cudaMalloc(&c->snap_feta, m * sizeof(double)));
         }
         c->frame_slots = slots;
         drop_iteration_graphs(c);          // the snapshot is a node of the iteration graph
@@ -773,6 +828,11 @@ int abm_download_frame(abm_ctx* c, int index, double* cm, int ld, int* n, double
         else
             launch_cells_to_colmajor(c->snap_geom + off, c->snap_vel + off, c->snap_phys + off, f.n, c->ncols, f.n,
                                      c->has_gamma, c->staging, c->st);
+        if (c->snap_feta)
+        {
+            rc = stage_eta_column(c, c->snap_feta + off, f.n);
+            if (rc) return rc;
+        }
         CK(cudaMemcpy2DAsync(cm, (size_t)ld * sizeof(double), c->staging, (size_t)f.n * sizeof(double),
                              (size_t)f.n * sizeof(double), c->ncols, cudaMemcpyDeviceToHost, c->st));
     }
@@ -898,8 +958,18 @@ static void enqueue_loop_pair_force(abm_ctx* c) { enqueue_pair_force(c, sum_in_a
 static PairGather loop_gather(abm_ctx* c)
 {
     const bool f32 = c->p.precision == ABM_PRECISION_MIXED && c->dims == 3;
-    PairGather pg = {sum_in_attempt(c) ? (f32 ? 3 : 2) : 0, c->row_ptr, c->lower_end, c->jbuf, c->fcc};
+    PairGather pg = {sum_in_attempt(c) ? (f32 ? 3 : 2) : 0, c->row_ptr, c->lower_end, c->jbuf, c->fcc,
+                     c->fbuf, c->fmask, c->ystage, c->cap};
     return pg;
+}
+
+// friction with a surface: the trial passes and decision checks that precede an attempt
+// of kind `kind` (no candidates without a surface)
+static void enqueue_friction_rounds(abm_ctx* c, int kind, PairGather pg, double eval_dt = 0.0, int eval_attempt = 0)
+{
+    if (!c->sp.fric || !c->fp.surface) return;
+    launch_friction_rounds(kind, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->k0buf,
+                           eval_dt, eval_attempt, c->cap, c->st, pg, c->pairs, c->fr_list, c->fmask, c->p.R);
 }
 
 
@@ -907,11 +977,16 @@ static void enqueue_attempts(abm_ctx* c)
 {
     cudaStream_t st = c->st;
     PairGather pg = loop_gather(c);
+    enqueue_friction_rounds(c, MODE_TRIAL, pg);
     launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
     for (int r = 0; r < c->p.max_tries_update_stepsize; ++r)
+    {
+        enqueue_friction_rounds(c, MODE_RETRY, pg);
         launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
+    }
+    enqueue_friction_rounds(c, MODE_FINAL, pg);
     launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                    c->k0buf, 0.0, 0, c->cap, st, 0, 0, pg, c->dims);
 }
@@ -920,7 +995,8 @@ static void enqueue_attempts(abm_ctx* c)
 static void enqueue_frame_snapshot(abm_ctx* c)
 {
     launch_frame_snapshot(c->geom, c->vel, c->phys, c->ctrl, c->snap_geom, c->snap_vel, c->snap_phys,
-                          c->frame_info, c->frame_slots, c->cap, c->st);
+                          c->frame_info, c->frame_slots, c->cap, c->st, c->sp.fric ? c->feta : nullptr,
+                          c->snap_feta);
 }
 
 static void enqueue_iteration(abm_ctx* c)
@@ -1049,7 +1125,7 @@ static void enqueue_basal_test(abm_ctx* c, unsigned long long cond, int use_cond
 static void enqueue_basal_compact(abm_ctx* c)
 {
     launch_basal_compact(c->geom, c->vel, c->phys, c->geom_c, c->vel_c, c->phys_c, c->ctrl, c->keep, c->keep_rank,
-                         c->cap, c->st);
+                         c->cap, c->st, c->sp.fric ? c->feta : nullptr, c->staging);
 }
 
 static void enqueue_switch_cells(abm_ctx* c)
@@ -1143,16 +1219,19 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
     PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
         enqueue_loop_pair_force(c);
+        enqueue_friction_rounds(c, MODE_TRIAL, pg);
         launch_attempt(MODE_TRIAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, h_retry, (retries ? 1 : 0) | (branch ? 2 : 0), pg, c->dims,
                        h_run);
     });
     if (rc) return rc;
     auto retry_attempt = [&](int use_cond) {
+        enqueue_friction_rounds(c, MODE_RETRY, pg);
         launch_attempt(MODE_RETRY, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c,
                        nullptr, c->k0buf, 0.0, 0, c->cap, c->st, h_retry, use_cond, pg, c->dims);
     };
     auto final_attempt = [&]() {
+        enqueue_friction_rounds(c, MODE_FINAL, pg);
         launch_attempt(MODE_FINAL, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, nullptr,
                        c->k0buf, 0.0, 0, c->cap, c->st, 0, 0, pg, c->dims);
     };
@@ -1395,14 +1474,18 @@ int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
     enqueue_pair_force(c, 1);
     k_clear_eval<<<1, 1, 0, c->st>>>(c->ctrl);
+    PairGather pg = {0, c->row_ptr, c->lower_end, c->jbuf, nullptr, c->fbuf, c->fmask, c->ystage, c->cap};
+    enqueue_friction_rounds(c, 3, pg, dt, attempt);
     launch_attempt(3, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->gen_tmp,
-                   c->k0buf, dt, attempt, c->cap, c->st, 0, 0, PairGather{0, 0, 0, 0, 0}, c->dims);
+                   c->k0buf, dt, attempt, c->cap, c->st, 0, 0, pg, c->dims);
     CK(cudaGetLastError());
     const int n = c->n_host;
     if (cells_out && n > 0)
     {
         if (c->dims == 2) launch_cells_to_colmajor_2d(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->staging, c->st);
         else launch_cells_to_colmajor(c->geom_c, c->vel_c, c->phys, n, c->ncols, n, c->has_gamma, c->staging, c->st);
+        rc = stage_eta_column(c, c->feta, n);
+        if (rc) return rc;
         CK(cudaMemcpyAsync(cells_out, c->staging, (size_t)n * c->ncols * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     }
     if (errors_out)

@@ -339,6 +339,7 @@ __global__ void k_div_commit(Geom* geom, Vel* vel, Phys* phys, const Ctrl* ctrl,
         if (dp.inherit && n + nd >= dp.n_start_switch) inherit_switch(dp, ctrl->iter, k, p1, p2);
         geom[i] = a; phys[i] = p1;
         geom[n + k] = b; phys[n + k] = p2; vel[n + k] = vm;
+        if (dp.feta) dp.feta[n + k] = dp.feta[i];
         parents[np + 2 * k] = parent_id;
         parents[np + 2 * k + 1] = parent_id;
     }

@@ -717,7 +717,7 @@ __device__ __forceinline__ double jkr_magnitude_variable(double dist, double gam
 // reference's j < i loop computes it): magnitude m along d, returned as
 // v = m d_hat with the body coordinates s (on i) and t (on j).  Cell i gains
 // (v, s v) in dE/dq and cell j gains (-v, -t v) (mechanics.hpp:1390-1659).
-struct PairOut { double vx, vy, vz, s, t, ovl; bool touch; };
+struct PairOut { double vx, vy, vz, s, t, ovl; bool touch; double dx, dy, dz, dist; };
 
 __device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& gj, const ForceParams& fp,
                                                    const double* td, const double* tr)
@@ -742,6 +742,7 @@ __device__ __forceinline__ PairOut pair_force_fp64(const Geom& gi, const Geom& g
     if (fp.adhesion && overlap > fp.max_overlap) m += fp.pf1 * pow15(overlap - fp.max_overlap);
     out.vx = m * ux; out.vy = m * uy; out.vz = m * uz;
     out.s = d.s; out.t = d.t; out.ovl = overlap; out.touch = true;
+    out.dx = d.dx; out.dy = d.dy; out.dz = d.dz; out.dist = dist;
     return out;
 }
 
@@ -1006,10 +1007,97 @@ __device__ __forceinline__ void zero_shares(double4* jbuf, int k, int r)
 // reference (all need overlap > 0).  Every share slot is written by exactly one
 // pair, so the order of the active list changes no result.  The last block
 // installs a new list and clears the drift.
+// mechanics.hpp:1031-1175 (cellCellFrictionForces, include_constraint = false) for one
+// touching pair (i, j), i = pr.x the larger index, from the pair's distance record: the
+// friction force on cell i is -eta sqrt(Req overlap) times the tangential part of the
+// relative velocity of the two contact points (dr + s dn of each cell's stored velocity),
+// eta the smaller of the two coefficients, its norm capped at
+// coulomb (4/3) E0 sqrt(Req) overlap^(3/2) when coulomb > 0.  A candidate contact
+// (surface present, |dz / d| < 1e-3) whose contact points both lie below 1.01 R is taken
+// in the xy-plane (distance, overlap and relative velocity without z).  Writes the force
+// for both decisions (planar only for a candidate) and the decision at these positions.
+__device__ __forceinline__ void friction_force(const X3 dv, double dist, bool planar, const double rv_in[3],
+                                               double eta, const ForceParams& fp, double f[3])
+{
+    const double Req = fp.R / 2;
+    X3 u;
+    double overlap;
+    double rv[3] = {rv_in[0], rv_in[1], rv_in[2]};
+    if (planar)
+    {
+        const double d2 = xnorm(x3(dv.x, dv.y, 0.0));
+        u = x3(dv.x / d2, dv.y / d2, 0.0);
+        overlap = 2 * fp.R - d2;
+        rv[2] = 0.0;
+    }
+    else
+    {
+        u = x3(dv.x / dist, dv.y / dist, dv.z / dist);
+        overlap = 2 * fp.R - dist;
+    }
+    const double dd = (rv[0] * u.x + rv[1] * u.y) + rv[2] * u.z;
+    const double c = -eta * sqrt(Req * overlap);
+    f[0] = c * (rv[0] - dd * u.x);
+    f[1] = c * (rv[1] - dd * u.y);
+    f[2] = c * (rv[2] - dd * u.z);
+    if (fp.coulomb_cc > 0)
+    {
+        const double fn = sqrt((f[0] * f[0] + f[1] * f[1]) + f[2] * f[2]);
+        const double max_norm = fp.coulomb_cc * (4. / 3.) * fp.E0 * sqrt(Req) * pow(overlap, 1.5);
+        if (fn > max_norm)
+        {
+            const double scale = max_norm / fn;
+            f[0] *= scale; f[1] *= scale; f[2] *= scale;
+        }
+    }
+}
+
+// the friction part of a touching pair's shares (FP64): v -= the force on i under the
+// decision at the attempt's positions; a candidate also records the change of v when the
+// decision flips, and is listed for the stage checks
+__device__ __forceinline__ void friction_shares(const Geom& gi, const Geom& gj, const int4& pr, const ForceParams& fp,
+                                                const Dist& d, double dist, double4& own, double4& other)
+{
+    const int i = pr.x, j = pr.y;
+    const X3 dv = x3(d.dx, d.dy, d.dz);
+    const Vel ui = fp.vel[i], uj = fp.vel[j];
+    const double eta = fmin(fp.feta[i], fp.feta[j]);
+    double rv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rv[c] = (ui.v[c] + d.s * ui.v[3 + c]) - (uj.v[c] + d.t * uj.v[3 + c]);
+    const bool cand = fp.surface && fabs(__ddiv_rn(d.dz, dist)) < 1e-3;
+    bool flat0 = false;
+    if (cand)
+    {
+        const double lim = 1.01 * fp.R;
+        flat0 = __dadd_rn(gi.rz, __dmul_rn(d.s, gi.nz)) < lim && __dadd_rn(gj.rz, __dmul_rn(d.t, gj.nz)) < lim;
+    }
+    double f[3];
+    friction_force(dv, dist, flat0, rv, eta, fp, f);
+    own.x -= f[0]; own.y -= f[1]; own.z -= f[2];
+    other.x -= f[0]; other.y -= f[1]; other.z -= f[2];
+    if (cand)
+    {
+        double g[3];
+        friction_force(dv, dist, !flat0, rv, eta, fp, g);
+        const double4 delta = make_double4(-(g[0] - f[0]), -(g[1] - f[1]), -(g[2] - f[2]), 0.0);
+        fp.fbuf[pr.z] = delta;
+        fp.fbuf[pr.w] = delta;
+        const int m = FR_CAND | (flat0 ? FR_D0 : 0);
+        fp.fmask[pr.z] = m;
+        fp.fmask[pr.w] = m;
+    }
+    else
+    {
+        fp.fmask[pr.z] = 0;
+        fp.fmask[pr.w] = 0;
+    }
+}
+
 template <bool MIXED, int DIM>
 __device__ __forceinline__ void pair_shares(const Geom& gi, const Geom& gj, const int4& pr, const ForceParams& fp,
                                             const double* __restrict__ td, const double* __restrict__ tr,
-                                            double4* __restrict__ jbuf, double& ovl_max)
+                                            double4* __restrict__ jbuf, double& ovl_max, bool* fr_cand = nullptr)
 {
     const int k = pr.z, r = pr.w;
     PairOut p;
@@ -1037,6 +1125,17 @@ __device__ __forceinline__ void pair_shares(const Geom& gi, const Geom& gj, cons
             own = make_double4(p.vx, p.vy, p.vz, p.s);
             other = make_double4(p.vx, p.vy, p.vz, p.t);
             ovl_max = fmax(ovl_max, p.ovl);
+            if (DIM == 3 && fp.fric)
+            {
+                const Dist d = {p.dx, p.dy, p.dz, p.s, p.t};
+                friction_shares(gi, gj, pr, fp, d, p.dist, own, other);
+                if (fr_cand) *fr_cand = (fp.fmask[k] & FR_CAND) != 0;
+            }
+        }
+        else if (DIM == 3 && fp.fric)
+        {
+            fp.fmask[k] = 0;
+            fp.fmask[r] = 0;
         }
         jbuf[k] = own;
         jbuf[r] = other;
@@ -1077,7 +1176,11 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
                 gi = load_geom(geom, pr.x);
                 gj = load_geom(geom, pr.y);
                 keep = may_touch(gi, gj, limit);
-                if (!keep) zero_shares<MIXED>(jbuf, pr.z, pr.w);
+                if (!keep)
+                {
+                    zero_shares<MIXED>(jbuf, pr.z, pr.w);
+                    if (!MIXED && DIM == 3 && fp.fric) { fp.fmask[pr.z] = 0; fp.fmask[pr.w] = 0; }
+                }
             }
             // warp-aggregated append of the active pairs
             const unsigned mask = __ballot_sync(0xffffffffu, keep);
@@ -1087,7 +1190,9 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
             if (keep)
             {
                 surv[pos + __popc(mask & ((1u << lane) - 1u))] = p;
-                pair_shares<MIXED, DIM>(gi, gj, pr, fp, td, tr, jbuf, ovl_max);
+                bool cand = false;
+                pair_shares<MIXED, DIM>(gi, gj, pr, fp, td, tr, jbuf, ovl_max, &cand);
+                if (cand) fp.fr_list[atomicAdd(&ctrl->fr_ncand_next, 1)] = p;
             }
         }
     }
@@ -1096,8 +1201,11 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
         const int m = ctrl->n_surv;
         for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride)
         {
-            const int4 pr = pairs[surv[q]];
-            pair_shares<MIXED, DIM>(load_geom(geom, pr.x), load_geom(geom, pr.y), pr, fp, td, tr, jbuf, ovl_max);
+            const int p = surv[q];
+            const int4 pr = pairs[p];
+            bool cand = false;
+            pair_shares<MIXED, DIM>(load_geom(geom, pr.x), load_geom(geom, pr.y), pr, fp, td, tr, jbuf, ovl_max, &cand);
+            if (cand) fp.fr_list[atomicAdd(&ctrl->fr_ncand_next, 1)] = p;
         }
     }
     if (fp.stats)
@@ -1123,6 +1231,13 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
             ctrl->n_surv_next = 0;
             ctrl->screen_valid = 1;
             ctrl->drift = 0.0;
+        }
+        if (fp.fric)
+        {
+            // the candidates of this pass; no stage has a changed decision yet
+            ctrl->fr_ncand = atomicAdd(&ctrl->fr_ncand_next, 0);
+            ctrl->fr_ncand_next = 0;
+            ctrl->fr_nflip = 0;
         }
         ctrl->surv_blocks = 0u;
     }
@@ -1572,6 +1687,27 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
     c->mode = MODE_FINAL;
 }
 
+// friction: the force of cell i at stage st, f0 minus the change of the dE/dq shares of its
+// candidate contacts whose planar decision at this stage differs from the one at y0; each
+// share enters as the pair sum does, (v, s v) from a lower entry, (-v, -t v) from a partner's
+__device__ __forceinline__ void friction_stage_force(const PairGather& pg, int i, int st, const double f0[6],
+                                                     double fs[6])
+{
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int le = pg.lower_end[i], r1 = pg.row_ptr[i + 1];
+    for (int e = pg.row_ptr[i]; e < r1; ++e)
+    {
+        if (!((pg.fmask[e] >> st) & 1)) continue;
+        const double4 dv = pg.fbuf[e];
+        const double w = pg.jbuf[e].w;
+        const double sg = e < le ? 1.0 : -1.0;
+        acc[0] += sg * dv.x; acc[1] += sg * dv.y; acc[2] += sg * dv.z;
+        acc[3] += sg * w * dv.x; acc[4] += sg * w * dv.y; acc[5] += sg * w * dv.z;
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fs[c] = f0[c] - acc[c];
+}
+
 // KIND: MODE_TRIAL / MODE_RETRY / MODE_FINAL inside the loop, 3 = API evaluation.
 // Without noise the stage-0 velocity k0 = f(y0) is the same for every attempt of an
 // iteration (y0 and the pair forces do not change), so the trial stores it in k0buf
@@ -1583,16 +1719,23 @@ __device__ void controller_finish(Ctrl* c, const StepParams& sp, int kind, doubl
 // that read y0 back from that copy.
 // use_cond bit 0: `cond` is the retry WHILE node's handle; bit 1: `cond_run` is the
 // handle of the IF node around the final attempt (0 after a committed proposal).
-template <int S, int KIND, bool NOISE, int DIM, bool F32>
+// V: 0 FP64; 1 mixed precision; 2 FP64 with cell-cell friction, whose candidate contacts
+// add, at each stage whose planar decision differs from the one at y0, the recorded change
+// of their shares; 3 the friction trial pass, which runs only the stages of the cells with
+// candidate contacts and records their stage states (z, n_z) for the decision check, with
+// no other effect.
+template <int S, int KIND, bool NOISE, int DIM, int V>
 __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
                                                  unsigned long long cond, int use_cond, PairGather pg,
                                                  unsigned long long cond_run)
 {
+    constexpr bool F32 = V == 1, FRIC = V >= 2, DRY = V == 3;
     __shared__ double sh_max[AT_T / 32], sh_drift[AT_T / 32];
     __shared__ double4 sh_stat[AT_T / 32];
     __shared__ bool last;
+    if (DRY && (!ctrl->fr_pending || (KIND != 3 && ctrl->halted))) return;
     if (KIND != 3 && ctrl->halted)
     {
         // a halted context takes no step: stop an enclosing WHILE node
@@ -1642,8 +1785,11 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     const bool commit = false;
     // a proposal (learned or PI) advances the state in place; the attempts after a failed
     // proposal start from the copy of y0 it kept
-    const bool in_place = (KIND == MODE_TRIAL) && sp.propose;
+    const bool in_place = !DRY && (KIND == MODE_TRIAL) && sp.propose;
     const bool from_backup = (KIND == MODE_RETRY || KIND == MODE_FINAL) && sp.propose;
+    if (DRY) store_k0 = false;
+    // friction: stages whose planar decisions differ from those at y0 somewhere
+    const bool flips = FRIC && ctrl->fr_nflip > 0;
 
     // the first attempt of an iteration sums the cell's pair shares (pg.fused); under
     // the reference controller the trial writes the total back for the rest, under the
@@ -1667,6 +1813,13 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
         const int t = g0 * 32 + lane_a;
         if (t >= n) continue;
         const int i = t < n_order ? sp.order[t] : t;
+        if (DRY)
+        {
+            // only cells with a candidate contact have stage states to report
+            bool any = false;
+            for (int e = pg.row_ptr[i]; e < pg.row_ptr[i + 1] && !any; ++e) any = (pg.fmask[e] & FR_CAND) != 0;
+            if (!any) continue;
+        }
         const Geom g = load_geom(from_backup ? geom_c : geom, i);
         const Vel* vprev = (from_backup ? vel_c : vel) + i;
         const double y0[6] = {g.rx, g.ry, g.rz, g.nx, g.ny, g.nz};
@@ -1691,7 +1844,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             cc = pg.fused == 3 ? sum_row_shares(pg.row_ptr, pg.lower_end, reinterpret_cast<const float4*>(pg.jbuf), i)
                : pg.fused == 2 ? sum_row_shares(pg.row_ptr, pg.lower_end, pg.jbuf, i)
                                : gather_pair_force(fcc, pg.row_ptr, pg.lower_end, pg.jbuf, i);
-            if (KIND == MODE_TRIAL && !sp.propose) pg.fcc_w[i] = cc;
+            if (KIND == MODE_TRIAL && !sp.propose && !DRY) pg.fcc_w[i] = cc;
         }
         else cc = (KIND == MODE_TRIAL) ? fcc[i] : load_gen6(fcc, i);
         double f0[6];
@@ -1734,7 +1887,23 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             }
             normalize_n(y);
             if constexpr (DIM == 2) velocity_2d(sp, y, l, eta0, eta1, cc, nz2, k[st]);
+            else if constexpr (FRIC)
+            {
+                if (DRY) pg.ystage[(size_t)st * pg.ystage_ld + i] = make_double2(y[2], y[5]);
+                if (flips)
+                {
+                    double fs[6];
+                    friction_stage_force(pg, i, st, f0, fs);
+                    cell_velocity_p<false>(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, fs, k[st]);
+                }
+                else cell_velocity_p<false>(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, f0, k[st]);
+            }
             else cell_velocity_p<F32>(sp, a2, y, l, g.h, eta0, eta1, sigma0, vprev, f0, k[st]);
+        }
+        if (DRY)
+        {
+            pg.ystage[i] = make_double2(y0[2], y0[5]);
+            continue;
         }
         double vf1[6], d1[6];
 #pragma unroll
@@ -1795,6 +1964,7 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
             }
         }
     }
+    if (DRY) return;
     if ((KIND == MODE_FINAL || in_place) && sp.stats_on)
     {
         // per-block partials of the step-size features, summed in block order later
@@ -1927,7 +2097,8 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
 // keeps running; the host downloads the slots when it writes the frames.
 __global__ void k_frame_snapshot(const Geom* __restrict__ geom, const Vel* __restrict__ vel,
                                  const Phys* __restrict__ phys, Ctrl* ctrl, Geom* snap_geom, Vel* snap_vel,
-                                 Phys* snap_phys, FrameInfo* info, int slots, int cap_cells)
+                                 Phys* snap_phys, FrameInfo* info, int slots, int cap_cells,
+                                 const double* __restrict__ feta, double* snap_feta)
 {
     __shared__ bool last;
     // frame_due changes only in the last block below, after every block has passed here
@@ -1939,6 +2110,7 @@ __global__ void k_frame_snapshot(const Geom* __restrict__ geom, const Vel* __res
         snap_geom[off + i] = geom[i];
         snap_vel[off + i] = vel[i];
         snap_phys[off + i] = phys[i];
+        if (feta) snap_feta[off + i] = feta[i];
     }
     __syncthreads();
     if (threadIdx.x == 0)
@@ -1964,11 +2136,11 @@ __global__ void k_frame_snapshot(const Geom* __restrict__ geom, const Vel* __res
 
 void launch_frame_snapshot(const Geom* geom, const Vel* vel, const Phys* phys, Ctrl* ctrl, Geom* snap_geom,
                            Vel* snap_vel, Phys* snap_phys, FrameInfo* info, int slots, int cap_cells,
-                           cudaStream_t st)
+                           cudaStream_t st, const double* feta, double* snap_feta)
 {
     const int blocks = max(min(cdiv(cap_cells, 256), 4 * 148), 1);
     k_frame_snapshot<<<blocks, 256, 0, st>>>(geom, vel, phys, ctrl, snap_geom, snap_vel, snap_phys, info, slots,
-                                             cap_cells);
+                                             cap_cells, feta, snap_feta);
 }
 
 // Attempt order (3-D): the cells whose velocity takes the full surface solve
@@ -2019,14 +2191,14 @@ static int one_wave_blocks(K kernel, int blocks_for_cap)
     return max(1, min(blocks_for_cap, occ * sms));
 }
 
-template <int S, bool NOISE, int DIM, bool F32>
+template <int S, bool NOISE, int DIM, int V>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
                              Gen6* k0buf, double eval_dt, int eval_attempt, cudaStream_t st,
                              unsigned long long cond, int use_cond, PairGather pg, unsigned long long cond_run)
 {
 #define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg, cond_run
-#define AT_LAUNCH(K) { auto kern = k_attempt<S, K, NOISE, DIM, F32>; \
+#define AT_LAUNCH(K) { auto kern = k_attempt<S, K, NOISE, DIM, V>; \
         kern<<<one_wave_blocks(kern, blocks), AT_T, 0, st>>>(AT_ARGS); }
     switch (kind)
     {
@@ -2049,9 +2221,10 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
     int blocks = attempt_blocks(cap_cells);
 #define AT_CALL(S, NZ, D, F) launch_attempt_s<S, NZ, D, F>(kind, blocks, geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, st, cond, use_cond, pg, cond_run)
 #define AT_CASE(S, D) case S: \
-        if (D == 3 && sp.mixed) { if (sp.noise_on) AT_CALL(S, true, D, D == 3); else AT_CALL(S, false, D, D == 3); } \
-        else if (sp.noise_on) AT_CALL(S, true, D, false); \
-        else AT_CALL(S, false, D, false); \
+        if (D == 3 && sp.mixed) { if (sp.noise_on) AT_CALL(S, true, D, (D == 3 ? 1 : 0)); else AT_CALL(S, false, D, (D == 3 ? 1 : 0)); } \
+        else if (D == 3 && sp.fric) { if (sp.noise_on) AT_CALL(S, true, D, (D == 3 ? 2 : 0)); else AT_CALL(S, false, D, (D == 3 ? 2 : 0)); } \
+        else if (sp.noise_on) AT_CALL(S, true, D, 0); \
+        else AT_CALL(S, false, D, 0); \
         break;
     if (dims == 2)
     {
@@ -2071,6 +2244,102 @@ void launch_attempt(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
     }
 #undef AT_CASE
 #undef AT_CALL
+}
+
+// Friction decision check over the candidate pairs of the last pair pass: the planar
+// decision of each stage from the two cells' stage states (the contact points
+// r + s n of both cells below 1.01 R, mechanics.hpp:1090-1110), compared with the one at
+// y0; a pair whose set of differing stages changed is updated in both entries.  The last
+// block schedules another trial pass when any pair changed.
+__global__ void k_fr_check(Ctrl* ctrl, const int4* __restrict__ pairs, const int* __restrict__ fr_list,
+                           const double4* __restrict__ jbuf, const double2* __restrict__ ystage, int ld, int S,
+                           int* fmask, double R)
+{
+    __shared__ bool last;
+    if (!ctrl->fr_pending) return;
+    const int m = ctrl->fr_ncand;
+    const double lim = 1.01 * R;
+    int changed = 0, nflip = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    {
+        const int4 pr = pairs[fr_list[q]];
+        const double s = jbuf[pr.z].w, t = jbuf[pr.w].w;
+        const int mk = fmask[pr.z];
+        const bool d0 = (mk & FR_D0) != 0;
+        int fl = 0;
+        for (int st = 1; st < S; ++st)
+        {
+            const double2 a = ystage[(size_t)st * ld + pr.x], b = ystage[(size_t)st * ld + pr.y];
+            const bool flat = __dadd_rn(a.x, __dmul_rn(s, a.y)) < lim && __dadd_rn(b.x, __dmul_rn(t, b.y)) < lim;
+            if (flat != d0) fl |= 1 << st;
+        }
+        if (fl != (mk & FR_FLIPS))
+        {
+            fmask[pr.z] = (mk & ~FR_FLIPS) | fl;
+            fmask[pr.w] = (fmask[pr.w] & ~FR_FLIPS) | fl;
+            changed = 1;
+        }
+        nflip += fl != 0;
+    }
+    changed = __syncthreads_or(changed);
+    if (nflip) atomicAdd(&ctrl->fr_nflip_next, nflip);
+    if (threadIdx.x == 0)
+    {
+        if (changed) atomicOr(&ctrl->fr_changed, 1);
+        __threadfence();
+        last = atomicAdd(&ctrl->fr_blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        __threadfence();
+        ctrl->fr_nflip = atomicAdd(&ctrl->fr_nflip_next, 0);
+        ctrl->fr_nflip_next = 0;
+        ctrl->fr_pending = atomicAdd(&ctrl->fr_changed, 0);
+        ctrl->fr_changed = 0;
+        ctrl->fr_blocks = 0u;
+    }
+}
+
+__global__ void k_fr_arm(Ctrl* ctrl) { ctrl->fr_pending = ctrl->fr_ncand > 0 && !ctrl->halted; }
+
+template <int S, int KIND, bool NOISE>
+static void launch_fr_rounds_s(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl, const StepParams& sp,
+                               Geom* geom_c, Vel* vel_c, Gen6* k0buf, double eval_dt, int eval_attempt, int blocks,
+                               cudaStream_t st, PairGather pg, const int4* pairs, const int* fr_list, int* fmask,
+                               double R, int check_blocks)
+{
+    auto kern = k_attempt<S, KIND, NOISE, 3, 3>;
+    const int b = one_wave_blocks(kern, blocks);
+    k_fr_arm<<<1, 1, 0, st>>>(ctrl);
+    for (int r = 1; r < S; ++r)
+    {
+        kern<<<b, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, nullptr, k0buf, eval_dt,
+                                 eval_attempt, 0ull, 0, pg, 0ull);
+        k_fr_check<<<check_blocks, 256, 0, st>>>(ctrl, pairs, fr_list, pg.jbuf, pg.ystage, pg.ystage_ld, S, fmask, R);
+    }
+}
+
+void launch_friction_rounds(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
+                            const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* k0buf, double eval_dt,
+                            int eval_attempt, int cap_cells, cudaStream_t st, PairGather pg, const int4* pairs,
+                            const int* fr_list, int* fmask, double R)
+{
+    const int blocks = attempt_blocks(cap_cells);
+    const int cb = 148 * 2;
+#define FR_K(S, K) { if (sp.noise_on) launch_fr_rounds_s<S, K, true>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, k0buf, eval_dt, eval_attempt, blocks, st, pg, pairs, fr_list, fmask, R, cb); \
+                     else launch_fr_rounds_s<S, K, false>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, k0buf, eval_dt, eval_attempt, blocks, st, pg, pairs, fr_list, fmask, R, cb); }
+#define FR_S(S) case S: \
+        switch (kind) { case MODE_TRIAL: FR_K(S, MODE_TRIAL) break; case MODE_RETRY: FR_K(S, MODE_RETRY) break; \
+                        case MODE_FINAL: FR_K(S, MODE_FINAL) break; default: FR_K(S, 3) break; } \
+        break;
+    switch (sp.s)
+    {
+        FR_S(2) FR_S(4) FR_S(6) FR_S(7)
+        default: break;
+    }
+#undef FR_S
+#undef FR_K
 }
 
 __global__ void k_velocities_2d(const Geom* __restrict__ geom, const Phys* __restrict__ phys,

@@ -89,6 +89,12 @@ struct Ctrl {
     double dt_write;                    // 0: no frames
     int frame_due, frames_taken;
     unsigned int frame_blocks;          // last-block counter of the snapshot kernel
+    // friction: candidate pairs of the last pair pass, pairs whose decisions change with the
+    // stage, and the trial loop's state (a trial pass is pending; a check changed a decision)
+    int fr_ncand, fr_ncand_next;
+    int fr_nflip, fr_nflip_next;
+    int fr_pending, fr_changed;
+    unsigned int fr_blocks;
     // basal-only compaction: cells kept by the last test, cells dropped so far
     int n_keep;
     long long basal_dropped;
@@ -122,6 +128,7 @@ struct StepParams {
     int pi;                     // 1: the PI rule makes the proposal after each accepted step
     int mixed;                  // 1: mixed precision (3-D): cells in surface contact take the FP32
                                 // contact branch of the velocity solve
+    int fric;                   // 1: cell-cell kinetic friction (3-D, FP64)
     int stats_on;               // accumulate the network's features (learned or logging)
     double near_div_length;     // 0.9 Ldiv
     double4* stat_part;         // per-block (max |v_r|, sum |v_r|^2, sum growth, near-division count)
@@ -150,7 +157,23 @@ struct ForceParams {
     double pf2d[3];
     double adh_strength, adh_mindist;
     const unsigned char* adhere;    // per CSR entry: to_adhere at the last rebuild
+    // cell-cell kinetic friction (cellCellFrictionForces, mechanics.hpp:1031-1175), FP64, 3-D
+    int fric;
+    int surface;                    // a surface is present (the planar-contact rule applies)
+    double coulomb_cc;              // Coulomb cap coefficient (not positive: no cap)
+    const Vel* vel;                 // stored velocities of the cells (dr, dn)
+    const double* feta;             // friction coefficient of each cell
+    double4* fbuf;                  // per CSR entry: share change when the contact is planar
+    int* fmask;                     // per CSR entry: FR_* bits
+    int* fr_list;                   // pairs with a planar-contact candidate, this pass
 };
+
+// Friction: a contact with |dz / d| < 1e-3 whose two contact points lie below 1.01 R is taken
+// in the xy-plane (mechanics.hpp:1090-1110).  The positions enter only through that test, so
+// an attempt's pair forces are fixed but for those candidate pairs, whose planar decision can
+// change from stage to stage.  Per CSR entry: FR_CAND, FR_D0 = the decision at y0, and bits
+// 0-7 = the stages whose decision differs from FR_D0.
+const int FR_CAND = 1 << 16, FR_D0 = 1 << 17, FR_FLIPS = 0xFF;
 
 struct BuildParams {
     double threshold;           // neighbor_threshold
@@ -169,6 +192,12 @@ struct PairGather {
     const int* lower_end;
     const double4* jbuf;
     Gen6* fcc_w;
+    // friction: the planar-contact corrections of each stage, and the stage states of the
+    // cells with candidate contacts (z and n_z per stage, written by the trial passes)
+    const double4* fbuf;
+    const int* fmask;
+    double2* ystage;
+    int ystage_ld;
 };
 
 // ---- launch wrappers (abm_kernels.cu) ----
@@ -247,7 +276,7 @@ struct FrameInfo {
 // copies the cells into ring slot frames_taken % slots when a frame is due
 void launch_frame_snapshot(const Geom* geom, const Vel* vel, const Phys* phys, Ctrl* ctrl, Geom* snap_geom,
                            Vel* snap_vel, Phys* snap_phys, FrameInfo* info, int slots, int cap_cells,
-                           cudaStream_t st);
+                           cudaStream_t st, const double* feta = nullptr, double* snap_feta = nullptr);
 void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int* flag, int* pos,
                           int* block_sums, int* order, int cap_cells, cudaStream_t st);
 void launch_velocities(const Geom* geom, const Vel* vel, const Phys* phys, const Gen6* fcc,
@@ -283,6 +312,7 @@ struct DivideParams {
     double gmean[2], gstd[2];
     int inherit, n_start_switch;
     double rates[4];
+    double* feta;               // friction coefficient of each cell (daughters inherit it), or null
 };
 void launch_div_count(const Phys* phys, Ctrl* ctrl, const DivideParams& dp, int* flags,
                       unsigned long long cond, int use_cond, cudaStream_t st);
@@ -336,7 +366,16 @@ void launch_basal_flags(const Geom* geom, const Ctrl* ctrl, const SwitchParams& 
 void launch_basal_decide(Ctrl* ctrl, const int* keep, const int* rank, unsigned long long cond, int use_cond,
                          cudaStream_t st);
 void launch_basal_compact(Geom* geom, Vel* vel, Phys* phys, Geom* geom_tmp, Vel* vel_tmp, Phys* phys_tmp,
-                          Ctrl* ctrl, const int* keep, const int* rank, int cap_cells, cudaStream_t st);
+                          Ctrl* ctrl, const int* keep, const int* rank, int cap_cells, cudaStream_t st,
+                          double* feta = nullptr, double* feta_tmp = nullptr);
 void launch_periodic_rebuild_cond(const Ctrl* ctrl, int every, unsigned long long cond, cudaStream_t st);
+
+// friction (abm_kernels.cu): before an attempt, trial passes that run the stages of the cells
+// with candidate contacts and checks that recompute the candidates' planar decisions from
+// the stage states, until the decisions agree with the states (at most stages - 1 rounds)
+void launch_friction_rounds(int kind, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc, Ctrl* ctrl,
+                            const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* k0buf, double eval_dt,
+                            int eval_attempt, int cap_cells, cudaStream_t st, PairGather pg, const int4* pairs,
+                            const int* fr_list, int* fmask, double R);
 
 }   // namespace abm

@@ -176,7 +176,8 @@ __global__ void k_basal_decide(Ctrl* ctrl, const int* keep, const int* rank, uns
 }
 
 __global__ void k_basal_scatter(const Geom* geom, const Vel* vel, const Phys* phys, Geom* geom_tmp, Vel* vel_tmp,
-                                Phys* phys_tmp, const Ctrl* ctrl, const int* keep, const int* rank)
+                                Phys* phys_tmp, const Ctrl* ctrl, const int* keep, const int* rank,
+                                const double* feta, double* feta_tmp)
 {
     const int n = ctrl->n;
     if (ctrl->n_keep >= n) return;
@@ -185,17 +186,19 @@ __global__ void k_basal_scatter(const Geom* geom, const Vel* vel, const Phys* ph
         {
             const int r = rank[i];
             geom_tmp[r] = geom[i]; vel_tmp[r] = vel[i]; phys_tmp[r] = phys[i];
+            if (feta) feta_tmp[r] = feta[i];
         }
 }
 
 __global__ void k_basal_gather(Geom* geom, Vel* vel, Phys* phys, const Geom* geom_tmp, const Vel* vel_tmp,
-                               const Phys* phys_tmp, const Ctrl* ctrl)
+                               const Phys* phys_tmp, const Ctrl* ctrl, double* feta, const double* feta_tmp)
 {
     const int m = ctrl->n_keep;
     if (m >= ctrl->n) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
     {
         geom[i] = geom_tmp[i]; vel[i] = vel_tmp[i]; phys[i] = phys_tmp[i];
+        if (feta) feta[i] = feta_tmp[i];
     }
 }
 
@@ -244,11 +247,13 @@ void launch_basal_decide(Ctrl* ctrl, const int* keep, const int* rank, unsigned 
 }
 
 void launch_basal_compact(Geom* geom, Vel* vel, Phys* phys, Geom* geom_tmp, Vel* vel_tmp, Phys* phys_tmp,
-                          Ctrl* ctrl, const int* keep, const int* rank, int cap_cells, cudaStream_t st)
+                          Ctrl* ctrl, const int* keep, const int* rank, int cap_cells, cudaStream_t st,
+                          double* feta, double* feta_tmp)
 {
     const int b = sw_blocks(cap_cells);
-    k_basal_scatter<<<b, SW_T, 0, st>>>(geom, vel, phys, geom_tmp, vel_tmp, phys_tmp, ctrl, keep, rank);
-    k_basal_gather<<<b, SW_T, 0, st>>>(geom, vel, phys, geom_tmp, vel_tmp, phys_tmp, ctrl);
+    k_basal_scatter<<<b, SW_T, 0, st>>>(geom, vel, phys, geom_tmp, vel_tmp, phys_tmp, ctrl, keep, rank, feta,
+                                        feta_tmp);
+    k_basal_gather<<<b, SW_T, 0, st>>>(geom, vel, phys, geom_tmp, vel_tmp, phys_tmp, ctrl, feta, feta_tmp);
     k_basal_commit<<<1, 1, 0, st>>>(ctrl);
 }
 

@@ -117,6 +117,12 @@ typedef struct abm_params {
     /* where each cell's pair shares are summed: 1 = inside the first RK attempt,
      * 2 = a separate light kernel before it (0 = 1, the faster on B200) */
     int pair_sum;
+    /* cell-cell kinetic friction (3-D, FP64): 0 = NONE, 1 = KINETIC (mechanics.hpp:61-65,
+     * 1031-1175), the coefficient of each cell in column 22 with adhesion, 21 without
+     * (simulation.hpp:1184-1186); its norm capped at cell_cell_coulomb_coeff (4/3) E0
+     * sqrt(R/2) overlap^(3/2) when that coefficient is positive (runSimulation's default 1) */
+    int friction_mode;
+    double cell_cell_coulomb_coeff;
 } abm_params;
 
 typedef struct abm_stats {

@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libabm_b200.so")
 ABM_OK = 0
 ERRORS = {-1: "ABM_ERR_ARG", -2: "ABM_ERR_CUDA", -3: "ABM_ERR_CAPACITY", -4: "ABM_ERR_NAN",
           -5: "ABM_ERR_STATE"}
-HEUN_EULER, BOGACKI_SHAMPINE, RUNGE_KUTTA_FEHLBERG, DORMAND_PRINCE = 1, 2, 3, 4
+VELOCITY_VERLET, HEUN_EULER, BOGACKI_SHAMPINE, RUNGE_KUTTA_FEHLBERG, DORMAND_PRINCE = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # Column indices of the 3-D cell array (ABM-3d/ABM-3d-cpp/include/indices.hpp:17-47)
@@ -64,6 +64,7 @@ class AbmParams(ctypes.Structure):
         ("pair_tile", ctypes.c_int), ("pair_blocks_per_sm", ctypes.c_int), ("pair_skin", ctypes.c_double),
         ("pair_sum", ctypes.c_int),
         ("friction_mode", ctypes.c_int), ("cell_cell_coulomb_coeff", ctypes.c_double),
+        ("M0", ctypes.c_double),
     ]
 
 
@@ -105,6 +106,7 @@ DEFAULTS = dict(
     cap_neighbors_per_cell=0, pair_lanes=8, use_graphs=1, controller=0, stepsize_log_capacity=0,
     dims=3, sigma0=100.0, adhesion_strength=0.0, adhesion_mindist=0.0, max_noise=0.0,
     pair_tile=0, pair_blocks_per_sm=0, pair_skin=0.0, pair_sum=0, friction_mode=0, cell_cell_coulomb_coeff=1.0,
+    M0=0.0,
 )
 
 # The 2-D driver (ABM-2d/ABM-2d-cpp/include/simulation.hpp:163-237): Bogacki-Shampine 3(2),

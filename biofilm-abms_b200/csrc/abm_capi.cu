@@ -74,6 +74,11 @@ struct abm_ctx {
     double2* ystage = nullptr;
     double* snap_feta = nullptr;
     int eta_col = 21;
+    // velocity Verlet (integration mode 0): JKR parts of the pair shares, half-step
+    // angular velocities, the cell density
+    bool verlet = false;
+    double4 *pbuf = nullptr, *whalf = nullptr;
+    double rho = 0.0;
     // phenotype switching, ramps, local viscosity, basal-only compaction (abm_switch.cu)
     SwitchParams sw;
     bool post_on = false;            // the post-step kernels run after each accepted step
@@ -198,7 +203,8 @@ static void free_all(abm_ctx* c)
                     c->mothers, c->div_check, c->div_sat, c->div_ok, c->parents_dev, c->d1, c->d2, c->dlen,
                     c->dgrowth, c->mlp_w, c->log_buf, c->adhere, c->stat_part, c->order, c->order_flag,
                     c->order_pos, c->snap_geom, c->snap_vel, c->snap_phys, c->frame_info, c->phys_c, c->keep,
-                    c->keep_rank, c->feta, c->fbuf, c->fmask, c->fr_list, c->ystage, c->snap_feta};
+                    c->keep_rank, c->feta, c->fbuf, c->fmask, c->fr_list, c->ystage, c->snap_feta, c->pbuf,
+                    c->whalf};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -290,8 +296,10 @@ int abm_create(const abm_params* q, abm_ctx** out)
         *out = c;
         return ABM_ERR_ARG;
     }
-    bool ok;
-    fill_tableau(c->sp, p.integration_mode, ok);
+    bool ok = true;
+    c->verlet = p.integration_mode == ABM_VELOCITY_VERLET;
+    if (c->verlet) { c->sp.s = 0; c->sp.inv_q1 = 0.0; }
+    else fill_tableau(c->sp, p.integration_mode, ok);
     if (!ok) { c->err = "unsupported integration_mode"; *out = c; return ABM_ERR_ARG; }
     if (p.pair_lanes == 0) p.pair_lanes = 8;
     if (p.pair_lanes != 4 && p.pair_lanes != 8 && p.pair_lanes != 16 && p.pair_lanes != 32)
@@ -423,6 +431,18 @@ int abm_create(const abm_params* q, abm_ctx** out)
         CK(cudaMalloc(&c->adhere, cap * c->cap_nbr));
         CK(cudaMemset(c->adhere, 0, cap * c->cap_nbr));
         fp.adhere = c->adhere;
+    }
+    // velocity Verlet (simulation.hpp:1279-1290, 1786-1798)
+    if (c->verlet)
+    {
+        if (c->dims != 3) return fail(c, ABM_ERR_ARG, "velocity Verlet belongs to the 3-D model");
+        if (p.precision != ABM_PRECISION_FP64) return fail(c, ABM_ERR_ARG, "velocity Verlet runs in FP64");
+        if (p.controller != ABM_CONTROLLER_REFERENCE)
+            return fail(c, ABM_ERR_ARG, "velocity Verlet takes a fixed step (reference controller)");
+        if (!(p.M0 > 0)) return fail(c, ABM_ERR_ARG, "Initial cell mass must be defined when using velocity Verlet");
+        c->rho = p.M0 / (M_PI * ((4. / 3.) * std::pow(p.R, 3) + p.R * p.R * p.L0));
+        CK(cudaMalloc(&c->pbuf, cap * c->cap_nbr * sizeof(double4)));
+        CK(cudaMalloc(&c->whalf, cap * sizeof(double4)));
     }
     // cell-cell kinetic friction (mechanics.hpp:1031-1175, 1339-1346)
     if (p.friction_mode != 0 && p.friction_mode != 1) return fail(c, ABM_ERR_ARG, "friction_mode must be 0 or 1");
@@ -694,7 +714,8 @@ int abm_upload_cells(abm_ctx* c, const double* cm, int n, int ncols, int ld)
     if (c->sp.fric && ncols <= c->eta_col)
         return fail(c, ABM_ERR_ARG, "friction needs the cell-cell friction column (22 with adhesion, 21 without)");
     c->ncols = ncols;
-    c->has_gamma = !two_d && (c->p.adhesion_mode != 0);
+    // the gamma column travels with the cells when present (used with adhesion only)
+    c->has_gamma = !two_d && ncols > 21;
     if (n > 0)
     {
         CK(cudaMemcpy2DAsync(c->staging, (size_t)n * sizeof(double), cm, (size_t)ld * sizeof(double),
@@ -967,11 +988,19 @@ static PairGather loop_gather(abm_ctx* c)
 // of kind `kind` (no candidates without a surface)
 static void enqueue_friction_rounds(abm_ctx* c, int kind, PairGather pg, double eval_dt = 0.0, int eval_attempt = 0)
 {
-    if (!c->sp.fric || !c->fp.surface) return;
+    if (!c->sp.fric || !c->fp.surface || c->verlet) return;
     launch_friction_rounds(kind, c->geom, c->vel, c->phys, c->fcc, c->ctrl, c->sp, c->geom_c, c->vel_c, c->k0buf,
                            eval_dt, eval_attempt, c->cap, c->st, pg, c->pairs, c->fr_list, c->fmask, c->p.R);
 }
 
+
+// one velocity-Verlet step (integration mode 0) at the context's dt, growth included
+static void enqueue_verlet_step(abm_ctx* c)
+{
+    launch_verlet_step(c->geom, c->vel, c->phys, c->geom_c, c->vel_c, c->whalf, c->ctrl, c->sp, c->fp,
+                       c->jkr_delta, c->jkr_radius, c->pairs, c->row_ptr, c->lower_end, c->jbuf, c->pbuf, c->rho,
+                       c->cap, c->cap * c->cap_nbr / 2, c->st);
+}
 
 static void enqueue_attempts(abm_ctx* c)
 {
@@ -1001,8 +1030,12 @@ static void enqueue_frame_snapshot(abm_ctx* c)
 
 static void enqueue_iteration(abm_ctx* c)
 {
-    enqueue_loop_pair_force(c);
-    enqueue_attempts(c);
+    if (c->verlet) enqueue_verlet_step(c);
+    else
+    {
+        enqueue_loop_pair_force(c);
+        enqueue_attempts(c);
+    }
     if (c->frame_slots > 0) enqueue_frame_snapshot(c);
 }
 
@@ -1215,6 +1248,18 @@ static int append_iteration(abm_ctx* c, cudaGraph_t G, std::vector<cudaGraphNode
         if (rc) return rc;
         rc = capture_division_body(c, body);
         if (rc) return rc;
+    }
+    if (c->verlet)
+    {
+        rc = capture_into(c, G, deps, [&]() { enqueue_verlet_step(c); });
+        if (rc) return rc;
+        if (c->post_on)
+        {
+            rc = append_post_step(c, G, deps);
+            if (rc) return rc;
+        }
+        if (c->frame_slots > 0) return capture_into(c, G, deps, [&]() { enqueue_frame_snapshot(c); });
+        return ABM_OK;
     }
     PairGather pg = loop_gather(c);
     rc = capture_into(c, G, deps, [&]() {
@@ -1469,6 +1514,7 @@ int abm_rk_attempt(abm_ctx* c, double dt, int attempt, double* cells_out, double
                    double* max_scaled_error)
 {
     if (!c || !(dt > 0)) return ABM_ERR_ARG;
+    if (c->verlet) return fail(c, ABM_ERR_STATE, "the context integrates with velocity Verlet (no RK attempt)");
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
@@ -1614,8 +1660,12 @@ int abm_iterate(abm_ctx* c, int n_iters, int n_cells_stop, abm_stats* stats)
             if (c->div_enabled) { rc = divide_now(c, true, nullptr); if (rc) return rc; }
             if (c->post_on)
             {
-                enqueue_loop_pair_force(c);
-                enqueue_attempts(c);
+                if (c->verlet) enqueue_verlet_step(c);
+                else
+                {
+                    enqueue_loop_pair_force(c);
+                    enqueue_attempts(c);
+                }
                 rc = post_step_direct(c);
                 if (rc) return rc;
                 if (c->frame_slots > 0) enqueue_frame_snapshot(c);
@@ -1641,6 +1691,7 @@ int abm_profile_iterations(abm_ctx* c, int n_iters, abm_profile* prof)
 {
     if (!c || !prof || n_iters < 0) return ABM_ERR_ARG;
     if (c->post_on) return fail(c, ABM_ERR_STATE, "the profile covers the loop without switching or basal-only compaction");
+    if (c->verlet) return fail(c, ABM_ERR_STATE, "the profile covers the Runge-Kutta loop");
     int rc = ready_for_forces(c);
     if (rc) return rc;
     if (c->sp.network && !c->mlp_loaded)

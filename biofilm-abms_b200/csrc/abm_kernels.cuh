@@ -370,6 +370,12 @@ void launch_basal_compact(Geom* geom, Vel* vel, Phys* phys, Geom* geom_tmp, Vel*
                           double* feta = nullptr, double* feta_tmp = nullptr);
 void launch_periodic_rebuild_cond(const Ctrl* ctrl, int every, unsigned long long cond, cudaStream_t st);
 
+// velocity Verlet (abm_verlet.cu): one step of integration mode 0 at ctrl->dt, growth included
+void launch_verlet_step(Geom* geom, Vel* vel, Phys* phys, Geom* geom_c, Vel* vel_c, double4* whalf, Ctrl* ctrl,
+                        const StepParams& sp, const ForceParams& fp, const double* td, const double* tr,
+                        const int4* pairs, const int* row_ptr, const int* lower_end, double4* jbuf, double4* pbuf,
+                        double rho, int cap_cells, int cap_pairs, cudaStream_t st);
+
 // friction (abm_kernels.cu): before an attempt, trial passes that run the stages of the cells
 // with candidate contacts and checks that recompute the candidates' planar decisions from
 // the stage states, until the decisions agree with the states (at most stages - 1 rounds)

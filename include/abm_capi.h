@@ -31,6 +31,7 @@ extern "C" {
 #define ABM_ERR_STATE -5        /* call order violated (e.g. iterate before upload) */
 
 /* Integration modes, as IntegrationMode in simulation.hpp:45-55 */
+#define ABM_VELOCITY_VERLET 0   /* 3-D, FP64, reference controller; needs abm_params.M0 > 0 */
 #define ABM_HEUN_EULER 1
 #define ABM_BOGACKI_SHAMPINE 2
 #define ABM_RUNGE_KUTTA_FEHLBERG 3
@@ -74,7 +75,7 @@ typedef struct abm_params {
     double neighbor_threshold;   /* abmConstAdhesion.cpp:53: 0.5 (2R + Ldiv) */
     double nz_threshold;
     int adhesion_mode;           /* 0 = NONE, 1 = JKR_ISOTROPIC with a fixed-gamma radius table */
-    int integration_mode;        /* ABM_HEUN_EULER ... ABM_DORMAND_PRINCE */
+    int integration_mode;        /* ABM_VELOCITY_VERLET, ABM_HEUN_EULER ... ABM_DORMAND_PRINCE */
     double max_stepsize, min_stepsize;
     double max_error_allowed, min_error;
     int max_tries_update_stepsize;
@@ -123,6 +124,9 @@ typedef struct abm_params {
      * sqrt(R/2) overlap^(3/2) when that coefficient is positive (runSimulation's default 1) */
     int friction_mode;
     double cell_cell_coulomb_coeff;
+    /* integration_mode ABM_VELOCITY_VERLET (0): the cell mass at length L0, which sets the
+     * density of every cell (simulation.hpp:1279-1290); must be positive in that mode */
+    double M0;
 } abm_params;
 
 typedef struct abm_stats {

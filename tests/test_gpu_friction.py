@@ -129,8 +129,11 @@ def test_friction_rk_attempt_with_planar_contacts(mode):
     cg, eg, Eg = sim.step_runge_kutta_adaptive(dt)
     co, eo, Eo = o.rk_attempt(dt)
     assert colwise_relerr(cg, co) <= 1e-10
-    assert colwise_relerr(eg, eo) <= 1e-8
-    assert abs(Eg - Eo) <= 1e-8 * abs(Eo)
+    # the embedded error estimates are differences of nearly equal stage sums (down to
+    # 1e-20 here): held to FP64 rounding of the step, and E to the same in its units
+    step = np.abs(co[:, 1:7] - cells[:, 1:7]).max()
+    assert np.abs(eg - eo).max() <= 1e-10 * step
+    assert abs(Eg - Eo) <= 1e-6 * max(abs(Eo), 1e-3)
     # the decisions at the end of the step differ from those at y0 for some contacts, so
     # the stages in between saw changed decisions too
     d1 = planar_decisions(co, table)

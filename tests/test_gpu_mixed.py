@@ -15,10 +15,11 @@ Bars, stated here:
     max_i |y1_mixed - y1_oracle| / (tol (1 + |y0|)) <= 0.05, i.e. the FP32 rounding
     moves the step by at most 5 % of what the error test accepts (measured: 0.011 at
     dt = 1e-6 h on the 100k state, 0.02 at 1e-5 h on a 3000-cell patch); and the scaled error
-    norm E agrees to 1e-3 relative above a floor of 1e-4: the FP32 stage velocities of
-    cells in surface contact put rounding noise of that size into the embedded error,
-    which matters only where E itself is that small (high-order tableaux at small dt),
-    far from the accept threshold E = 1.
+    norm E agrees to 1e-3 relative above a floor of 1e-3: the FP32 stage velocities of
+    cells in surface contact put rounding noise into the embedded error, about
+    eps_32 |k| dt / (tol (1 + |y|)) (measured up to 1.8e-4 at dt = 1e-5 h, where the FP64
+    oracle's E is 6e-12), which matters only where E itself is that small (high-order
+    tableaux at small dt), three orders below the accept threshold E = 1.
 """
 import numpy as np
 import pytest
@@ -35,7 +36,7 @@ TOL = 1e-8
 RTOL_FORCE = 1e-4
 RK_UNITS_MAX = 0.05
 E_RTOL = 1e-3
-E_FLOOR = 1e-4
+E_FLOOR = 1e-3
 
 
 def rk_units(c_mixed, c_oracle, cells, tol=TOL):

@@ -1578,13 +1578,16 @@ __device__ __forceinline__ void friction_stage_force(const PairGather& pg, int i
 // that read y0 back from that copy.
 // use_cond bit 0: `cond` is the retry WHILE node's handle; bit 1: `cond_run` is the
 // handle of the IF node around the final attempt (0 after a committed proposal).
+// Launch bounds: six blocks per SM (85 registers) for the 2- and 4-stage tableaux, the
+// fastest measured for the 100k-cell step (three for their friction trial pass, which
+// would spill at six); no bound for the 6- and 7-stage ones, which spill below ~130.
 // V: 0 FP64; 1 mixed precision; 2 FP64 with cell-cell friction, whose candidate contacts
 // add, at each stage whose planar decision differs from the one at y0, the recorded change
 // of their shares; 3 the friction trial pass, which runs only the stages of the cells with
 // candidate contacts and records their stage states (z, n_z) for the decision check, with
 // no other effect.
 template <int S, int KIND, bool NOISE, int DIM, int V>
-__global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
+__global__ void __launch_bounds__(AT_T, (S <= 4 ? (V == 3 ? 3 : 6) : 1)) k_attempt(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                                                  Ctrl* ctrl, StepParams sp, Geom* geom_c, Vel* vel_c,
                                                  Gen6* err_out, Gen6* k0buf, double eval_dt, int eval_attempt,
                                                  unsigned long long cond, int use_cond, PairGather pg,
@@ -1660,17 +1663,11 @@ __global__ void __launch_bounds__(AT_T) k_attempt(Geom* geom, Vel* vel, Phys* ph
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
     double local_drift = 0.0;
-    // The grid holds one wave of resident blocks and strides over the attempt order in
-    // groups of 32 consecutive positions, one group per warp: group g goes to block
-    // g mod gridDim.x, so the full-surface cells at the head of the order spread over all
-    // blocks, while each warp still runs cells of one class.  Position t of the order is
-    // cell order[t] (cells appended after the order was made, in index order).
-    const int wpb = AT_T / 32, lane_a = threadIdx.x & 31, warp_b = threadIdx.x >> 5;
-    const int groups_per_pass = gridDim.x * wpb;
-    for (int g0 = warp_b * gridDim.x + blockIdx.x; g0 * 32 < n; g0 += groups_per_pass)
+    // one cell per thread: the grid covers the capacity (attempt_blocks), so each thread
+    // runs at most one pass; thread t takes the t-th cell of the attempt order (cells
+    // appended after the order was made, in index order)
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     {
-        const int t = g0 * 32 + lane_a;
-        if (t >= n) continue;
         const int i = t < n_order ? sp.order[t] : t;
         if (DRY)
         {
@@ -2039,17 +2036,6 @@ void launch_attempt_order(const Geom* geom, Ctrl* ctrl, const MechParams& P, int
     k_attempt_order<<<blocks, 256, 0, st>>>(ctrl, flag, pos, order);
 }
 
-// One wave: at most as many blocks as are resident at once (the kernel strides over the
-// cells), and no more than the capacity needs.
-template <class K>
-static int one_wave_blocks(K kernel, int blocks_for_cap)
-{
-    int dev = 0, sms = 148, occ = 1;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, AT_T, 0) != cudaSuccess || occ < 1) occ = 1;
-    return max(1, min(blocks_for_cap, occ * sms));
-}
-
 template <int S, bool NOISE, int DIM, int V>
 static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc,
                              Ctrl* ctrl, const StepParams& sp, Geom* geom_c, Vel* vel_c, Gen6* err_out,
@@ -2057,8 +2043,7 @@ static void launch_attempt_s(int kind, int blocks, Geom* geom, Vel* vel, Phys* p
                              unsigned long long cond, int use_cond, PairGather pg, unsigned long long cond_run)
 {
 #define AT_ARGS geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, err_out, k0buf, eval_dt, eval_attempt, cond, use_cond, pg, cond_run
-#define AT_LAUNCH(K) { auto kern = k_attempt<S, K, NOISE, DIM, V>; \
-        kern<<<one_wave_blocks(kern, blocks), AT_T, 0, st>>>(AT_ARGS); }
+#define AT_LAUNCH(K) k_attempt<S, K, NOISE, DIM, V><<<blocks, AT_T, 0, st>>>(AT_ARGS);
     switch (kind)
     {
         case MODE_TRIAL: AT_LAUNCH(MODE_TRIAL) break;
@@ -2168,12 +2153,10 @@ static void launch_fr_rounds_s(Geom* geom, Vel* vel, Phys* phys, const Gen6* fcc
                                cudaStream_t st, PairGather pg, const int4* pairs, const int* fr_list, int* fmask,
                                double R, int check_blocks)
 {
-    auto kern = k_attempt<S, KIND, NOISE, 3, 3>;
-    const int b = one_wave_blocks(kern, blocks);
     k_fr_arm<<<1, 1, 0, st>>>(ctrl);
     for (int r = 1; r < S; ++r)
     {
-        kern<<<b, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, nullptr, k0buf, eval_dt,
+        k_attempt<S, KIND, NOISE, 3, 3><<<blocks, AT_T, 0, st>>>(geom, vel, phys, fcc, ctrl, sp, geom_c, vel_c, nullptr, k0buf, eval_dt,
                                  eval_attempt, 0ull, 0, pg, 0ull);
         k_fr_check<<<check_blocks, 256, 0, st>>>(ctrl, pairs, fr_list, pg.jbuf, pg.ystage, pg.ystage_ld, S, fmask, R);
     }

@@ -9,8 +9,8 @@ statistical.  Bars:
     compaction: bit for bit;
   * local viscosity eta0: bit for bit (integer contact counts, correctly rounded
     arithmetic) from identical inputs;
-  * ramped attributes and gamma: 1e-12 relative (they advance by rate x dt, and dt is set
-    by the error norm, which the device sums in another order);
+  * ramped attributes and gamma: 1e-12 relative, dt and the clock 1e-10 (the ramps advance
+    by rate x dt, and dt is set by the error norm, which the device sums in another order);
   * the other columns: 1e-9 normwise, the loop tests' bar.
 """
 import numpy as np
@@ -95,7 +95,7 @@ def test_markov_switching_and_ramps_follow_the_oracle(graphs):
         prev = co[:, 20].copy()
         t, dt, i = sim.clock()
         to, dto, io = o.clock()
-        assert i == io and abs(dt - dto) <= 1e-12 * dto and abs(t - to) <= 1e-9 * to
+        assert i == io and abs(dt - dto) <= 1e-10 * dto and abs(t - to) <= 1e-10 * to
     assert switched > len(cells)                     # many switches, both ways
     g1 = cg[:, 20] == 1
     assert 0 < g1.sum() < len(cg)
@@ -192,10 +192,13 @@ def test_inherited_switching_at_division(stay):
     compare(cg, co, exact=(0, 16, 20))
     assert np.array_equal(sim.parents(), o.parents())
     moved = (cg[:n, 20] != cells[:, 20]) | (cg[n:, 20] != cells[:, 20])
+    both = (cg[:n, 20] != cells[:, 20]) & (cg[n:, 20] != cells[:, 20])
+    g1 = cells[:, 20] == 1
+    assert not both.any() and not moved[~g1].any()      # P(2, 2) = 1: group-2 pairs stay
     if stay == 0.0:
-        assert moved.all() and not np.any((cg[:n, 20] != cells[:, 20]) & (cg[n:, 20] != cells[:, 20]))
+        assert moved[g1].all()
     else:
-        assert 0 < moved.sum() < n
+        assert 0 < moved[g1].sum() < g1.sum()
     sim.close()
 
 

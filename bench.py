@@ -490,7 +490,7 @@ def oracle_step_outputs(o, dt=1e-6):
     return dict(forces=o.cell_cell_forces(), velocities=o.get_velocities(), cells=c1, E=e)
 
 
-def survey_b_step(P, E, s, K=100):
+def step_byte_model(P, E, s, K=100):
     """Algorithmic bytes per accepted cell-step of the FP64 plain path, B_step(s, P, E, K):
     pair refresh and force [8P + 56 + 48], E evaluations of B_eval(s) = 232 s + 24 s (s - 1)
     + 144 + 48 s, growth 24, and the cell list and pair build amortised over K."""
@@ -602,7 +602,7 @@ def run_b200(args):
     h = results[head]
     P = h["pairs"] / args.n
     E = h["attempts"] / max(h["iterations"], 1)
-    b_step = survey_b_step(P, E, STAGES[args.tableau])
+    b_step = step_byte_model(P, E, STAGES[args.tableau])
     roof = roofline(h["kernels"], h["rebuild_extra_ms"])
     peak = roof["peak"]
     roof["b_step_model"] = {"bytes_per_cell_step": b_step, "pairs_per_cell": P, "rk_evals_per_step": E,

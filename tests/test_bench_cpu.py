@@ -50,12 +50,12 @@ def test_byte_model_per_cell():
     assert bench.pair_force_bytes(n, n_dir) == 120 * n + 4 * n_dir
 
 
-def test_survey_byte_model_worked_values():
+def test_step_byte_model_worked_values():
     # B_step(s, P, E, K) at P = 10, E = 1, K = 100: ~962 B (Heun-Euler) and ~1762 B (BS3(2))
-    assert abs(bench.survey_b_step(10, 1, 2) - 961.56) < 1e-9
-    assert abs(bench.survey_b_step(10, 1, 4) - 1761.56) < 1e-9
+    assert abs(bench.step_byte_model(10, 1, 2) - 961.56) < 1e-9
+    assert abs(bench.step_byte_model(10, 1, 4) - 1761.56) < 1e-9
     # each extra evaluation adds B_eval(s): 752 B and 1552 B
-    assert abs(bench.survey_b_step(10, 2, 2) - bench.survey_b_step(10, 1, 2) - 752) < 1e-9
+    assert abs(bench.step_byte_model(10, 2, 2) - bench.step_byte_model(10, 1, 2) - 752) < 1e-9
 
 
 def test_rk_units_scale_by_the_error_test():

@@ -197,3 +197,46 @@ def test_friction_arguments_are_checked():
     with pytest.raises(RuntimeError, match="friction column"):
         sim.upload_cells(patch_state(10, 76)[:, :22])
     sim.close()
+
+
+def test_friction_with_the_pi_controller():
+    """Friction under a proposing controller (the PI rule): the trial passes run before the
+    proposal's in-place attempt and before the retries that start from its backup."""
+    cells = with_friction(monolayer(14, 11), 0, 77)
+    sim, o = pair(cells, adhesion_mode=0, integration_mode=2, max_rz_noise=2000.0, rng_seed=6,
+                  max_stepsize=1e-4, controller=abm_b200.CONTROLLER_PI)
+    sim.get_cell_neighbors()
+    o.loop_init()
+    for it in range(8):
+        sim.iterate(1)
+        o.iterate(1)
+        assert colwise_relerr(sim.download_cells(), o.cells()) <= 1e-9, it
+    assert sim.stats()["attempts"] == o.stats()["attempts"]
+    sim.close()
+
+
+def test_friction_coefficients_travel_through_frames_and_compaction():
+    """The coefficient column comes back in frames, and basal-only compaction keeps each
+    kept cell's coefficient."""
+    cells = with_friction(patch_state(800, 78), 1, 78)
+    sim, o = pair(cells, adhesion_mode=1, max_stepsize=1e-5)
+    sim.set_basal_only(True, 0.01)
+    o.set_basal_only(True, 0.01)
+    sim.set_frames(1e-5, slots=4)
+    sim.get_cell_neighbors()
+    o.loop_init()
+    frames = 0
+    for it in range(3):
+        k0 = sim.frames_taken()
+        sim.iterate(1)
+        o.iterate(1)
+        cg, co = sim.download_cells(), o.cells()
+        assert len(cg) == len(co)
+        assert np.array_equal(cg[:, 0], co[:, 0]) and np.array_equal(cg[:, 22], co[:, 22])
+        assert colwise_relerr(cg, co) <= 1e-9
+        if sim.frames_taken() > k0:                 # a frame of this iteration's end state
+            fc = sim.download_frame(sim.frames_taken() - 1)[0]
+            assert np.array_equal(fc[:, 22], cg[:, 22])
+            frames += 1
+    assert len(cg) < len(cells) and frames >= 1
+    sim.close()

@@ -133,3 +133,25 @@ def test_verlet_arguments_are_checked():
     with pytest.raises(RuntimeError, match="Verlet"):
         sim.step_runge_kutta_adaptive(1e-6)
     sim.close()
+
+
+def test_verlet_with_markov_switching():
+    """The post-step kernels follow a Verlet step as they follow a Runge-Kutta one."""
+    cells = moving(patch_state(800, 86), 86)
+    cells[:, 20] = 1.0
+    cells[:, 21] = 10.0
+    sw = dict(mode=1, rates=(0.0, 2e4, 1e4, 0.0), growth=((0.0, 0.0), (0.0, 0.0)), timescale=2e-4,
+              attrs=[(18, 720.0, 300.0)], max_gamma=60.0)
+    sim, o = pair(cells, adhesion_mode=1, max_stepsize=1e-5, iter_update_neighbors=3)
+    sim.set_switching(**sw)
+    o.set_switching(**sw)
+    sim.get_cell_neighbors()
+    o.loop_init()
+    for it in range(6):
+        sim.iterate(1)
+        o.iterate(1)
+        cg, co = sim.download_cells(), o.cells()
+        assert np.array_equal(cg[:, 20], co[:, 20]), it
+        assert colwise_relerr(cg, co) <= 1e-9, it
+    assert np.count_nonzero(cg[:, 20] == 2) > 0
+    sim.close()

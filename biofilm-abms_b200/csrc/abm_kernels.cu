@@ -1663,10 +1663,11 @@ __global__ void __launch_bounds__(AT_T, (S <= 4 ? (V == 3 ? 3 : 6) : 1)) k_attem
     double st_vmax = 0.0, st_v2 = 0.0, st_g = 0.0, st_near = 0.0;
     // motion bound of each new segment: |dr| + h' |dn| + |dh| (a Hausdorff bound)
     double local_drift = 0.0;
-    // one cell per thread: the grid covers the capacity (attempt_blocks), so each thread
-    // runs at most one pass; thread t takes the t-th cell of the attempt order (cells
-    // appended after the order was made, in index order)
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    // one cell per thread: the grid covers the capacity (attempt_blocks); thread t takes
+    // the t-th cell of the attempt order (cells appended after the order was made, in
+    // index order).  The body is a do-while(false) block so that `continue` leaves it.
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) do
     {
         const int i = t < n_order ? sp.order[t] : t;
         if (DRY)
@@ -1819,7 +1820,7 @@ __global__ void __launch_bounds__(AT_T, (S <= 4 ? (V == 3 ? 3 : 6) : 1)) k_attem
                 vel_c[i] = vo;
             }
         }
-    }
+    } while (false);
     if (DRY) return;
     if ((KIND == MODE_FINAL || in_place) && sp.stats_on)
     {

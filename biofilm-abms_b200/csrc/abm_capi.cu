@@ -957,7 +957,7 @@ static void enqueue_rebuild(abm_ctx* c)
 // final attempt (simulation.hpp:1677-1769), each an early exit when idle
 // the screened pass writes both shares of every pair; with_gather also sums them
 // per cell into fcc (the API paths; the loop's first attempt sums them itself)
-// in_loop: the pass of a loop iteration, whose last block also makes the iteration's
+// in_loop: the pass of a loop iteration, one of whose blocks also makes the iteration's
 // step-size features (and, learned, the proposed dt)
 static void enqueue_pair_force(abm_ctx* c, int with_gather, bool in_loop = false)
 {

@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(PF_T) k_pair_force(const Geom* __restrict__ ge
     {
         ovl_max = warp_max(ovl_max);
         if ((threadIdx.x & 31) == 0 && ovl_max > 0)
-            atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
+            atomicMax(&ctrl->st_ovl_bits[ctrl->iter & 1], (unsigned long long)__double_as_longlong(ovl_max));
     }
 }
 
@@ -1001,24 +1001,35 @@ __device__ __forceinline__ void pair_shares(const Geom& gi, const Geom& gj, cons
     }
 }
 
-// With `propose` the last block then runs the step-size proposal of the iteration
-// (mlp_propose_block), once every block's overlaps are in; it reads their maximum
-// with an atomic, the one field of the control record that other blocks change
-// during the pass.
-template <bool MIXED, int DIM>
-__global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
-                                                   Ctrl* ctrl, ForceParams fp, const double* __restrict__ td,
-                                                   const double* __restrict__ tr, double4* __restrict__ jbuf,
-                                                   int* __restrict__ surv, StepParams sp,
-                                                   const float* __restrict__ mlp_w, int propose)
+// With PROPOSE the pass also makes the iteration's step-size proposal
+// (mlp_propose_block). Its features read the previous iteration's overlap maximum
+// (st_ovl_bits of the other parity, which no block of this pass writes), so the
+// proposal depends on nothing this pass computes: the grid's last block makes it
+// while the other blocks stride over the pairs, and its chain of dependent reads
+// and three network layers runs beside the pair work instead of after it. A grid of
+// one block computes its pairs first and proposes at the end. The proposal is a
+// template parameter so that the passes without it carry none of its code, and the
+// bound of two resident blocks per SM (at most 128 registers) holds the pair loop's
+// occupancy whatever the proposal adds.
+template <bool MIXED, int DIM, bool PROPOSE>
+__global__ void __launch_bounds__(PS_T, 2) k_pair_pass(const Geom* __restrict__ geom, const int4* __restrict__ pairs,
+                                                      Ctrl* ctrl, ForceParams fp, const double* __restrict__ td,
+                                                      const double* __restrict__ tr, double4* __restrict__ jbuf,
+                                                      int* __restrict__ surv, StepParams sp,
+                                                      const float* __restrict__ mlp_w)
 {
     __shared__ bool last;
     if (ctrl->halted) return;
+    const bool split = PROPOSE && gridDim.x > 1;
+    const bool proposer = split && blockIdx.x == gridDim.x - 1;
+    const int work_blocks = split ? gridDim.x - 1 : gridDim.x;
     const bool refresh = !ctrl->screen_valid || !(2.0 * ctrl->drift * (1.0 + 1e-6) + 1e-9 < fp.skin);
     const int lane = threadIdx.x & 31;
-    const int stride = gridDim.x * blockDim.x;
+    const int stride = work_blocks * blockDim.x;
     double ovl_max = 0.0;
-    if (refresh)
+    if (proposer)
+        mlp_propose_block(ctrl, sp, mlp_w);
+    else if (refresh)
     {
         const int n_pairs = ctrl->n_dir >> 1;
         const double limit = 2 * fp.R + fp.skin;
@@ -1067,11 +1078,11 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
             if (cand) fp.fr_list[atomicAdd(&ctrl->fr_ncand_next, 1)] = p;
         }
     }
-    if (fp.stats)
+    if (fp.stats && !proposer)
     {
         ovl_max = warp_max(ovl_max);
         if (lane == 0 && ovl_max > 0)
-            atomicMax(&ctrl->st_ovl_bits, (unsigned long long)__double_as_longlong(ovl_max));
+            atomicMax(&ctrl->st_ovl_bits[ctrl->iter & 1], (unsigned long long)__double_as_longlong(ovl_max));
     }
     __syncthreads();
     if (threadIdx.x == 0)
@@ -1100,7 +1111,7 @@ __global__ void __launch_bounds__(PS_T) k_pair_pass(const Geom* __restrict__ geo
         }
         ctrl->surv_blocks = 0u;
     }
-    if (propose)
+    if (PROPOSE && !split)
     {
         __syncthreads();
         mlp_propose_block(ctrl, sp, mlp_w);
@@ -1179,14 +1190,27 @@ void launch_pair_screened(const Geom* geom, const int* row_ptr, const int* lower
         const int per_sm = blocks_per_sm > 0 ? min(blocks_per_sm, occ_cache) : occ_cache;
         return max(1, min(cdiv(max_pairs, tile), num_sms * per_sm));
     };
-    static int occ2 = 0, occ3m = 0, occ3 = 0;
-#define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv, spv, mlp_w, propose
+    // resident blocks per SM of each instantiation (without, with the proposal)
+    static int occ2[2] = {0, 0}, occ3m[2] = {0, 0}, occ3[2] = {0, 0};
+#define PX_ARGS geom, pairs, ctrl, fp, jkr_delta, jkr_radius, jbuf, surv, spv, mlp_w
+#define PX_LAUNCH(M, D, P, occ) \
+    k_pair_pass<M, D, P><<<grid((const void*)k_pair_pass<M, D, P>, occ[P ? 1 : 0]), PS_T, 0, st>>>(PX_ARGS)
     if (dims == 2)
-        k_pair_pass<false, 2><<<grid((const void*)k_pair_pass<false, 2>, occ2), PS_T, 0, st>>>(PX_ARGS);
+    {
+        if (propose) PX_LAUNCH(false, 2, true, occ2);
+        else PX_LAUNCH(false, 2, false, occ2);
+    }
     else if (f32)
-        k_pair_pass<true, 3><<<grid((const void*)k_pair_pass<true, 3>, occ3m), PS_T, 0, st>>>(PX_ARGS);
+    {
+        if (propose) PX_LAUNCH(true, 3, true, occ3m);
+        else PX_LAUNCH(true, 3, false, occ3m);
+    }
     else
-        k_pair_pass<false, 3><<<grid((const void*)k_pair_pass<false, 3>, occ3), PS_T, 0, st>>>(PX_ARGS);
+    {
+        if (propose) PX_LAUNCH(false, 3, true, occ3);
+        else PX_LAUNCH(false, 3, false, occ3);
+    }
+#undef PX_LAUNCH
 #undef PX_ARGS
     if (with_sum)
         k_pair_sum_rows<<<max(cdiv(cap_cells, 128), 1), 128, 0, st>>>(row_ptr, lower_end, ctrl, jbuf, fcc, f32);

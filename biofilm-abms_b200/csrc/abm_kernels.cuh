@@ -60,7 +60,7 @@ struct Ctrl {
     // step-size features (filled when StepParams::stats_on)
     // sums in fixed point so that their value does not depend on the order of the atomics
     unsigned long long st_vmax_bits;    // max |v_r| of the last accepted step (ordered bits)
-    unsigned long long st_ovl_bits;     // max overlap of the last pair-force pass
+    unsigned long long st_ovl_bits[2];  // max overlap of the pair-force passes of even / odd iterations
     unsigned long long st_v2_fx;        // sum |v_r|^2 * 2^STAT_V2_SHIFT
     unsigned long long st_g_fx;         // sum of growth rates * 2^STAT_G_SHIFT
     unsigned long long st_near_div;     // cells with l > 0.9 Ldiv

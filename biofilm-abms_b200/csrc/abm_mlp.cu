@@ -7,7 +7,7 @@
 //   k_mlp_forward    batch inference, 16-row tiles per warp
 //   k_mlp_grad       loss and gradient of a batch (checked against a CPU restatement)
 //   k_mlp_train      mini-batch Adam on a logged data set, one block of 4 warps
-//   mlp_propose_block  inside the loop, in the last block of the pair pass
+//   mlp_propose_block  inside the loop, in one block of the pair pass
 //                    (abm_propose.cuh): the features of the iteration -> log row, and
 //                    (learned controller) the network's dt
 //

@@ -112,7 +112,9 @@ __global__ void k_na_setup(Ctrl* ctrl, int n_entries, const __grid_constant__ Jk
         ctrl->n_dir = n_entries;
         ctrl->status = 0;
         ctrl->halted = 0;
-        ctrl->st_ovl_bits = 0ull;
+        ctrl->iter = 0;
+        ctrl->st_ovl_bits[0] = 0ull;
+        ctrl->st_ovl_bits[1] = 0ull;
     }
     for (int k = threadIdx.x; k < jkr.n; k += blockDim.x)
     {

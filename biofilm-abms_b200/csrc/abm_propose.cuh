@@ -1,5 +1,5 @@
 // Step-size proposal of the learned controller, shared by the network kernels
-// (abm_mlp.cu) and the pair pass (abm_kernels.cu), which runs it in its last block.
+// (abm_mlp.cu) and the pair pass (abm_kernels.cu), which runs it in one of its blocks.
 // BF16 operands, FP32 accumulation on the tensor cores (mma.sync m16n8k16).
 #pragma once
 #include <cuda_bf16.h>
@@ -28,7 +28,7 @@ __device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, u
 //   0       ln(n) / 10
 //   1       log10(max |v_r| + 1e-12) / 4     (velocities of the last accepted step)
 //   2       log10(rms |v_r| + 1e-12) / 4
-//   3       max overlap / (2 (R - Rcell))    (this iteration's pair pass)
+//   3       max overlap / (2 (R - Rcell))    (the previous iteration's pair pass)
 //   4..11   log10(dt / max_stepsize) of the last 8 accepted steps, newest first
 //   12..19  log10(scaled error) / 10 of those steps
 //   20..27  1 if that step's first attempt passed the error test
@@ -74,8 +74,8 @@ __device__ __forceinline__ void row0_tile(const float* __restrict__ W, int w_off
 
 // One block of 8 warps (blockDim.x == 256): features, then layer 1 and layer 2 one
 // 8-unit tile per warp, then the output unit on warp 0 (bit-identical to
-// mlp_tile_forward_regs for row 0).  Runs as its own kernel or in the last block of
-// the pair pass, once that pass's overlaps are in.
+// mlp_tile_forward_regs for row 0).  Runs in one block of the pair pass, beside the
+// blocks that compute the pairs: nothing it reads is written during that pass.
 static __device__ __forceinline__ void mlp_propose_block(Ctrl* ctrl, const StepParams& sp, const float* __restrict__ W)
 {
     __shared__ float feat[MLP_IN], h1[MLP_H], h2[MLP_H];
@@ -85,25 +85,52 @@ static __device__ __forceinline__ void mlp_propose_block(Ctrl* ctrl, const StepP
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = ctrl->n;
     const double inv_n = 1.0 / (double)max(n, 1);
-    if (tid == 0)
+    // The step statistics, one feature per thread (the FP64 logarithms run side by
+    // side rather than one after another): the sums of the last accepted step (final
+    // attempt or accepted proposal) and the previous pass's overlap maximum, each read
+    // and then reset by the thread that uses it.
+    switch (tid)
     {
-        // sums of the last accepted step (final attempt or accepted proposal), then reset
+    case 0: feat[0] = (float)(log((double)max(n, 1)) / 10.0); break;
+    case 1:
+    {
         const double vmax = __longlong_as_double((long long)ctrl->st_vmax_bits);
-        const double v2 = ldexp((double)ctrl->st_v2_fx, -STAT_V2_SHIFT);
-        const double gs = ldexp((double)ctrl->st_g_fx, -STAT_G_SHIFT);
-        const double near = (double)ctrl->st_near_div;
-        // this pass's overlap maximum, made by every block's atomicMax: read at L2
-        const double ovl = __longlong_as_double((long long)atomicAdd(&ctrl->st_ovl_bits, 0ull));
-        ctrl->st_vmax_bits = 0ull; ctrl->st_v2_fx = 0ull; ctrl->st_g_fx = 0ull; ctrl->st_near_div = 0ull;
-        ctrl->st_ovl_bits = 0ull;
-        feat[0] = (float)(log((double)max(n, 1)) / 10.0);
+        ctrl->st_vmax_bits = 0ull;
         feat[1] = (float)(log10(vmax + 1e-12) / 4.0);
+        break;
+    }
+    case 2:
+    {
+        const double v2 = ldexp((double)ctrl->st_v2_fx, -STAT_V2_SHIFT);
+        ctrl->st_v2_fx = 0ull;
         feat[2] = (float)(log10(sqrt(v2 * inv_n) + 1e-12) / 4.0);
+        break;
+    }
+    case 3:
+    {
+        // the previous iteration's pass (the other parity), made by its blocks'
+        // atomicMax: taken and cleared at L2 for the next iteration's pass
+        const double ovl = __longlong_as_double((long long)atomicExch(&ctrl->st_ovl_bits[(ctrl->iter + 1) & 1], 0ull));
         feat[3] = (float)(ovl / (2 * (sp.mp.R - sp.mp.Rcell)));
+        break;
+    }
+    case 4:
+    {
+        const double gs = ldexp((double)ctrl->st_g_fx, -STAT_G_SHIFT);
+        ctrl->st_g_fx = 0ull;
         feat[28] = (float)(gs * inv_n);
+        break;
+    }
+    case 5:
+    {
+        const double near = (double)ctrl->st_near_div;
+        ctrl->st_near_div = 0ull;
         feat[29] = (float)(near * inv_n);
-        feat[30] = (float)log10(1.0 + (double)ctrl->n_divide);
-        feat[31] = (float)(log1p((double)ctrl->since_div) / 5.0);
+        break;
+    }
+    case 6: feat[30] = (float)log10(1.0 + (double)ctrl->n_divide); break;
+    case 7: feat[31] = (float)(log1p((double)ctrl->since_div) / 5.0); break;
+    default: break;
     }
     if (tid >= 32 && tid < 32 + HIST)
     {

@@ -157,6 +157,8 @@ def _load():
         "abm_build_neighbors": ([vp, ip], i),
         "abm_download_neighbors": ([vp, dp, i, i, ip], i),
         "abm_upload_neighbors": ([vp, dp, i, i], i),
+        "abm_save_checkpoint": ([vp, ctypes.c_char_p], i),
+        "abm_load_checkpoint": ([vp, ctypes.c_char_p], i),
         "abm_cell_cell_forces": ([vp, dp], i),
         "abm_get_velocities": ([vp, dp], i),
         "abm_rk_attempt": ([vp, d, i, dp, dp, dp], i),
@@ -220,6 +222,7 @@ EXPORTED = ("abm_create abm_destroy abm_last_error abm_get_stream abm_synchroniz
             "abm_jkr_radius_table_variable abm_set_jkr_table_variable abm_upload_cells "
             "abm_download_cells abm_get_num_cells abm_set_clock abm_get_clock abm_set_parents "
             "abm_get_parents abm_build_neighbors abm_download_neighbors abm_upload_neighbors "
+            "abm_save_checkpoint abm_load_checkpoint "
             "abm_cell_cell_forces abm_get_velocities abm_rk_attempt abm_grow abm_divide "
             "abm_iterate abm_get_stats abm_profile_iterations abm_last_division_tries abm_graph_info "
             "abm_cell_cell_forces_noalloc abm_cell_cell_forces_noalloc_status abm_noalloc_last_error "
@@ -422,6 +425,22 @@ class Simulation:
         a = np.ascontiguousarray(parents, dtype=np.int32)
         self._check(LIB.abm_set_parents(self._ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(a)),
                     "abm_set_parents")
+
+    def save_checkpoint(self, path):
+        """Exact binary checkpoint (cells, neighbor set, lineage, clock, controller state)."""
+        self._check(LIB.abm_save_checkpoint(self._ctx, os.fsencode(path)), "abm_save_checkpoint")
+
+    def load_checkpoint(self, path):
+        """Resume from abm_save_checkpoint's file; the context must have the saving one's
+        parameters, JKR table and network weights."""
+        self._check(LIB.abm_load_checkpoint(self._ctx, os.fsencode(path)), "abm_load_checkpoint")
+        self.ncols = self._ckpt_cols(path)
+
+    @staticmethod
+    def _ckpt_cols(path):
+        with open(path, "rb") as f:
+            head = f.read(16)
+        return int(np.frombuffer(head[8:16], dtype=np.int32)[1])
 
     def parents(self):
         n = ctypes.c_int()

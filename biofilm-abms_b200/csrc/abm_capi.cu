@@ -7,6 +7,7 @@
 // CSR).  All sizes that change during a run (cell count, pair count, bin
 // count) live in device memory, so the graphs are captured once and replayed.
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1451,6 +1452,157 @@ int abm_upload_neighbors(abm_ctx* c, const double* rows, int m, int ld)
         launch_adhere_flags(c->ctrl, c->row_ptr, c->col, c->geom, c->p.R, c->p.Rcell, c->adhere, c->cap, c->st);
     CK(cudaGetLastError());
     c->nbrs_valid = true;
+    return ABM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Exact binary checkpoints. The reference resumes a run from its text frames, whose
+// 10 significant digits move each value by up to 5e-10 of itself. A checkpoint keeps
+// the FP64 bits of the cells, the neighbor set, the lineage, the clock and the state
+// the controllers carry from one iteration to the next (the last HIST steps' dt,
+// scaled errors and accept flags, the step statistics the proposal reads, the loop's
+// counters). Everything else on the device is rebuilt or reset by the upload: the
+// active pair list and the attempt order depend on nothing but the cells and the
+// neighbor set, and they change no result bit. The random draws are keyed by the
+// iteration, which the checkpoint restores. So a context created with the same
+// parameters (and network weights), loaded from a checkpoint written at an
+// iteration boundary, continues bit for bit where the uninterrupted run continues.
+//
+// File: "ABMCKP01", six int32 (dims, ncols, n, pairs m, lineage length, 0), the
+// CkState block, cells (ncols x n doubles, column-major), pair cell indices (m int32
+// i, then m int32 j, each pair once as the neighbor table lists it), lineage (int32).
+// Host byte order.
+struct CkState {
+    double t, dt, dt_try, factor, last_max_error, last_trial_error, dt_prev;
+    double hist_dt[HIST], hist_err[HIST];
+    long long iter, since_div, hist_pos, first_passed, hist_acc[HIST];
+    long long attempts, retries, iterations, rebuilds, divisions, div_events, rejected, cell_steps,
+        basal_dropped, last_div_tries;
+    unsigned long long st_vmax_bits, st_ovl_bits[2], st_v2_fx, st_g_fx, st_near_div;
+};
+static_assert(sizeof(CkState) % 8 == 0, "checkpoint state block is made of 8-byte fields");
+static const char CK_MAGIC[8] = {'A', 'B', 'M', 'C', 'K', 'P', '0', '1'};
+
+static void ck_from_ctrl(const Ctrl& h, CkState& s)
+{
+    s.t = h.t; s.dt = h.dt; s.dt_try = h.dt_try; s.factor = h.factor;
+    s.last_max_error = h.last_max_error; s.last_trial_error = h.last_trial_error; s.dt_prev = h.dt_prev;
+    for (int k = 0; k < HIST; ++k)
+    {
+        s.hist_dt[k] = h.hist_dt[k]; s.hist_err[k] = h.hist_err[k]; s.hist_acc[k] = h.hist_acc[k];
+    }
+    s.iter = h.iter; s.since_div = h.since_div; s.hist_pos = h.hist_pos; s.first_passed = h.first_passed;
+    s.attempts = h.attempts; s.retries = h.retries; s.iterations = h.iterations; s.rebuilds = h.rebuilds;
+    s.divisions = h.divisions; s.div_events = h.div_events; s.rejected = h.rejected;
+    s.cell_steps = h.cell_steps; s.basal_dropped = h.basal_dropped; s.last_div_tries = h.last_div_tries;
+    s.st_vmax_bits = h.st_vmax_bits; s.st_ovl_bits[0] = h.st_ovl_bits[0]; s.st_ovl_bits[1] = h.st_ovl_bits[1];
+    s.st_v2_fx = h.st_v2_fx; s.st_g_fx = h.st_g_fx; s.st_near_div = h.st_near_div;
+}
+
+static void ck_to_ctrl(const CkState& s, Ctrl& h)
+{
+    h.t = s.t; h.dt = s.dt; h.dt_try = s.dt_try; h.factor = s.factor;
+    h.last_max_error = s.last_max_error; h.last_trial_error = s.last_trial_error; h.dt_prev = s.dt_prev;
+    for (int k = 0; k < HIST; ++k)
+    {
+        h.hist_dt[k] = s.hist_dt[k]; h.hist_err[k] = s.hist_err[k]; h.hist_acc[k] = (int)s.hist_acc[k];
+    }
+    h.iter = (int)s.iter; h.since_div = (int)s.since_div; h.hist_pos = (int)s.hist_pos;
+    h.first_passed = (int)s.first_passed;
+    h.attempts = s.attempts; h.retries = s.retries; h.iterations = s.iterations; h.rebuilds = s.rebuilds;
+    h.divisions = s.divisions; h.div_events = s.div_events; h.rejected = s.rejected;
+    h.cell_steps = s.cell_steps; h.basal_dropped = s.basal_dropped; h.last_div_tries = (int)s.last_div_tries;
+    h.st_vmax_bits = s.st_vmax_bits; h.st_ovl_bits[0] = s.st_ovl_bits[0]; h.st_ovl_bits[1] = s.st_ovl_bits[1];
+    h.st_v2_fx = s.st_v2_fx; h.st_g_fx = s.st_g_fx; h.st_near_div = s.st_near_div;
+}
+
+int abm_save_checkpoint(abm_ctx* c, const char* path)
+{
+    if (!c || !path) return ABM_ERR_ARG;
+    if (!c->cells_loaded) return fail(c, ABM_ERR_STATE, "no cells uploaded");
+    if (!c->nbrs_valid) return fail(c, ABM_ERR_STATE, "neighbors not built");
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const int n = h.n, ncols = c->ncols, n_par = h.n_parents;
+    std::vector<double> cells((size_t)std::max(n, 1) * ncols);
+    int rc = abm_download_cells(c, cells.data(), std::max(n, 1));
+    if (rc) return rc;
+    int m = 0;
+    rc = abm_download_neighbors(c, nullptr, 0, 0, &m);
+    if (rc) return rc;
+    const int tcols = c->dims == 2 ? 6 : 7;
+    std::vector<double> rows((size_t)std::max(m, 1) * tcols);
+    if (m > 0 && (rc = abm_download_neighbors(c, rows.data(), m, m, &m))) return rc;
+    std::vector<int> pairs((size_t)2 * m);
+    for (int k = 0; k < m; ++k) { pairs[k] = (int)rows[k]; pairs[(size_t)m + k] = (int)rows[(size_t)m + k]; }
+    std::vector<int> parents((size_t)std::max(n_par, 0));
+    if (n_par > 0 && (rc = abm_get_parents(c, parents.data(), n_par, nullptr))) return rc;
+    CkState s;
+    std::memset(&s, 0, sizeof(s));
+    ck_from_ctrl(h, s);
+    const int hdr[6] = {c->dims, ncols, n, m, n_par, 0};
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(c, ABM_ERR_ARG, std::string("cannot open ") + path + " for writing");
+    bool ok = std::fwrite(CK_MAGIC, 1, 8, f) == 8 && std::fwrite(hdr, sizeof(int), 6, f) == 6 &&
+              std::fwrite(&s, sizeof(s), 1, f) == 1;
+    if (ok && n > 0) ok = std::fwrite(cells.data(), sizeof(double), (size_t)n * ncols, f) == (size_t)n * ncols;
+    if (ok && m > 0) ok = std::fwrite(pairs.data(), sizeof(int), pairs.size(), f) == pairs.size();
+    if (ok && n_par > 0) ok = std::fwrite(parents.data(), sizeof(int), parents.size(), f) == parents.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(c, ABM_ERR_ARG, std::string("write failed: ") + path);
+    return ABM_OK;
+}
+
+int abm_load_checkpoint(abm_ctx* c, const char* path)
+{
+    if (!c || !path) return ABM_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(c, ABM_ERR_ARG, std::string("cannot open ") + path);
+    char magic[8];
+    int hdr[6];
+    CkState s;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, CK_MAGIC, 8) == 0 &&
+              std::fread(hdr, sizeof(int), 6, f) == 6 && std::fread(&s, sizeof(s), 1, f) == 1;
+    const int dims = ok ? hdr[0] : 0, ncols = ok ? hdr[1] : 0, n = ok ? hdr[2] : -1, m = ok ? hdr[3] : -1,
+              n_par = ok ? hdr[4] : -1;
+    if (!ok || n < 0 || m < 0 || n_par < 0 || ncols <= 0 || ncols > STAGING_COLS)
+    {
+        std::fclose(f);
+        return fail(c, ABM_ERR_ARG, std::string("not a checkpoint of this library: ") + path);
+    }
+    if (dims != c->dims)
+    {
+        std::fclose(f);
+        return fail(c, ABM_ERR_ARG, "the checkpoint belongs to the other model (2-D / 3-D)");
+    }
+    if (n > c->cap)
+    {
+        std::fclose(f);
+        return fail(c, ABM_ERR_CAPACITY, "the checkpoint holds more cells than cap_cells");
+    }
+    std::vector<double> cells((size_t)std::max(n, 1) * ncols);
+    std::vector<int> pairs((size_t)2 * m), parents((size_t)n_par);
+    if (n > 0) ok = std::fread(cells.data(), sizeof(double), (size_t)n * ncols, f) == (size_t)n * ncols;
+    if (ok && m > 0) ok = std::fread(pairs.data(), sizeof(int), pairs.size(), f) == pairs.size();
+    if (ok && n_par > 0) ok = std::fread(parents.data(), sizeof(int), parents.size(), f) == parents.size();
+    if (ok) ok = std::fgetc(f) == EOF;                // nothing after the lineage
+    std::fclose(f);
+    if (!ok) return fail(c, ABM_ERR_ARG, std::string("truncated or oversized checkpoint: ") + path);
+    if (!(s.dt > 0) || s.iter < 0 || s.iter > INT_MAX || s.hist_pos < 0 || s.hist_pos >= HIST)
+        return fail(c, ABM_ERR_ARG, "the checkpoint's clock or controller history is out of range");
+    int rc = abm_upload_cells(c, cells.data(), n, ncols, std::max(n, 1));
+    if (rc) return rc;
+    if ((rc = abm_set_parents(c, n_par > 0 ? parents.data() : nullptr, n_par))) return rc;
+    std::vector<double> rows((size_t)std::max(m, 1) * 2);
+    for (int k = 0; k < m; ++k) { rows[k] = pairs[k]; rows[(size_t)m + k] = pairs[(size_t)m + k]; }
+    if ((rc = abm_upload_neighbors(c, rows.data(), m, std::max(m, 1)))) return rc;
+    if ((rc = abm_set_clock(c, s.t, s.dt, (int)s.iter))) return rc;
+    Ctrl h;
+    CK(cudaMemcpyAsync(&h, c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    ck_to_ctrl(s, h);
+    CK(cudaMemcpy(c->ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice));
     return ABM_OK;
 }
 

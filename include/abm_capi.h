@@ -423,6 +423,21 @@ int abm_frames_taken(abm_ctx* ctx, int* taken);
 int abm_download_frame(abm_ctx* ctx, int index, double* cells, int ld, int* n, double* t, int* iter,
                        int* n_parents);
 
+/* Exact binary checkpoints: the resume the reference makes from its text frames
+ * (readCells and readLineage, utils.hpp:96-139 and 265-287, whose 10-digit values
+ * move a resumed run off its course), without the rounding.  A checkpoint holds the
+ * FP64 cells, the neighbor set, the lineage, the clock and what the step-size
+ * controllers carry between iterations (the last steps' dt, scaled errors and
+ * accept flags, the network's step statistics, the loop's counters).  Save at an
+ * iteration boundary (between abm_iterate calls) after the neighbors exist; load
+ * into a context created with the same parameters, JKR table and network weights,
+ * and it continues bit for bit as the saved run would.  Frames, the cell limit and
+ * switching settings are not part of it: set them again.  Host byte order;
+ * ABM_ERR_ARG for a file that is not a complete checkpoint of this library or
+ * belongs to the other model, ABM_ERR_CAPACITY when it holds more than cap_cells. */
+int abm_save_checkpoint(abm_ctx* ctx, const char* path);
+int abm_load_checkpoint(abm_ctx* ctx, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1591,6 +1591,17 @@ int abm_load_checkpoint(abm_ctx* c, const char* path)
     if (!ok) return fail(c, ABM_ERR_ARG, std::string("truncated or oversized checkpoint: ") + path);
     if (!(s.dt > 0) || s.iter < 0 || s.iter > INT_MAX || s.hist_pos < 0 || s.hist_pos >= HIST)
         return fail(c, ABM_ERR_ARG, "the checkpoint's clock or controller history is out of range");
+    // the checks abm_upload_neighbors makes, before anything reaches the context, so
+    // that a rejected file leaves it as it was
+    std::vector<int> degree((size_t)std::max(n, 1), 0);
+    for (int k = 0; k < m; ++k)
+    {
+        const int i = pairs[k], j = pairs[(size_t)m + k];
+        if (i < 0 || j < 0 || i >= n || j >= n || i == j)
+            return fail(c, ABM_ERR_ARG, "the checkpoint's neighbor set names a cell it does not hold");
+        if (++degree[i] > c->cap_nbr || ++degree[j] > c->cap_nbr)
+            return fail(c, ABM_ERR_CAPACITY, "the checkpoint's neighbors per cell exceed cap_neighbors_per_cell");
+    }
     int rc = abm_upload_cells(c, cells.data(), n, ncols, std::max(n, 1));
     if (rc) return rc;
     if ((rc = abm_set_parents(c, n_par > 0 ? parents.data() : nullptr, n_par))) return rc;

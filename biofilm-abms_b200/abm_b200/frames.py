@@ -78,11 +78,12 @@ def read_lineage(path):
     return out
 
 
-def write_frames(sim, outprefix, params=None, start=0, extra_cols=None, dims=3):
+def write_frames(sim, outprefix, params=None, start=0, extra_cols=None, dims=3, log=None):
     """Write frames start .. taken-1 of a Simulation with frames on, as runSimulation
     writes at its dt_write crossings (simulation.hpp:2045-2058): "<outprefix>_iter<i>.txt"
     with the parameters plus t_curr, then "<outprefix>_lineage.txt" with the lineage up
-    to the last frame written.  Returns the index of the next frame to write."""
+    to the last frame written.  With a RunLog `log`, one line of the loop's state and
+    counters follows the files.  Returns the index of the next frame to write."""
     taken = sim.frames_taken()
     params = dict(params or {})
     n_parents = None
@@ -92,4 +93,52 @@ def write_frames(sim, outprefix, params=None, start=0, extra_cols=None, dims=3):
         write_cells("%s_iter%d.txt" % (outprefix, it), cells, params, extra_cols, dims)
     if n_parents is not None:
         write_lineage("%s_lineage.txt" % outprefix, np.asarray(sim.parents())[:n_parents])
+    if log is not None and taken > start:
+        log.record(sim, frames_written=taken - start)
     return taken
+
+
+class RunLog:
+    """One JSON line per frame write, in place of the line runSimulation prints there
+    (simulation.hpp:2030-2039: iteration, cells, time, time elapsed since the last write,
+    dt).  The reference also prints the max and mean absolute RK error of the last step;
+    the device keeps the scaled max error E of the accepted attempt instead, logged as
+    `max_scaled_error`.  The loop's counters (attempts, retries, rejected first attempts,
+    rebuilds, divisions, neighbor pairs, cell-steps) come with each line, so a run's
+    controller behaviour can be read back without re-running it.
+
+    `sim` is anything with a `stats()` method returning the abm_stats fields as a dict
+    (abm_b200.Simulation does).  Lines are appended and flushed as they are written."""
+
+    def __init__(self, path, clock=None):
+        import time
+        self._clock = clock or time.monotonic
+        self._last = self._clock()
+        self._f = open(path, "a")
+
+    def record(self, sim, **extra):
+        """Append the line for the state `sim` is in now; `extra` keys go into it as given."""
+        import json
+        s = sim.stats()
+        now = self._clock()
+        line = {"iteration": int(s["iterations"]), "cells": int(s["n_cells"]), "t": float(s["t"]),
+                "time_elapsed_s": now - self._last, "dt": float(s["dt"]),
+                "max_scaled_error": float(s["last_max_error"])}
+        for k in ("attempts", "retries", "rejected", "rebuilds", "divisions", "n_pairs", "cell_steps"):
+            line[k] = int(s[k])
+        line.update(extra)
+        self._last = now
+        self._f.write(json.dumps(line) + "\n")
+        self._f.flush()
+        return line
+
+    def close(self):
+        if self._f:
+            self._f.close()
+            self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

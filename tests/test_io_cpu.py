@@ -100,3 +100,56 @@ def test_sparse_lineage_marks_absent_ids(tmp_path):
     path = tmp_path / "sparse.txt"
     path.write_text("0\t-1\n3\t0\n")
     assert list(frames.read_lineage(str(path))) == [-1, frames.ABSENT, frames.ABSENT, 0]
+
+
+class FramesStandIn:
+    """The calls write_frames and RunLog make on a Simulation, over host arrays: two
+    frames of a growing population, the lineage, and the loop's counters."""
+
+    def __init__(self):
+        self.states = [state_3d(200, 5), state_3d(260, 6)]
+        self.times, self.iters = [0.1, 0.2], [1000, 2150]
+        self.lineage = np.arange(-1, 259, dtype=np.int32)
+        self.counters = dict(iterations=2150, attempts=4400, retries=12, rebuilds=31, divisions=60, t=0.2,
+                             dt=9.5e-5, last_max_error=0.42, n_cells=260, n_pairs=1900, rejected=11,
+                             log_rows=0, cell_steps=512345)
+
+    def frames_taken(self):
+        return 2
+
+    def download_frame(self, k):
+        return self.states[k], self.times[k], self.iters[k], len(self.states[k])
+
+    def parents(self):
+        return self.lineage
+
+    def stats(self):
+        return dict(self.counters)
+
+
+def test_run_log_lines_beside_the_frames(tmp_path):
+    import json
+    sim = FramesStandIn()
+    ticks = iter([10.0, 12.5, 20.0])
+    prefix = str(tmp_path / "run")
+    with frames.RunLog(str(tmp_path / "run.jsonl"), clock=lambda: next(ticks)) as log:
+        assert frames.write_frames(sim, prefix, PARAMS, log=log) == 2
+        assert frames.write_frames(sim, prefix, PARAMS, start=2, log=log) == 2     # nothing new: no line
+        sim.counters.update(iterations=2300, t=0.21)
+        log.record(sim, note="end")
+    lines = [json.loads(x) for x in open(str(tmp_path / "run.jsonl"))]
+    assert len(lines) == 2
+    first, last = lines
+    # the reference's per-write fields (simulation.hpp:2035-2039) and the device counters
+    assert first["iteration"] == 2150 and first["cells"] == 260 and first["t"] == 0.2 and first["dt"] == 9.5e-5
+    assert first["time_elapsed_s"] == 2.5 and first["max_scaled_error"] == 0.42
+    assert first["frames_written"] == 2 and first["rejected"] == 11 and first["cell_steps"] == 512345
+    assert last["iteration"] == 2300 and last["time_elapsed_s"] == 7.5 and last["note"] == "end"
+    # the frame files themselves are the reference's, with t_curr of each frame
+    for k in range(2):
+        cells, params = frames.read_cells("%s_iter%d.txt" % (prefix, sim.iters[k]))
+        # ID through group (columns 0-20); gamma goes out only as a requested extra column
+        assert cells.shape == (len(sim.states[k]), 21)
+        assert np.array_equal(cells[:, [0, 20]], sim.states[k][:, [0, 20]])
+        assert params["t_curr"] == "%.10g" % sim.times[k]
+    assert np.array_equal(frames.read_lineage(prefix + "_lineage.txt"), sim.lineage[:260])

@@ -250,6 +250,92 @@ inline Neighbors get_cell_neighbors(const Cells& cells, double neighbor_threshol
     return nb;
 }
 
+// The same table as get_cell_neighbors from a uniform grid of bins no smaller than the
+// prefilter radius, so that every pair that passes the prefilter lies in adjacent bins:
+// each cell's row is made from the cells of its 27 surrounding bins (OpenMP over the
+// rows), with the same prefilter and distance arithmetic on (i, j), and sorted by j.
+// Not the reference's procedure: the "optimized CPU" figure reported beside the
+// reference-faithful CPU run uses it (with cpu_optimized in the parameters).
+inline Neighbors get_cell_neighbors_grid(const Cells& cells, double neighbor_threshold, double R, double Ldiv)
+{
+    Neighbors nb;
+    const int n = cells.n;
+    if (n <= 1) return nb;
+    const double prefilter = neighbor_threshold + Ldiv + 2 * R;
+    double lo[3] = {cells(0, C_RX), cells(0, C_RY), cells(0, C_RZ)}, hi[3] = {lo[0], lo[1], lo[2]};
+    for (int i = 1; i < n; ++i)
+    {
+        const double r[3] = {cells(i, C_RX), cells(i, C_RY), cells(i, C_RZ)};
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], r[a]); hi[a] = std::max(hi[a], r[a]); }
+    }
+    // bins of edge >= prefilter, at most about 4 n of them (a sparse state widens the edge)
+    double edge = prefilter;
+    long long dims[3];
+    for (;;)
+    {
+        long long total = 1;
+        for (int a = 0; a < 3; ++a)
+        {
+            dims[a] = (long long)std::floor((hi[a] - lo[a]) / edge) + 1;
+            total *= dims[a];
+        }
+        if (total <= 4LL * n + 64) break;
+        edge *= 2;
+    }
+    auto bin_of = [&](int i, long long b[3]) {
+        const double r[3] = {cells(i, C_RX), cells(i, C_RY), cells(i, C_RZ)};
+        for (int a = 0; a < 3; ++a)
+            b[a] = std::min(dims[a] - 1, std::max(0LL, (long long)std::floor((r[a] - lo[a]) / edge)));
+    };
+    const long long nbins = dims[0] * dims[1] * dims[2];
+    std::vector<int> start((size_t)nbins + 1, 0), members((size_t)n);
+    std::vector<long long> key((size_t)n);
+    for (int i = 0; i < n; ++i)
+    {
+        long long b[3];
+        bin_of(i, b);
+        key[i] = (b[2] * dims[1] + b[1]) * dims[0] + b[0];
+        ++start[key[i] + 1];
+    }
+    for (long long b = 0; b < nbins; ++b) start[b + 1] += start[b];
+    {
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int i = 0; i < n; ++i) members[fill[key[i]]++] = i;
+    }
+    struct Row { int j; DistResult res; };
+    std::vector<std::vector<Row> > rows((size_t)n);
+    #pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i)
+    {
+        long long b[3];
+        bin_of(i, b);
+        const V3 ri = cell_r(cells, i);
+        std::vector<Row>& out = rows[i];
+        for (long long z = std::max(0LL, b[2] - 1); z <= std::min(dims[2] - 1, b[2] + 1); ++z)
+            for (long long y = std::max(0LL, b[1] - 1); y <= std::min(dims[1] - 1, b[1] + 1); ++y)
+                for (long long x = std::max(0LL, b[0] - 1); x <= std::min(dims[0] - 1, b[0] + 1); ++x)
+                {
+                    const long long bb = (z * dims[1] + y) * dims[0] + x;
+                    for (int q = start[bb]; q < start[bb + 1]; ++q)
+                    {
+                        const int j = members[q];
+                        if (j >= i || !(norm(ri - cell_r(cells, j)) < prefilter)) continue;
+                        const DistResult res = dist_cells(cells, i, j);
+                        if (norm(res.d) < neighbor_threshold) out.push_back(Row{j, res});
+                    }
+                }
+        std::sort(out.begin(), out.end(), [](const Row& a, const Row& c) { return a.j < c.j; });
+    }
+    for (int i = 0; i < n; ++i)
+        for (const Row& r : rows[i])
+        {
+            nb.i.push_back(i); nb.j.push_back(r.j);
+            nb.dx.push_back(r.res.d.x); nb.dy.push_back(r.res.d.y); nb.dz.push_back(r.res.d.z);
+            nb.si.push_back(r.res.s); nb.sj.push_back(r.res.t);
+        }
+    return nb;
+}
+
 // mechanics.hpp:604-648 (updateNeighborDistances)
 inline void update_neighbor_distances(const Cells& cells, Neighbors& nb)
 {
@@ -537,7 +623,18 @@ struct Params3 {
     // variable-gamma JKR table (IsotropicJKRDataVariableGamma, mechanics.hpp:159-199): radii on the
     // overlap mesh jkr_overlaps x the gamma mesh jkr_gammas, overlap-major; used when non-empty
     std::vector<double> jkr_gammas, jkr_radii2;
+    // not the reference's procedure: the "optimized CPU" context figure (cell-list neighbor
+    // build, pair forces with OpenMP over the pairs); off for every parity comparison
+    int cpu_optimized = 0;
 };
+
+// getCellNeighbors as the loop calls it: the reference's O(n^2) procedure, or the
+// cell-list build with cpu_optimized (the same table)
+inline Neighbors build_neighbors(const Cells& cells, const Params3& p)
+{
+    return p.cpu_optimized ? get_cell_neighbors_grid(cells, p.neighbor_threshold, p.R, p.Ldiv)
+                           : get_cell_neighbors(cells, p.neighbor_threshold, p.R, p.Ldiv);
+}
 
 struct Tableau {
     int s = 0; double error_order = 0;
@@ -727,16 +824,15 @@ inline std::vector<double> jkr_radius_table2(const std::vector<double>& overlaps
 // the friction term (add_friction adds it).  Returns dE/dq (n x 6).  `constraint` selects
 // include_constraint = true, the form velocity Verlet uses: the Hertz and hard-core rows
 // become (s n) x v (mechanics.hpp:1298-1311, 1554-1566, 1608-1617).
-inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
-                             bool constraint = false)
+// the pairs k0 <= k < k1 of the table, added into dEdq (n x 6) in table order
+inline void cell_cell_forces_range(const Cells& cells, const Neighbors& nb, const Params3& p, bool constraint,
+                                   int k0, int k1, Arr6& dEdq)
 {
-    const int n = cells.n, m = nb.size();
-    Arr6 dEdq((size_t)n * 6, 0.0);
-    if (m == 0) return dEdq;
+    const int n = cells.n;
     const double R = p.R, Rcell = p.Rcell;
     double pf[3]; repulsion_prefactors(p, pf);
     const bool adhesion = (p.adhesion_mode != 0);
-    for (int k = 0; k < m; ++k)
+    for (int k = k0; k < k1; ++k)
     {
         int i = nb.i[k], j = nb.j[k];
         V3 dij = v3(nb.dx[k], nb.dy[k], nb.dz[k]);
@@ -797,6 +893,40 @@ inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Para
                 h[1][3] = tj.x; h[1][4] = tj.y; h[1][5] = tj.z;
             }
             for (int c = 0; c < 6; ++c) { A6(dEdq, n, i, c) += h[0][c]; A6(dEdq, n, j, c) += h[1][c]; }
+        }
+    }
+}
+
+// mechanics.hpp:1209-1350, 1390-1659 (cellCellInteractionForces): the pair loop in table
+// order.  With cpu_optimized, each OpenMP thread sums a contiguous range of pairs into its
+// own buffer and the buffers are added per cell in thread order (the sums then differ
+// from the table-order ones by rounding only).
+inline Arr6 cell_cell_forces(const Cells& cells, const Neighbors& nb, const Params3& p,
+                             bool constraint = false)
+{
+    const int n = cells.n, m = nb.size();
+    Arr6 dEdq((size_t)n * 6, 0.0);
+    if (m == 0) return dEdq;
+    if (!p.cpu_optimized)
+    {
+        cell_cell_forces_range(cells, nb, p, constraint, 0, m, dEdq);
+        return dEdq;
+    }
+    const int T = std::max(1, std::min(omp_get_max_threads(), m));
+    std::vector<Arr6> part((size_t)T);
+    #pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const int k0 = (int)((long long)m * t / nt), k1 = (int)((long long)m * (t + 1) / nt);
+        part[t].assign((size_t)n * 6, 0.0);
+        cell_cell_forces_range(cells, nb, p, constraint, k0, k1, part[t]);
+        #pragma omp barrier
+        #pragma omp for
+        for (int e = 0; e < n * 6; ++e)
+        {
+            double acc = 0.0;
+            for (int u = 0; u < nt; ++u) acc += part[u][e];
+            dEdq[e] = acc;
         }
     }
     return dEdq;
@@ -1841,7 +1971,7 @@ inline double pi_next_dt(double dt, double E, double E_prev, double error_order,
 inline void loop_init(LoopState& st, const Params3& p)
 {
     st.dt = p.max_stepsize;                      // simulation.hpp:1167
-    st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);   // :1277
+    st.nb = build_neighbors(st.cells, p);   // :1277
     st.rebuilds = 1;
 }
 
@@ -1865,7 +1995,7 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
                 if (to_divide[i]) pairs.push_back(std::make_pair(i, n_before + m++));
             switch_groups_inherit(st.cells, pairs, p, st.iter);
         }
-        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.nb = build_neighbors(st.cells, p);
         st.rebuilds++;
     }
     if (p.integration_mode == 0)
@@ -1927,14 +2057,14 @@ inline void loop_iteration(LoopState& st, const Params3& p, bool cc_once = false
     update_neighbor_distances(st.cells, st.nb);
     if (!p.no_surface && p.basal_only && basal_compact(st.cells, p) > 0)
     {
-        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.nb = build_neighbors(st.cells, p);
         st.rebuilds++;
     }
     st.t += st.dt;
     st.iter++;
     if (st.iter % p.iter_update_neighbors == 0)
     {
-        st.nb = get_cell_neighbors(st.cells, p.neighbor_threshold, p.R, p.Ldiv);
+        st.nb = build_neighbors(st.cells, p);
         st.rebuilds++;
     }
     // simulation.hpp:1866-2022.  The reference compares its cell count from before the

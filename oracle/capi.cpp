@@ -162,9 +162,13 @@ void oracle_get_clock(oracle_ctx* c, double* t, double* dt, int* iter)
 // mechanics.hpp:520-593
 int oracle_build_neighbors(oracle_ctx* c)
 {
-    c->st.nb = get_cell_neighbors(c->st.cells, c->p.neighbor_threshold, c->p.R, c->p.Ldiv);
+    c->st.nb = build_neighbors(c->st.cells, c->p);
     return c->st.nb.size();
 }
+
+// the "optimized CPU" procedures (cell-list neighbor build, OpenMP over the pairs), for
+// the context figure beside the reference-faithful CPU run; off by default
+void oracle_set_cpu_optimized(oracle_ctx* c, int on) { c->p.cpu_optimized = on ? 1 : 0; }
 
 int oracle_num_neighbors(oracle_ctx* c) { return c->st.nb.size(); }
 

@@ -63,6 +63,7 @@ def _load():
         "oracle_set_clock": ([vp, d, d, i], None),
         "oracle_get_clock": ([vp, dp, dp, ip], None),
         "oracle_build_neighbors": ([vp], i),
+        "oracle_set_cpu_optimized": ([vp, i], None),
         "oracle_num_neighbors": ([vp], i),
         "oracle_get_neighbors": ([vp, dp, i], i),
         "oracle_set_neighbors": ([vp, dp, i, i], i),
@@ -143,7 +144,9 @@ def jkr_table(R, Rcell, E0, gamma, n_mesh=100):
 class Oracle:
     """The oracle's loop state; parameters use the same names as abm_b200.DEFAULTS."""
 
-    def __init__(self, pdict, jkr=None, n_threads=0, n_start_multithread=50):
+    def __init__(self, pdict, jkr=None, n_threads=0, n_start_multithread=50, cpu_optimized=False):
+        """cpu_optimized: the cell-list neighbor build and OpenMP over the pairs (the
+        "optimized CPU" context figure), in place of the reference's procedures."""
         p = OracleParams()
         for name, _ in OracleParams._fields_:
             if name in pdict:
@@ -153,6 +156,7 @@ class Oracle:
         self.pdict = dict(pdict)
         self._c = ctypes.c_void_p()
         LIB.oracle_create(ctypes.byref(p), ctypes.byref(self._c))
+        LIB.oracle_set_cpu_optimized(self._c, 1 if cpu_optimized else 0)
         if jkr is not None:
             self.set_jkr_table(*jkr)
         self.ncols = None

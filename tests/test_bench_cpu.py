@@ -99,3 +99,16 @@ def test_both_builds_of_the_generator_draw_the_same_state():
     assert np.array_equal(a, b) and ia == ib
     c = workloads.biofilm_2d(3000, seed=4)
     assert c.shape == (3000, 17)
+
+
+def test_optimized_cpu_leg_runs_on_the_benchmark_state():
+    # the context figure beside the faithful CPU run: same state and parameters, the
+    # cell-list build and parallel pair forces; a small case of the same workload
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ref as orc
+    args = bench.parse_args(["--cells", "3000"])
+    cells, _ = bench.workload(args.n, 1, lib=orc.LIB)
+    r = bench.cpu_optimized_rate(cells, args, 2, 2)
+    assert r["value"] > 0 and r["cores"] == 2 and r["unit"] == bench.UNIT
+    assert "2 accepted steps at n=3000" in r["sample"]
+    json.dumps(r)

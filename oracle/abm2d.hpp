@@ -1,6 +1,6 @@
 // ORACLE — test infrastructure only.  A plain C++17 restatement of the 2-D
-// mechanics step of kmnam/biofilm-ABMs (ABM-2d/ABM-2d-cpp), used by tests/ as
-// the checker of the 2-D CUDA path.  The product library never links, includes
+// mechanics step of kmnam/biofilm-ABMs (ABM-2d/ABM-2d-cpp), against which tests/
+// compare the 2-D CUDA path.  The product library never links, includes
 // or calls anything under oracle/.
 //
 // Geometry is shared with the 3-D restatement (abm3d.hpp): the 2-D reference

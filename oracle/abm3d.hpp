@@ -1,7 +1,7 @@
 // ORACLE — test infrastructure only.  A plain C++17 restatement of the 3-D
-// mechanics step of kmnam/biofilm-ABMs (ABM-3d/ABM-3d-cpp), used by tests/,
-// __graft_entry__.smoke() and bench.py's CPU baseline leg as the checker.  The
-// product library never links, includes or calls anything under oracle/.
+// mechanics step of kmnam/biofilm-ABMs (ABM-3d/ABM-3d-cpp), against which tests/ and
+// __graft_entry__.smoke() compare the CUDA path, and which bench.py's CPU baseline leg
+// times.  The product library never links, includes or calls anything under oracle/.
 // Beyond the adaptive Runge-Kutta loop it restates, for the steps next to that path:
 // cell-cell kinetic friction, the velocity-Verlet integrator with the constrained force
 // forms, phenotype switching with its ramps, local viscosity and basal-only compaction,

@@ -1,5 +1,5 @@
 """ORACLE — test infrastructure only.  A restatement in Python of the reference's
-frame and lineage writers, used by tests/ as the checker of the library's files:
+frame and lineage writers, against which tests/ compare the library's files:
 
   writeCells (ABM-3d/ABM-3d-cpp/include/utils.hpp:153-198; ABM-2d the same with the
   group in column 16): every parameter of the std::map (so in sorted key order) as

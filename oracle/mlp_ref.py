@@ -1,5 +1,5 @@
-"""CPU restatement of the step-size network (test infrastructure: the checker of the
-GPU forward, backward and training kernels; nothing in the product imports it).
+"""CPU restatement of the step-size network (test infrastructure: the GPU forward,
+backward and training kernels are compared against it; nothing in the product imports it).
 
 The network is 32 -> 64 -> 64 -> 1 with ReLU, flat FP32 parameters
 W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3.  The GPU kernels round the

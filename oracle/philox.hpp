@@ -1,6 +1,6 @@
 // ORACLE — test infrastructure only.  Nothing in the product library links or
 // includes this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
-// baseline leg use the oracle, and only as the checker.
+// baseline leg use the oracle, and only to compare results against (or to time it).
 //
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11), restated from the

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (oracle/_build/liboracle_abm.so) for the tests.
 
 The oracle is test infrastructure: a C++ restatement of the reference's 3-D
-mechanics step (see oracle/abm3d.hpp).  It is only used here as the checker.
+mechanics step (see oracle/abm3d.hpp).  Here it is only what results are compared against.
 """
 import ctypes
 import os

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdint>
 #include <limits>
+#include <random>
 #include <stdexcept>
 #include <utility>
 #include <vector>
@@ -575,6 +576,8 @@ inline int nearest_value(const std::vector<double>& values, double x)
 // ------------------------------------------------------------------------
 // Parameters
 // ------------------------------------------------------------------------
+struct RngStream;
+
 struct Params3 {
     double R = 0.8, Rcell = 0.5, E0 = 3900.0, Ecell = 3.9e6;
     double L0 = 2.0, Ldiv = 5.6;
@@ -626,6 +629,30 @@ struct Params3 {
     // not the reference's procedure: the "optimized CPU" context figure (cell-list neighbor
     // build, pair forces with OpenMP over the pairs); off for every parity comparison
     int cpu_optimized = 0;
+    // Random draws: the counter-based Philox policy (null, the default, which the CUDA path
+    // shares), or one sequential stream drawn in the reference's order (a semantics check).
+    RngStream* stream = nullptr;
+};
+
+// The reference's random source (simulation.hpp:1173, 1298): one mt19937 (Matsumoto and
+// Nishimura 1998) seeded with rng_seed, read through boost::random::uniform_01<>, which
+// scales a 32-bit output x to x / 2^32.  Every draw of the loop comes from it in the
+// reference's order: per try of divideCells the four daughter angles of each mother,
+// then each mother's length fraction (two uniforms, Box-Muller), then the growth rates
+// of the mothers and of the daughters (two each) (growth.hpp:252-350); n x 6 noise
+// uniforms, cell-major, per stepRungeKuttaAdaptive call (mechanics.hpp:2493-2509); one
+// uniform per cell, and two more for a switched cell's growth rate, in Markov switching
+// (switch.hpp:55-75), and per daughter pair one, then two more uniforms and a growth
+// rate for a switch, in inherited switching (switch.hpp:107-135).  `draws` counts them.
+struct RngStream {
+    std::mt19937 engine;
+    long long draws = 0;
+    explicit RngStream(uint32_t seed) : engine(seed) {}
+    double uniform01()
+    {
+        ++draws;
+        return (double)engine() * (1.0 / 4294967296.0);
+    }
 };
 
 // getCellNeighbors as the loop calls it: the reference's O(n^2) procedure, or the
@@ -1293,10 +1320,20 @@ inline Arr6 sample_noise(int n, const Params3& p, int iter, int attempt)
     Arr6 noise((size_t)n * 6, 0.0);
     if (!(p.max_rxy_noise > 0 || p.max_rz_noise > 0 || p.max_nxy_noise > 0 || p.max_nz_noise > 0))
         return noise;
-    uint32_t k0, k1;
-    rng_key(p.rng_seed, RNG_PURPOSE_NOISE, k0, k1);
     const double mx[6] = {p.max_rxy_noise, p.max_rxy_noise, p.max_rz_noise,
                           p.max_nxy_noise, p.max_nxy_noise, p.max_nz_noise};
+    if (p.stream)
+    {
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 6; ++c)
+            {
+                const double u = p.stream->uniform01();
+                A6(noise, n, i, c) = -mx[c] + 2 * mx[c] * u;
+            }
+        return noise;
+    }
+    uint32_t k0, k1;
+    rng_key(p.rng_seed, RNG_PURPOSE_NOISE, k0, k1);
     for (int i = 0; i < n; ++i)
     {
         for (int c = 0; c < 3; ++c)
@@ -1443,6 +1480,7 @@ inline double growth_std_of(const Params3& p, double group)
 
 inline double div_uniform(const Params3& p, int iter, int k, int tr, int slot)
 {
+    if (p.stream) return p.stream->uniform01();
     return rng_uniform(p.rng_seed, RNG_PURPOSE_DIVIDE, (uint32_t)iter, (uint32_t)k,
                        (uint32_t)tr, (uint32_t)slot);
 }
@@ -1501,8 +1539,9 @@ inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double 
         }
         for (int m = 0; m < n_divide; ++m)
         {
-            double r = 0.5 + p.daughter_length_std *
-                standard_normal(div_uniform(p, iter, m, ntries, 4), div_uniform(p, iter, m, ntries, 5));
+            // u before v, as standardNormal draws them (utils.hpp:648-655)
+            const double u = div_uniform(p, iter, m, ntries, 4), v = div_uniform(p, iter, m, ntries, 5);
+            double r = 0.5 + p.daughter_length_std * standard_normal(u, v);
             double M = (r < 0) ? 0.0 : (r > 1 ? 1.0 : r);
             int im = idx_divide[m];
             double Ld = total(im, C_L) - 2 * R;
@@ -1519,12 +1558,17 @@ inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double 
             total(im, C_T0) = t; nc(m, C_T0) = t;
         }
         for (int m = 0; m < n_divide; ++m)
+        {
+            const double u = div_uniform(p, iter, m, ntries, 6), v = div_uniform(p, iter, m, ntries, 7);
             total(idx_divide[m], C_GROWTH) = growth_mean_of(p, total(idx_divide[m], C_GROUP)) +
-                growth_std_of(p, total(idx_divide[m], C_GROUP)) *
-                standard_normal(div_uniform(p, iter, m, ntries, 6), div_uniform(p, iter, m, ntries, 7));
+                growth_std_of(p, total(idx_divide[m], C_GROUP)) * standard_normal(u, v);
+        }
         for (int m = 0; m < n_divide; ++m)
+        {
+            const double u = div_uniform(p, iter, m, ntries, 8), v = div_uniform(p, iter, m, ntries, 9);
             nc(m, C_GROWTH) = growth_mean_of(p, nc(m, C_GROUP)) + growth_std_of(p, nc(m, C_GROUP)) *
-                standard_normal(div_uniform(p, iter, m, ntries, 8), div_uniform(p, iter, m, ntries, 9));
+                standard_normal(u, v);
+        }
         for (int m = 0; m < n_divide; ++m)
             for (int c = 0; c < cells.ncols; ++c) total(n + m, c) = nc(m, c);
         std::vector<double> md1(n_divide, 0), md2(n_divide, 0);
@@ -1784,13 +1828,14 @@ inline Cells step_velocity_verlet(const Cells& cells, const Neighbors& nb, doubl
 // ------------------------------------------------------------------------
 inline double switch_uniform(const Params3& p, int iter, int k, int slot)
 {
+    if (p.stream) return p.stream->uniform01();
     return rng_uniform(p.rng_seed, RNG_PURPOSE_SWITCH, (uint32_t)iter, (uint32_t)k, (uint32_t)slot, 0u);
 }
 
 inline double switch_growth(const Params3& p, int group0, int iter, int k, int slot)
 {
-    return p.group_growth_mean[group0] + p.group_growth_std[group0] *
-           standard_normal(switch_uniform(p, iter, k, slot), switch_uniform(p, iter, k, slot + 1));
+    const double u = switch_uniform(p, iter, k, slot), v = switch_uniform(p, iter, k, slot + 1);
+    return p.group_growth_mean[group0] + p.group_growth_std[group0] * standard_normal(u, v);
 }
 
 // switch.hpp:45-95 (switchGroupsMarkov): each cell leaves its group g for group j when a

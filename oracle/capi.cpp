@@ -4,6 +4,7 @@
 // neighbor rows are column-major m x 7 doubles (i, j, dx, dy, dz, si, sj),
 // exactly the reference's layouts.
 #include <cstring>
+#include <memory>
 #include <string>
 #include <chrono>
 #include "abm3d.hpp"
@@ -36,6 +37,7 @@ struct oracle_ctx {
     Params3 p;
     LoopState st;
     std::string err;
+    std::unique_ptr<RngStream> stream;   // the reference's sequential source, when selected
 };
 
 static std::string g_last_error;
@@ -169,6 +171,24 @@ int oracle_build_neighbors(oracle_ctx* c)
 // the "optimized CPU" procedures (cell-list neighbor build, OpenMP over the pairs), for
 // the context figure beside the reference-faithful CPU run; off by default
 void oracle_set_cpu_optimized(oracle_ctx* c, int on) { c->p.cpu_optimized = on ? 1 : 0; }
+
+// on = 1: every random draw comes from one mt19937 seeded with `seed`, in the reference's
+// order (the semantics check of its random source); on = 0: the Philox counter policy
+void oracle_set_rng_stream(oracle_ctx* c, int on, unsigned seed)
+{
+    c->stream.reset(on ? new RngStream(seed) : nullptr);
+    c->p.stream = c->stream.get();
+}
+
+// uniforms drawn from the stream so far (0 without one)
+long long oracle_rng_stream_draws(oracle_ctx* c) { return c->stream ? c->stream->draws : 0; }
+
+// the first k uniforms of a fresh stream seeded with `seed`
+void oracle_rng_stream_uniforms(unsigned seed, int k, double* out)
+{
+    RngStream r(seed);
+    for (int i = 0; i < k; ++i) out[i] = r.uniform01();
+}
 
 int oracle_num_neighbors(oracle_ctx* c) { return c->st.nb.size(); }
 

@@ -64,6 +64,9 @@ def _load():
         "oracle_get_clock": ([vp, dp, dp, ip], None),
         "oracle_build_neighbors": ([vp], i),
         "oracle_set_cpu_optimized": ([vp, i], None),
+        "oracle_set_rng_stream": ([vp, i, ctypes.c_uint], None),
+        "oracle_rng_stream_draws": ([vp], ctypes.c_longlong),
+        "oracle_rng_stream_uniforms": ([ctypes.c_uint, i, dp], None),
         "oracle_num_neighbors": ([vp], i),
         "oracle_get_neighbors": ([vp, dp, i], i),
         "oracle_set_neighbors": ([vp, dp, i, i], i),
@@ -133,6 +136,13 @@ def jkr_table_variable(R, Rcell, E0, max_gamma, n_delta=100, n_gamma=100):
     r = np.zeros(n_delta * n_gamma)
     LIB.oracle_jkr_table2(R, Rcell, E0, max_gamma, n_delta, n_gamma, _dp(d), _dp(g), _dp(r))
     return d, g, r.reshape(n_delta, n_gamma)
+
+
+def rng_stream_uniforms(seed, k):
+    """The first k uniforms of the reference's random source seeded with `seed`."""
+    out = np.zeros(k)
+    LIB.oracle_rng_stream_uniforms(int(seed), k, _dp(out))
+    return out
 
 
 def jkr_table(R, Rcell, E0, gamma, n_mesh=100):
@@ -282,6 +292,14 @@ class Oracle:
 
     def divide(self, t, iteration):
         return LIB.oracle_divide(self._c, t, iteration)
+
+    def set_rng_stream(self, seed):
+        """Draw every random number from one mt19937 seeded with `seed`, in the reference's
+        order (simulation.hpp:1173), instead of the Philox counter policy; None: Philox."""
+        LIB.oracle_set_rng_stream(self._c, 0 if seed is None else 1, 0 if seed is None else int(seed))
+
+    def rng_stream_draws(self):
+        return LIB.oracle_rng_stream_draws(self._c)
 
     def min_dist_to_cell(self, i):
         return LIB.oracle_min_dist_to_cell(self._c, i)

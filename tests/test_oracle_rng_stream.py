@@ -1,0 +1,104 @@
+"""The oracle's sequential random source, the semantics check of the reference's own:
+one mt19937 seeded with rng_seed (simulation.hpp:1173) read through
+boost::random::uniform_01<> (a 32-bit output x becomes x / 2^32), drawn in the
+reference's order.  The Philox counter policy that the CUDA path shares stays the
+default; this mode shows that the oracle consumes the reference's stream draw for draw
+where the reference does: n x 6 noise uniforms per RK attempt, cell-major
+(mechanics.hpp:2493-2509), and per try of divideCells four angles per mother, then
+each mother's length fraction, then the mothers' and the daughters' growth rates, two
+uniforms (Box-Muller, utils.hpp:648-655) each (growth.hpp:252-350)."""
+import numpy as np
+
+import abm_b200
+import oracle_ref as orc
+
+
+def test_stream_is_mt19937_read_through_uniform_01():
+    # the value the C++ standard requires of the 10000th output of a default-seeded mt19937
+    u = orc.rng_stream_uniforms(5489, 10000)
+    assert u[-1] * 2.0 ** 32 == 4123659995
+    # numpy's MT19937 with the same integer seeding, raw 32-bit outputs over 2^32
+    raw = np.random.RandomState(42).randint(0, 2 ** 32, size=2000, dtype=np.uint32)
+    assert np.array_equal(orc.rng_stream_uniforms(42, 2000), raw / 2.0 ** 32)
+
+
+def lone_cells(k, spacing=40.0, length=3.0):
+    """k horizontal cells along x, `spacing` apart: no pairs, no contact with each other."""
+    cells = np.zeros((k, 22))
+    cells[:, 0] = np.arange(k)
+    cells[:, 1] = spacing * np.arange(k)
+    cells[:, 3] = 5.0
+    cells[:, 4] = 1.0
+    cells[:, 13] = length
+    cells[:, 14] = length / 2
+    cells[:, 17] = 100.0
+    cells[:, 18] = 720.0
+    cells[:, 19] = 100.0
+    cells[:, 20] = 1
+    return cells
+
+
+def test_noise_is_drawn_cell_major_in_component_order():
+    k, seed, dt, amp = 3, 11, 1e-3, 0.5
+    cells = lone_cells(k)
+    _, p = abm_b200.make_params(no_surface=1, adhesion_mode=0, max_rz_noise=amp)
+    o = orc.Oracle(p)
+    o.set_cells(cells)
+    o.set_rng_stream(seed)
+    o.build_neighbors()
+    new, _, _ = o.rk_attempt(dt)
+    assert o.rng_stream_draws() == 6 * k
+    # only the rz noise is on: a free cell moves by dt * noise_z / (eta0 l), and cell i's
+    # z noise is the third of its six uniforms
+    u = orc.rng_stream_uniforms(seed, 6 * k)
+    expect = dt * (-amp + 2 * amp * u[6 * np.arange(k) + 2]) / (cells[:, 17] * cells[:, 13])
+    # the displacement is a difference from z = 5: a few ulps of z bound its rounding
+    np.testing.assert_allclose(new[:, 3] - cells[:, 3], expect, rtol=1e-9, atol=8 * np.spacing(5.0))
+    assert np.array_equal(new[:, 1:3], cells[:, 1:3])
+
+
+def normal(u, v):
+    return np.sqrt(-2 * np.log(u)) * np.cos(2 * np.pi * v)
+
+
+def test_division_draws_follow_the_reference_order():
+    k, seed, R = 5, 3, 0.8
+    cells = lone_cells(k, length=5.9)                 # every cell is past Ldiv = 5.6
+    _, p = abm_b200.make_params(growth_mean=1.5, growth_std=0.1, daughter_length_std=0.05,
+                                daughter_angle_xy_bound=0.3, daughter_angle_z_bound=0.1)
+    o = orc.Oracle(p)
+    o.set_cells(cells)
+    o.set_parents(-np.ones(k, dtype=np.int32))
+    o.set_rng_stream(seed)
+    tries = o.divide(0.25, 0)
+    assert tries == 1                                 # lone mothers: the first try satisfies all
+    assert o.rng_stream_draws() == 10 * k
+    u = orc.rng_stream_uniforms(seed, 10 * k)
+    out = o.cells()
+    assert out.shape[0] == 2 * k
+    # after 4k angle draws: each mother's length fraction M from (u, v), in mother order
+    m = np.arange(k)
+    frac = np.clip(0.5 + 0.05 * normal(u[4 * k + 2 * m], u[4 * k + 2 * m + 1]), 0, 1)
+    np.testing.assert_allclose(out[:k, 13], frac * (5.9 - 2 * R), rtol=1e-12)
+    np.testing.assert_allclose(out[k:, 13], (1 - frac) * (5.9 - 2 * R), rtol=1e-12)
+    # then the mothers' growth rates, then the daughters'
+    np.testing.assert_allclose(out[:k, 16], 1.5 + 0.1 * normal(u[6 * k + 2 * m], u[6 * k + 2 * m + 1]), rtol=1e-12)
+    np.testing.assert_allclose(out[k:, 16], 1.5 + 0.1 * normal(u[8 * k + 2 * m], u[8 * k + 2 * m + 1]), rtol=1e-12)
+
+
+def test_philox_stays_the_default_and_comes_back():
+    cells = lone_cells(4, length=5.9)
+    _, p = abm_b200.make_params(growth_mean=1.5, growth_std=0.1, daughter_length_std=0.05,
+                                daughter_angle_xy_bound=0.3, daughter_angle_z_bound=0.1)
+    out = []
+    for stream in (False, True):
+        o = orc.Oracle(p)
+        o.set_cells(cells)
+        o.set_parents(-np.ones(4, dtype=np.int32))
+        if stream:
+            o.set_rng_stream(9)
+            o.set_rng_stream(None)
+        o.divide(0.25, 0)
+        assert o.rng_stream_draws() == 0
+        out.append(o.cells())
+    assert np.array_equal(out[0], out[1])

@@ -45,6 +45,7 @@ struct Params2 {
     // their own, 2D/test/src/testHertz.cpp:201-204); unused when use_pf == 0
     int use_pf = 0;
     double pf[3] = {0, 0, 0};
+    RngStream* stream = nullptr;           // the reference's sequential source (abm3d.hpp), or Philox
 };
 
 // 2D/include/simulation.hpp:232-235 (the code's exponents: 0.5, 2.5 and 0.5)
@@ -251,6 +252,17 @@ inline Arr4 sample_noise_2d(int n, const Params2& p, int iter, int attempt)
 {
     Arr4 noise((size_t)n * 4, 0.0);
     if (!(p.max_noise > 0)) return noise;
+    if (p.stream)
+    {
+        // 2D/include/mechanics.hpp:1760-1771: four uniforms per cell, cell-major
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 4; ++c)
+            {
+                const double u = p.stream->uniform01();
+                A4(noise, n, i, c) = -p.max_noise + 2 * p.max_noise * u;
+            }
+        return noise;
+    }
     uint32_t k0, k1;
     rng_key(p.rng_seed, RNG_PURPOSE_NOISE, k0, k1);
     const double m = p.max_noise;
@@ -375,6 +387,8 @@ inline Params3 division_params(const Params2& p)
     q.daughter_angle_xy_bound = p.daughter_angle_bound;
     q.daughter_angle_z_bound = 0.0;
     q.rng_seed = p.rng_seed;
+    q.stream = p.stream;
+    q.planar_division = 1;
     return q;
 }
 

@@ -632,6 +632,10 @@ struct Params3 {
     // Random draws: the counter-based Philox policy (null, the default, which the CUDA path
     // shares), or one sequential stream drawn in the reference's order (a semantics check).
     RngStream* stream = nullptr;
+    // divideCells of the 2-D model (2D/include/growth.hpp:252-258) draws one angle per daughter,
+    // in the plane; with planar_division the restatement draws no out-of-plane angles (their
+    // bound is 0 there, so only the stream's order changes)
+    int planar_division = 0;
 };
 
 // The reference's random source (simulation.hpp:1173, 1298): one mt19937 (Matsumoto and
@@ -1523,9 +1527,9 @@ inline Cells divide_cells(const Cells& cells, std::vector<int>& parents, double 
             {
                 double bxy = p.daughter_angle_xy_bound, bz = p.daughter_angle_z_bound;
                 txy1[m] = -bxy + 2 * bxy * div_uniform(p, iter, m, ntries, 0);
-                tz1[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 1);
+                if (!p.planar_division) tz1[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 1);
                 txy2[m] = -bxy + 2 * bxy * div_uniform(p, iter, m, ntries, 2);
-                tz2[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 3);
+                if (!p.planar_division) tz2[m] = -bz + 2 * bz * div_uniform(p, iter, m, ntries, 3);
             }
         }
         for (int m = 0; m < n_divide; ++m)

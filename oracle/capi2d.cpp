@@ -3,6 +3,7 @@
 // doubles in the 2-D reference layout (ABM-2d/ABM-2d-cpp/include/indices.hpp),
 // neighbor rows are column-major m x 6 doubles (i, j, dx, dy, si, sj).
 #include <cstring>
+#include <memory>
 #include <string>
 #include "abm2d.hpp"
 
@@ -26,7 +27,18 @@ struct oracle2d_params {
 struct oracle2d_ctx {
     Params2 p;
     LoopState2 st;
+    std::unique_ptr<RngStream> stream;   // the reference's sequential source, when selected
 };
+
+// on = 1: every random draw comes from one mt19937 seeded with `seed`, in the 2-D
+// reference's order; on = 0: the Philox counter policy
+void oracle2d_set_rng_stream(oracle2d_ctx* c, int on, unsigned seed)
+{
+    c->stream.reset(on ? new RngStream(seed) : nullptr);
+    c->p.stream = c->stream.get();
+}
+
+long long oracle2d_rng_stream_draws(oracle2d_ctx* c) { return c->stream ? c->stream->draws : 0; }
 
 int oracle2d_create(const oracle2d_params* q, oracle2d_ctx** out)
 {

@@ -348,6 +348,8 @@ def _load2d(lib):
         "oracle2d_iterate": ([vp, i, i], i),
         "oracle2d_get_stats": ([vp, ll, ll, ll, dp], None),
         "oracle2d_divide": ([vp, d, i, ip], i),
+        "oracle2d_set_rng_stream": ([vp, i, ctypes.c_uint], None),
+        "oracle2d_rng_stream_draws": ([vp], ctypes.c_longlong),
         "oracle2d_grow": ([vp, d], i),
         "oracle2d_jkr_lagrange_pair": ([dp, dp, dp, d, d, d, d, dp], None),
     }
@@ -471,5 +473,11 @@ class Oracle2D:
         nd = LIB.oracle2d_divide(self._c, t, iteration, ctypes.byref(tr))
         return nd, tr.value
 
+    def set_rng_stream(self, seed):
+        """The reference's sequential mt19937 source seeded with `seed`; None: Philox."""
+        LIB.oracle2d_set_rng_stream(self._c, 0 if seed is None else 1, 0 if seed is None else int(seed))
+
+    def rng_stream_draws(self):
+        return LIB.oracle2d_rng_stream_draws(self._c)
     def grow(self, dt):
         LIB.oracle2d_grow(self._c, dt)

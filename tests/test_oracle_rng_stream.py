@@ -102,3 +102,65 @@ def test_philox_stays_the_default_and_comes_back():
         assert o.rng_stream_draws() == 0
         out.append(o.cells())
     assert np.array_equal(out[0], out[1])
+
+
+def lone_cells_2d(k, spacing=40.0, length=3.0):
+    """k 2-D cells along x, `spacing` apart (ABM-2d column order, indices.hpp)."""
+    cells = np.zeros((k, 17))
+    cells[:, 0] = np.arange(k)
+    cells[:, 1] = spacing * np.arange(k)
+    cells[:, 3] = 1.0
+    cells[:, 9] = length
+    cells[:, 10] = length / 2
+    cells[:, 13] = 100.0
+    cells[:, 14] = 100.0
+    cells[:, 15] = 100.0
+    cells[:, 16] = 1
+    return cells
+
+
+def test_2d_noise_is_drawn_cell_major_four_per_cell():
+    # 2D/include/mechanics.hpp:1760-1771: (rx, ry, nx, ny) per cell, cells in order
+    k, seed, amp = 3, 21, 0.5
+    cells = lone_cells_2d(k)
+    o = orc.Oracle2D(dict(max_noise=amp, adhesion_mode=0))
+    o.set_cells(cells)
+    o.set_rng_stream(seed)
+    o.build_neighbors()
+    new, _, _ = o.rk_attempt(1e-3)
+    assert o.rng_stream_draws() == 4 * k
+    u = orc.rng_stream_uniforms(seed, 4 * k)
+    nx, ny = -amp + 2 * amp * u[4 * np.arange(k)], -amp + 2 * amp * u[4 * np.arange(k) + 1]
+    # a lone cell's translational mobility is one scalar: x and y move in the noise's ratio
+    dx, dy = new[:, 1] - cells[:, 1], new[:, 2] - cells[:, 2]
+    # dx is a difference from x (up to 80 um): a few ulps of x bound its rounding
+    np.testing.assert_allclose(dx * ny, dy * nx, rtol=1e-9, atol=8 * np.spacing(cells[:, 1].max()) * amp)
+    assert np.all(np.sign(dx) == -np.sign(nx)) or np.all(np.sign(dx) == np.sign(nx))
+
+
+def test_2d_division_draws_one_angle_per_daughter():
+    # 2D/include/growth.hpp:252-335: per try two angles per mother (one per daughter), then
+    # the length fractions, then the mothers' and the daughters' growth rates
+    k, seed, R, L = 4, 5, 0.8, 5.9
+    cells = lone_cells_2d(k, length=L)
+    o = orc.Oracle2D(dict(growth_mean=1.5, growth_std=0.1, daughter_length_std=0.05,
+                          daughter_angle_xy_bound=0.3, Ldiv=5.6))
+    o.set_cells(cells)
+    o.set_parents(-np.ones(k, dtype=np.int32))
+    o.set_rng_stream(seed)
+    nd, tries = o.divide(0.25, 0)
+    assert tries == 1
+    assert o.rng_stream_draws() == 8 * k
+    u = orc.rng_stream_uniforms(seed, 8 * k)
+    out = o.cells()
+    m = np.arange(k)
+    frac = np.clip(0.5 + 0.05 * normal(u[2 * k + 2 * m], u[2 * k + 2 * m + 1]), 0, 1)
+    np.testing.assert_allclose(out[:k, 9], frac * (L - 2 * R), rtol=1e-12)
+    np.testing.assert_allclose(out[k:, 9], (1 - frac) * (L - 2 * R), rtol=1e-12)
+    np.testing.assert_allclose(out[:k, 12], 1.5 + 0.1 * normal(u[4 * k + 2 * m], u[4 * k + 2 * m + 1]), rtol=1e-12)
+    np.testing.assert_allclose(out[k:, 12], 1.5 + 0.1 * normal(u[6 * k + 2 * m], u[6 * k + 2 * m + 1]), rtol=1e-12)
+    # the daughters' orientations turn by the two drawn angles
+    ang1 = -0.3 + 0.6 * u[2 * m]
+    ang2 = -0.3 + 0.6 * u[2 * m + 1]
+    np.testing.assert_allclose(np.arctan2(out[:k, 4], out[:k, 3]), ang1, atol=1e-12)
+    np.testing.assert_allclose(np.arctan2(out[k:, 4], out[k:, 3]), ang2, atol=1e-12)

@@ -164,3 +164,34 @@ def test_2d_division_draws_one_angle_per_daughter():
     ang2 = -0.3 + 0.6 * u[2 * m + 1]
     np.testing.assert_allclose(np.arctan2(out[:k, 4], out[:k, 3]), ang1, atol=1e-12)
     np.testing.assert_allclose(np.arctan2(out[k:, 4], out[k:, 3]), ang2, atol=1e-12)
+
+
+def test_philox_and_the_reference_stream_give_the_same_division_statistics():
+    """Parity with the reference's own draws is statistical: dividing the same 3000 lone
+    mothers once under the Philox policy and once under the mt19937 stream gives daughters
+    whose length fractions, orientations and growth rates are alike in distribution."""
+    from scipy import stats
+    k, L, R = 3000, 5.9, 0.8
+    cells = lone_cells(k, spacing=20.0, length=L)
+    _, p = abm_b200.make_params(growth_mean=1.5, growth_std=0.1, daughter_length_std=0.05,
+                                daughter_angle_xy_bound=0.3, daughter_angle_z_bound=0.1, rng_seed=17)
+    out = {}
+    for source in ("philox", "stream"):
+        o = orc.Oracle(p)
+        o.set_cells(cells)
+        o.set_parents(-np.ones(k, dtype=np.int32))
+        if source == "stream":
+            o.set_rng_stream(17)
+        assert o.divide(0.25, 0) == 1
+        c = o.cells()
+        out[source] = dict(frac=c[:k, 13] / (L - 2 * R), growth=c[:, 16],
+                           azimuth=np.arctan2(c[:, 5], c[:, 4]), tilt=np.arcsin(np.clip(c[:, 6], -1, 1)))
+    for key in ("frac", "growth", "azimuth", "tilt"):
+        a, b = out["philox"][key], out["stream"][key]
+        assert not np.array_equal(a, b)                      # different draws ...
+        assert stats.ks_2samp(a, b).pvalue > 1e-3, key       # ... from the same distributions
+    # and the distributions the reference asks for
+    for src in out.values():
+        assert abs(src["frac"].mean() - 0.5) < 5 * 0.05 / np.sqrt(k)
+        assert abs(src["growth"].std() - 0.1) < 0.01
+        assert np.abs(src["azimuth"]).max() <= 0.3 + 1e-12 and np.abs(src["tilt"]).max() <= 0.1 + 1e-12
